@@ -1,0 +1,369 @@
+// C ABI of the assembler (include/fem_alls.h): workspace layout, argument
+// checks, stream-ordered orchestration of the kernels, status decoding and the
+// host-buffer entry point.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "launch.h"
+
+using namespace fem;
+
+namespace {
+
+thread_local int32_t g_last_cuda_error = 0;
+
+fem_status cuda_fail(cudaError_t err) {
+    g_last_cuda_error = (int32_t)err;
+    return FEM_ERR_CUDA;
+}
+
+constexpr size_t kAlign = 256;
+size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+
+int kind_dpn(int kind) { return kind == FEM_HEX20 ? 3 : 2; }
+
+fem_status check_mesh(const fem_mesh* m, bool device_pointers_needed = true) {
+    (void)device_pointers_needed;
+    if (!m) return FEM_ERR_BAD_ARG;
+    if (m->kind < FEM_Q4 || m->kind > FEM_MIXED_2D) return FEM_ERR_BAD_ARG;
+    if (m->num_nodes <= 0 || m->num_elems < 0) return FEM_ERR_BAD_ARG;
+    const int need_stride = m->kind == FEM_Q4 ? 4 : m->kind == FEM_T3 ? 3 : m->kind == FEM_HEX20 ? 20 : 4;
+    if (m->conn_stride != need_stride) return FEM_ERR_BAD_ARG;
+    if (!m->x || !m->y || (m->num_elems > 0 && !m->conn)) return FEM_ERR_BAD_ARG;
+    if (m->kind == FEM_HEX20 && !m->z) return FEM_ERR_BAD_ARG;
+    if (m->kind == FEM_MIXED_2D && m->num_elems > 0 && !m->elem_type) return FEM_ERR_BAD_ARG;
+    if ((long long)m->num_nodes * kind_dpn(m->kind) + 1 > 0x7FFFFFFFll) return FEM_ERR_RANGE;
+    return FEM_OK;
+}
+
+fem_status make_layout(const fem_mesh* m, const fem_opts* o, HostLayout& h) {
+    fem_status st = check_mesh(m);
+    if (st) return st;
+    fem_opts d{};
+    if (!o) o = &d;
+    h = HostLayout{};
+    h.kind = m->kind;
+    h.dpn = kind_dpn(m->kind);
+    h.B = h.dpn * h.dpn;
+    h.N = m->num_nodes;
+    h.E = m->num_elems;
+    if (h.dpn == 2) {
+        // 2-D chunk rows are fixed at 16 words (the scatter reads them as 4 x 16 bytes).
+        if ((o->first_slots && o->first_slots != k2DSlots) || (o->chunk_slots && o->chunk_slots != k2DSlots))
+            return FEM_ERR_BAD_ARG;
+        h.S1 = h.S2 = k2DSlots;
+    } else {
+        h.S1 = o->first_slots ? o->first_slots : 94;
+        h.S2 = o->chunk_slots ? o->chunk_slots : 30;
+        if (h.S1 < 2 || h.S2 < 2 || (h.S1 + 2) % 4 || (h.S2 + 2) % 4 || h.S1 > 4094 || h.S2 > 4094)
+            return FEM_ERR_BAD_ARG;
+    }
+    h.H1 = h.S1 + 2;
+    h.H2 = h.S2 + 2;
+    const double pf = o->pool_factor > 0 ? o->pool_factor : (h.dpn == 3 ? 0.5 : 0.125);
+    const double cap2 = std::ceil(pf * (double)h.N) + 64;
+    if (cap2 > 2e9) return FEM_ERR_RANGE;
+    h.cap2 = (int)cap2;
+    const double slots = (double)h.N * h.S1 + (double)h.cap2 * h.S2;
+    if (slots >= 2147483648.0) return FEM_ERR_RANGE;  // slot ids carry a flag in bit 31
+    h.nodes_per_tile = consolidate_nodes_per_tile(h.dpn);
+    h.num_tiles = (h.N + h.nodes_per_tile - 1) / h.nodes_per_tile;
+    size_t off = 0;
+    h.off_info = off;
+    off += align_up(sizeof(DevInfo));
+    h.off_meta1 = off;
+    h.meta1_bytes = (size_t)h.N * h.H1 * sizeof(int);
+    off += align_up(h.meta1_bytes);
+    h.off_meta2 = off;
+    off += align_up((size_t)h.cap2 * h.H2 * sizeof(int));
+    h.off_vals = off;
+    off += align_up((size_t)slots * h.B * sizeof(double));
+    h.off_tiles = off;
+    off += align_up((size_t)h.num_tiles * sizeof(unsigned long long));
+    h.off_elist = off;
+    if (h.kind == FEM_MIXED_2D) off += align_up(2 * sizeof(int)) + 2 * align_up((size_t)h.E * sizeof(int));
+    h.total = off;
+    return FEM_OK;
+}
+
+ListLayout device_layout(const HostLayout& h, void* ws) {
+    unsigned char* b = static_cast<unsigned char*>(ws);
+    ListLayout L;
+    L.N = h.N;
+    L.S1 = h.S1;
+    L.S2 = h.S2;
+    L.H1 = h.H1;
+    L.H2 = h.H2;
+    L.B = h.B;
+    L.cap2 = h.cap2;
+    L.meta1 = reinterpret_cast<int*>(b + h.off_meta1);
+    L.meta2 = reinterpret_cast<int*>(b + h.off_meta2);
+    L.vals = reinterpret_cast<double*>(b + h.off_vals);
+    L.info = reinterpret_cast<DevInfo*>(b + h.off_info);
+    return L;
+}
+
+MeshView mesh_view(const fem_mesh* m) {
+    MeshView v;
+    v.x = m->x;
+    v.y = m->y;
+    v.z = m->z;
+    v.conn = m->conn;
+    v.types = m->elem_type;
+    v.E = m->E;
+    v.nu = m->nu;
+    v.E0 = m->E0;
+    v.nu0 = m->nu0;
+    v.t = m->thickness;
+    v.N = m->num_nodes;
+    v.E_count = m->num_elems;
+    v.stride = m->conn_stride;
+    return v;
+}
+
+fem_status check_ws(const HostLayout& h, const void* ws, size_t bytes) {
+    if (!ws || bytes < h.total || (reinterpret_cast<uintptr_t>(ws) % kAlign)) return FEM_ERR_WORKSPACE;
+    return FEM_OK;
+}
+
+// Most severe status among the device bits.
+fem_status decode_bits(int bits) {
+    static const int order[] = {FEM_ERR_BAD_MESH,  FEM_ERR_POOL_OVERFLOW, FEM_ERR_TIMEOUT, FEM_ERR_ROW_TOO_LONG,
+                                FEM_ERR_RANGE,     FEM_ERR_CAPACITY,      FEM_ERR_DETJ};
+    for (int code : order)
+        if (bits & (1 << code)) return code;
+    return FEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t fem_abi_version(void) { return FEM_ALLS_ABI_VERSION; }
+int32_t fem_last_cuda_error(void) { return g_last_cuda_error; }
+
+const char* fem_status_string(fem_status s) {
+    switch (s) {
+        case FEM_OK: return "ok";
+        case FEM_ERR_BAD_ARG: return "bad argument";
+        case FEM_ERR_BAD_MESH: return "bad mesh (node id out of range)";
+        case FEM_ERR_POOL_OVERFLOW: return "list pool overflow (retry with a larger pool_factor)";
+        case FEM_ERR_DETJ: return "non-positive Jacobian determinant";
+        case FEM_ERR_CUDA: return "CUDA error";
+        case FEM_ERR_CAPACITY: return "output capacity smaller than nnz";
+        case FEM_ERR_WORKSPACE: return "workspace too small or misaligned";
+        case FEM_ERR_TIMEOUT: return "bounded wait gave up";
+        case FEM_ERR_RANGE: return "size exceeds the int32 range";
+        case FEM_ERR_ROW_TOO_LONG: return "row list longer than the consolidation capacity";
+        default: return "unknown status";
+    }
+}
+
+fem_status fem_alls_workspace_size(const fem_mesh* mesh, const fem_opts* opts, size_t* bytes) {
+    if (!bytes) return FEM_ERR_BAD_ARG;
+    HostLayout h;
+    fem_status st = make_layout(mesh, opts, h);
+    if (st) return st;
+    *bytes = h.total;
+    return FEM_OK;
+}
+
+fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* workspace, size_t workspace_bytes,
+                            void* stream) {
+    HostLayout h;
+    fem_status st = make_layout(mesh, opts, h);
+    if (st) return st;
+    if ((st = check_ws(h, workspace, workspace_bytes))) return st;
+    if (opts && opts->precision != FEM_PREC_FP64) return FEM_ERR_BAD_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    ListLayout L = device_layout(h, workspace);
+    unsigned char* b = static_cast<unsigned char*>(workspace);
+    cudaError_t err = cudaMemsetAsync(b + h.off_info, 0, sizeof(DevInfo), s);
+    if (!err) err = launch_info_init(L.info, h.cap2, s);
+    if (!err) err = cudaMemsetAsync(b + h.off_meta1, 0, h.meta1_bytes, s);
+    if (err) return cuda_fail(err);
+    if (h.E == 0) return FEM_OK;
+    MeshView m = mesh_view(mesh);
+    switch (h.kind) {
+        case FEM_Q4: err = launch_scatter_2d(m, L, 4, nullptr, nullptr, s); break;
+        case FEM_T3: err = launch_scatter_2d(m, L, 3, nullptr, nullptr, s); break;
+        case FEM_HEX20: err = launch_scatter_hex20(m, L, s); break;
+        default: {
+            int* counts = reinterpret_cast<int*>(b + h.off_elist);
+            int* lq = reinterpret_cast<int*>(b + h.off_elist + align_up(2 * sizeof(int)));
+            int* lt = reinterpret_cast<int*>(b + h.off_elist + align_up(2 * sizeof(int)) + align_up((size_t)h.E * sizeof(int)));
+            err = launch_partition_2d(m, lq, lt, counts, s);
+            if (!err) err = launch_scatter_2d(m, L, 4, lq, counts + 0, s);
+            if (!err) err = launch_scatter_2d(m, L, 3, lt, counts + 1, s);
+        }
+    }
+    return err ? cuda_fail(err) : FEM_OK;
+}
+
+fem_status fem_alls_consolidate(const fem_mesh* mesh, const fem_opts* opts, void* workspace, size_t workspace_bytes,
+                                int32_t* row_ptr, int32_t* col_idx, double* values, int64_t capacity, void* stream) {
+    HostLayout h;
+    fem_status st = make_layout(mesh, opts, h);
+    if (st) return st;
+    if ((st = check_ws(h, workspace, workspace_bytes))) return st;
+    if (!row_ptr || capacity < 0 || (capacity > 0 && (!col_idx || !values))) return FEM_ERR_BAD_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    ListLayout L = device_layout(h, workspace);
+    unsigned long long* tiles = reinterpret_cast<unsigned long long*>(static_cast<unsigned char*>(workspace) + h.off_tiles);
+    cudaError_t err = launch_consolidate(L, h.dpn, row_ptr, col_idx, values, capacity, tiles, h.num_tiles, s);
+    return err ? cuda_fail(err) : FEM_OK;
+}
+
+fem_status fem_alls_read_info(const void* workspace, fem_info* info, void* stream) {
+    if (!workspace || !info) return FEM_ERR_BAD_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t err = cudaMemcpyAsync(info, workspace, sizeof(fem_info), cudaMemcpyDeviceToHost, s);
+    if (!err) err = cudaStreamSynchronize(s);
+    if (err) return cuda_fail(err);
+    return decode_bits(info->status_bits);
+}
+
+fem_status fem_assemble_async(const fem_mesh* mesh, const fem_opts* opts, void* workspace, size_t workspace_bytes,
+                              fem_csr* out, void* stream) {
+    if (!out) return FEM_ERR_BAD_ARG;
+    fem_status st = fem_alls_scatter(mesh, opts, workspace, workspace_bytes, stream);
+    if (st) return st;
+    return fem_alls_consolidate(mesh, opts, workspace, workspace_bytes, out->row_ptr, out->col_idx, out->values,
+                                out->capacity, stream);
+}
+
+fem_status fem_assemble(const fem_mesh* mesh, const fem_opts* opts, void* workspace, size_t workspace_bytes,
+                        fem_csr* out, void* stream) {
+    fem_status st = fem_assemble_async(mesh, opts, workspace, workspace_bytes, out, stream);
+    if (st) return st;
+    fem_info info;
+    st = fem_alls_read_info(workspace, &info, stream);
+    out->nnz = info.nnz;
+    out->n_rows = mesh->num_nodes * kind_dpn(mesh->kind);
+    return st;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Host-buffer entry point
+// ---------------------------------------------------------------------------
+
+struct fem_context {
+    struct Buf {
+        void* p = nullptr;
+        size_t n = 0;
+    };
+    Buf x, y, z, conn, types, E, nu, ws, row_ptr, col_idx, values;
+    double pool_factor = 0.0;
+    ~fem_context() {
+        for (Buf* b : {&x, &y, &z, &conn, &types, &E, &nu, &ws, &row_ptr, &col_idx, &values})
+            if (b->p) cudaFree(b->p);
+    }
+    // Grow-only device buffer.
+    cudaError_t need(Buf& b, size_t bytes) {
+        if (bytes <= b.n && b.p) return cudaSuccess;
+        if (b.p) cudaFree(b.p);
+        b.p = nullptr;
+        b.n = 0;
+        cudaError_t err = cudaMalloc(&b.p, bytes ? bytes : 1);
+        if (!err) b.n = bytes;
+        return err;
+    }
+};
+
+extern "C" {
+
+fem_status fem_context_create(fem_context** ctx) {
+    if (!ctx) return FEM_ERR_BAD_ARG;
+    *ctx = new (std::nothrow) fem_context();
+    return *ctx ? FEM_OK : FEM_ERR_BAD_ARG;
+}
+
+void fem_context_destroy(fem_context* ctx) { delete ctx; }
+
+fem_status fem_assemble_host(fem_context* ctx, const fem_mesh* hm, const fem_opts* opts, fem_csr* out, void* stream) {
+    if (!ctx || !out || !out->row_ptr) return FEM_ERR_BAD_ARG;
+    fem_status st = check_mesh(hm);
+    if (st) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int dpn = kind_dpn(hm->kind);
+    const size_t N = (size_t)hm->num_nodes, E = (size_t)hm->num_elems;
+    cudaError_t err = cudaSuccess;
+    auto up = [&](fem_context::Buf& b, const void* src, size_t bytes) {
+        if (err || !src) return;
+        err = ctx->need(b, bytes);
+        if (!err) err = cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, s);
+    };
+    up(ctx->x, hm->x, N * sizeof(double));
+    up(ctx->y, hm->y, N * sizeof(double));
+    up(ctx->z, hm->z, N * sizeof(double));
+    up(ctx->conn, hm->conn, E * hm->conn_stride * sizeof(int32_t));
+    up(ctx->types, hm->elem_type, E);
+    up(ctx->E, hm->E, E * sizeof(double));
+    up(ctx->nu, hm->nu, E * sizeof(double));
+    if (err) return cuda_fail(err);
+    fem_mesh dm = *hm;
+    dm.x = static_cast<const double*>(ctx->x.p);
+    dm.y = static_cast<const double*>(ctx->y.p);
+    dm.z = hm->z ? static_cast<const double*>(ctx->z.p) : nullptr;
+    dm.conn = static_cast<const int32_t*>(ctx->conn.p);
+    dm.elem_type = hm->elem_type ? static_cast<const uint8_t*>(ctx->types.p) : nullptr;
+    dm.E = hm->E ? static_cast<const double*>(ctx->E.p) : nullptr;
+    dm.nu = hm->nu ? static_cast<const double*>(ctx->nu.p) : nullptr;
+
+    fem_opts o = opts ? *opts : fem_opts{};
+    if (ctx->pool_factor > o.pool_factor) o.pool_factor = ctx->pool_factor;
+    const size_t n_rows = N * dpn;
+    if ((err = ctx->need(ctx->row_ptr, (n_rows + 1) * sizeof(int32_t)))) return cuda_fail(err);
+    fem_info info{};
+    for (int attempt = 0; attempt < 4; attempt++) {
+        size_t wsb = 0;
+        if ((st = fem_alls_workspace_size(&dm, &o, &wsb))) return st;
+        if ((err = ctx->need(ctx->ws, wsb))) return cuda_fail(err);
+        if ((st = fem_alls_scatter(&dm, &o, ctx->ws.p, ctx->ws.n, stream))) return st;
+        long long cap = (long long)(ctx->values.n / sizeof(double));
+        if ((st = fem_alls_consolidate(&dm, &o, ctx->ws.p, ctx->ws.n, static_cast<int32_t*>(ctx->row_ptr.p),
+                                       static_cast<int32_t*>(ctx->col_idx.p), static_cast<double*>(ctx->values.p),
+                                       cap, stream)))
+            return st;
+        st = fem_alls_read_info(ctx->ws.p, &info, stream);
+        if (st == FEM_ERR_POOL_OVERFLOW) {
+            // Grow the overflow pool and assemble again.
+            HostLayout h;
+            make_layout(&dm, &o, h);
+            o.pool_factor = 2.0 * ((double)h.cap2 / (double)h.N + 0.25);
+            ctx->pool_factor = o.pool_factor;
+            continue;
+        }
+        if (st == FEM_ERR_CAPACITY) {
+            if ((err = ctx->need(ctx->col_idx, (size_t)info.nnz * sizeof(int32_t)))) return cuda_fail(err);
+            if ((err = ctx->need(ctx->values, (size_t)info.nnz * sizeof(double)))) return cuda_fail(err);
+            if ((st = fem_alls_consolidate(&dm, &o, ctx->ws.p, ctx->ws.n, static_cast<int32_t*>(ctx->row_ptr.p),
+                                           static_cast<int32_t*>(ctx->col_idx.p), static_cast<double*>(ctx->values.p),
+                                           info.nnz, stream)))
+                return st;
+            st = fem_alls_read_info(ctx->ws.p, &info, stream);
+        }
+        break;
+    }
+    out->n_rows = (int32_t)n_rows;
+    out->nnz = info.nnz;
+    if (st != FEM_OK && st != FEM_ERR_DETJ) return st;
+    err = cudaMemcpyAsync(out->row_ptr, ctx->row_ptr.p, (n_rows + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (err) return cuda_fail(err);
+    if (out->capacity < info.nnz || !out->col_idx || !out->values) {
+        if ((err = cudaStreamSynchronize(s))) return cuda_fail(err);
+        return FEM_ERR_CAPACITY;
+    }
+    err = cudaMemcpyAsync(out->col_idx, ctx->col_idx.p, (size_t)info.nnz * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (!err)
+        err = cudaMemcpyAsync(out->values, ctx->values.p, (size_t)info.nnz * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (!err) err = cudaStreamSynchronize(s);
+    if (err) return cuda_fail(err);
+    return st;
+}
+
+}  // extern "C"

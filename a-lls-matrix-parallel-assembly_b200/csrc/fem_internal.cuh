@@ -1,0 +1,152 @@
+// Internal definitions shared by the kernels and the C ABI of the assembler.
+//
+// Row lists ("A-LLS" lists, after the reference's ALLSNode pool,
+// ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:63-67,384-391) live in a device
+// pool of fixed-size chunks. Every node n owns chunk n (its "first chunk");
+// further chunks come from an overflow pool through an atomic bump counter and
+// are linked with atomicCAS on the previous chunk's `next` word. A list entry
+// (slot) holds one column NODE and the dof_per_node^2 block of values of that
+// (row node, column node) pair, so the dpn rows of a node share one list.
+//
+// Chunk metadata is a row of H = S + 2 int32 words:
+//     word 0 = fill  (slots claimed so far; may overshoot S, readers clamp)
+//     word 1 = next  (chunk id + 1 of the next chunk, 0 = none)
+//     word 2+s = col (column node id + 1 of slot s, 0 = not yet written)
+// Slot values are stored slot-major: vals[gid * B + v], B = dpn^2, where gid is
+// the global slot id (first-chunk slots first, then overflow-chunk slots).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fem_alls.h"
+
+namespace fem {
+
+constexpr int kBlockThreads = 256;
+
+// Device-resident info word; its first bytes are laid out exactly as fem_info.
+struct DevInfo {
+    long long nnz;
+    long long list_entries;
+    int status_bits;
+    int overflow_chunks;   // overflow-pool bump counter (may overshoot the capacity)
+    int pool_chunks;
+    int max_row_entries;
+    int tile_ticket;       // consolidation tile dispenser
+    int pad0;
+    long long pad1[3];
+};
+static_assert(sizeof(DevInfo) == 64, "DevInfo size");
+static_assert(offsetof(DevInfo, max_row_entries) == offsetof(fem_info, max_row_entries), "fem_info layout");
+
+struct ListLayout {
+    int N;          // nodes (= first chunks)
+    int S1, S2;     // slots per first / overflow chunk
+    int H1, H2;     // int32 words per first / overflow chunk meta row (S + 2)
+    int B;          // values per slot (dpn^2)
+    int cap2;       // overflow chunk capacity
+    int* meta1;     // [N * H1]
+    int* meta2;     // [cap2 * H2]
+    double* vals;   // [(N*S1 + cap2*S2) * B]
+    DevInfo* info;
+};
+
+// Bits of DevInfo::status_bits are 1 << FEM_ERR_*.
+__device__ __forceinline__ void raise_status(DevInfo* info, int code) {
+    atomicOr(&info->status_bits, 1 << code);
+}
+
+__device__ __forceinline__ int* chunk_meta(const ListLayout& L, int c) {
+    return c < L.N ? L.meta1 + (size_t)c * L.H1 : L.meta2 + (size_t)(c - L.N) * L.H2;
+}
+__device__ __forceinline__ int chunk_cap(const ListLayout& L, int c) { return c < L.N ? L.S1 : L.S2; }
+__device__ __forceinline__ unsigned slot_gid(const ListLayout& L, int c, int s) {
+    return c < L.N ? (unsigned)c * (unsigned)L.S1 + (unsigned)s
+                   : (unsigned)L.N * (unsigned)L.S1 + (unsigned)(c - L.N) * (unsigned)L.S2 + (unsigned)s;
+}
+// Chunk id and slot of a global slot id.
+__device__ __forceinline__ void gid_chunk(const ListLayout& L, unsigned gid, int& c, int& s) {
+    unsigned first = (unsigned)L.N * (unsigned)L.S1;
+    if (gid < first) {
+        c = (int)(gid / (unsigned)L.S1);
+        s = (int)(gid % (unsigned)L.S1);
+    } else {
+        unsigned g2 = gid - first;
+        c = L.N + (int)(g2 / (unsigned)L.S2);
+        s = (int)(g2 % (unsigned)L.S2);
+    }
+}
+
+// L2-coherent loads (bypass L1: list words change under other SMs' writes).
+__device__ __forceinline__ int ld_cg(const int* p) { return __ldcg(p); }
+__device__ __forceinline__ int4 ld_cg4(const int* p) { return __ldcg(reinterpret_cast<const int4*>(p)); }
+
+// Takes one chunk from the overflow pool and zeroes its meta row. Returns the
+// chunk id, or -1 (and raises FEM_ERR_POOL_OVERFLOW) when the pool is empty.
+// The caller must __threadfence() before publishing the chunk.
+__device__ __forceinline__ int alloc_chunk(const ListLayout& L) {
+    int k = atomicAdd(&L.info->overflow_chunks, 1);
+    if (k >= L.cap2) {
+        raise_status(L.info, FEM_ERR_POOL_OVERFLOW);
+        return -1;
+    }
+    int* m = L.meta2 + (size_t)k * L.H2;
+    for (int i = 0; i < L.H2; i += 4) *reinterpret_cast<int4*>(m + i) = make_int4(0, 0, 0, 0);
+    return L.N + k;
+}
+
+// Bound on retry loops (chunk chains, claims); hitting it raises FEM_ERR_TIMEOUT.
+constexpr int kMaxChainSteps = 1 << 20;
+
+// A run of consecutive claimed slots gid .. gid + n - 1 (all in one chunk).
+struct ClaimRun {
+    unsigned gid;
+    int n;
+};
+
+// Claims up to `want` consecutive slots of one row, starting at chunk c (the
+// last chunk the caller scanned; c is advanced along the chain). Slots are
+// claimed with atomicAdd on the chunk's fill word; a full chunk is followed
+// through `next`, allocating and atomicCAS-linking a new chunk when there is
+// none. Returns an empty run only on pool overflow or timeout (status raised).
+// `spare` carries an allocated-but-unpublished chunk between calls (-1 = none).
+__device__ __forceinline__ ClaimRun claim_run(const ListLayout& L, int& c, int want, int& spare) {
+    for (int step = 0; step < kMaxChainSteps; step++) {
+        int* m = chunk_meta(L, c);
+        int cap = chunk_cap(L, c);
+        if (ld_cg(m) < cap) {  // skip the atomic on chunks already seen full
+            int base = atomicAdd(m, want);
+            int got = min(want, cap - base);
+            if (got > 0) return ClaimRun{slot_gid(L, c, base), got};
+        }
+        int nx = ld_cg(m + 1);
+        if (nx == 0) {
+            int nc = spare >= 0 ? spare : alloc_chunk(L);
+            spare = -1;
+            if (nc < 0) return ClaimRun{0u, 0};
+            __threadfence();  // the zeroed meta row is visible before the link
+            int old = atomicCAS(m + 1, 0, nc + 1);
+            if (old == 0) {
+                nx = nc + 1;
+            } else {
+                spare = nc;  // lost the race: keep it for this thread's next allocation
+                nx = old;
+            }
+        }
+        c = nx - 1;
+    }
+    raise_status(L.info, FEM_ERR_TIMEOUT);
+    return ClaimRun{0u, 0};
+}
+
+// Host-side layout description (sizes in bytes, offsets from the workspace base).
+struct HostLayout {
+    int kind, dpn, B, N, E;
+    int S1, S2, H1, H2, cap2;
+    int nodes_per_tile, num_tiles;
+    size_t off_info, off_meta1, off_meta2, off_vals, off_tiles, off_elist, total;
+    size_t meta1_bytes;
+};
+
+}  // namespace fem

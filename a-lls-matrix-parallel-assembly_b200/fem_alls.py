@@ -1,0 +1,262 @@
+"""Python binding of the assembler's C ABI (include/fem_alls.h) over ctypes.
+
+The library is ``lib/libfem_alls.so`` (built by build.py from csrc/); this
+module only marshals arguments. Device memory for meshes and CSR outputs comes
+from torch tensors on a CUDA device (torch is used as an allocator and stream
+provider, nothing else). Every call goes through the C ABI; there is no Python
+or CPU fallback: if the library or a GPU is missing the calls raise.
+
+Names mirror the reference's host-side assembly steps:
+``alls_scatter`` ~ assembleGlobalStiffnessKernelALLS
+(ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:394-468), ``alls_consolidate`` ~
+buildCSRStructure + convertALLStoCSRKernel (Q4A:605-645, Q4A:471-501), and
+``assemble`` the whole sequence of the reference driver (Q4A:794-827).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libfem_alls.so")
+
+FEM_OK = 0
+STATUS_NAMES = {0: "FEM_OK", 1: "FEM_ERR_BAD_ARG", 2: "FEM_ERR_BAD_MESH", 3: "FEM_ERR_POOL_OVERFLOW",
+                4: "FEM_ERR_DETJ", 5: "FEM_ERR_CUDA", 6: "FEM_ERR_CAPACITY", 7: "FEM_ERR_WORKSPACE",
+                8: "FEM_ERR_TIMEOUT", 9: "FEM_ERR_RANGE", 10: "FEM_ERR_ROW_TOO_LONG"}
+globals().update({v: k for k, v in STATUS_NAMES.items()})
+
+# C ABI exports (kept in sync with include/fem_alls.h by tests/test_abi.py).
+EXPORTS = ["fem_alls_workspace_size", "fem_alls_scatter", "fem_alls_consolidate", "fem_alls_read_info",
+           "fem_assemble", "fem_assemble_async", "fem_context_create", "fem_context_destroy",
+           "fem_assemble_host", "fem_status_string", "fem_last_cuda_error", "fem_abi_version"]
+
+
+class FemMesh(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("num_nodes", C.c_int32), ("num_elems", C.c_int32),
+                ("conn_stride", C.c_int32), ("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p),
+                ("conn", C.c_void_p), ("elem_type", C.c_void_p), ("E", C.c_void_p), ("nu", C.c_void_p),
+                ("E0", C.c_double), ("nu0", C.c_double), ("thickness", C.c_double)]
+
+
+class FemOpts(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("first_slots", C.c_int32), ("chunk_slots", C.c_int32),
+                ("flags", C.c_int32), ("pool_factor", C.c_double)]
+
+
+class FemCsr(C.Structure):
+    _fields_ = [("n_rows", C.c_int32), ("pad", C.c_int32), ("nnz", C.c_int64), ("capacity", C.c_int64),
+                ("row_ptr", C.c_void_p), ("col_idx", C.c_void_p), ("values", C.c_void_p)]
+
+
+class FemInfo(C.Structure):
+    _fields_ = [("nnz", C.c_int64), ("list_entries", C.c_int64), ("status_bits", C.c_int32),
+                ("overflow_chunks", C.c_int32), ("pool_chunks", C.c_int32), ("max_row_entries", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class FemError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        name = STATUS_NAMES.get(status, str(status))
+        extra = ""
+        if status == 5:
+            extra = f" (cudaError {load().fem_last_cuda_error()})"
+        super().__init__(f"{what}: {name}{extra}")
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load lib/libfem_alls.so (building it first if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            import build as _b  # noqa: WPS433 (local build script)
+            _b.build()
+        L = C.CDLL(LIB_PATH)
+        vp, p = C.c_void_p, C.POINTER
+        L.fem_alls_workspace_size.argtypes = [p(FemMesh), p(FemOpts), p(C.c_size_t)]
+        L.fem_alls_scatter.argtypes = [p(FemMesh), p(FemOpts), vp, C.c_size_t, vp]
+        L.fem_alls_consolidate.argtypes = [p(FemMesh), p(FemOpts), vp, C.c_size_t, vp, vp, vp, C.c_int64, vp]
+        L.fem_alls_read_info.argtypes = [vp, p(FemInfo), vp]
+        L.fem_assemble.argtypes = [p(FemMesh), p(FemOpts), vp, C.c_size_t, p(FemCsr), vp]
+        L.fem_assemble_async.argtypes = [p(FemMesh), p(FemOpts), vp, C.c_size_t, p(FemCsr), vp]
+        L.fem_context_create.argtypes = [p(vp)]
+        L.fem_context_destroy.argtypes = [vp]
+        L.fem_context_destroy.restype = None
+        L.fem_assemble_host.argtypes = [vp, p(FemMesh), p(FemOpts), p(FemCsr), vp]
+        L.fem_status_string.argtypes = [C.c_int32]
+        L.fem_status_string.restype = C.c_char_p
+        for f in EXPORTS:
+            if f not in ("fem_context_destroy", "fem_status_string"):
+                getattr(L, f).restype = C.c_int32
+        _lib = L
+    return _lib
+
+
+def opts(first_slots: int = 0, chunk_slots: int = 0, pool_factor: float = 0.0) -> FemOpts:
+    return FemOpts(0, first_slots, chunk_slots, 0, pool_factor)
+
+
+def _ptr(t) -> Optional[int]:
+    if t is None:
+        return None
+    if isinstance(t, np.ndarray):
+        return t.ctypes.data
+    return t.data_ptr()
+
+
+def fem_mesh_struct(mesh, arrays: dict) -> FemMesh:
+    """FemMesh over the buffers in `arrays` (device tensors or host numpy arrays)."""
+    return FemMesh(mesh.kind, mesh.num_nodes, mesh.num_elems, mesh.stride, _ptr(arrays["x"]), _ptr(arrays["y"]),
+                   _ptr(arrays.get("z")), _ptr(arrays["conn"]), _ptr(arrays.get("types")), _ptr(arrays.get("E")),
+                   _ptr(arrays.get("nu")), float(mesh.E0), float(mesh.nu0), float(mesh.thickness))
+
+
+def host_arrays(mesh) -> dict:
+    a = {"x": np.ascontiguousarray(mesh.x, np.float64), "y": np.ascontiguousarray(mesh.y, np.float64),
+         "conn": np.ascontiguousarray(mesh.conn, np.int32)}
+    if mesh.z is not None:
+        a["z"] = np.ascontiguousarray(mesh.z, np.float64)
+    if mesh.types is not None:
+        a["types"] = np.ascontiguousarray(mesh.types, np.uint8)
+    if mesh.E is not None:
+        a["E"] = np.ascontiguousarray(mesh.E, np.float64)
+    if mesh.nu is not None:
+        a["nu"] = np.ascontiguousarray(mesh.nu, np.float64)
+    return a
+
+
+def device_arrays(mesh, device="cuda"):
+    import torch
+    return {k: torch.from_numpy(v).to(device) for k, v in host_arrays(mesh).items()}
+
+
+def check(status: int, what: str, allow=(FEM_OK,)):
+    if status not in allow:
+        raise FemError(status, what)
+    return status
+
+
+def workspace_size(mesh, o: Optional[FemOpts] = None) -> int:
+    """Bytes of workspace (pure host computation; works without a GPU)."""
+    m = fem_mesh_struct(mesh, host_arrays(mesh))
+    n = C.c_size_t(0)
+    check(load().fem_alls_workspace_size(C.byref(m), C.byref(o) if o else None, C.byref(n)), "workspace_size")
+    return n.value
+
+
+class Assembler:
+    """Device-resident assembly of one mesh through the C ABI.
+
+    Holds the mesh arrays, workspace and CSR outputs as torch CUDA tensors so
+    repeated assemblies (benchmarks) allocate nothing."""
+
+    def __init__(self, mesh, o: Optional[FemOpts] = None, device="cuda", capacity: Optional[int] = None):
+        import torch
+        self.torch = torch
+        self.mesh = mesh
+        self.opts = o if o is not None else opts()
+        self.dev = device_arrays(mesh, device)
+        self.cm = fem_mesh_struct(mesh, self.dev)
+        self.ws_bytes = workspace_size(mesh, self.opts)
+        self.ws = torch.empty(self.ws_bytes + 256, dtype=torch.uint8, device=device)
+        base = self.ws.data_ptr()
+        self.ws_ptr = (base + 255) // 256 * 256
+        self.n_rows = mesh.num_dofs
+        self.row_ptr = torch.empty(self.n_rows + 1, dtype=torch.int32, device=device)
+        self.capacity = 0
+        self.col_idx = None
+        self.values = None
+        if capacity:
+            self.reserve(capacity)
+        self.lib = load()
+
+    def reserve(self, capacity: int):
+        if capacity > self.capacity:
+            self.col_idx = self.torch.empty(capacity, dtype=self.torch.int32, device=self.row_ptr.device)
+            self.values = self.torch.empty(capacity, dtype=self.torch.float64, device=self.row_ptr.device)
+            self.capacity = capacity
+
+    def _stream(self):
+        return self.torch.cuda.current_stream().cuda_stream
+
+    def scatter(self):
+        check(self.lib.fem_alls_scatter(C.byref(self.cm), C.byref(self.opts), self.ws_ptr, self.ws_bytes,
+                                        self._stream()), "fem_alls_scatter")
+
+    def consolidate(self, capacity: Optional[int] = None):
+        cap = self.capacity if capacity is None else capacity
+        check(self.lib.fem_alls_consolidate(C.byref(self.cm), C.byref(self.opts), self.ws_ptr, self.ws_bytes,
+                                            _ptr(self.row_ptr), _ptr(self.col_idx) if cap else None,
+                                            _ptr(self.values) if cap else None, cap, self._stream()),
+              "fem_alls_consolidate")
+
+    def read_info(self) -> tuple:
+        info = FemInfo()
+        st = self.lib.fem_alls_read_info(self.ws_ptr, C.byref(info), self._stream())
+        return st, info
+
+    def assemble_async(self):
+        """scatter + consolidate into the reserved capacity, no host sync."""
+        out = FemCsr(self.n_rows, 0, 0, self.capacity, _ptr(self.row_ptr), _ptr(self.col_idx),
+                     _ptr(self.values))
+        check(self.lib.fem_assemble_async(C.byref(self.cm), C.byref(self.opts), self.ws_ptr, self.ws_bytes,
+                                          C.byref(out), self._stream()), "fem_assemble_async")
+
+    def assemble(self, allow=(FEM_OK,)):
+        """Full assembly; sizes the outputs on first use. Returns (row_ptr, col_idx, values, info) tensors."""
+        self.scatter()
+        self.consolidate()
+        st, info = self.read_info()
+        if st == FEM_ERR_CAPACITY:
+            self.reserve(int(info.nnz))
+            self.consolidate()
+            st, info = self.read_info()
+        check(st, "assemble", allow)
+        nnz = int(info.nnz)
+        if self.col_idx is None:
+            self.reserve(max(nnz, 1))
+        return self.row_ptr, self.col_idx[:nnz], self.values[:nnz], info
+
+
+def assemble(mesh, o: Optional[FemOpts] = None, allow=(FEM_OK,)):
+    """Assemble on the GPU; returns numpy (row_ptr, col_idx, values, info dict)."""
+    a = Assembler(mesh, o)
+    rp, ci, v, info = a.assemble(allow)
+    return rp.cpu().numpy(), ci.cpu().numpy(), v.cpu().numpy(), info.as_dict()
+
+
+class HostContext:
+    """fem_assemble_host: host arrays in, host CSR out (copies inside the call)."""
+
+    def __init__(self):
+        self.lib = load()
+        self.ctx = C.c_void_p()
+        check(self.lib.fem_context_create(C.byref(self.ctx)), "fem_context_create")
+
+    def close(self):
+        if self.ctx:
+            self.lib.fem_context_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def assemble(self, mesh, arrays: dict, row_ptr: np.ndarray, col_idx: Optional[np.ndarray],
+                 values: Optional[np.ndarray], o: Optional[FemOpts] = None, stream=None) -> tuple:
+        m = fem_mesh_struct(mesh, arrays)
+        cap = 0 if col_idx is None else int(min(col_idx.shape[0], values.shape[0]))
+        out = FemCsr(mesh.num_dofs, 0, 0, cap, _ptr(row_ptr), _ptr(col_idx), _ptr(values))
+        st = self.lib.fem_assemble_host(self.ctx, C.byref(m), C.byref(o) if o else None, C.byref(out), stream)
+        return st, int(out.nnz)

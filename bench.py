@@ -1,0 +1,370 @@
+"""Benchmark of the FEM global-stiffness assembly (A-LLS path) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload t3|q4|mixed|hex20]
+                    [--impl ours|reference]
+
+A step is one full device assembly of a seeded synthetic mesh: list reset,
+fused element stiffness + A-LLS scatter, and list -> CSR consolidation (pattern
+and FP64 values), inputs resident in HBM. The default workload is the T3
+unstructured configuration (1000x1000 grid, random diagonals, shuffled
+elements, lognormal E). ``value`` is elements/s over the whole job; nnz/s,
+the roofline, the end-to-end figure through the host-buffer C ABI entry point
+(host<->device copies inside the timed region) and a CPU baseline are added to
+the same JSON line. With --gpus N > 1 (one process per GPU under torchrun) every
+rank assembles its own replica (the path has no exchange step): weak scaling.
+
+``--impl reference`` times the reference's own CPU path for the same workload:
+its host CSR pattern builder (buildCSRStructure, compiled from the reference
+sources into oracle/_ref) plus the serial FP64 value scatter of
+assembleGlobalStiffnessHost (ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:329-380;
+the reference's own function for Q4, the oracle's restatement of it for the
+other element kinds), on a bounded sample, in parallel on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "a-lls-matrix-parallel-assembly_b200"), os.path.join(ROOT, "oracle")]
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    "q4": ("q4_100x100", "Q4 plane stress 100x100 unit square, jitter 0.1h, E=1, nu=0.3, t=1, natural order"),
+    "t3": ("t3_1000x1000", "T3 1000x1000 grid, random diagonals, jitter 0.2h, shuffled, E~LogNormal(0,0.5), nu=0.3"),
+    "mixed": ("mixed_1500x1500", "Q4+T3 1500x1500 grid (p_Q4=0.5), jitter 0.15h, shuffled, E~LogNormal(0,0.5), nu~U[0.2,0.4]"),
+    "hex20": ("hex20_64x64x64", "Hex20 64^3 compact serendipity mesh, jitter 0.05h, E=1, nu=0.3, 3x3x3 Gauss"),
+}
+# A smaller instance of each workload's generator, for the CPU legs.
+CPU_SAMPLES = {"q4": ("q4", {}), "t3": ("t3", {"nx": 400, "ny": 400}),
+               "mixed": ("mixed", {"nx": 450, "ny": 450}), "hex20": ("hex20", {"nx": 12})}
+L2_BYTES = 126 * 2 ** 20
+
+
+def make_mesh(workload: str, **kw):
+    import meshgen as mg
+    if workload == "q4":
+        return mg.q4_grid(**kw) if kw else mg.q4_grid(100, 100)
+    if workload == "t3":
+        return mg.t3_grid(**kw) if kw else mg.t3_grid(1000, 1000)
+    if workload == "mixed":
+        return mg.mixed_grid(**kw) if kw else mg.mixed_grid(1500, 1500)
+    if workload == "hex20":
+        return mg.hex20_grid(**kw) if kw else mg.hex20_grid(64)
+    raise ValueError(workload)
+
+
+def algorithmic_bytes(mesh, nnz: int) -> dict:
+    """Algorithmic bytes of one assembly: inputs, CSR output and the A-LLS list
+    entries written once and read once (16 B each way per nnz)."""
+    dim = 3 if mesh.z is not None else 2
+    conn = int(np.sum(mesh.nodes_per_elem())) * 4
+    b_in = mesh.num_nodes * dim * 8 + conn + mesh.num_elems * 16 + (mesh.num_elems if mesh.types is not None else 0)
+    b_out = 4 * (mesh.num_dofs + 1) + 12 * nnz
+    b_list = 32 * nnz
+    return {"in": b_in, "out": b_out, "list": b_list, "total": b_in + b_out + b_list}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self) -> dict:
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (oracle / reference code)
+# ---------------------------------------------------------------------------
+
+def _cpu_sample_worker(args):
+    workload, use_reference = args
+    name, kw = CPU_SAMPLES[workload]
+    mesh = make_mesh(name, **kw)
+    import oracle as O
+    t0 = time.perf_counter()
+    if use_reference and O.ref_available("t3"):
+        rp, ci = O.ref_pattern(mesh)
+        if mesh.kind == 0:
+            vals = O.ref_q4a_host_assemble(mesh, rp, ci)  # noqa: F841 (reference material)
+        else:
+            O.assemble(mesh, rp, ci)
+        kind = "reference" if mesh.kind == 0 else "reference pattern + ported value scatter"
+    else:
+        O.assemble(mesh)
+        kind = "port"
+    dt = time.perf_counter() - t0
+    return mesh.num_elems, dt, kind, mesh.name
+
+
+def cpu_baseline(workload: str, use_reference: bool, workers: int) -> dict:
+    """Serial assembly on a bounded sample; `workers` independent copies in parallel."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    if workers <= 1:
+        res = [_cpu_sample_worker((workload, use_reference))]
+    else:
+        with ctx.Pool(workers) as pool:
+            res = pool.map(_cpu_sample_worker, [(workload, use_reference)] * workers)
+    wall = time.perf_counter() - t0
+    elems = sum(r[0] for r in res)
+    per = [r[0] / r[1] for r in res]
+    kind = res[0][2]
+    return {"value": float(sum(per)), "unit": "elements/s", "cores": workers,
+            "kind": "reference" if kind == "reference" else "port",
+            "sample": f"{len(res)} x {res[0][3]} ({res[0][0]} elements each), {kind}; serial pattern build + FP64 "
+                      f"values per copy, copies in parallel processes; wall {wall:.1f}s",
+            "elements": elems}
+
+
+# ---------------------------------------------------------------------------
+# GPU leg
+# ---------------------------------------------------------------------------
+
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import torch
+    import fem_alls as fem
+    import build
+    build.build()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    name, desc = WORKLOADS[args.workload]
+    mesh = make_mesh(args.workload)
+    asm = fem.Assembler(mesh, device=dev)
+    _, _, _, info = asm.assemble()          # sizes the outputs
+    nnz = int(info.nnz)
+    flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        asm.assemble_async()
+    torch.cuda.synchronize()
+    st, info = asm.read_info()
+    fem.check(st, "warmup assembly")
+
+    # per-kernel breakdown (untimed pass)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(stream)
+    asm.scatter()
+    ev[1].record(stream)
+    asm.consolidate()
+    ev[2].record(stream)
+    torch.cuda.synchronize()
+    t_scatter, t_cons = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        for i in range(args.steps):
+            flush.zero_()                      # evict L2 between steps (outside the step events)
+            starts[i].record(stream)
+            asm.assemble_async()
+            stops[i].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    times = [s.elapsed_time(e) for s, e in zip(starts, stops)]
+    st, info = asm.read_info()
+    fem.check(st, "timed assembly")
+    total_ms = sum(times)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms = total_ms / args.steps
+    clocks = clk.summary()
+
+    # end to end through the host-buffer entry point
+    e2e = None
+    if not args.no_e2e:
+        pinned = {k: torch.from_numpy(v).pin_memory() for k, v in fem.host_arrays(mesh).items()}
+        harr = {k: v.numpy() for k, v in pinned.items()}
+        rp = torch.empty(mesh.num_dofs + 1, dtype=torch.int32).pin_memory().numpy()
+        ci = torch.empty(nnz, dtype=torch.int32).pin_memory().numpy()
+        vv = torch.empty(nnz, dtype=torch.float64).pin_memory().numpy()
+        ctx = fem.HostContext()
+        s = stream.cuda_stream
+        for _ in range(max(1, args.warmup)):
+            fem.check(ctx.assemble(mesh, harr, rp, ci, vv, stream=s)[0], "fem_assemble_host")
+        torch.cuda.synchronize()
+        e_times = []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fem.check(ctx.assemble(mesh, harr, rp, ci, vv, stream=s)[0], "fem_assemble_host")
+            b.record(stream)
+            b.synchronize()
+            e_times.append(a.elapsed_time(b))
+        ctx.close()
+        te = torch.tensor([sum(e_times)], dtype=torch.float64, device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+        e_ms = float(te.item()) / args.steps
+        h2d = sum(v.nbytes for v in harr.values())
+        d2h = rp.nbytes + ci.nbytes + vv.nbytes
+        e2e = {"value": world * mesh.num_elems / (e_ms / 1e3), "unit": "elements/s", "ms_per_step": e_ms,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "api": "fem_assemble_host (pinned host buffers, copies inside the call)"}
+
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peak()
+    ab = algorithmic_bytes(mesh, nnz)
+    achieved = ab["total"] / (ms / 1e3) / 1e9
+    traffic = read_profile_traffic(args.workload)
+    line = {
+        "metric": "elements/s (device FP64 A-LLS assembly: element stiffness, list scatter, CSR pattern + values)",
+        "value": world * mesh.num_elems / (ms / 1e3),
+        "unit": "elements/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded mesh generator)",
+        "config": {"workload": name, "description": desc, "elements": mesh.num_elems, "nodes": mesh.num_nodes,
+                   "dofs": mesh.num_dofs, "nnz": nnz, "contributions": mesh.contributions(),
+                   "l2": "2x L2 buffer zeroed between steps, outside the per-step events",
+                   "parallelism": f"replicas{world}"},
+        "nnz_per_s": world * nnz / (ms / 1e3),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": traffic,
+                     "kernel": "one assembly step (scatter + consolidate kernels)",
+                     "algorithmic_bytes": ab, "frac_nominal_8tbs": achieved / 8000.0,
+                     "compulsory_frac": (ab["in"] + ab["out"]) / (ms / 1e3) / 1e9 / peak},
+        "kernels_ms": {"scatter": t_scatter, "consolidate": t_cons},
+        "list": {"entries": int(info.list_entries), "unique": nnz // mesh.dpn ** 2,
+                 "max_row_entries": int(info.max_row_entries), "overflow_chunks": int(info.overflow_chunks)},
+        "clocks": clocks,
+        "gpu_launches": KERNELS_PER_STEP[args.workload] * args.steps,
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(args.workload, use_reference=False, workers=1)
+    print(json.dumps(line), flush=True)
+
+
+# k_info_init, scatter kernel(s) (+ partition for mixed), k_consolidate_reset, k_consolidate
+KERNELS_PER_STEP = {"q4": 4, "t3": 4, "mixed": 6, "hex20": 4}
+
+
+def read_profile_traffic(workload: str):
+    """DRAM bytes per step from the committed ncu summary, if there is one."""
+    p = os.path.join(ROOT, "profiles", f"traffic_{workload}.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p)).get("dram_bytes_per_step")
+        except (ValueError, OSError):
+            return None
+    return None
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    workers = max(1, min(mp.cpu_count(), 16))
+    name, desc = WORKLOADS[args.workload]
+    vals = []
+    for _ in range(max(1, args.steps)):
+        cb = cpu_baseline(args.workload, use_reference=True, workers=workers)
+        vals.append(cb["value"])
+    v = statistics.median(vals)
+    cb["value"] = v
+    line = {"impl": "reference", "metric": "elements/s (device FP64 A-LLS assembly: element stiffness, list scatter, "
+            "CSR pattern + values)", "value": v, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded mesh generator)", "config": {"workload": name, "description": desc},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": "elements/s", "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="t3", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

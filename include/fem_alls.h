@@ -1,0 +1,185 @@
+/*
+ * fem_alls.h - C ABI of the B200 FEM global-stiffness assembler (A-LLS method).
+ *
+ * A mesh (node coordinates, connectivity, element type Q4 / T3 / Hex20 / mixed
+ * Q4+T3, per-element E and nu) goes in; a CSR matrix (row_ptr, col_idx sorted
+ * within each row, FP64 values) comes out. Element stiffness, the atomic
+ * row-list scatter and the list-to-CSR consolidation run as sm_100a CUDA
+ * kernels; there is no CPU fallback.
+ *
+ * The reference has no library API. Its de facto assembly call is a host
+ * sequence inside each benchmark driver; each entry point below names the step
+ * it replaces (file:line in zhou1533/A-LLS-Matrix-Parallel-Assembly):
+ *
+ *   buildCSRStructure           ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:605-645
+ *   (host pattern)              ALLS_T3_Unstructed_Elements_Assemble_Performance.cu:458-482
+ *                               ALLS_Q4_T3_Mixed_Elements_Assembly_Performance.cu:488-512
+ *                               ALLS_Hex20_3D_Assembly_Performance.cu:364-392
+ *   pool setup + resets         ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:776-813
+ *   assembleGlobalStiffness-    ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:394-468
+ *     KernelALLS(...)           ALLS_T3_Unstructed_Elements_Assemble_Performance.cu:227-290
+ *                               ALLS_Q4_T3_Mixed_Elements_Assembly_Performance.cu:248-312
+ *   ...ALLSFixedArray (Hex20)   ALLS_Hex20_3D_Assembly_Performance.cu:208-257
+ *   convertALLStoCSRKernel      ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:471-501
+ *   ...FixedArray (Hex20)       ALLS_Hex20_3D_Assembly_Performance.cu:259-278
+ *   CHECK_CUDA_ERROR -> exit(1) ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:15-23
+ *
+ * Differences a caller of the reference must know:
+ *  - the CSR pattern is built on the device (the reference builds it on the host
+ *    with std::set); it is identical to the reference's pattern;
+ *  - errors are returned as fem_status codes instead of exit(1);
+ *  - everything is stream-ordered and re-entrant: no __device__ globals (the
+ *    reference reaches its pool through __device__ pointers, Q4A:384-391);
+ *  - memory the library needs beyond inputs and outputs is a caller-provided
+ *    workspace (size from fem_alls_workspace_size).
+ *
+ * All pointers in fem_mesh / fem_csr are DEVICE pointers unless a function says
+ * otherwise. cudaStream_t is passed as void* so this header needs no CUDA header.
+ */
+#ifndef FEM_ALLS_H
+#define FEM_ALLS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FEM_ALLS_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define FEM_API __attribute__((visibility("default")))
+#else
+#define FEM_API
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+typedef int32_t fem_status;
+#define FEM_OK 0
+#define FEM_ERR_BAD_ARG 1        /* null pointer, bad size, unknown kind */
+#define FEM_ERR_BAD_MESH 2       /* node id < 0 or >= num_nodes in conn */
+#define FEM_ERR_POOL_OVERFLOW 3  /* list pool exhausted; retry with a larger pool_factor */
+#define FEM_ERR_DETJ 4           /* non-positive Jacobian determinant at a Gauss point
+                                    (the matrix is still assembled) */
+#define FEM_ERR_CUDA 5           /* a CUDA call failed (fem_last_cuda_error gives the code) */
+#define FEM_ERR_CAPACITY 6       /* col_idx/values capacity < nnz; info.nnz has the size */
+#define FEM_ERR_WORKSPACE 7      /* workspace too small or misaligned */
+#define FEM_ERR_TIMEOUT 8        /* a bounded wait inside a kernel gave up */
+#define FEM_ERR_RANGE 9          /* nnz or a pool index exceeds the int32/uint32 range */
+#define FEM_ERR_ROW_TOO_LONG 10  /* a row's list exceeded the consolidation capacity */
+
+/* ---- element kinds -------------------------------------------------------- */
+#define FEM_Q4 0        /* 4-node quadrilateral, plane stress, 2x2 Gauss, 2 dof/node */
+#define FEM_T3 1        /* 3-node triangle (CST), plane stress, 1 point, 2 dof/node */
+#define FEM_HEX20 2     /* 20-node serendipity hexahedron, 3x3x3 Gauss, 3 dof/node */
+#define FEM_MIXED_2D 3  /* Q4 and T3 in one mesh; conn_stride 4, elem_type per element */
+
+/* ---- precision of the element stiffness --------------------------------- */
+#define FEM_PREC_FP64 0  /* plain FP64 element stiffness (the oracle path) */
+
+typedef struct fem_mesh {
+    int32_t kind;          /* FEM_Q4, FEM_T3, FEM_HEX20, FEM_MIXED_2D */
+    int32_t num_nodes;
+    int32_t num_elems;
+    int32_t conn_stride;   /* ints per connectivity row: Q4 4, T3 3, HEX20 20, MIXED_2D 4 */
+    const double* x;       /* [num_nodes] node coordinates (structure of arrays) */
+    const double* y;       /* [num_nodes] */
+    const double* z;       /* [num_nodes], HEX20 only (else NULL) */
+    const int32_t* conn;   /* [num_elems * conn_stride] node ids, reference node order */
+    const uint8_t* elem_type; /* MIXED_2D: [num_elems] FEM_Q4 or FEM_T3; else NULL */
+    const double* E;       /* [num_elems] Young's modulus, or NULL for E0 everywhere */
+    const double* nu;      /* [num_elems] Poisson ratio, or NULL for nu0 everywhere */
+    double E0;
+    double nu0;
+    double thickness;      /* plane-stress thickness (2-D kinds) */
+} fem_mesh;
+
+typedef struct fem_opts {
+    int32_t precision;     /* FEM_PREC_FP64 */
+    int32_t first_slots;   /* list slots in each node's first chunk; 0 = default */
+    int32_t chunk_slots;   /* list slots per overflow chunk; 0 = default */
+    int32_t flags;         /* reserved, 0 */
+    double pool_factor;    /* overflow chunks per node in the pool; 0 = default */
+} fem_opts;
+
+typedef struct fem_csr {
+    int32_t n_rows;        /* num_nodes * dof per node */
+    int32_t pad;
+    int64_t nnz;           /* set by the library */
+    int64_t capacity;      /* entries available in col_idx / values */
+    int32_t* row_ptr;      /* [n_rows + 1] */
+    int32_t* col_idx;      /* [capacity] */
+    double* values;        /* [capacity] */
+} fem_csr;
+
+/* Device-side result word of the last assembly in a workspace. */
+typedef struct fem_info {
+    int64_t nnz;              /* CSR nonzeros */
+    int64_t list_entries;     /* list slots filled by the scatter (nnz/dof^2 + duplicates) */
+    int32_t status_bits;      /* OR of (1 << FEM_ERR_*) raised on the device */
+    int32_t overflow_chunks;  /* overflow chunks taken from the pool */
+    int32_t pool_chunks;      /* overflow chunk capacity of the pool */
+    int32_t max_row_entries;  /* longest row list (node granularity, duplicates included) */
+} fem_info;
+
+/* ---- workspace ------------------------------------------------------------ */
+
+/* Bytes of device workspace an assembly of this mesh needs (256-byte aligned).
+ * Depends on num_nodes, num_elems, kind and opts only. */
+FEM_API fem_status fem_alls_workspace_size(const fem_mesh* mesh, const fem_opts* opts, size_t* bytes);
+
+/* ---- the A-LLS path -------------------------------------------------------- */
+
+/* Resets the workspace lists and runs the fused element-stiffness + list
+ * scatter kernel(s). Replaces the reference's pool resets and
+ * assembleGlobalStiffnessKernelALLS / ...FixedArray launches. Asynchronous. */
+FEM_API fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* workspace,
+                            size_t workspace_bytes, void* stream);
+
+/* Consolidates the lists into CSR: per row sort + duplicate merge, device scan
+ * for row_ptr, coalesced writes of col_idx/values. Replaces the host
+ * buildCSRStructure and convertALLStoCSRKernel. row_ptr is always written; if
+ * capacity < nnz nothing else is written and the device info gets
+ * FEM_ERR_CAPACITY (the lists stay intact, so it can be re-run with larger
+ * buffers). capacity 0 with NULL col_idx/values just counts. Asynchronous. */
+FEM_API fem_status fem_alls_consolidate(const fem_mesh* mesh, const fem_opts* opts, void* workspace,
+                                size_t workspace_bytes, int32_t* row_ptr, int32_t* col_idx,
+                                double* values, int64_t capacity, void* stream);
+
+/* Copies the device info word of the last assembly to the host (synchronizes
+ * the stream) and returns the most severe status it holds. */
+FEM_API fem_status fem_alls_read_info(const void* workspace, fem_info* info, void* stream);
+
+/* scatter + consolidate + read_info. out->nnz is set. */
+FEM_API fem_status fem_assemble(const fem_mesh* mesh, const fem_opts* opts, void* workspace,
+                        size_t workspace_bytes, fem_csr* out, void* stream);
+
+/* scatter + consolidate without the host synchronization (graph capturable);
+ * read the outcome later with fem_alls_read_info. */
+FEM_API fem_status fem_assemble_async(const fem_mesh* mesh, const fem_opts* opts, void* workspace,
+                              size_t workspace_bytes, fem_csr* out, void* stream);
+
+/* ---- host-buffer entry point ------------------------------------------------ */
+
+typedef struct fem_context fem_context;
+
+FEM_API fem_status fem_context_create(fem_context** ctx);
+FEM_API void fem_context_destroy(fem_context* ctx);
+
+/* Same as fem_assemble, but mesh arrays and out arrays are HOST pointers (pinned
+ * memory is fastest). The context keeps grow-only device buffers between calls.
+ * If out->capacity < nnz, returns FEM_ERR_CAPACITY with out->nnz set and
+ * row_ptr filled. Synchronous. */
+FEM_API fem_status fem_assemble_host(fem_context* ctx, const fem_mesh* host_mesh, const fem_opts* opts,
+                             fem_csr* host_out, void* stream);
+
+/* ---- misc ------------------------------------------------------------------- */
+FEM_API const char* fem_status_string(fem_status s);
+FEM_API int32_t fem_last_cuda_error(void);   /* cudaError_t of the last FEM_ERR_CUDA (per thread) */
+FEM_API int32_t fem_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FEM_ALLS_H */

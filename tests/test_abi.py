@@ -1,0 +1,98 @@
+"""The C ABI library: it loads, exports every symbol include/*.h declares, and its
+host-side argument checking and workspace sizing behave (CPU, no kernel launches)."""
+import ctypes as C
+import glob
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def declared_functions():
+    names = []
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"^\s*FEM_API\s+[^(;]*?\b(fem_[A-Za-z0-9_]+)\s*\(", text, re.M)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol(fem):
+    lib = fem.load()
+    decl = declared_functions()
+    assert len(decl) >= 12
+    for name in decl:
+        assert hasattr(lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", fem.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (fem_\w+)", out))
+    assert exported == set(decl), (exported ^ set(decl))
+    assert set(fem.EXPORTS) == set(decl)
+
+
+def test_abi_version_and_status_strings(fem):
+    lib = fem.load()
+    assert lib.fem_abi_version() == 1
+    assert lib.fem_status_string(0) == b"ok"
+    assert b"pool" in lib.fem_status_string(3)
+
+
+def test_workspace_size_host_only(fem):
+    import meshgen as mg
+    m = mg.by_name("q4_small")
+    n = fem.workspace_size(m)
+    assert n > 0 and n % 256 == 0
+    # grows with the pool factor
+    assert fem.workspace_size(m, fem.opts(pool_factor=2.0)) > n
+    h = mg.by_name("hex20_small")
+    nh = fem.workspace_size(h)
+    nh2 = fem.workspace_size(h, fem.opts(first_slots=126, chunk_slots=62))
+    assert nh2 > nh
+
+
+def test_bad_arguments_are_rejected_before_any_launch(fem):
+    import meshgen as mg
+    lib = fem.load()
+    m = mg.by_name("q4_small")
+    arrays = fem.host_arrays(m)
+    cm = fem.fem_mesh_struct(m, arrays)
+    n = C.c_size_t()
+    assert lib.fem_alls_workspace_size(None, None, C.byref(n)) == fem.FEM_ERR_BAD_ARG
+    bad = fem.fem_mesh_struct(m, arrays)
+    bad.conn_stride = 3
+    assert lib.fem_alls_workspace_size(C.byref(bad), None, C.byref(n)) == fem.FEM_ERR_BAD_ARG
+    bad = fem.fem_mesh_struct(m, arrays)
+    bad.kind = 7
+    assert lib.fem_alls_workspace_size(C.byref(bad), None, C.byref(n)) == fem.FEM_ERR_BAD_ARG
+    # 2-D chunk rows are fixed
+    o = fem.opts(first_slots=30)
+    assert lib.fem_alls_workspace_size(C.byref(cm), C.byref(o), C.byref(n)) == fem.FEM_ERR_BAD_ARG
+    # Hex20 chunk rows must be a multiple of 16 bytes
+    h = mg.by_name("hex20_small")
+    ch = fem.fem_mesh_struct(h, fem.host_arrays(h))
+    o = fem.opts(first_slots=31)
+    assert lib.fem_alls_workspace_size(C.byref(ch), C.byref(o), C.byref(n)) == fem.FEM_ERR_BAD_ARG
+    # a workspace that is too small is refused before touching the device
+    assert lib.fem_alls_scatter(C.byref(cm), None, C.c_void_p(256), 16, None) == fem.FEM_ERR_WORKSPACE
+    # misaligned workspace
+    size = fem.workspace_size(m)
+    assert lib.fem_alls_scatter(C.byref(cm), None, C.c_void_p(257), size, None) == fem.FEM_ERR_WORKSPACE
+    # consolidate: capacity without buffers
+    assert lib.fem_alls_consolidate(C.byref(cm), None, C.c_void_p(256), size, C.c_void_p(512), None, None, 10,
+                                    None) == fem.FEM_ERR_BAD_ARG
+    assert lib.fem_alls_read_info(None, None, None) == fem.FEM_ERR_BAD_ARG
+
+
+def test_host_entry_point_checks_arguments(fem):
+    import meshgen as mg
+    ctx = fem.HostContext()
+    m = mg.by_name("q4_small")
+    arrays = fem.host_arrays(m)
+    bad = fem.fem_mesh_struct(m, arrays)
+    bad.num_nodes = 0
+    out = fem.FemCsr()
+    assert fem.load().fem_assemble_host(ctx.ctx, C.byref(bad), None, C.byref(out), None) == fem.FEM_ERR_BAD_ARG
+    ctx.close()
