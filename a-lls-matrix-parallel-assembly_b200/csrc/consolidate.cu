@@ -8,11 +8,13 @@
 //
 // One CTA handles a tile of NPT consecutive nodes; a group of G lanes serves
 // one node (all dpn dof rows of it):
-//   1. gather the node's list entries (column node, slot) from its chunk chain
-//      into shared memory as 64-bit keys (col << 32 | slot);
+//   1. gather the node's list entries (column node, slot) — the non-empty
+//      hashed slots of its chunk chain — into shared memory as 64-bit keys
+//      (col << 32 | slot);
 //   2. bitonic sort of the G*KPL keys across the group (shuffles + registers);
-//   3. mark the first key of every column run (duplicates are adjacent) and
-//      count unique columns u;
+//   3. mark the first key of every column run and count unique columns u (the
+//      scatter inserts each column once per row; runs longer than one would be
+//      summed all the same);
 //   4. tile-wide scan of u, then a single-pass decoupled look-back over tiles
 //      (tiles are handed out in launch order through an atomic ticket, so every
 //      predecessor is already running; waits are bounded);
@@ -94,10 +96,10 @@ __device__ int long_row_next_col(const ListLayout& L, int n, int after, int glan
     int c = n;
     for (int step = 0; step < kMaxChainSteps; step++) {
         const int* meta = chunk_meta(L, c);
-        const int fill = min(__ldg(meta), chunk_cap(L, c));
+        const int cap = chunk_cap(L, c);
         const int next = __ldg(meta + 1);
-        for (int s = glane; s < fill; s += G) {
-            const int col = __ldg(meta + 2 + s) - 1;
+        for (int s = glane; s < cap; s += G) {
+            const int col = (__ldg(meta + 2 + s) & kColMask) - 1;
             if (col > after && col < best) best = col;
         }
         if (next == 0) break;
@@ -134,10 +136,10 @@ __device__ void long_row_write(const ListLayout& L, int n, int u, long long base
         int c = n;
         for (int step = 0; step < kMaxChainSteps; step++) {
             const int* meta = chunk_meta(L, c);
-            const int fill = min(__ldg(meta), chunk_cap(L, c));
+            const int cap = chunk_cap(L, c);
             const int next = __ldg(meta + 1);
-            for (int s = glane; s < fill; s += G) {
-                if (__ldg(meta + 2 + s) - 1 == col) {
+            for (int s = glane; s < cap; s += G) {
+                if ((__ldg(meta + 2 + s) & kColMask) - 1 == col) {
                     const double* p = L.vals + (size_t)slot_gid(L, c, s) * B;
 #pragma unroll
                     for (int v = 0; v < B; v++) sum[v] += __ldg(p + v);
@@ -187,21 +189,26 @@ __global__ void __launch_bounds__(kBlockThreads) k_consolidate(ListLayout L, int
     const int n = tile * NPT + grp;
     const bool valid = n < L.N;
 
-    // 1. gather
+    const unsigned gmask = group_mask<G>((tid & 31) / G);
+    const int gshift = G == 32 ? 0 : ((tid & 31) / G) * G;
+    // 1. gather (non-empty hashed slots of every chunk of the row)
     int T = 0;
     bool long_row = false;
     if (valid) {
         int c = n;
         for (int step = 0; step < kMaxChainSteps; step++) {
             const int* meta = chunk_meta(L, c);
-            const int fill = min(__ldg(meta), chunk_cap(L, c));
+            const int cap = chunk_cap(L, c);
             const int next = __ldg(meta + 1);
-            for (int s = glane; s < fill; s += G) {
-                const int e = T + s;
-                const int col = __ldg(meta + 2 + s);
-                if (e < NK) s_keys[grp][e] = ((unsigned long long)(unsigned)(col - 1) << 32) | slot_gid(L, c, s);
+            for (int s0 = 0; s0 < cap; s0 += G) {
+                const int s = s0 + glane;
+                const int col = s < cap ? (__ldg(meta + 2 + s) & kColMask) : 0;
+                const unsigned used = __ballot_sync(gmask, col != 0) >> gshift;
+                const int e = T + __popc(used & ((1u << glane) - 1u));
+                if (col != 0 && e < NK)
+                    s_keys[grp][e] = ((unsigned long long)(unsigned)(col - 1) << 32) | slot_gid(L, c, s);
+                T += __popc(used);
             }
-            T += fill;
             if (next == 0) break;
             c = next - 1;
         }
@@ -240,7 +247,6 @@ __global__ void __launch_bounds__(kBlockThreads) k_consolidate(ListLayout L, int
 #pragma unroll
     for (int i = 0; i < KPL; i++)
         if (is_head[i]) s_head[grp][k++] = (short)(glane * KPL + i);
-    const unsigned gmask = group_mask<G>((tid & 31) / G);
     if (long_row) u = long_row_count<DPN, G>(L, n, T, glane, gmask);
     if (glane == 0) {
         s_head[grp][u < NK ? u : NK] = (short)Ts;

@@ -9,9 +9,17 @@
 // (row node, column node) pair, so the dpn rows of a node share one list.
 //
 // Chunk metadata is a row of H = S + 2 int32 words:
-//     word 0 = fill  (slots claimed so far; may overshoot S, readers clamp)
+//     word 0 = reserved (0)
 //     word 1 = next  (chunk id + 1 of the next chunk, 0 = none)
-//     word 2+s = col (column node id + 1 of slot s, 0 = not yet written)
+//     word 2+s = slot s: 0 = empty, col+1 = column node col (published),
+//                (col+1) | kPending = claimed, values being written
+// Within a chunk a column's slot is found by open addressing (linear probing
+// from a hash of the column); a chunk with no free slot on the probe sequence
+// continues in the next chunk. A slot is claimed by atomicCAS(0 -> col|pending),
+// so every column appears at most once per row. The claimer stores the initial
+// block values, fences, and publishes the column (clears kPending); other
+// contributors atomicAdd into published slots and wait (bounded) for pending
+// ones, but only after publishing their own claims, so no wait is circular.
 // Slot values are stored slot-major: vals[gid * B + v], B = dpn^2, where gid is
 // the global slot id (first-chunk slots first, then overflow-chunk slots).
 #pragma once
@@ -99,45 +107,46 @@ __device__ __forceinline__ int alloc_chunk(const ListLayout& L) {
 // Bound on retry loops (chunk chains, claims); hitting it raises FEM_ERR_TIMEOUT.
 constexpr int kMaxChainSteps = 1 << 20;
 
-// A run of consecutive claimed slots gid .. gid + n - 1 (all in one chunk).
-struct ClaimRun {
-    unsigned gid;
-    int n;
-};
+constexpr int kPending = (int)0x80000000;
+constexpr int kColMask = 0x7FFFFFFF;
 
-// Claims up to `want` consecutive slots of one row, starting at chunk c (the
-// last chunk the caller scanned; c is advanced along the chain). Slots are
-// claimed with atomicAdd on the chunk's fill word; a full chunk is followed
-// through `next`, allocating and atomicCAS-linking a new chunk when there is
-// none. Returns an empty run only on pool overflow or timeout (status raised).
-// `spare` carries an allocated-but-unpublished chunk between calls (-1 = none).
-__device__ __forceinline__ ClaimRun claim_run(const ListLayout& L, int& c, int want, int& spare) {
-    for (int step = 0; step < kMaxChainSteps; step++) {
-        int* m = chunk_meta(L, c);
-        int cap = chunk_cap(L, c);
-        if (ld_cg(m) < cap) {  // skip the atomic on chunks already seen full
-            int base = atomicAdd(m, want);
-            int got = min(want, cap - base);
-            if (got > 0) return ClaimRun{slot_gid(L, c, base), got};
+// Start of the probe sequence of column key `key` (col + 1) in a chunk of S slots.
+__device__ __forceinline__ int probe_start(int key, int S) {
+    return (int)__umulhi((unsigned)key * 2654435761u, (unsigned)S);
+}
+
+// Next chunk of chunk c, allocating and atomicCAS-linking a new one if there is
+// none. Returns -1 on pool overflow (status raised). `spare` keeps a chunk that
+// lost a link race for this thread's next allocation (-1 = none).
+__device__ __forceinline__ int next_chunk(const ListLayout& L, int c, int& spare) {
+    int* m = chunk_meta(L, c);
+    int nx = ld_cg(m + 1);
+    if (nx == 0) {
+        int nc = spare >= 0 ? spare : alloc_chunk(L);
+        spare = -1;
+        if (nc < 0) return -1;
+        __threadfence();  // the zeroed meta row is visible before the link
+        int old = atomicCAS(m + 1, 0, nc + 1);
+        if (old == 0) {
+            nx = nc + 1;
+        } else {
+            spare = nc;
+            nx = old;
         }
-        int nx = ld_cg(m + 1);
-        if (nx == 0) {
-            int nc = spare >= 0 ? spare : alloc_chunk(L);
-            spare = -1;
-            if (nc < 0) return ClaimRun{0u, 0};
-            __threadfence();  // the zeroed meta row is visible before the link
-            int old = atomicCAS(m + 1, 0, nc + 1);
-            if (old == 0) {
-                nx = nc + 1;
-            } else {
-                spare = nc;  // lost the race: keep it for this thread's next allocation
-                nx = old;
-            }
-        }
-        c = nx - 1;
+    }
+    return nx - 1;
+}
+
+// Bounded wait until a pending slot is published. Returns false (and raises
+// FEM_ERR_TIMEOUT) if it is not published within the bound.
+constexpr int kMaxPendingSpins = 1 << 22;
+__device__ __forceinline__ bool wait_published(const ListLayout& L, const int* word) {
+    for (int i = 0; i < kMaxPendingSpins; i++) {
+        if ((ld_cg(word) & kPending) == 0) return true;
+        __nanosleep(32);
     }
     raise_status(L.info, FEM_ERR_TIMEOUT);
-    return ClaimRun{0u, 0};
+    return false;
 }
 
 // Host-side layout description (sizes in bytes, offsets from the workspace base).

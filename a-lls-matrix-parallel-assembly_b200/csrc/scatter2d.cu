@@ -7,27 +7,30 @@
 //
 // One thread per element, as in the reference, but:
 //  * Ke is computed in registers in node-block form (upper blocks only);
-//  * each row node's list is read one 64-byte chunk row at a time (fill, next
-//    and 14 column slots in four 16-byte L2 loads) and all of the element's
-//    column nodes are matched against it at once, instead of a pointer walk per
-//    (row, col) pair;
-//  * missing columns are claimed as a run of consecutive slots with one
-//    atomicAdd on the chunk's fill word (full chunks are followed through `next`
-//    and new chunks are atomicCAS-linked); the claimer stores its block values
-//    with plain 16-byte stores, fences, and only then publishes the column ids,
-//    so every later atomicAdd lands on initialised values;
-//  * found columns are accumulated with atomicAdd (red.global.add.f64).
-// A reader that scans a chunk while a claim is in flight may miss that column
-// and append a duplicate; the consolidation merges duplicates, so no
-// contribution is lost (the reference can lose one, its head-insert race).
+//  * each row node's list is read one 64-byte chunk row at a time (next pointer
+//    and 14 hashed slots in four 16-byte L2 loads) and all of the element's
+//    column nodes are resolved against that view: a column is looked up along
+//    its probe sequence and, if absent, its slot is claimed with atomicCAS
+//    (empty -> col|pending) — one slot per column and row, never a duplicate;
+//  * the claimer stores its block values with plain 16-byte stores, fences, and
+//    publishes the column; found columns are accumulated with atomicAdd
+//    (red.global.add.f64), after a bounded wait if the slot is still pending.
+//    A thread publishes its own claims before it waits on anyone else's, so
+//    no wait can be circular.
+// The reference instead walks a pointer list per (row, col) pair and can lose a
+// contribution or insert a column twice (its head-insert race, Q4A:452-463).
 #include "element2d.cuh"
 #include "launch.h"
 
 namespace fem {
 namespace {
 
-constexpr unsigned kNone = 0xFFFFFFFFu;
-constexpr unsigned kNewBit = 0x80000000u;
+enum SlotState : int { kUnresolved = 0, kFound = 1, kFoundPending = 2, kClaimed = 3 };
+constexpr int kMask14 = (1 << k2DSlots) - 1;
+
+__device__ __forceinline__ unsigned rot14(unsigned m, int h) {
+    return ((m >> h) | (m << (k2DSlots - h))) & kMask14;
+}
 
 template <int NPE>
 __device__ __forceinline__ void scatter_element_2d(const MeshView& m, const ListLayout& L, int e, int& spare) {
@@ -60,75 +63,80 @@ __device__ __forceinline__ void scatter_element_2d(const MeshView& m, const List
     }
     if (!(det > 0.0)) raise_status(L.info, FEM_ERR_DETJ);
 
-    // Phase 1: find existing slots of (row node a, column node b).
-    unsigned slot[NPE][NPE];
-    int lastc[NPE];
 #pragma unroll
     for (int a = 0; a < NPE; a++) {
+        int state[NPE];
+        unsigned gid[NPE];
+        int* word[NPE];
 #pragma unroll
-        for (int b = 0; b < NPE; b++) slot[a][b] = kNone;
+        for (int b = 0; b < NPE; b++) {
+            state[b] = kUnresolved;
+            gid[b] = 0;
+            word[b] = nullptr;
+        }
+        // Resolve the slot of every column node of the element in row node a.
         int c = nodes[a];
         for (int step = 0; step < kMaxChainSteps; step++) {
-            const int* meta = chunk_meta(L, c);
-            int4 w0 = ld_cg4(meta), w1 = ld_cg4(meta + 4), w2 = ld_cg4(meta + 8), w3 = ld_cg4(meta + 12);
+            int* meta = chunk_meta(L, c);
+            const int4 w0 = ld_cg4(meta), w1 = ld_cg4(meta + 4), w2 = ld_cg4(meta + 8), w3 = ld_cg4(meta + 12);
             const int cols[k2DSlots] = {w0.z, w0.w, w1.x, w1.y, w1.z, w1.w, w2.x,
                                         w2.y, w2.z, w2.w, w3.x, w3.y, w3.z, w3.w};
-            const int fill = min(w0.x, k2DSlots);
+            unsigned empty = 0, pend = 0;
+#pragma unroll
+            for (int s = 0; s < k2DSlots; s++) {
+                empty |= (cols[s] == 0 ? 1u : 0u) << s;
+                pend |= (cols[s] < 0 ? 1u : 0u) << s;
+            }
             bool all = true;
 #pragma unroll
             for (int b = 0; b < NPE; b++) {
-                if (slot[a][b] == kNone) {
+                if (state[b] == kUnresolved) {
+                    const int key = nodes[b] + 1;
+                    unsigned match = 0;
 #pragma unroll
-                    for (int s = 0; s < k2DSlots; s++)
-                        if (s < fill && cols[s] == nodes[b] + 1) slot[a][b] = slot_gid(L, c, s);
-                }
-                all &= slot[a][b] != kNone;
-            }
-            lastc[a] = c;
-            if (all || w0.y == 0) break;
-            c = w0.y - 1;
-        }
-    }
-
-    // Phase 2: claim slots for the missing columns, a run per row.
-#pragma unroll
-    for (int a = 0; a < NPE; a++) {
-        int missing = 0;
-#pragma unroll
-        for (int b = 0; b < NPE; b++) missing += slot[a][b] == kNone;
-        if (missing) {
-            int c = lastc[a];
-            ClaimRun run{0u, 0};
-#pragma unroll
-            for (int b = 0; b < NPE; b++) {
-                if (slot[a][b] == kNone) {
-                    if (run.n == 0) run = claim_run(L, c, missing, spare);
-                    if (run.n > 0) {
-                        slot[a][b] = run.gid | kNewBit;
-                        run.gid++;
-                        run.n--;
+                    for (int s = 0; s < k2DSlots; s++) match |= (((cols[s] & kColMask) == key) ? 1u : 0u) << s;
+                    const int h = probe_start(key, k2DSlots);
+                    for (int tries = 0; tries <= k2DSlots; tries++) {
+                        const unsigned cand = rot14(match | empty, h);
+                        if (!cand) break;  // no free slot on this chunk's probe sequence
+                        int pos = h + __ffs(cand) - 1;
+                        pos -= pos >= k2DSlots ? k2DSlots : 0;
+                        if (match & (1u << pos)) {
+                            state[b] = (pend >> pos) & 1u ? kFoundPending : kFound;
+                        } else {
+                            const int old = atomicCAS(meta + 2 + pos, 0, key | kPending);
+                            empty &= ~(1u << pos);
+                            if (old == 0) {
+                                state[b] = kClaimed;
+                            } else if ((old & kColMask) == key) {
+                                state[b] = old < 0 ? kFoundPending : kFound;
+                            } else {
+                                continue;
+                            }
+                        }
+                        gid[b] = slot_gid(L, c, pos);
+                        word[b] = meta + 2 + pos;
+                        break;
                     }
-                    missing--;
                 }
+                all &= state[b] != kUnresolved;
             }
+            if (all) break;
+            c = next_chunk(L, c, spare);
+            if (c < 0) break;  // pool overflow: status raised, the rest of the row is dropped
         }
-    }
-
-    // Phase 3: values. New slots get plain stores, found slots atomic adds.
-    bool any_new = false;
-#pragma unroll
-    for (int a = 0; a < NPE; a++) {
+        // Claimed slots: store values, fence, publish. Found slots: atomicAdd.
+        bool claimed = false;
 #pragma unroll
         for (int b = 0; b < NPE; b++) {
-            const unsigned sl = slot[a][b];
-            if (sl == kNone) continue;  // dropped on pool overflow (status raised)
-            double* p = L.vals + (size_t)(sl & ~kNewBit) * 4;
+            if (state[b] == kUnresolved || state[b] == kFoundPending) continue;
+            double* p = L.vals + (size_t)gid[b] * 4;
             const double v0 = block_entry<NPE>(kb, a, b, 0), v1 = block_entry<NPE>(kb, a, b, 1);
             const double v2 = block_entry<NPE>(kb, a, b, 2), v3 = block_entry<NPE>(kb, a, b, 3);
-            if (sl & kNewBit) {
+            if (state[b] == kClaimed) {
                 reinterpret_cast<double2*>(p)[0] = make_double2(v0, v1);
                 reinterpret_cast<double2*>(p)[1] = make_double2(v2, v3);
-                any_new = true;
+                claimed = true;
             } else {
                 atomicAdd(p + 0, v0);
                 atomicAdd(p + 1, v1);
@@ -136,22 +144,20 @@ __device__ __forceinline__ void scatter_element_2d(const MeshView& m, const List
                 atomicAdd(p + 3, v3);
             }
         }
-    }
-
-    // Phase 4: publish the column ids of new slots after their values.
-    if (any_new) {
-        __threadfence();
+        if (claimed) {
+            __threadfence();
 #pragma unroll
-        for (int a = 0; a < NPE; a++) {
+            for (int b = 0; b < NPE; b++)
+                if (state[b] == kClaimed) atomicExch(word[b], nodes[b] + 1);
+        }
+        // Columns another thread is still writing: wait for them, then add.
 #pragma unroll
-            for (int b = 0; b < NPE; b++) {
-                const unsigned sl = slot[a][b];
-                if (sl != kNone && (sl & kNewBit)) {
-                    int c, s;
-                    gid_chunk(L, sl & ~kNewBit, c, s);
-                    chunk_meta(L, c)[2 + s] = nodes[b] + 1;
-                }
-            }
+        for (int b = 0; b < NPE; b++) {
+            if (state[b] != kFoundPending) continue;
+            if (!wait_published(L, word[b])) continue;
+            double* p = L.vals + (size_t)gid[b] * 4;
+#pragma unroll
+            for (int v = 0; v < 4; v++) atomicAdd(p + v, block_entry<NPE>(kb, a, b, v));
         }
     }
 }

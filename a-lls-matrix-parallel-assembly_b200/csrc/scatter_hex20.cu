@@ -15,21 +15,23 @@
 //    Ke_IJ = lambda M_IJ + mu M_IJ^T + mu tr(M_IJ) I  — algebraically the
 //    reference's per-Gauss-point block formula (H20:173-191) with
 //    c1 = lambda + 2 mu, c2 = lambda, c3 = mu, in double;
-//  * scatter: warp w serves row nodes w, w+8, w+16; each warp reads the row's
-//    chunk rows with lane-parallel L2 loads, matches all 20 column nodes at
-//    once, claims the missing ones as one run (atomicAdd on fill, atomicCAS
-//    chunk links), stores new blocks, atomicAdds found ones, fences and then
-//    publishes the new column ids.
+//  * scatter: warp w serves row nodes w, w+8, w+16. The warp copies the row's
+//    chunk slots into shared memory with lane-parallel L2 loads; lane j then
+//    resolves column node j along its hashed probe sequence, claiming a free
+//    slot with atomicCAS (empty -> col|pending) if the column is absent, and
+//    following / atomicCAS-linking overflow chunks when the probe sequence is
+//    full. Claimed blocks are stored, the warp fences and publishes them; found
+//    blocks are accumulated with atomicAdd (after a bounded wait for slots
+//    another warp is still writing).
 #include "launch.h"
 
 namespace fem {
 namespace {
 
-constexpr unsigned kNone = 0xFFFFFFFFu;
-constexpr unsigned kNewBit = 0x80000000u;
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kPairs = 210;
+constexpr int kMaxHex20Slots = 128;  // upper bound of S1, S2 (checked on the host)
 
 __device__ __forceinline__ int pair_index(int I, int J) { return I * 20 - I * (I - 1) / 2 + (J - I); }
 
@@ -71,12 +73,95 @@ struct Hex20Smem {
     double w[27];           // Gauss weight * detJ
     double G[27][60];       // physical gradients G[g][3*node + dir]
     double K[kPairs][9];    // upper node-pair blocks of Ke
-    unsigned slot[kWarps][20];
+    int view[kWarps][kMaxHex20Slots];   // per-warp copy of the chunk slots being probed
+    unsigned gid[kWarps][20];
+    int state[kWarps][20];
     int nodes[20];
     unsigned char pI[kPairs], pJ[kPairs];
     double lam, mu;
     int bad;
 };
+
+enum SlotState : int { kUnresolved = 0, kFound = 1, kFoundPending = 2, kClaimed = 3 };
+
+// Resolves the 20 column slots of row node I of the current element and
+// scatters its 20 Ke blocks (warp-cooperative; lane j owns column node j).
+__device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, int I, int warp, int lane,
+                                            int& spare) {
+    int* view = sm.view[warp];
+    const int key = lane < 20 ? sm.nodes[lane] + 1 : 0;
+    int state = lane < 20 ? kUnresolved : kFound;
+    unsigned gid = 0;
+    int* word = nullptr;
+    int c = sm.nodes[I];
+    for (int step = 0; step < kMaxChainSteps; step++) {
+        int* meta = chunk_meta(L, c);
+        const int cap = chunk_cap(L, c);
+        for (int s = lane; s < cap; s += 32) view[s] = ld_cg(meta + 2 + s);
+        __syncwarp();
+        if (state == kUnresolved) {
+            int p = probe_start(key, cap);
+            for (int tries = 0; tries < cap; tries++) {
+                int v = view[p];
+                if (v == 0) {
+                    v = atomicCAS(meta + 2 + p, 0, key | kPending);
+                    if (v == 0) {
+                        state = kClaimed;
+                        view[p] = key | kPending;
+                    } else {
+                        view[p] = v;
+                    }
+                }
+                if (state != kClaimed && (v & kColMask) == key) state = v < 0 ? kFoundPending : kFound;
+                if (state != kUnresolved) {
+                    gid = slot_gid(L, c, p);
+                    word = meta + 2 + p;
+                    break;
+                }
+                p = p + 1 == cap ? 0 : p + 1;
+            }
+        }
+        __syncwarp();
+        if (!__any_sync(0xFFFFFFFFu, state == kUnresolved)) break;
+        int nc = 0;
+        if (lane == 0) nc = next_chunk(L, c, spare);
+        c = __shfl_sync(0xFFFFFFFFu, nc, 0);
+        if (c < 0) break;  // pool overflow: status raised, unresolved columns dropped
+    }
+    if (lane < 20) {
+        sm.state[warp][lane] = state;
+        sm.gid[warp][lane] = gid;
+    }
+    __syncwarp();
+    // Claimed blocks: plain stores. Found (published) blocks: atomicAdd.
+    for (int idx = lane; idx < 20 * 9; idx += 32) {
+        const int j = idx / 9, v = idx - j * 9;
+        const int st = sm.state[warp][j];
+        if (st == kUnresolved || st == kFoundPending) continue;
+        const int a = v / 3, b = v - a * 3;
+        const double val = I <= j ? sm.K[pair_index(I, j)][3 * a + b] : sm.K[pair_index(j, I)][3 * b + a];
+        double* p = L.vals + (size_t)sm.gid[warp][j] * 9 + v;
+        if (st == kClaimed)
+            *p = val;
+        else
+            atomicAdd(p, val);
+    }
+    const bool any_claimed = __any_sync(0xFFFFFFFFu, state == kClaimed);
+    if (any_claimed) {
+        __threadfence();
+        __syncwarp();
+        if (state == kClaimed) atomicExch(word, key);
+    }
+    // Blocks of slots another warp is still writing: wait, then add.
+    if (state == kFoundPending && wait_published(L, word)) {
+        double* p = L.vals + (size_t)gid * 9;
+        for (int v = 0; v < 9; v++) {
+            const int a = v / 3, b = v - a * 3;
+            atomicAdd(p + v, I <= lane ? sm.K[pair_index(I, lane)][3 * a + b] : sm.K[pair_index(lane, I)][3 * b + a]);
+        }
+    }
+    __syncwarp();
+}
 
 __global__ void __launch_bounds__(kThreads) k_scatter_hex20(MeshView m, ListLayout L) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -188,71 +273,7 @@ __global__ void __launch_bounds__(kThreads) k_scatter_hex20(MeshView m, ListLayo
         __syncthreads();
 
         // Scatter: warp w serves row nodes w, w + 8, w + 16.
-        for (int I = warp; I < 20; I += kWarps) {
-            const int n = sm.nodes[I];
-            if (lane < 20) sm.slot[warp][lane] = kNone;
-            __syncwarp();
-            int c = n, lastc = n;
-            for (int step = 0; step < kMaxChainSteps; step++) {
-                const int* meta = chunk_meta(L, c);
-                const int cap = chunk_cap(L, c);
-                // fill / next change under other warps: take lane 0's view so the
-                // loop below stays warp-uniform
-                const int fill = min(__shfl_sync(0xFFFFFFFFu, ld_cg(meta), 0), cap);
-                const int next = __shfl_sync(0xFFFFFFFFu, ld_cg(meta + 1), 0);
-                for (int s = lane; s < fill; s += 32) {
-                    const int col = ld_cg(meta + 2 + s);
-                    if (col != 0) {
-#pragma unroll
-                        for (int j = 0; j < 20; j++)
-                            if (col == sm.nodes[j] + 1) sm.slot[warp][j] = slot_gid(L, c, s);
-                    }
-                }
-                lastc = c;
-                __syncwarp();
-                const bool found = lane >= 20 || sm.slot[warp][lane] != kNone;
-                if (__all_sync(0xFFFFFFFFu, found) || next == 0) break;
-                c = next - 1;
-            }
-            const unsigned missing = __ballot_sync(0xFFFFFFFFu, lane < 20 && sm.slot[warp][lane] == kNone);
-            if (lane == 0 && missing) {
-                int cc = lastc, want = __popc(missing);
-                ClaimRun run{0u, 0};
-                for (int j = 0; j < 20; j++) {
-                    if (!(missing & (1u << j))) continue;
-                    if (run.n == 0) run = claim_run(L, cc, want, spare);
-                    if (run.n == 0) break;  // pool overflow: status raised, rest dropped
-                    sm.slot[warp][j] = run.gid | kNewBit;
-                    run.gid++;
-                    run.n--;
-                    want--;
-                }
-            }
-            __syncwarp();
-            for (int idx = lane; idx < 20 * 9; idx += 32) {
-                const int j = idx / 9, v = idx % 9;
-                const unsigned sl = sm.slot[warp][j];
-                if (sl == kNone) continue;
-                const int a = v / 3, b = v % 3;
-                const double val = I <= j ? sm.K[pair_index(I, j)][3 * a + b] : sm.K[pair_index(j, I)][3 * b + a];
-                double* p = L.vals + (size_t)(sl & ~kNewBit) * 9 + v;
-                if (sl & kNewBit)
-                    *p = val;
-                else
-                    atomicAdd(p, val);
-            }
-            __threadfence();
-            __syncwarp();
-            if (lane < 20) {
-                const unsigned sl = sm.slot[warp][lane];
-                if (sl != kNone && (sl & kNewBit)) {
-                    int cc, s;
-                    gid_chunk(L, sl & ~kNewBit, cc, s);
-                    chunk_meta(L, cc)[2 + s] = sm.nodes[lane] + 1;
-                }
-            }
-            __syncwarp();
-        }
+        for (int I = warp; I < 20; I += kWarps) scatter_row(L, sm, I, warp, lane, spare);
         __syncthreads();
     }
 }
