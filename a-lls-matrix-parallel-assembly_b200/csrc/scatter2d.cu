@@ -75,6 +75,9 @@ __device__ __forceinline__ void scatter_element_2d(const MeshView& m, const List
             word[b] = nullptr;
         }
         // Resolve the slot of every column node of the element in row node a.
+        // A failed CAS means the register view of the chunk is stale; the chunk
+        // is then re-read before the remaining columns are resolved (a column
+        // another thread has just claimed must be found, not claimed again).
         int c = nodes[a];
         for (int step = 0; step < kMaxChainSteps; step++) {
             int* meta = chunk_meta(L, c);
@@ -87,41 +90,44 @@ __device__ __forceinline__ void scatter_element_2d(const MeshView& m, const List
                 empty |= (cols[s] == 0 ? 1u : 0u) << s;
                 pend |= (cols[s] < 0 ? 1u : 0u) << s;
             }
-            bool all = true;
+            bool all = true, full = false, stale = false;
 #pragma unroll
             for (int b = 0; b < NPE; b++) {
-                if (state[b] == kUnresolved) {
+                if (state[b] == kUnresolved && !stale) {
                     const int key = nodes[b] + 1;
                     unsigned match = 0;
 #pragma unroll
                     for (int s = 0; s < k2DSlots; s++) match |= (((cols[s] & kColMask) == key) ? 1u : 0u) << s;
                     const int h = probe_start(key, k2DSlots);
-                    for (int tries = 0; tries <= k2DSlots; tries++) {
-                        const unsigned cand = rot14(match | empty, h);
-                        if (!cand) break;  // no free slot on this chunk's probe sequence
+                    const unsigned cand = rot14(match | empty, h);
+                    if (!cand) {
+                        full = true;  // no free slot on this chunk's probe sequence
+                    } else {
                         int pos = h + __ffs(cand) - 1;
                         pos -= pos >= k2DSlots ? k2DSlots : 0;
                         if (match & (1u << pos)) {
                             state[b] = (pend >> pos) & 1u ? kFoundPending : kFound;
                         } else {
                             const int old = atomicCAS(meta + 2 + pos, 0, key | kPending);
-                            empty &= ~(1u << pos);
                             if (old == 0) {
                                 state[b] = kClaimed;
+                                empty &= ~(1u << pos);
                             } else if ((old & kColMask) == key) {
                                 state[b] = old < 0 ? kFoundPending : kFound;
                             } else {
-                                continue;
+                                stale = true;  // slot taken by another column: re-read the chunk
                             }
                         }
-                        gid[b] = slot_gid(L, c, pos);
-                        word[b] = meta + 2 + pos;
-                        break;
+                        if (state[b] != kUnresolved) {
+                            gid[b] = slot_gid(L, c, pos);
+                            word[b] = meta + 2 + pos;
+                        }
                     }
                 }
                 all &= state[b] != kUnresolved;
             }
             if (all) break;
+            if (stale || !full) continue;  // same chunk, fresh view
             c = next_chunk(L, c, spare);
             if (c < 0) break;  // pool overflow: status raised, the rest of the row is dropped
         }

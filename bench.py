@@ -48,8 +48,10 @@ CPU_SAMPLES = {"q4": ("q4", {}), "t3": ("t3", {"nx": 400, "ny": 400}),
 L2_BYTES = 126 * 2 ** 20
 
 
-def make_mesh(workload: str, **kw):
+def make_mesh(workload: str, size: int = 0, **kw):
     import meshgen as mg
+    if size:
+        kw = {"nx": size} if workload == "hex20" else {"nx": size, "ny": size}
     if workload == "q4":
         return mg.q4_grid(**kw) if kw else mg.q4_grid(100, 100)
     if workload == "t3":
@@ -183,7 +185,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     name, desc = WORKLOADS[args.workload]
-    mesh = make_mesh(args.workload)
+    mesh = make_mesh(args.workload, args.size)
+    if args.size:
+        name = mesh.name
     asm = fem.Assembler(mesh, device=dev)
     _, _, _, info = asm.assemble()          # sizes the outputs
     nnz = int(info.nnz)
@@ -344,6 +348,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="t3", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=0,
+                    help="grid cells per side instead of the configuration's (profiling a smaller case)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

@@ -26,7 +26,8 @@ def _check(fem, oracle_mod, m, o=None, allow=(0,)):
     bad = np.abs(v - ov) > RTOL * scale
     assert not bad.any(), f"{bad.sum()} entries off; max rel {rel:.3e}, max scaled {scaled:.3e}"
     assert info["nnz"] == oci.shape[0]
-    assert info["list_entries"] >= oci.shape[0] // (m.dpn * m.dpn)
+    # every column is inserted once per row: the lists hold no duplicates
+    assert info["list_entries"] == oci.shape[0] // (m.dpn * m.dpn)
     return rel, scaled, info
 
 
@@ -55,7 +56,10 @@ def test_reference_material_q4_values(fem, oracle_mod, cuda_device):
         conn, x, y = g["q4_ref10x100/conn"], g["q4_ref10x100/x"], g["q4_ref10x100/y"]
     m = mg.Mesh(mg.Q4, x, y, None, conn, None, None, None, E0=2.1e11, nu0=0.3, thickness=0.01)
     rel, scaled, _ = _check(fem, oracle_mod, m)
-    assert rel < 1e-13
+    # On this unperturbed mesh many off-diagonal entries cancel exactly between
+    # elements, so the per-entry relative error is meaningless there; the
+    # error relative to the row/column scale is what is bounded.
+    assert scaled < 1e-13
 
 
 def test_hex20_reference_lattice_with_orphan_nodes(fem, oracle_mod, cuda_device):
