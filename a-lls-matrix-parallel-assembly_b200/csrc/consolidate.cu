@@ -1,4 +1,5 @@
-// K2-K4 fused: list -> CSR consolidation.
+// List -> CSR consolidation: per-row counts -> device scan -> row_ptr, then a
+// per-row sort and coalesced write of col_idx / values.
 //
 // Replaces both the reference's host pattern build (buildCSRStructure,
 // ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:605-645; buildCSRStructureHex20,
@@ -6,39 +7,132 @@
 // (convertALLStoCSRKernel, Q4A:471-501; ...FixedArray, H20:259-278), which walk
 // each row's list and binary-search the host-built col_ind.
 //
-// One CTA handles a tile of NPT consecutive nodes; a group of G lanes serves
-// one node (all dpn dof rows of it):
-//   1. gather the node's list entries (column node, slot) — the non-empty
-//      hashed slots of its chunk chain — into shared memory as 64-bit keys
-//      (col << 32 | slot);
-//   2. bitonic sort of the G*KPL keys across the group (shuffles + registers);
-//   3. mark the first key of every column run and count unique columns u (the
-//      scatter inserts each column once per row; runs longer than one would be
-//      summed all the same);
-//   4. tile-wide scan of u, then a single-pass decoupled look-back over tiles
-//      (tiles are handed out in launch order through an atomic ticket, so every
-//      predecessor is already running; waits are bounded);
-//   5. write row_ptr and, row by row, col_idx = col*dpn + b and the value
-//      (sum of the run's slot values) with consecutive lanes on consecutive
-//      entries.
-// The result is the reference's pattern exactly: every dof row of node n holds
-// {c*dpn + b : c in adj(n)} in increasing order.
+// The scatter inserts every column once per row and counts the entries of each
+// row node in counts[n], so the CSR layout is known before any list is read:
+//   k_scan_reduce  per tile of 4096 nodes: sum of dpn^2 * counts
+//   k_scan_tiles   one CTA: exclusive scan of the tile sums, nnz, capacity check
+//   k_row_ptr      per tile: block scan of counts -> row_ptr of all dpn rows
+//   k_write        a group of G lanes per row node: gather the node's non-empty
+//                  hashed slots as 64-bit keys (col << 32 | slot), bitonic sort
+//                  across the group, then write each dof row's entries
+//                  (col*dpn + b, block value) with consecutive lanes on
+//                  consecutive entries. Rows longer than the group's sort
+//                  capacity take an exact slow path.
+// Every dof row of node n holds {c*dpn + b : c in adj(n)} in increasing order,
+// which is the reference's pattern.
+#include <algorithm>
+
 #include "launch.h"
 
 namespace fem {
 namespace {
 
 constexpr unsigned long long kEmptyKey = ~0ull;
-constexpr unsigned long long kFlagAggregate = 1ull << 62;
-constexpr unsigned long long kFlagPrefix = 2ull << 62;
-constexpr unsigned long long kValueMask = (1ull << 62) - 1;
-constexpr long long kMaxSpin = 1ll << 22;
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = kScanTile / kScanThreads;  // 16 nodes per thread
 
 __device__ __forceinline__ unsigned long long shfl_xor_u64(unsigned long long v, int m) {
     unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
     lo = __shfl_xor_sync(0xFFFFFFFFu, lo, m);
     hi = __shfl_xor_sync(0xFFFFFFFFu, hi, m);
     return ((unsigned long long)hi << 32) | lo;
+}
+
+// Block-wide exclusive scan of one long long per thread (kScanThreads threads).
+__device__ __forceinline__ long long block_exclusive_scan(long long v, long long* s_warp, long long& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long long inc = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const long long o = __shfl_up_sync(0xFFFFFFFFu, inc, d);
+        if (lane >= d) inc += o;
+    }
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        long long w = lane < kScanThreads / 32 ? s_warp[lane] : 0;
+        long long wi = w;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const long long o = __shfl_up_sync(0xFFFFFFFFu, wi, d);
+            if (lane >= d) wi += o;
+        }
+        if (lane < kScanThreads / 32) s_warp[lane] = wi - w;
+        if (lane == kScanThreads / 32 - 1) s_warp[kScanThreads / 32] = wi;
+    }
+    __syncthreads();
+    total = s_warp[kScanThreads / 32];
+    const long long out = s_warp[warp] + inc - v;
+    __syncthreads();  // s_warp may be reused by the caller's next scan
+    return out;
+}
+
+// Tile sums of dpn^2 * counts.
+template <int B>
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int* __restrict__ counts, int N,
+                                                              long long* __restrict__ tile_sums) {
+    __shared__ long long s_warp[kScanThreads / 32 + 1];
+    const long long base = (long long)blockIdx.x * kScanTile;
+    long long sum = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        const long long n = base + (long long)i * kScanThreads + threadIdx.x;
+        if (n < N) sum += __ldg(counts + n);
+    }
+    long long total;
+    block_exclusive_scan(sum, s_warp, total);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = (long long)B * total;
+}
+
+// Exclusive scan of the tile sums in place (one CTA), nnz, last row_ptr entry.
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(long long* __restrict__ tile_sums, int num_tiles,
+                                                             DevInfo* info, int* __restrict__ row_ptr_end,
+                                                             long long capacity) {
+    __shared__ long long s_warp[kScanThreads / 32 + 1];
+    long long carry = 0;
+    for (int base = 0; base < num_tiles; base += kScanThreads) {
+        const int t = base + threadIdx.x;
+        const long long v = t < num_tiles ? tile_sums[t] : 0;
+        long long total;
+        const long long ex = block_exclusive_scan(v, s_warp, total);
+        if (t < num_tiles) tile_sums[t] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) {
+        info->nnz = carry;
+        *row_ptr_end = (int)carry;
+        if (carry > 0x7FFFFFFFll) raise_status(info, FEM_ERR_RANGE);
+        if (carry > capacity) raise_status(info, FEM_ERR_CAPACITY);
+    }
+}
+
+// row_ptr of every dof row: node n's rows start at dpn^2 * (exclusive count sum).
+template <int DPN>
+__global__ void __launch_bounds__(kScanThreads) k_row_ptr(const int* __restrict__ counts, int N,
+                                                          const long long* __restrict__ tile_offsets,
+                                                          int* __restrict__ row_ptr) {
+    constexpr int B = DPN * DPN;
+    __shared__ long long s_warp[kScanThreads / 32 + 1];
+    const long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+    int c[kScanItems];
+    long long sum = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        const long long n = base + i;
+        c[i] = n < N ? __ldg(counts + n) : 0;
+        sum += c[i];
+    }
+    long long total;
+    long long off = tile_offsets[blockIdx.x] + (long long)B * block_exclusive_scan(sum, s_warp, total);
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        const long long n = base + i;
+        if (n < N) {
+#pragma unroll
+            for (int a = 0; a < DPN; a++) row_ptr[n * DPN + a] = (int)(off + (long long)a * DPN * c[i]);
+        }
+        off += (long long)B * c[i];
+    }
 }
 
 // Ascending bitonic sort of G*KPL keys held as keys[i] at position lane*KPL + i
@@ -80,16 +174,14 @@ __device__ __forceinline__ void group_sort(unsigned long long (&keys)[KPL], int 
     }
 }
 
-// Slow path for rows with more list entries than a group can sort at once (a
-// node of unusually high degree). Iterated minimum extraction: each unique
-// column is found as the smallest column above the previous one, with a
-// group-wide min over the row's entries; duplicate slots are summed by the same
-// walk. O(unique * entries / G) work, exact for any row length.
 template <int G>
 __device__ __forceinline__ unsigned group_mask(int grp_in_warp) {
     return G == 32 ? 0xFFFFFFFFu : (((1u << G) - 1u) << (grp_in_warp * G));
 }
 
+// Slow path for a row with more entries than a group can sort at once (a node
+// of unusually high degree): iterated minimum extraction over the row's chunk
+// chain. O(u * entries / G) work, exact for any row length.
 template <int G>
 __device__ int long_row_next_col(const ListLayout& L, int n, int after, int glane, unsigned mask) {
     int best = 0x7FFFFFFF;
@@ -108,18 +200,6 @@ __device__ int long_row_next_col(const ListLayout& L, int n, int after, int glan
 #pragma unroll
     for (int d = G / 2; d > 0; d >>= 1) best = min(best, __shfl_xor_sync(mask, best, d));
     return best;
-}
-
-template <int DPN, int G>
-__device__ int long_row_count(const ListLayout& L, int n, int T, int glane, unsigned mask) {
-    int u = 0, last = -1;
-    for (int it = 0; it < T; it++) {
-        const int c = long_row_next_col<G>(L, n, last, glane, mask);
-        if (c == 0x7FFFFFFF) break;
-        u++;
-        last = c;
-    }
-    return u;
 }
 
 template <int DPN, int G>
@@ -167,175 +247,95 @@ __device__ void long_row_write(const ListLayout& L, int n, int u, long long base
 }
 
 template <int DPN, int G, int KPL>
-__global__ void __launch_bounds__(kBlockThreads) k_consolidate(ListLayout L, int* __restrict__ row_ptr,
-                                                               int* __restrict__ col_idx, double* __restrict__ values,
-                                                               long long capacity, unsigned long long* tile_state,
-                                                               int num_tiles) {
-    constexpr int NPT = kBlockThreads / G;  // nodes per tile
-    constexpr int NK = G * KPL;             // key capacity per node
+__global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int* __restrict__ row_ptr,
+                                                         int* __restrict__ col_idx, double* __restrict__ values,
+                                                         long long capacity) {
+    constexpr int NPB = kBlockThreads / G;  // nodes per batch
+    constexpr int NK = G * KPL;             // sort capacity per node
     constexpr int B = DPN * DPN;
-    __shared__ unsigned long long s_keys[NPT][NK];
-    __shared__ short s_head[NPT][NK + 1];
-    __shared__ int s_u[NPT], s_ex[NPT], s_T[NPT];
-    __shared__ int s_tile;
-    __shared__ long long s_prefix, s_total;
-
+    __shared__ unsigned long long s_keys[NPB][NK];
+    if (L.info->nnz > capacity) return;  // FEM_ERR_CAPACITY already raised; write nothing
     const int tid = threadIdx.x;
-    if (tid == 0) s_tile = atomicAdd(&L.info->tile_ticket, 1);
-    __syncthreads();
-    const int tile = s_tile;
-    if (tile >= num_tiles) return;  // uniform
     const int grp = tid / G, glane = tid % G;
-    const int n = tile * NPT + grp;
-    const bool valid = n < L.N;
-
     const unsigned gmask = group_mask<G>((tid & 31) / G);
     const int gshift = G == 32 ? 0 : ((tid & 31) / G) * G;
-    // 1. gather (non-empty hashed slots of every chunk of the row)
-    int T = 0;
-    bool long_row = false;
-    if (valid) {
-        int c = n;
-        for (int step = 0; step < kMaxChainSteps; step++) {
-            const int* meta = chunk_meta(L, c);
-            const int cap = chunk_cap(L, c);
-            const int next = __ldg(meta + 1);
-            for (int s0 = 0; s0 < cap; s0 += G) {
-                const int s = s0 + glane;
-                const int col = s < cap ? (__ldg(meta + 2 + s) & kColMask) : 0;
-                const unsigned used = __ballot_sync(gmask, col != 0) >> gshift;
-                const int e = T + __popc(used & ((1u << glane) - 1u));
-                if (col != 0 && e < NK)
-                    s_keys[grp][e] = ((unsigned long long)(unsigned)(col - 1) << 32) | slot_gid(L, c, s);
-                T += __popc(used);
-            }
-            if (next == 0) break;
-            c = next - 1;
+    int t_sum = 0, t_max = 0;
+    for (long long nb = (long long)blockIdx.x * NPB; nb < L.N; nb += (long long)gridDim.x * NPB) {
+        const int n = (int)(nb + grp);
+        const bool valid = n < L.N;
+        int u = 0;
+        long long base = 0;
+        if (valid) {
+            base = __ldg(row_ptr + (size_t)n * DPN);
+            u = (__ldg(row_ptr + (size_t)n * DPN + 1) - (int)base) / DPN;
         }
-        long_row = T > NK;
-    }
-    const int Ts = long_row ? 0 : T;  // entries sorted in registers
-    __syncwarp();
-    // 2. sort
-    unsigned long long keys[KPL];
-#pragma unroll
-    for (int i = 0; i < KPL; i++) {
-        const int p = glane * KPL + i;
-        keys[i] = p < Ts ? s_keys[grp][p] : kEmptyKey;
-    }
-    group_sort<G, KPL>(keys, glane);
-#pragma unroll
-    for (int i = 0; i < KPL; i++) s_keys[grp][glane * KPL + i] = keys[i];
-    __syncwarp();
-    // 3. run heads
-    int heads = 0;
-    bool is_head[KPL];
-#pragma unroll
-    for (int i = 0; i < KPL; i++) {
-        const int p = glane * KPL + i;
-        is_head[i] = p < Ts && (p == 0 || (s_keys[grp][p] >> 32) != (s_keys[grp][p - 1] >> 32));
-        heads += is_head[i];
-    }
-    int incl = heads;
-#pragma unroll
-    for (int d = 1; d < G; d <<= 1) {
-        const int v = __shfl_up_sync(0xFFFFFFFFu, incl, d, G);
-        if (glane >= d) incl += v;
-    }
-    int u = __shfl_sync(0xFFFFFFFFu, incl, G - 1, G);
-    int k = incl - heads;
-#pragma unroll
-    for (int i = 0; i < KPL; i++)
-        if (is_head[i]) s_head[grp][k++] = (short)(glane * KPL + i);
-    if (long_row) u = long_row_count<DPN, G>(L, n, T, glane, gmask);
-    if (glane == 0) {
-        s_head[grp][u < NK ? u : NK] = (short)Ts;
-        s_u[grp] = valid ? u : 0;
-        s_T[grp] = valid ? T : 0;
-    }
-    __syncthreads();
-    // 4. tile scan + decoupled look-back
-    if (tid < 32) {
-        int v = tid < NPT ? s_u[tid] : 0;
-        int t = tid < NPT ? s_T[tid] : 0;
-        int inc = v;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const int o = __shfl_up_sync(0xFFFFFFFFu, inc, d);
-            if (tid >= d) inc += o;
-        }
-        if (tid < NPT) s_ex[tid] = inc - v;
-        int tmax = t, tsum = t;
-#pragma unroll
-        for (int d = 16; d > 0; d >>= 1) {
-            tmax = max(tmax, __shfl_xor_sync(0xFFFFFFFFu, tmax, d));
-            tsum += __shfl_xor_sync(0xFFFFFFFFu, tsum, d);
-        }
-        const long long agg = (long long)B * __shfl_sync(0xFFFFFFFFu, inc, 31);
-        if (tid == 0) {
-            atomicAdd(reinterpret_cast<unsigned long long*>(&L.info->list_entries), (unsigned long long)tsum);
-            atomicMax(&L.info->max_row_entries, tmax);
-            volatile unsigned long long* st = tile_state;
-            long long prefix = 0;
-            if (tile == 0) {
-                st[0] = kFlagPrefix | (unsigned long long)agg;
-            } else {
-                st[tile] = kFlagAggregate | (unsigned long long)agg;
-                int j = tile - 1;
-                long long spins = 0;
-                while (j >= 0) {
-                    const unsigned long long w = st[j];
-                    const unsigned long long flag = w & ~kValueMask;
-                    if (flag == 0) {
-                        if (++spins > kMaxSpin) {
-                            raise_status(L.info, FEM_ERR_TIMEOUT);
-                            break;
-                        }
-                        __nanosleep(64);
-                        continue;
-                    }
-                    prefix += (long long)(w & kValueMask);
-                    if (flag == kFlagPrefix) break;
-                    j--;
+        // 1. gather the non-empty slots of the node's chunk chain
+        int T = 0;
+        if (valid) {
+            int c = n;
+            for (int step = 0; step < kMaxChainSteps; step++) {
+                const int* meta = chunk_meta(L, c);
+                const int cap = chunk_cap(L, c);
+                const int next = __ldg(meta + 1);
+                for (int s0 = 0; s0 < cap; s0 += G) {
+                    const int s = s0 + glane;
+                    const int col = s < cap ? (__ldg(meta + 2 + s) & kColMask) : 0;
+                    const unsigned used = (__ballot_sync(gmask, col != 0) >> gshift) & gmask >> gshift;
+                    const int e = T + __popc(used & ((1u << glane) - 1u));
+                    if (col != 0 && e < NK)
+                        s_keys[grp][e] = ((unsigned long long)(unsigned)(col - 1) << 32) | slot_gid(L, c, s);
+                    T += __popc(used);
                 }
-                __threadfence();
-                st[tile] = kFlagPrefix | (unsigned long long)(prefix + agg);
+                if (next == 0) break;
+                c = next - 1;
             }
-            s_prefix = prefix;
-            s_total = prefix + agg;
-            if (tile == num_tiles - 1) {
-                row_ptr[(size_t)L.N * DPN] = (int)(prefix + agg);
-                L.info->nnz = prefix + agg;
-                if (prefix + agg > 0x7FFFFFFFll) raise_status(L.info, FEM_ERR_RANGE);
-            }
-            if (prefix + agg > capacity) raise_status(L.info, FEM_ERR_CAPACITY);
+            if (glane == 0 && T != u) raise_status(L.info, FEM_ERR_INTERNAL);
         }
-    }
-    __syncthreads();
-    // 5. writes
-    if (!valid) return;
-    const long long base = s_prefix + (long long)B * s_ex[grp];
-    if (glane < DPN) row_ptr[(size_t)n * DPN + glane] = (int)(base + (long long)glane * DPN * u);
-    if (s_total > capacity) return;
-    if (long_row) {
-        long_row_write<DPN, G>(L, n, u, base, glane, gmask, col_idx, values);
-        return;
-    }
-    const int row_len = DPN * u;
-    for (int a = 0; a < DPN; a++) {
-        const long long rbase = base + (long long)a * row_len;
-        for (int r = glane; r < row_len; r += G) {
-            const int kk = r / DPN, b = r - kk * DPN;
-            const int h0 = s_head[grp][kk], h1 = s_head[grp][kk + 1];
-            const unsigned long long key0 = s_keys[grp][h0];
-            double sum = 0.0;
-            for (int h = h0; h < h1; h++) {
-                const unsigned gid = (unsigned)s_keys[grp][h];
-                sum += __ldg(L.vals + (size_t)gid * B + a * DPN + b);
-            }
-            col_idx[rbase + r] = (int)(key0 >> 32) * DPN + b;
-            values[rbase + r] = sum;
+        t_sum += T;
+        t_max = max(t_max, T);
+        const bool long_row = T > NK;
+        const int Ts = long_row ? 0 : min(T, u);
+        __syncwarp();
+        // 2. sort
+        unsigned long long keys[KPL];
+#pragma unroll
+        for (int i = 0; i < KPL; i++) {
+            const int p = glane * KPL + i;
+            keys[i] = p < Ts ? s_keys[grp][p] : kEmptyKey;
         }
+        group_sort<G, KPL>(keys, glane);
+#pragma unroll
+        for (int i = 0; i < KPL; i++) s_keys[grp][glane * KPL + i] = keys[i];
+        __syncwarp();
+        // 3. write the dpn rows of the node
+        if (valid) {
+            if (long_row) {
+                long_row_write<DPN, G>(L, n, u, base, glane, gmask, col_idx, values);
+            } else {
+                const int row_len = DPN * Ts;
+                for (int a = 0; a < DPN; a++) {
+                    const long long rbase = base + (long long)a * DPN * u;
+                    for (int r = glane; r < row_len; r += G) {
+                        const int k = r / DPN, b = r - k * DPN;
+                        const unsigned long long key = s_keys[grp][k];
+                        col_idx[rbase + r] = (int)(key >> 32) * DPN + b;
+                        values[rbase + r] = __ldg(L.vals + (size_t)(unsigned)key * B + a * DPN + b);
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+    // list statistics (one atomic per warp)
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        t_max = max(t_max, __shfl_xor_sync(0xFFFFFFFFu, t_max, d));
+        t_sum += __shfl_xor_sync(0xFFFFFFFFu, t_sum, d);
+    }
+    if ((tid & 31) == 0) {
+        // every lane of a group counted the same rows: divide by G
+        atomicAdd(reinterpret_cast<unsigned long long*>(&L.info->list_entries), (unsigned long long)(t_sum / G));
+        atomicMax(&L.info->max_row_entries, t_max);
     }
 }
 
@@ -346,31 +346,36 @@ __global__ void k_info_init(DevInfo* info, int pool_chunks) {
 // Clears what a consolidation pass owns, so the pass can be re-run on the same
 // lists (e.g. after FEM_ERR_CAPACITY with larger output buffers).
 __global__ void k_consolidate_reset(DevInfo* info) {
-    constexpr int kOwned = (1 << FEM_ERR_CAPACITY) | (1 << FEM_ERR_RANGE) | (1 << FEM_ERR_ROW_TOO_LONG) |
-                           (1 << FEM_ERR_TIMEOUT);
+    constexpr int kOwned = (1 << FEM_ERR_CAPACITY) | (1 << FEM_ERR_RANGE) | (1 << FEM_ERR_INTERNAL);
     info->status_bits &= ~kOwned;
     info->nnz = 0;
     info->list_entries = 0;
     info->max_row_entries = 0;
-    info->tile_ticket = 0;
+}
+
+template <int DPN, int G, int KPL>
+cudaError_t launch_all(const ListLayout& L, int* row_ptr, int* col_idx, double* values, long long capacity,
+                       long long* tile_sums, int num_tiles, cudaStream_t s) {
+    k_consolidate_reset<<<1, 1, 0, s>>>(L.info);
+    k_scan_reduce<DPN * DPN><<<num_tiles, kScanThreads, 0, s>>>(L.counts, L.N, tile_sums);
+    k_scan_tiles<<<1, kScanThreads, 0, s>>>(tile_sums, num_tiles, L.info, row_ptr + (size_t)L.N * DPN, capacity);
+    k_row_ptr<DPN><<<num_tiles, kScanThreads, 0, s>>>(L.counts, L.N, tile_sums, row_ptr);
+    if (capacity > 0) {
+        constexpr int NPB = kBlockThreads / G;
+        const long long batches = ((long long)L.N + NPB - 1) / NPB;
+        const long long grid = std::min<long long>(batches, (long long)sm_count() * 8);
+        k_write<DPN, G, KPL><<<(int)(grid > 0 ? grid : 1), kBlockThreads, 0, s>>>(L, row_ptr, col_idx, values,
+                                                                                capacity);
+    }
+    return cudaGetLastError();
 }
 
 }  // namespace
 
 cudaError_t launch_consolidate(const ListLayout& L, int dpn, int* row_ptr, int* col_idx, double* values,
-                               long long capacity, unsigned long long* tile_state, int num_tiles, cudaStream_t s) {
-    cudaError_t err = cudaMemsetAsync(tile_state, 0, (size_t)num_tiles * sizeof(unsigned long long), s);
-    if (err) return err;
-    k_consolidate_reset<<<1, 1, 0, s>>>(L.info);
-    err = cudaGetLastError();
-    if (err) return err;
-    if (dpn == 3)
-        k_consolidate<3, 32, 8><<<num_tiles, kBlockThreads, 0, s>>>(L, row_ptr, col_idx, values, capacity, tile_state,
-                                                                    num_tiles);
-    else
-        k_consolidate<2, 16, 2><<<num_tiles, kBlockThreads, 0, s>>>(L, row_ptr, col_idx, values, capacity, tile_state,
-                                                                    num_tiles);
-    return cudaGetLastError();
+                               long long capacity, long long* tile_sums, int num_tiles, cudaStream_t s) {
+    if (dpn == 3) return launch_all<3, 32, 4>(L, row_ptr, col_idx, values, capacity, tile_sums, num_tiles, s);
+    return launch_all<2, 8, 2>(L, row_ptr, col_idx, values, capacity, tile_sums, num_tiles, s);
 }
 
 cudaError_t launch_info_init(DevInfo* info, int pool_chunks, cudaStream_t s) {

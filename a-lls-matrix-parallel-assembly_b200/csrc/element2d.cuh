@@ -102,6 +102,81 @@ __device__ __forceinline__ double ke_t3_blocks(const double (&x)[3], const doubl
     return det;
 }
 
+// Row a of Ke only: blocks K_ab for all b (used when one thread serves one row).
+template <int NPE>
+__device__ __forceinline__ void accumulate_row_2d(const double (&gx)[NPE], const double (&gy)[NPE], int a, double w,
+                                                  double d11, double d12, double d33, double (&kr)[NPE][4]) {
+    double xa = gx[0], ya = gy[0];
+#pragma unroll
+    for (int i = 1; i < NPE; i++) {
+        xa = a == i ? gx[i] : xa;
+        ya = a == i ? gy[i] : ya;
+    }
+    const double wxa = w * xa, wya = w * ya;
+#pragma unroll
+    for (int b = 0; b < NPE; b++) {
+        kr[b][0] = fma(d11 * wxa, gx[b], fma(d33 * wya, gy[b], kr[b][0]));
+        kr[b][1] = fma(d12 * wxa, gy[b], fma(d33 * wya, gx[b], kr[b][1]));
+        kr[b][2] = fma(d12 * wya, gx[b], fma(d33 * wxa, gy[b], kr[b][2]));
+        kr[b][3] = fma(d11 * wya, gy[b], fma(d33 * wxa, gx[b], kr[b][3]));
+    }
+}
+
+// Row a of a Q4 Ke (2x2 Gauss). Returns the minimum detJ.
+__device__ __forceinline__ double ke_q4_row(const double (&x)[4], const double (&y)[4], double E, double nu, double t,
+                                            int a, double (&kr)[4][4]) {
+    constexpr double g = 0.577350269189626;
+    double d11, d12, d33;
+    plane_stress_d(E, nu, d11, d12, d33);
+#pragma unroll
+    for (int b = 0; b < 4; b++) kr[b][0] = kr[b][1] = kr[b][2] = kr[b][3] = 0.0;
+    double min_det = 1e300;
+#pragma unroll
+    for (int gi = 0; gi < 2; gi++) {
+#pragma unroll
+        for (int gj = 0; gj < 2; gj++) {
+            const double xi = gi ? g : -g, eta = gj ? g : -g;
+            const double dxi[4] = {-0.25 * (1.0 - eta), 0.25 * (1.0 - eta), 0.25 * (1.0 + eta), -0.25 * (1.0 + eta)};
+            const double deta[4] = {-0.25 * (1.0 - xi), -0.25 * (1.0 + xi), 0.25 * (1.0 + xi), 0.25 * (1.0 - xi)};
+            double j0 = 0.0, j1 = 0.0, j2 = 0.0, j3 = 0.0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                j0 = fma(dxi[k], x[k], j0);
+                j1 = fma(dxi[k], y[k], j1);
+                j2 = fma(deta[k], x[k], j2);
+                j3 = fma(deta[k], y[k], j3);
+            }
+            const double det = j0 * j3 - j1 * j2;
+            min_det = fmin(min_det, det);
+            const double i0 = j3 / det, i1 = -j1 / det, i2 = -j2 / det, i3 = j0 / det;
+            double gx[4], gy[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                gx[k] = fma(i0, dxi[k], i1 * deta[k]);
+                gy[k] = fma(i2, dxi[k], i3 * deta[k]);
+            }
+            accumulate_row_2d<4>(gx, gy, a, det * t, d11, d12, d33, kr);
+        }
+    }
+    return min_det;
+}
+
+// Row a of a T3 Ke. Returns detJ.
+__device__ __forceinline__ double ke_t3_row(const double (&x)[3], const double (&y)[3], double E, double nu, double t,
+                                            int a, double (&kr)[3][4]) {
+    double d11, d12, d33;
+    plane_stress_d(E, nu, d11, d12, d33);
+#pragma unroll
+    for (int b = 0; b < 3; b++) kr[b][0] = kr[b][1] = kr[b][2] = kr[b][3] = 0.0;
+    const double j0 = x[1] - x[0], j1 = y[1] - y[0], j2 = x[2] - x[0], j3 = y[2] - y[0];
+    const double det = j0 * j3 - j1 * j2;
+    const double i0 = j3 / det, i1 = -j1 / det, i2 = -j2 / det, i3 = j0 / det;
+    const double gx[3] = {-i0 - i1, i0, i1};
+    const double gy[3] = {-i2 - i3, i2, i3};
+    accumulate_row_2d<3>(gx, gy, a, 0.5 * det * t, d11, d12, d33, kr);
+    return det;
+}
+
 // Entry v (= a_dof * 2 + b_dof) of block (a, b) from the upper blocks.
 template <int NPE>
 __device__ __forceinline__ double block_entry(const double (&kb)[Blocks2D<NPE>::kCount][4], int a, int b, int v) {

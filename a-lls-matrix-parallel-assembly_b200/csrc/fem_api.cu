@@ -10,6 +10,19 @@
 
 using namespace fem;
 
+namespace fem {
+int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+}  // namespace fem
+
 namespace {
 
 thread_local int32_t g_last_cuda_error = 0;
@@ -68,8 +81,7 @@ fem_status make_layout(const fem_mesh* m, const fem_opts* o, HostLayout& h) {
     h.cap2 = (int)cap2;
     const double slots = (double)h.N * h.S1 + (double)h.cap2 * h.S2;
     if (slots >= 2147483648.0) return FEM_ERR_RANGE;  // slot ids carry a flag in bit 31
-    h.nodes_per_tile = consolidate_nodes_per_tile(h.dpn);
-    h.num_tiles = (h.N + h.nodes_per_tile - 1) / h.nodes_per_tile;
+    h.num_tiles = (h.N + kScanTile - 1) / kScanTile;
     size_t off = 0;
     h.off_info = off;
     off += align_up(sizeof(DevInfo));
@@ -80,10 +92,14 @@ fem_status make_layout(const fem_mesh* m, const fem_opts* o, HostLayout& h) {
     off += align_up((size_t)h.cap2 * h.H2 * sizeof(int));
     h.off_vals = off;
     off += align_up((size_t)slots * h.B * sizeof(double));
+    h.off_counts = off;
+    off += align_up((size_t)h.N * sizeof(int));
     h.off_tiles = off;
-    off += align_up((size_t)h.num_tiles * sizeof(unsigned long long));
-    h.off_elist = off;
-    if (h.kind == FEM_MIXED_2D) off += align_up(2 * sizeof(int)) + 2 * align_up((size_t)h.E * sizeof(int));
+    off += align_up((size_t)h.num_tiles * sizeof(long long));
+    h.off_elist = off;  // 2-D: visit order of the elements (perm), ranges, bucket histogram
+    if (h.dpn == 2)
+        off += align_up((size_t)h.E * sizeof(int)) + align_up(4 * sizeof(int)) +
+               align_up((size_t)2 * reorder_buckets(h.N) * sizeof(int));
     h.total = off;
     return FEM_OK;
 }
@@ -101,6 +117,7 @@ ListLayout device_layout(const HostLayout& h, void* ws) {
     L.meta1 = reinterpret_cast<int*>(b + h.off_meta1);
     L.meta2 = reinterpret_cast<int*>(b + h.off_meta2);
     L.vals = reinterpret_cast<double*>(b + h.off_vals);
+    L.counts = reinterpret_cast<int*>(b + h.off_counts);
     L.info = reinterpret_cast<DevInfo*>(b + h.off_info);
     return L;
 }
@@ -130,8 +147,8 @@ fem_status check_ws(const HostLayout& h, const void* ws, size_t bytes) {
 
 // Most severe status among the device bits.
 fem_status decode_bits(int bits) {
-    static const int order[] = {FEM_ERR_BAD_MESH,  FEM_ERR_POOL_OVERFLOW, FEM_ERR_TIMEOUT, FEM_ERR_ROW_TOO_LONG,
-                                FEM_ERR_RANGE,     FEM_ERR_CAPACITY,      FEM_ERR_DETJ};
+    static const int order[] = {FEM_ERR_BAD_MESH, FEM_ERR_POOL_OVERFLOW, FEM_ERR_TIMEOUT, FEM_ERR_INTERNAL,
+                                FEM_ERR_RANGE,    FEM_ERR_CAPACITY,      FEM_ERR_DETJ};
     for (int code : order)
         if (bits & (1 << code)) return code;
     return FEM_OK;
@@ -156,7 +173,7 @@ const char* fem_status_string(fem_status s) {
         case FEM_ERR_WORKSPACE: return "workspace too small or misaligned";
         case FEM_ERR_TIMEOUT: return "bounded wait gave up";
         case FEM_ERR_RANGE: return "size exceeds the int32 range";
-        case FEM_ERR_ROW_TOO_LONG: return "row list longer than the consolidation capacity";
+        case FEM_ERR_INTERNAL: return "list consistency check failed";
         default: return "unknown status";
     }
 }
@@ -183,21 +200,20 @@ fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* wo
     cudaError_t err = cudaMemsetAsync(b + h.off_info, 0, sizeof(DevInfo), s);
     if (!err) err = launch_info_init(L.info, h.cap2, s);
     if (!err) err = cudaMemsetAsync(b + h.off_meta1, 0, h.meta1_bytes, s);
+    if (!err) err = cudaMemsetAsync(b + h.off_counts, 0, (size_t)h.N * sizeof(int), s);
     if (err) return cuda_fail(err);
     if (h.E == 0) return FEM_OK;
     MeshView m = mesh_view(mesh);
-    switch (h.kind) {
-        case FEM_Q4: err = launch_scatter_2d(m, L, 4, nullptr, nullptr, s); break;
-        case FEM_T3: err = launch_scatter_2d(m, L, 3, nullptr, nullptr, s); break;
-        case FEM_HEX20: err = launch_scatter_hex20(m, L, s); break;
-        default: {
-            int* counts = reinterpret_cast<int*>(b + h.off_elist);
-            int* lq = reinterpret_cast<int*>(b + h.off_elist + align_up(2 * sizeof(int)));
-            int* lt = reinterpret_cast<int*>(b + h.off_elist + align_up(2 * sizeof(int)) + align_up((size_t)h.E * sizeof(int)));
-            err = launch_partition_2d(m, lq, lt, counts, s);
-            if (!err) err = launch_scatter_2d(m, L, 4, lq, counts + 0, s);
-            if (!err) err = launch_scatter_2d(m, L, 3, lt, counts + 1, s);
-        }
+    if (h.kind == FEM_HEX20) {
+        err = launch_scatter_hex20(m, L, s);
+    } else {
+        int* perm = reinterpret_cast<int*>(b + h.off_elist);
+        int* ranges = reinterpret_cast<int*>(b + h.off_elist + align_up((size_t)h.E * sizeof(int)));
+        int* hist = reinterpret_cast<int*>(b + h.off_elist + align_up((size_t)h.E * sizeof(int)) +
+                                           align_up(4 * sizeof(int)));
+        err = launch_reorder(m, hist, ranges, perm, sm_count(), s);
+        if (!err && h.kind != FEM_T3) err = launch_scatter_2d(m, L, 4, perm, ranges + 0, s);
+        if (!err && h.kind != FEM_Q4) err = launch_scatter_2d(m, L, 3, perm, ranges + 2, s);
     }
     return err ? cuda_fail(err) : FEM_OK;
 }
@@ -211,7 +227,7 @@ fem_status fem_alls_consolidate(const fem_mesh* mesh, const fem_opts* opts, void
     if (!row_ptr || capacity < 0 || (capacity > 0 && (!col_idx || !values))) return FEM_ERR_BAD_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     ListLayout L = device_layout(h, workspace);
-    unsigned long long* tiles = reinterpret_cast<unsigned long long*>(static_cast<unsigned char*>(workspace) + h.off_tiles);
+    long long* tiles = reinterpret_cast<long long*>(static_cast<unsigned char*>(workspace) + h.off_tiles);
     cudaError_t err = launch_consolidate(L, h.dpn, row_ptr, col_idx, values, capacity, tiles, h.num_tiles, s);
     return err ? cuda_fail(err) : FEM_OK;
 }

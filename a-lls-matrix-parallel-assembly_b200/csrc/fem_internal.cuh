@@ -32,6 +32,7 @@
 namespace fem {
 
 constexpr int kBlockThreads = 256;
+constexpr int kScanTile = 4096;  // nodes per scan tile (256 threads x 16)
 
 // Device-resident info word; its first bytes are laid out exactly as fem_info.
 struct DevInfo {
@@ -57,6 +58,7 @@ struct ListLayout {
     int* meta1;     // [N * H1]
     int* meta2;     // [cap2 * H2]
     double* vals;   // [(N*S1 + cap2*S2) * B]
+    int* counts;    // [N] list entries of each row node (incremented by the claimers)
     DevInfo* info;
 };
 
@@ -153,8 +155,8 @@ __device__ __forceinline__ bool wait_published(const ListLayout& L, const int* w
 struct HostLayout {
     int kind, dpn, B, N, E;
     int S1, S2, H1, H2, cap2;
-    int nodes_per_tile, num_tiles;
-    size_t off_info, off_meta1, off_meta2, off_vals, off_tiles, off_elist, total;
+    int num_tiles;  // scan tiles of kScanTile nodes
+    size_t off_info, off_meta1, off_meta2, off_vals, off_counts, off_tiles, off_elist, total;
     size_t meta1_bytes;
 };
 

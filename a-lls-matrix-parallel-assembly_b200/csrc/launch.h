@@ -24,16 +24,17 @@ struct MeshView {
 // 2-D chunk rows are 16 int32 words (14 slots + fill + next).
 constexpr int k2DSlots = 14;
 
-cudaError_t launch_scatter_2d(const MeshView& m, const ListLayout& L, int npe, const int* elist,
-                              const int* ecount, cudaStream_t s);
-cudaError_t launch_partition_2d(const MeshView& m, int* list_q4, int* list_t3, int* counts, cudaStream_t s);
+// perm: element visit order; range: device ints {begin, end} into perm.
+cudaError_t launch_scatter_2d(const MeshView& m, const ListLayout& L, int npe, const int* perm, const int* range,
+                              cudaStream_t s);
+// Node-local element order (perm) and the element ranges {q4 begin, q4 end, t3 begin, t3 end}.
+int reorder_buckets(int num_nodes);
+cudaError_t launch_reorder(const MeshView& m, int* hist, int* ranges, int* perm, int sms, cudaStream_t s);
+int sm_count();
 cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, cudaStream_t s);
 cudaError_t launch_consolidate(const ListLayout& L, int dpn, int* row_ptr, int* col_idx, double* values,
-                               long long capacity, unsigned long long* tile_state, int num_tiles,
-                               cudaStream_t s);
+                               long long capacity, long long* tile_sums, int num_tiles, cudaStream_t s);
 cudaError_t launch_info_init(DevInfo* info, int pool_chunks, cudaStream_t s);
 
-// Nodes handled by one consolidation tile (one CTA).
-inline int consolidate_nodes_per_tile(int dpn) { return dpn == 3 ? 8 : 16; }
 
 }  // namespace fem

@@ -5,20 +5,24 @@
 //  ALLS_T3_Unstructed_Elements_Assemble_Performance.cu:227-290,
 //  ALLS_Q4_T3_Mixed_Elements_Assembly_Performance.cu:248-312).
 //
-// One thread per element, as in the reference, but:
-//  * Ke is computed in registers in node-block form (upper blocks only);
-//  * each row node's list is read one 64-byte chunk row at a time (next pointer
-//    and 14 hashed slots in four 16-byte L2 loads) and all of the element's
-//    column nodes are resolved against that view: a column is looked up along
-//    its probe sequence and, if absent, its slot is claimed with atomicCAS
-//    (empty -> col|pending) — one slot per column and row, never a duplicate;
+// One thread per (element, row node) instead of one per element:
+//  * elements are visited in a node-local order (reorder.cu) so the lists they
+//    touch stay in L2;
+//  * the thread computes its row of Ke in registers (node-block form) and reads
+//    its row node's list one 64-byte chunk row at a time (next pointer and 14
+//    hashed slots in four 16-byte L2 loads); every column node of the element
+//    is looked up along its probe sequence and, if absent, its slot is claimed
+//    with atomicCAS (empty -> col|pending) — one slot per column and row, never
+//    a duplicate; a failed CAS re-reads the chunk before the next column;
 //  * the claimer stores its block values with plain 16-byte stores, fences, and
 //    publishes the column; found columns are accumulated with atomicAdd
 //    (red.global.add.f64), after a bounded wait if the slot is still pending.
 //    A thread publishes its own claims before it waits on anyone else's, so
-//    no wait can be circular.
+//    no wait can be circular. Claims are counted per row node for the scan.
 // The reference instead walks a pointer list per (row, col) pair and can lose a
 // contribution or insert a column twice (its head-insert race, Q4A:452-463).
+#include <algorithm>
+
 #include "element2d.cuh"
 #include "launch.h"
 
@@ -33,8 +37,7 @@ __device__ __forceinline__ unsigned rot14(unsigned m, int h) {
 }
 
 template <int NPE>
-__device__ __forceinline__ void scatter_element_2d(const MeshView& m, const ListLayout& L, int e, int& spare) {
-    using Blk = Blocks2D<NPE>;
+__device__ __forceinline__ void scatter_row_2d(const MeshView& m, const ListLayout& L, int e, int a, int& spare) {
     int nodes[NPE];
     bool bad = false;
 #pragma unroll
@@ -43,7 +46,7 @@ __device__ __forceinline__ void scatter_element_2d(const MeshView& m, const List
         bad |= (nodes[a] < 0) | (nodes[a] >= m.N);
     }
     if (bad) {
-        raise_status(L.info, FEM_ERR_BAD_MESH);
+        if (a == 0) raise_status(L.info, FEM_ERR_BAD_MESH);
         return;
     }
     double xe[NPE], ye[NPE];
@@ -54,17 +57,18 @@ __device__ __forceinline__ void scatter_element_2d(const MeshView& m, const List
     }
     const double E = m.E ? __ldg(m.E + e) : m.E0;
     const double nu = m.nu ? __ldg(m.nu + e) : m.nu0;
-    double kb[Blk::kCount][4];
+    double kr[NPE][4];  // blocks K_ab of this thread's row a
     double det;
     if constexpr (NPE == 4) {
-        det = ke_q4_blocks(xe, ye, E, nu, m.t, kb);
+        det = ke_q4_row(xe, ye, E, nu, m.t, a, kr);
     } else {
-        det = ke_t3_blocks(xe, ye, E, nu, m.t, kb);
+        det = ke_t3_row(xe, ye, E, nu, m.t, a, kr);
     }
-    if (!(det > 0.0)) raise_status(L.info, FEM_ERR_DETJ);
-
+    if (a == 0 && !(det > 0.0)) raise_status(L.info, FEM_ERR_DETJ);
+    int row_node = nodes[0];
 #pragma unroll
-    for (int a = 0; a < NPE; a++) {
+    for (int i = 1; i < NPE; i++) row_node = a == i ? nodes[i] : row_node;
+    {
         int state[NPE];
         unsigned gid[NPE];
         int* word[NPE];
@@ -78,7 +82,7 @@ __device__ __forceinline__ void scatter_element_2d(const MeshView& m, const List
         // A failed CAS means the register view of the chunk is stale; the chunk
         // is then re-read before the remaining columns are resolved (a column
         // another thread has just claimed must be found, not claimed again).
-        int c = nodes[a];
+        int c = row_node;
         for (int step = 0; step < kMaxChainSteps; step++) {
             int* meta = chunk_meta(L, c);
             const int4 w0 = ld_cg4(meta), w1 = ld_cg4(meta + 4), w2 = ld_cg4(meta + 8), w3 = ld_cg4(meta + 12);
@@ -132,13 +136,16 @@ __device__ __forceinline__ void scatter_element_2d(const MeshView& m, const List
             if (c < 0) break;  // pool overflow: status raised, the rest of the row is dropped
         }
         // Claimed slots: store values, fence, publish. Found slots: atomicAdd.
+        int nclaimed = 0;
+#pragma unroll
+        for (int b = 0; b < NPE; b++) nclaimed += state[b] == kClaimed;
+        if (nclaimed) atomicAdd(L.counts + row_node, nclaimed);
         bool claimed = false;
 #pragma unroll
         for (int b = 0; b < NPE; b++) {
             if (state[b] == kUnresolved || state[b] == kFoundPending) continue;
             double* p = L.vals + (size_t)gid[b] * 4;
-            const double v0 = block_entry<NPE>(kb, a, b, 0), v1 = block_entry<NPE>(kb, a, b, 1);
-            const double v2 = block_entry<NPE>(kb, a, b, 2), v3 = block_entry<NPE>(kb, a, b, 3);
+            const double v0 = kr[b][0], v1 = kr[b][1], v2 = kr[b][2], v3 = kr[b][3];
             if (state[b] == kClaimed) {
                 reinterpret_cast<double2*>(p)[0] = make_double2(v0, v1);
                 reinterpret_cast<double2*>(p)[1] = make_double2(v2, v3);
@@ -163,78 +170,35 @@ __device__ __forceinline__ void scatter_element_2d(const MeshView& m, const List
             if (!wait_published(L, word[b])) continue;
             double* p = L.vals + (size_t)gid[b] * 4;
 #pragma unroll
-            for (int v = 0; v < 4; v++) atomicAdd(p + v, block_entry<NPE>(kb, a, b, v));
+            for (int v = 0; v < 4; v++) atomicAdd(p + v, kr[b][v]);
         }
     }
 }
 
 template <int NPE>
-__global__ void __launch_bounds__(128) k_scatter_2d(MeshView m, ListLayout L, const int* __restrict__ elist,
-                                                   const int* __restrict__ ecount) {
-    const int count = ecount ? *ecount : m.E_count;
+__global__ void __launch_bounds__(256, NPE == 3 ? 3 : 2) k_scatter_2d(MeshView m, ListLayout L, const int* __restrict__ perm,
+                                                   const int* __restrict__ range) {
+    const int begin = range[0], count = range[1] - range[0];
+    const long long work = (long long)count * NPE;
     int spare = -1;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        const int e = elist ? __ldg(elist + i) : i;
-        scatter_element_2d<NPE>(m, L, e, spare);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < work;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / NPE), a = (int)(t - (long long)i * NPE);
+        scatter_row_2d<NPE>(m, L, __ldg(perm + begin + i), a, spare);
     }
-}
-
-// Splits a mixed mesh into Q4 and T3 element lists (warp-aggregated appends).
-__global__ void k_partition_2d(MeshView m, int* __restrict__ list_q4, int* __restrict__ list_t3,
-                               int* __restrict__ counts) {
-    const int lane = threadIdx.x & 31;
-    for (int base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; base < m.E_count;
-         base += gridDim.x * blockDim.x) {
-        const int e = base + lane;
-        const bool valid = e < m.E_count;
-        const bool q4 = valid && __ldg(m.types + e) == FEM_Q4;
-        const bool t3 = valid && !q4;
-        const unsigned mq = __ballot_sync(0xFFFFFFFFu, q4), mt = __ballot_sync(0xFFFFFFFFu, t3);
-        int bq = 0, bt = 0;
-        if (lane == 0) {
-            if (mq) bq = atomicAdd(counts + 0, __popc(mq));
-            if (mt) bt = atomicAdd(counts + 1, __popc(mt));
-        }
-        bq = __shfl_sync(0xFFFFFFFFu, bq, 0);
-        bt = __shfl_sync(0xFFFFFFFFu, bt, 0);
-        const unsigned below = (1u << lane) - 1u;
-        if (q4) list_q4[bq + __popc(mq & below)] = e;
-        if (t3) list_t3[bt + __popc(mt & below)] = e;
-    }
-}
-
-int sm_count() {
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
-    return n;
 }
 
 }  // namespace
 
-cudaError_t launch_scatter_2d(const MeshView& m, const ListLayout& L, int npe, const int* elist,
-                              const int* ecount, cudaStream_t s) {
-    const int threads = 128;
-    long long want = ((long long)m.E_count + threads - 1) / threads;
-    int grid = (int)(want < (long long)sm_count() * 64 ? (want > 0 ? want : 1) : (long long)sm_count() * 64);
-    if (npe == 4)
-        k_scatter_2d<4><<<grid, threads, 0, s>>>(m, L, elist, ecount);
-    else
-        k_scatter_2d<3><<<grid, threads, 0, s>>>(m, L, elist, ecount);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_partition_2d(const MeshView& m, int* list_q4, int* list_t3, int* counts, cudaStream_t s) {
-    cudaError_t err = cudaMemsetAsync(counts, 0, 2 * sizeof(int), s);
-    if (err) return err;
+cudaError_t launch_scatter_2d(const MeshView& m, const ListLayout& L, int npe, const int* perm, const int* range,
+                              cudaStream_t s) {
     const int threads = 256;
-    long long want = ((long long)m.E_count + threads - 1) / threads;
-    int grid = (int)(want < (long long)sm_count() * 16 ? (want > 0 ? want : 1) : (long long)sm_count() * 16);
-    k_partition_2d<<<grid, threads, 0, s>>>(m, list_q4, list_t3, counts);
+    const long long want = ((long long)m.E_count * npe + threads - 1) / threads;
+    const int grid = (int)std::min<long long>(want > 0 ? want : 1, (long long)sm_count() * 8);
+    if (npe == 4)
+        k_scatter_2d<4><<<grid, threads, 0, s>>>(m, L, perm, range);
+    else
+        k_scatter_2d<3><<<grid, threads, 0, s>>>(m, L, perm, range);
     return cudaGetLastError();
 }
 

@@ -146,8 +146,9 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
         else
             atomicAdd(p, val);
     }
-    const bool any_claimed = __any_sync(0xFFFFFFFFu, state == kClaimed);
-    if (any_claimed) {
+    const unsigned claimed = __ballot_sync(0xFFFFFFFFu, state == kClaimed);
+    if (lane == 0 && claimed) atomicAdd(L.counts + sm.nodes[I], __popc(claimed));
+    if (claimed) {
         __threadfence();
         __syncwarp();
         if (state == kClaimed) atomicExch(word, key);

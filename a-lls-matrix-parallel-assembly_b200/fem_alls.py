@@ -26,7 +26,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libfem_alls.so")
 FEM_OK = 0
 STATUS_NAMES = {0: "FEM_OK", 1: "FEM_ERR_BAD_ARG", 2: "FEM_ERR_BAD_MESH", 3: "FEM_ERR_POOL_OVERFLOW",
                 4: "FEM_ERR_DETJ", 5: "FEM_ERR_CUDA", 6: "FEM_ERR_CAPACITY", 7: "FEM_ERR_WORKSPACE",
-                8: "FEM_ERR_TIMEOUT", 9: "FEM_ERR_RANGE", 10: "FEM_ERR_ROW_TOO_LONG"}
+                8: "FEM_ERR_TIMEOUT", 9: "FEM_ERR_RANGE", 10: "FEM_ERR_INTERNAL"}
 globals().update({v: k for k, v in STATUS_NAMES.items()})
 
 # C ABI exports (kept in sync with include/fem_alls.h by tests/test_abi.py).

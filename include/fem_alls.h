@@ -67,7 +67,7 @@ typedef int32_t fem_status;
 #define FEM_ERR_WORKSPACE 7      /* workspace too small or misaligned */
 #define FEM_ERR_TIMEOUT 8        /* a bounded wait inside a kernel gave up */
 #define FEM_ERR_RANGE 9          /* nnz or a pool index exceeds the int32/uint32 range */
-#define FEM_ERR_ROW_TOO_LONG 10  /* a row's list exceeded the consolidation capacity */
+#define FEM_ERR_INTERNAL 10      /* a list failed a consistency check (entries != count) */
 
 /* ---- element kinds -------------------------------------------------------- */
 #define FEM_Q4 0        /* 4-node quadrilateral, plane stress, 2x2 Gauss, 2 dof/node */
