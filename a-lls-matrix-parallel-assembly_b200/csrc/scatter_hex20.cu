@@ -5,35 +5,42 @@
 // 14.9 KB of local memory per thread and whose fixed 300-entry rows silently
 // drop overflow.
 //
-// One CTA (8 warps) per element, persistent over the element range:
-//  * the 27 Gauss points' shape-function derivatives (H20:95-128) are built once
-//    per CTA in shared memory;
-//  * per element: J (243 dot products), det/inverse (27 threads), the
-//    physical gradients G[g][node][dir] (1620 values), then the node-pair
-//    matrix  M_IJ[a][b] = sum_g w_g detJ_g G[g][I][a] G[g][J][b]  for the 210
-//    upper node pairs, from which the isotropic block is
-//    Ke_IJ = lambda M_IJ + mu M_IJ^T + mu tr(M_IJ) I  — algebraically the
-//    reference's per-Gauss-point block formula (H20:173-191) with
-//    c1 = lambda + 2 mu, c2 = lambda, c3 = mu, in double;
-//  * scatter: warp w serves row nodes w, w+8, w+16. The warp copies the row's
-//    chunk slots into shared memory with lane-parallel L2 loads; lane j then
-//    resolves column node j along its hashed probe sequence, claiming a free
-//    slot with atomicCAS (empty -> col|pending) if the column is absent, and
-//    following / atomicCAS-linking overflow chunks when the probe sequence is
-//    full. Claimed blocks are stored, the warp fences and publishes them; found
-//    blocks are accumulated with atomicAdd (after a bounded wait for slots
-//    another warp is still writing).
+// One CTA (10 warps) per element at a time, persistent over the element range.
+//
+// Element stiffness, in double. With the physical shape-function gradients
+// G_g (a 60-vector per Gauss point g, dof r = 3 node + dir) and
+// w_g = gauss weight * detJ_g, the node-pair matrix
+//     M = sum_g w_g G_g G_g^T          (60 x 60, contraction length 27)
+// gives every 3x3 block of the isotropic stiffness as
+//     Ke_IJ[a][b] = lambda M[3I+a][3J+b] + mu M[3I+b][3J+a] + mu delta_ab tr(M_IJ)
+// which is algebraically the reference's per-Gauss-point block formula
+// (H20:173-191, c1 = lambda + 2 mu, c2 = lambda, c3 = mu). M is one 64x64x28
+// FP64 matrix product per element, computed on the FP64 tensor cores with
+// mma.sync.m8n8k4.f64 (8 warps x 8 tiles x 7 k-steps); Ke is never stored, its
+// entries are formed from M while they are scattered. The Gauss-point shape
+// derivatives (H20:95-128) are tabulated once per CTA.
+//
+// Scatter. Warp w serves row nodes w and w+10. It copies the row's chunk row
+// (512 bytes: next pointer + 126 hashed slots) to shared memory with one 16-byte
+// load per lane, matches every slot against a shared-memory hash of the
+// element's 20 nodes, and builds ballot bitmaps of the empty slots. Lane j then
+// claims the first empty slot on column node j's probe sequence with atomicCAS
+// (empty -> col|pending) if the column is absent — re-trying past slots another
+// warp has just taken — and follows / atomicCAS-links overflow chunks when the
+// probe sequence is full. Claimed blocks are stored, the warp fences and
+// publishes them; found blocks are accumulated with atomicAdd (after a bounded
+// wait for slots another warp is still writing).
 #include "launch.h"
 
 namespace fem {
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 320;
 constexpr int kWarps = kThreads / 32;
-constexpr int kPairs = 210;
-constexpr int kMaxHex20Slots = 128;  // upper bound of S1, S2 (checked on the host)
-
-__device__ __forceinline__ int pair_index(int I, int J) { return I * 20 - I * (I - 1) / 2 + (J - I); }
+constexpr int kMaxHex20Words = 128;  // chunk meta rows of at most 128 words (S <= 126, checked on the host)
+constexpr int PS = 28;               // row stride of P (doubles): conflict-free m8n8k4 fragment loads
+constexpr int MS = 61;               // row stride of M (doubles)
+constexpr int kHash = 64;            // element-node hash slots
 
 // Natural coordinates of the 20 nodes in the reference order (H20:97-99).
 __constant__ signed char c_xin[20] = {-1, 1, 1, -1, -1, 1, 1, -1, 0, 1, 0, -1, 0, 1, 0, -1, -1, 1, 1, -1};
@@ -66,72 +73,140 @@ __device__ void hex20_dshape_node(int n, double xi, double eta, double zeta, dou
     }
 }
 
+enum SlotState : int { kUnresolved = 0, kFound = 1, kFoundPending = 2, kClaimed = 3 };
+
 struct Hex20Smem {
-    double dN[27][3][20];   // shape derivatives at the Gauss points
-    double X[20][3];        // element node coordinates
-    double J[27][9];        // Jacobians, then their inverses
-    double w[27];           // Gauss weight * detJ
-    double G[27][60];       // physical gradients G[g][3*node + dir]
-    double K[kPairs][9];    // upper node-pair blocks of Ke
-    int view[kWarps][kMaxHex20Slots];   // per-warp copy of the chunk slots being probed
+    double dN[27][3][20];      // shape derivatives at the Gauss points
+    double P[64][PS];          // P[3n+a][g] = G_g[n][a]; rows 60..63 and column 27 stay zero
+    double M[60][MS];          // node-pair matrix of the current element
+    double X[20][3];           // element node coordinates
+    double J[27][9];           // Jacobians, then their inverses
+    double w[PS];              // Gauss weight * detJ (w[27] = 0 pads the contraction)
+    int view[kWarps][kMaxHex20Words];  // per-warp copy of the chunk row being resolved
     unsigned gid[kWarps][20];
     int state[kWarps][20];
+    int hkey[kHash];           // element-node hash: node + 1 -> local index
+    int hval[kHash];
     int nodes[20];
-    unsigned char pI[kPairs], pJ[kPairs];
     double lam, mu;
     int bad;
 };
 
-enum SlotState : int { kUnresolved = 0, kFound = 1, kFoundPending = 2, kClaimed = 3 };
+__device__ __forceinline__ unsigned hash_slot(int key) { return ((unsigned)key * 2654435761u) >> 26; }
+
+// Local index of node key (node + 1) in the current element, or -1.
+__device__ __forceinline__ int element_lookup(const Hex20Smem& sm, int key) {
+    unsigned h = hash_slot(key);
+    for (int i = 0; i < kHash; i++) {
+        const int k = sm.hkey[h];
+        if (k == key) return sm.hval[h];
+        if (k == 0) return -1;
+        h = (h + 1) & (kHash - 1);
+    }
+    return -1;
+}
+
+__device__ __forceinline__ unsigned pick(const unsigned (&bm)[4], int k) {
+    return k == 0 ? bm[0] : (k == 1 ? bm[1] : (k == 2 ? bm[2] : bm[3]));
+}
+
+// First set bit at word position >= p0, cyclically over the nw bitmap words; -1 if none.
+__device__ __forceinline__ int first_empty_from(const unsigned (&bm)[4], int nw, int p0) {
+    int k = p0 >> 5;
+    unsigned m = pick(bm, k) & (0xFFFFFFFFu << (p0 & 31));
+    for (int it = 0; it <= nw; it++) {
+        if (m) return (k << 5) + __ffs(m) - 1;
+        k = k + 1 == nw ? 0 : k + 1;
+        m = pick(bm, k);
+    }
+    return -1;
+}
+
+// Entry (a, b) of block Ke_IJ from the node-pair matrix.
+__device__ __forceinline__ double ke_entry(const Hex20Smem& sm, int I, int J, int a, int b) {
+    double v = sm.lam * sm.M[3 * I + a][3 * J + b] + sm.mu * sm.M[3 * I + b][3 * J + a];
+    if (a == b) v += sm.mu * (sm.M[3 * I][3 * J] + sm.M[3 * I + 1][3 * J + 1] + sm.M[3 * I + 2][3 * J + 2]);
+    return v;
+}
 
 // Resolves the 20 column slots of row node I of the current element and
 // scatters its 20 Ke blocks (warp-cooperative; lane j owns column node j).
 __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, int I, int warp, int lane,
                                             int& spare) {
+    constexpr unsigned kFull = 0xFFFFFFFFu;
     int* view = sm.view[warp];
     const int key = lane < 20 ? sm.nodes[lane] + 1 : 0;
     int state = lane < 20 ? kUnresolved : kFound;
     unsigned gid = 0;
-    int* word = nullptr;
+    if (lane < 20) sm.state[warp][lane] = kUnresolved;
     int c = sm.nodes[I];
     for (int step = 0; step < kMaxChainSteps; step++) {
         int* meta = chunk_meta(L, c);
-        const int cap = chunk_cap(L, c);
-        for (int s = lane; s < cap; s += 32) view[s] = ld_cg(meta + 2 + s);
+        const int H = c < L.N ? L.H1 : L.H2;
+        for (int q = lane * 4; q < H; q += 128) *reinterpret_cast<int4*>(view + q) = ld_cg4(meta + q);
         __syncwarp();
+        // columns already in this chunk
+        for (int p = 2 + lane; p < H; p += 32) {
+            const int v = view[p];
+            if (v != 0) {
+                const int j = element_lookup(sm, v & kColMask);
+                if (j >= 0) {
+                    sm.gid[warp][j] = slot_gid(L, c, p - 2);
+                    sm.state[warp][j] = v < 0 ? kFoundPending : kFound;
+                }
+            }
+        }
+        unsigned bm[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int p = 32 * k + lane;
+            bm[k] = __ballot_sync(kFull, p >= 2 && p < H && view[p] == 0);
+        }
+        __syncwarp();
+        if (state == kUnresolved && sm.state[warp][lane] != kUnresolved) {
+            state = sm.state[warp][lane];
+            gid = sm.gid[warp][lane];
+        }
+        // claim the first empty slot on the probe sequence of each absent column
         if (state == kUnresolved) {
-            int p = probe_start(key, cap);
-            for (int tries = 0; tries < cap; tries++) {
-                int v = view[p];
-                if (v == 0) {
-                    v = atomicCAS(meta + 2 + p, 0, key | kPending);
-                    if (v == 0) {
-                        state = kClaimed;
-                        view[p] = key | kPending;
-                    } else {
-                        view[p] = v;
-                    }
+            int p0 = 2 + probe_start(key, H - 2);
+            for (int tries = 0; tries < H; tries++) {
+                const int p = first_empty_from(bm, (H + 31) >> 5, p0);
+                if (p < 0) break;  // probe sequence full: continue in the next chunk
+                const int old = atomicCAS(meta + p, 0, key | kPending);
+                if (old == 0) {
+                    state = kClaimed;
+                } else if ((old & kColMask) == key) {
+                    state = old < 0 ? kFoundPending : kFound;
+                } else {
+                    const unsigned bit = 1u << (p & 31);
+                    const int k = p >> 5;
+                    bm[0] &= k == 0 ? ~bit : 0xFFFFFFFFu;
+                    bm[1] &= k == 1 ? ~bit : 0xFFFFFFFFu;
+                    bm[2] &= k == 2 ? ~bit : 0xFFFFFFFFu;
+                    bm[3] &= k == 3 ? ~bit : 0xFFFFFFFFu;
+                    p0 = p;
+                    continue;
                 }
-                if (state != kClaimed && (v & kColMask) == key) state = v < 0 ? kFoundPending : kFound;
-                if (state != kUnresolved) {
-                    gid = slot_gid(L, c, p);
-                    word = meta + 2 + p;
-                    break;
-                }
-                p = p + 1 == cap ? 0 : p + 1;
+                gid = slot_gid(L, c, p - 2);
+                break;
             }
         }
         __syncwarp();
-        if (!__any_sync(0xFFFFFFFFu, state == kUnresolved)) break;
+        if (!__any_sync(kFull, state == kUnresolved)) break;
         int nc = 0;
         if (lane == 0) nc = next_chunk(L, c, spare);
-        c = __shfl_sync(0xFFFFFFFFu, nc, 0);
+        c = __shfl_sync(kFull, nc, 0);
         if (c < 0) break;  // pool overflow: status raised, unresolved columns dropped
+        if (lane < 20 && state == kUnresolved) sm.state[warp][lane] = kUnresolved;
+        __syncwarp();
     }
     if (lane < 20) {
         sm.state[warp][lane] = state;
         sm.gid[warp][lane] = gid;
     }
+    const unsigned claimed = __ballot_sync(kFull, state == kClaimed);
+    if (lane == 0 && claimed) atomicAdd(L.counts + sm.nodes[I], __popc(claimed));
     __syncwarp();
     // Claimed blocks: plain stores. Found (published) blocks: atomicAdd.
     for (int idx = lane; idx < 20 * 9; idx += 32) {
@@ -139,32 +214,41 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
         const int st = sm.state[warp][j];
         if (st == kUnresolved || st == kFoundPending) continue;
         const int a = v / 3, b = v - a * 3;
-        const double val = I <= j ? sm.K[pair_index(I, j)][3 * a + b] : sm.K[pair_index(j, I)][3 * b + a];
+        const double val = ke_entry(sm, I, j, a, b);
         double* p = L.vals + (size_t)sm.gid[warp][j] * 9 + v;
         if (st == kClaimed)
             *p = val;
         else
             atomicAdd(p, val);
     }
-    const unsigned claimed = __ballot_sync(0xFFFFFFFFu, state == kClaimed);
-    if (lane == 0 && claimed) atomicAdd(L.counts + sm.nodes[I], __popc(claimed));
     if (claimed) {
         __threadfence();
         __syncwarp();
-        if (state == kClaimed) atomicExch(word, key);
+        if (state == kClaimed) {
+            int cc, s;
+            gid_chunk(L, gid, cc, s);
+            atomicExch(chunk_meta(L, cc) + 2 + s, key);
+        }
     }
     // Blocks of slots another warp is still writing: wait, then add.
-    if (state == kFoundPending && wait_published(L, word)) {
-        double* p = L.vals + (size_t)gid * 9;
-        for (int v = 0; v < 9; v++) {
-            const int a = v / 3, b = v - a * 3;
-            atomicAdd(p + v, I <= lane ? sm.K[pair_index(I, lane)][3 * a + b] : sm.K[pair_index(lane, I)][3 * b + a]);
+    if (state == kFoundPending) {
+        int cc, s;
+        gid_chunk(L, gid, cc, s);
+        if (wait_published(L, chunk_meta(L, cc) + 2 + s)) {
+            double* p = L.vals + (size_t)gid * 9;
+            for (int v = 0; v < 9; v++) atomicAdd(p + v, ke_entry(sm, I, lane, v / 3, v % 3));
         }
     }
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(kThreads) k_scatter_hex20(MeshView m, ListLayout L) {
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListLayout L) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Hex20Smem& sm = *reinterpret_cast<Hex20Smem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -177,17 +261,14 @@ __global__ void __launch_bounds__(kThreads) k_scatter_hex20(MeshView m, ListLayo
         sm.dN[g][1][n] = dy;
         sm.dN[g][2][n] = dz;
     }
-    if (tid < kPairs) {
-        int I = 0, r = tid;
-        while (r >= 20 - I) { r -= 20 - I; I++; }
-        sm.pI[tid] = (unsigned char)I;
-        sm.pJ[tid] = (unsigned char)(I + r);
-    }
+    for (int idx = tid; idx < 64 * PS; idx += kThreads) (&sm.P[0][0])[idx] = 0.0;
+    if (tid < PS) sm.w[tid] = 0.0;
     int spare = -1;
     __syncthreads();
 
     for (int e = blockIdx.x; e < m.E_count; e += gridDim.x) {
         if (tid == 0) sm.bad = 0;
+        if (tid < kHash) sm.hkey[tid] = 0;
         __syncthreads();
         if (tid < 20) {
             const int n = __ldg(m.conn + (size_t)e * 20 + tid);
@@ -198,6 +279,17 @@ __global__ void __launch_bounds__(kThreads) k_scatter_hex20(MeshView m, ListLayo
                 sm.X[tid][0] = __ldg(m.x + n);
                 sm.X[tid][1] = __ldg(m.y + n);
                 sm.X[tid][2] = __ldg(m.z + n);
+                // element-node hash (node ids of an element are distinct)
+                const int key = n + 1;
+                unsigned h = hash_slot(key);
+                for (int i = 0; i < kHash; i++) {
+                    const int old = atomicCAS(&sm.hkey[h], 0, key);
+                    if (old == 0 || old == key) {
+                        sm.hval[h] = tid;
+                        break;
+                    }
+                    h = (h + 1) & (kHash - 1);
+                }
             }
         }
         if (tid == 32) {
@@ -242,38 +334,40 @@ __global__ void __launch_bounds__(kThreads) k_scatter_hex20(MeshView m, ListLayo
             sm.w[tid] = weight3(tid / 9) * weight3((tid / 3) % 3) * weight3(tid % 3) * det;
         }
         __syncthreads();
-        // Physical gradients G[g][3n+a] = sum_i iJ[g][3a+i] dN[g][i][n]
+        // Physical gradients P[3n+a][g] = sum_i iJ[g][3a+i] dN[g][i][n]
         for (int idx = tid; idx < 27 * 60; idx += kThreads) {
             const int g = idx / 60, r = idx % 60, n = r / 3, a = r % 3;
             const double* iJ = sm.J[g];
-            sm.G[g][r] = fma(iJ[3 * a], sm.dN[g][0][n], fma(iJ[3 * a + 1], sm.dN[g][1][n], iJ[3 * a + 2] * sm.dN[g][2][n]));
+            sm.P[r][g] = fma(iJ[3 * a], sm.dN[g][0][n], fma(iJ[3 * a + 1], sm.dN[g][1][n], iJ[3 * a + 2] * sm.dN[g][2][n]));
         }
         __syncthreads();
-        // Upper node-pair blocks.
-        if (tid < kPairs) {
-            const int I = sm.pI[tid], J = sm.pJ[tid];
-            double acc[9];
+        // M = (P diag(w)) P^T on the FP64 tensor cores: warp mt owns tile row mt.
+        if (warp < 8) {
+            double acc[8][2];
 #pragma unroll
-            for (int k = 0; k < 9; k++) acc[k] = 0.0;
-            for (int g = 0; g < 27; g++) {
-                const double w = sm.w[g];
-                const double a0 = w * sm.G[g][3 * I], a1 = w * sm.G[g][3 * I + 1], a2 = w * sm.G[g][3 * I + 2];
-                const double b0 = sm.G[g][3 * J], b1 = sm.G[g][3 * J + 1], b2 = sm.G[g][3 * J + 2];
-                acc[0] = fma(a0, b0, acc[0]); acc[1] = fma(a0, b1, acc[1]); acc[2] = fma(a0, b2, acc[2]);
-                acc[3] = fma(a1, b0, acc[3]); acc[4] = fma(a1, b1, acc[4]); acc[5] = fma(a1, b2, acc[5]);
-                acc[6] = fma(a2, b0, acc[6]); acc[7] = fma(a2, b1, acc[7]); acc[8] = fma(a2, b2, acc[8]);
+            for (int nt = 0; nt < 8; nt++) acc[nt][0] = acc[nt][1] = 0.0;
+            const int fr = lane >> 2, fc = lane & 3;
+#pragma unroll
+            for (int ks = 0; ks < 7; ks++) {
+                const int k = 4 * ks + fc;
+                const double a = sm.w[k] * sm.P[8 * warp + fr][k];
+#pragma unroll
+                for (int nt = 0; nt < 8; nt++) dmma_8x8x4(acc[nt][0], acc[nt][1], a, sm.P[8 * nt + fr][k]);
             }
-            const double lam = sm.lam, mu = sm.mu;
-            const double tr = mu * (acc[0] + acc[4] + acc[8]);
+            const int row = 8 * warp + fr;
+            if (row < 60) {
 #pragma unroll
-            for (int a = 0; a < 3; a++)
-#pragma unroll
-                for (int b = 0; b < 3; b++)
-                    sm.K[tid][3 * a + b] = fma(lam, acc[3 * a + b], mu * acc[3 * b + a]) + (a == b ? tr : 0.0);
+                for (int nt = 0; nt < 8; nt++) {
+                    const int col = 8 * nt + 2 * fc;
+                    if (col < 60) {
+                        sm.M[row][col] = acc[nt][0];
+                        sm.M[row][col + 1] = acc[nt][1];
+                    }
+                }
+            }
         }
         __syncthreads();
-
-        // Scatter: warp w serves row nodes w, w + 8, w + 16.
+        // Scatter: warp w serves row nodes w and w + 10.
         for (int I = warp; I < 20; I += kWarps) scatter_row(L, sm, I, warp, lane, spare);
         __syncthreads();
     }
@@ -289,9 +383,7 @@ cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, cudaStr
         if (err) return err;
         err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_scatter_hex20, kThreads, smem);
         if (err) return err;
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        sms = sm_count();
         if (blocks_per_sm < 1) blocks_per_sm = 1;
     }
     long long grid = (long long)blocks_per_sm * sms;
