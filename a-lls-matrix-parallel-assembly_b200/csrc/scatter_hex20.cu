@@ -82,7 +82,7 @@ struct Hex20Smem {
     double X[20][3];           // element node coordinates
     double J[27][9];           // Jacobians, then their inverses
     double w[PS];              // Gauss weight * detJ (w[27] = 0 pads the contraction)
-    int view[kWarps][kMaxHex20Words];  // per-warp copy of the chunk row being resolved
+    alignas(16) int view[kWarps][kMaxHex20Words];  // per-warp copy of the chunk row (16-byte stores)
     unsigned gid[kWarps][20];
     int state[kWarps][20];
     int hkey[kHash];           // element-node hash: node + 1 -> local index
@@ -91,6 +91,9 @@ struct Hex20Smem {
     double lam, mu;
     int bad;
 };
+
+static_assert(offsetof(Hex20Smem, view) % 16 == 0, "int4 stores into view need 16-byte alignment");
+static_assert((kMaxHex20Words * sizeof(int)) % 16 == 0, "view rows must stay 16-byte aligned");
 
 __device__ __forceinline__ unsigned hash_slot(int key) { return ((unsigned)key * 2654435761u) >> 26; }
 
