@@ -83,7 +83,8 @@ struct Hex20Smem {
     double J[27][9];           // Jacobians, then their inverses
     double w[PS];              // Gauss weight * detJ (w[27] = 0 pads the contraction)
     alignas(16) int view[kWarps][kMaxHex20Words];  // per-warp copy of the chunk row (16-byte stores)
-    unsigned gid[kWarps][20];
+    int chunk[kWarps][20];     // chunk and slot of each column node's entry in the row
+    int slot[kWarps][20];
     int state[kWarps][20];
     int hkey[kHash];           // element-node hash: node + 1 -> local index
     int hval[kHash];
@@ -125,11 +126,28 @@ __device__ __forceinline__ int first_empty_from(const unsigned (&bm)[4], int nw,
     return -1;
 }
 
-// Entry (a, b) of block Ke_IJ from the node-pair matrix.
-__device__ __forceinline__ double ke_entry(const Hex20Smem& sm, int I, int J, int a, int b) {
-    double v = sm.lam * sm.M[3 * I + a][3 * J + b] + sm.mu * sm.M[3 * I + b][3 * J + a];
-    if (a == b) v += sm.mu * (sm.M[3 * I][3 * J] + sm.M[3 * I + 1][3 * J + 1] + sm.M[3 * I + 2][3 * J + 2]);
-    return v;
+// Writes (store) or accumulates (atomicAdd) block Ke_IJ into slot s of chunk c:
+//   Ke_IJ[a][b] = lambda M[3I+a][3J+b] + mu M[3I+b][3J+a] + mu delta_ab tr(M_IJ)
+// The 3x3 block M_IJ is read once; value v = 3a+b goes to row v of the chunk.
+__device__ __forceinline__ void write_block(const ListLayout& L, const Hex20Smem& sm, int I, int J, int c, int s,
+                                            bool store) {
+    const double* m0 = &sm.M[3 * I][3 * J];
+    const double m00 = m0[0], m01 = m0[1], m02 = m0[2];
+    const double m10 = m0[MS], m11 = m0[MS + 1], m12 = m0[MS + 2];
+    const double m20 = m0[2 * MS], m21 = m0[2 * MS + 1], m22 = m0[2 * MS + 2];
+    const double lam = sm.lam, mu = sm.mu, mtr = mu * (m00 + m11 + m22);
+    const double k[9] = {fma(lam, m00, fma(mu, m00, mtr)), fma(lam, m01, mu * m10), fma(lam, m02, mu * m20),
+                         fma(lam, m10, mu * m01), fma(lam, m11, fma(mu, m11, mtr)), fma(lam, m12, mu * m21),
+                         fma(lam, m20, mu * m02), fma(lam, m21, mu * m12), fma(lam, m22, fma(mu, m22, mtr))};
+    double* base = L.vals + chunk_vbase(L, c) + s;
+    const int stride = chunk_cap(L, c);
+    if (store) {
+#pragma unroll
+        for (int v = 0; v < 9; v++) base[(size_t)v * stride] = k[v];
+    } else {
+#pragma unroll
+        for (int v = 0; v < 9; v++) atomicAdd(base + (size_t)v * stride, k[v]);
+    }
 }
 
 // Resolves the 20 column slots of row node I of the current element and
@@ -140,7 +158,7 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
     int* view = sm.view[warp];
     const int key = lane < 20 ? sm.nodes[lane] + 1 : 0;
     int state = lane < 20 ? kUnresolved : kFound;
-    unsigned gid = 0;
+    int my_c = 0, my_s = 0;
     if (lane < 20) sm.state[warp][lane] = kUnresolved;
     int c = sm.nodes[I];
     for (int step = 0; step < kMaxChainSteps; step++) {
@@ -154,7 +172,8 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
             if (v != 0) {
                 const int j = element_lookup(sm, v & kColMask);
                 if (j >= 0) {
-                    sm.gid[warp][j] = slot_gid(L, c, p - 2);
+                    sm.chunk[warp][j] = c;
+                    sm.slot[warp][j] = p - 2;
                     sm.state[warp][j] = v < 0 ? kFoundPending : kFound;
                 }
             }
@@ -168,7 +187,8 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
         __syncwarp();
         if (state == kUnresolved && sm.state[warp][lane] != kUnresolved) {
             state = sm.state[warp][lane];
-            gid = sm.gid[warp][lane];
+            my_c = sm.chunk[warp][lane];
+            my_s = sm.slot[warp][lane];
         }
         // claim the first empty slot on the probe sequence of each absent column
         if (state == kUnresolved) {
@@ -191,7 +211,8 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
                     p0 = p;
                     continue;
                 }
-                gid = slot_gid(L, c, p - 2);
+                my_c = c;
+                my_s = p - 2;
                 break;
             }
         }
@@ -204,44 +225,18 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
         if (lane < 20 && state == kUnresolved) sm.state[warp][lane] = kUnresolved;
         __syncwarp();
     }
-    if (lane < 20) {
-        sm.state[warp][lane] = state;
-        sm.gid[warp][lane] = gid;
-    }
     const unsigned claimed = __ballot_sync(kFull, state == kClaimed);
     if (lane == 0 && claimed) atomicAdd(L.counts + sm.nodes[I], __popc(claimed));
-    __syncwarp();
     // Claimed blocks: plain stores. Found (published) blocks: atomicAdd.
-    for (int idx = lane; idx < 20 * 9; idx += 32) {
-        const int j = idx / 9, v = idx - j * 9;
-        const int st = sm.state[warp][j];
-        if (st == kUnresolved || st == kFoundPending) continue;
-        const int a = v / 3, b = v - a * 3;
-        const double val = ke_entry(sm, I, j, a, b);
-        double* p = L.vals + (size_t)sm.gid[warp][j] * 9 + v;
-        if (st == kClaimed)
-            *p = val;
-        else
-            atomicAdd(p, val);
-    }
+    if (state == kClaimed || (state == kFound && lane < 20)) write_block(L, sm, I, lane, my_c, my_s, state == kClaimed);
     if (claimed) {
         __threadfence();
         __syncwarp();
-        if (state == kClaimed) {
-            int cc, s;
-            gid_chunk(L, gid, cc, s);
-            atomicExch(chunk_meta(L, cc) + 2 + s, key);
-        }
+        if (state == kClaimed) atomicExch(chunk_meta(L, my_c) + 2 + my_s, key);
     }
     // Blocks of slots another warp is still writing: wait, then add.
-    if (state == kFoundPending) {
-        int cc, s;
-        gid_chunk(L, gid, cc, s);
-        if (wait_published(L, chunk_meta(L, cc) + 2 + s)) {
-            double* p = L.vals + (size_t)gid * 9;
-            for (int v = 0; v < 9; v++) atomicAdd(p + v, ke_entry(sm, I, lane, v / 3, v % 3));
-        }
-    }
+    if (state == kFoundPending && wait_published(L, chunk_meta(L, my_c) + 2 + my_s))
+        write_block(L, sm, I, lane, my_c, my_s, false);
     __syncwarp();
 }
 
@@ -338,10 +333,12 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
         }
         __syncthreads();
         // Physical gradients P[3n+a][g] = sum_i iJ[g][3a+i] dN[g][i][n]
-        for (int idx = tid; idx < 27 * 60; idx += kThreads) {
-            const int g = idx / 60, r = idx % 60, n = r / 3, a = r % 3;
+        for (int idx = tid; idx < 27 * 20; idx += kThreads) {
+            const int g = idx / 20, n = idx - 20 * g;
             const double* iJ = sm.J[g];
-            sm.P[r][g] = fma(iJ[3 * a], sm.dN[g][0][n], fma(iJ[3 * a + 1], sm.dN[g][1][n], iJ[3 * a + 2] * sm.dN[g][2][n]));
+            const double d0 = sm.dN[g][0][n], d1 = sm.dN[g][1][n], d2 = sm.dN[g][2][n];
+#pragma unroll
+            for (int a = 0; a < 3; a++) sm.P[3 * n + a][g] = fma(iJ[3 * a], d0, fma(iJ[3 * a + 1], d1, iJ[3 * a + 2] * d2));
         }
         __syncthreads();
         // M = (P diag(w)) P^T on the FP64 tensor cores: warp mt owns tile row mt.
