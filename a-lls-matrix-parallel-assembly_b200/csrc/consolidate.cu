@@ -220,8 +220,9 @@ __device__ void long_row_write(const ListLayout& L, int n, int u, long long base
             const int next = __ldg(meta + 1);
             for (int s = glane; s < cap; s += G) {
                 if ((__ldg(meta + 2 + s) & kColMask) - 1 == col) {
+                    const double* p = L.vals + (size_t)slot_gid(L, c, s) * B;
 #pragma unroll
-                    for (int v = 0; v < B; v++) sum[v] += __ldg(slot_value<B>(L, c, s, v));
+                    for (int v = 0; v < B; v++) sum[v] += __ldg(p + v);
                 }
             }
             if (next == 0) break;
@@ -253,9 +254,6 @@ __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int
     constexpr int NK = G * KPL;             // sort capacity per node
     constexpr int B = DPN * DPN;
     __shared__ unsigned long long s_keys[NPB][NK];
-    // Hex20 (value rows per chunk): first value and row stride of each sorted slot
-    __shared__ size_t s_vbase[DPN == 3 ? NPB : 1][DPN == 3 ? NK : 1];
-    __shared__ int s_vstride[DPN == 3 ? NPB : 1][DPN == 3 ? NK : 1];
     if (L.info->nnz > capacity) return;  // FEM_ERR_CAPACITY already raised; write nothing
     const int tid = threadIdx.x;
     const int grp = tid / G, glane = tid % G;
@@ -307,18 +305,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int
         }
         group_sort<G, KPL>(keys, glane);
 #pragma unroll
-        for (int i = 0; i < KPL; i++) {
-            const int p = glane * KPL + i;
-            s_keys[grp][p] = keys[i];
-            if constexpr (DPN == 3) {
-                if (p < Ts) {
-                    int c, sl;
-                    gid_chunk(L, (unsigned)keys[i], c, sl);
-                    s_vbase[grp][p] = chunk_vbase(L, c) + sl;
-                    s_vstride[grp][p] = chunk_cap(L, c);
-                }
-            }
-        }
+        for (int i = 0; i < KPL; i++) s_keys[grp][glane * KPL + i] = keys[i];
         __syncwarp();
         // 3. write the dpn rows of the node
         if (valid) {
@@ -332,10 +319,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int
                         const int k = r / DPN, b = r - k * DPN;
                         const unsigned long long key = s_keys[grp][k];
                         col_idx[rbase + r] = (int)(key >> 32) * DPN + b;
-                        if constexpr (DPN == 3)
-                            values[rbase + r] = __ldg(L.vals + s_vbase[grp][k] + (size_t)(a * DPN + b) * s_vstride[grp][k]);
-                        else
-                            values[rbase + r] = __ldg(L.vals + (size_t)(unsigned)key * B + a * DPN + b);
+                        values[rbase + r] = __ldg(L.vals + (size_t)(unsigned)key * B + a * DPN + b);
                     }
                 }
             }

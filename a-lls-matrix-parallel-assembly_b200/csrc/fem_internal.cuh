@@ -20,11 +20,9 @@
 // block values, fences, and publishes the column (clears kPending); other
 // contributors atomicAdd into published slots and wait (bounded) for pending
 // ones, but only after publishing their own claims, so no wait is circular.
-// Slot values live in one array, chunk after chunk (first chunks, then overflow
-// chunks), B = dpn^2 values per slot. 2-D lists (B = 4) keep each slot's block
-// contiguous (one 32-byte sector per slot); Hex20 lists (B = 9) store a chunk's
-// values as B rows of `cap` slots, so a warp writing value v of the 20 slots an
-// element touches in one row chunk writes within one contiguous row.
+// Slot values are stored slot-major: vals[gid * B + v], B = dpn^2, where gid is
+// the global slot id (first-chunk slots first, then overflow-chunk slots), so a
+// slot's block is contiguous (one 32-byte sector in 2-D, 72 bytes for Hex20).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -89,18 +87,6 @@ __device__ __forceinline__ void gid_chunk(const ListLayout& L, unsigned gid, int
         c = L.N + (int)(g2 / (unsigned)L.S2);
         s = (int)(g2 % (unsigned)L.S2);
     }
-}
-
-// First value of chunk c in the value array.
-__device__ __forceinline__ size_t chunk_vbase(const ListLayout& L, int c) {
-    return c < L.N ? (size_t)c * L.S1 * L.B
-                   : (size_t)L.N * L.S1 * L.B + (size_t)(c - L.N) * L.S2 * L.B;
-}
-// Value v of slot s of chunk c (layout as described above, chosen by B).
-template <int B>
-__device__ __forceinline__ double* slot_value(const ListLayout& L, int c, int s, int v) {
-    if (B == 9) return L.vals + chunk_vbase(L, c) + (size_t)v * chunk_cap(L, c) + s;
-    return L.vals + chunk_vbase(L, c) + (size_t)s * B + v;
 }
 
 // L2-coherent loads (bypass L1: list words change under other SMs' writes).

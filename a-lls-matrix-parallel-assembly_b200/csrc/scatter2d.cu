@@ -135,33 +135,32 @@ __device__ __forceinline__ void scatter_row_2d(const MeshView& m, const ListLayo
             c = next_chunk(L, c, spare);
             if (c < 0) break;  // pool overflow: status raised, the rest of the row is dropped
         }
-        // Claimed slots: store values, fence, publish. Found slots: atomicAdd.
+        // Claimed slots: store values, fence, publish — before any atomic, so the
+        // fence waits only for these stores and the slots stay pending briefly.
         int nclaimed = 0;
 #pragma unroll
         for (int b = 0; b < NPE; b++) nclaimed += state[b] == kClaimed;
-        if (nclaimed) atomicAdd(L.counts + row_node, nclaimed);
-        bool claimed = false;
+        if (nclaimed) {
+            atomicAdd(L.counts + row_node, nclaimed);
 #pragma unroll
-        for (int b = 0; b < NPE; b++) {
-            if (state[b] == kUnresolved || state[b] == kFoundPending) continue;
-            double* p = L.vals + (size_t)gid[b] * 4;
-            const double v0 = kr[b][0], v1 = kr[b][1], v2 = kr[b][2], v3 = kr[b][3];
-            if (state[b] == kClaimed) {
-                reinterpret_cast<double2*>(p)[0] = make_double2(v0, v1);
-                reinterpret_cast<double2*>(p)[1] = make_double2(v2, v3);
-                claimed = true;
-            } else {
-                atomicAdd(p + 0, v0);
-                atomicAdd(p + 1, v1);
-                atomicAdd(p + 2, v2);
-                atomicAdd(p + 3, v3);
+            for (int b = 0; b < NPE; b++) {
+                if (state[b] != kClaimed) continue;
+                double* p = L.vals + (size_t)gid[b] * 4;
+                reinterpret_cast<double2*>(p)[0] = make_double2(kr[b][0], kr[b][1]);
+                reinterpret_cast<double2*>(p)[1] = make_double2(kr[b][2], kr[b][3]);
             }
-        }
-        if (claimed) {
             __threadfence();
 #pragma unroll
             for (int b = 0; b < NPE; b++)
                 if (state[b] == kClaimed) atomicExch(word[b], nodes[b] + 1);
+        }
+        // Found (published) slots: atomicAdd.
+#pragma unroll
+        for (int b = 0; b < NPE; b++) {
+            if (state[b] != kFound) continue;
+            double* p = L.vals + (size_t)gid[b] * 4;
+#pragma unroll
+            for (int v = 0; v < 4; v++) atomicAdd(p + v, kr[b][v]);
         }
         // Columns another thread is still writing: wait for them, then add.
 #pragma unroll

@@ -16,9 +16,10 @@
 // which is algebraically the reference's per-Gauss-point block formula
 // (H20:173-191, c1 = lambda + 2 mu, c2 = lambda, c3 = mu). M is one 64x64x28
 // FP64 matrix product per element, computed on the FP64 tensor cores with
-// mma.sync.m8n8k4.f64 (8 warps x 8 tiles x 7 k-steps); Ke is never stored, its
-// entries are formed from M while they are scattered. The Gauss-point shape
-// derivatives (H20:95-128) are tabulated once per CTA.
+// mma.sync.m8n8k4.f64 (8 warps x 8 tiles x 7 k-steps); only its 210 upper 3x3
+// node blocks are kept (so every Ke is exactly symmetric), in the shared memory
+// the gradients occupied. Ke blocks are formed from M per scattered row. The
+// Gauss-point shape derivatives (H20:95-128) are tabulated once per CTA.
 //
 // Scatter. Warp w serves row nodes w and w+10. It copies the row's chunk row
 // (512 bytes: next pointer + 126 hashed slots) to shared memory with one 16-byte
@@ -39,7 +40,6 @@ constexpr int kThreads = 320;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxHex20Words = 128;  // chunk meta rows of at most 128 words (S <= 126, checked on the host)
 constexpr int PS = 28;               // row stride of P (doubles): conflict-free m8n8k4 fragment loads
-constexpr int MS = 61;               // row stride of M (doubles)
 constexpr int kHash = 64;            // element-node hash slots
 
 // Natural coordinates of the 20 nodes in the reference order (H20:97-99).
@@ -77,15 +77,17 @@ enum SlotState : int { kUnresolved = 0, kFound = 1, kFoundPending = 2, kClaimed 
 
 struct Hex20Smem {
     double dN[27][3][20];      // shape derivatives at the Gauss points
-    double P[64][PS];          // P[3n+a][g] = G_g[n][a]; rows 60..63 and column 27 stay zero
-    double M[60][MS];          // node-pair matrix of the current element
+    union {
+        double P[64][PS];      // P[3n+a][g] = G_g[n][a]; rows 60..63 and column 27 zeroed per element
+        double Mb[210][9];     // upper 3x3 node blocks of the node-pair matrix: Mb[pair(I,J)][3a+b]
+    };
     double X[20][3];           // element node coordinates
     double J[27][9];           // Jacobians, then their inverses
     double w[PS];              // Gauss weight * detJ (w[27] = 0 pads the contraction)
     alignas(16) int view[kWarps][kMaxHex20Words];  // per-warp copy of the chunk row (16-byte stores)
-    int chunk[kWarps][20];     // chunk and slot of each column node's entry in the row
-    int slot[kWarps][20];
+    unsigned gid[kWarps][20];  // slot of each column node's entry in the row
     int state[kWarps][20];
+    double stage[kWarps][20 * 9];  // the row's 20 Ke blocks, entry j*9 + v
     int hkey[kHash];           // element-node hash: node + 1 -> local index
     int hval[kHash];
     int nodes[20];
@@ -126,28 +128,28 @@ __device__ __forceinline__ int first_empty_from(const unsigned (&bm)[4], int nw,
     return -1;
 }
 
-// Writes (store) or accumulates (atomicAdd) block Ke_IJ into slot s of chunk c:
+// Block Ke_IJ into out[0..9) (row-major 3x3):
 //   Ke_IJ[a][b] = lambda M[3I+a][3J+b] + mu M[3I+b][3J+a] + mu delta_ab tr(M_IJ)
-// The 3x3 block M_IJ is read once; value v = 3a+b goes to row v of the chunk.
-__device__ __forceinline__ void write_block(const ListLayout& L, const Hex20Smem& sm, int I, int J, int c, int s,
-                                            bool store) {
-    const double* m0 = &sm.M[3 * I][3 * J];
-    const double m00 = m0[0], m01 = m0[1], m02 = m0[2];
-    const double m10 = m0[MS], m11 = m0[MS + 1], m12 = m0[MS + 2];
-    const double m20 = m0[2 * MS], m21 = m0[2 * MS + 1], m22 = m0[2 * MS + 2];
+__device__ __forceinline__ int pair_index(int I, int J) { return I * 20 - I * (I - 1) / 2 + (J - I); }
+
+__device__ __forceinline__ void ke_block(const Hex20Smem& sm, int I, int J, double* out) {
+    // M is symmetric: block (I, J) with I > J is the transpose of block (J, I).
+    const bool t = I > J;
+    const double* m0 = sm.Mb[t ? pair_index(J, I) : pair_index(I, J)];
+    const double m00 = m0[0], m11 = m0[4], m22 = m0[8];
+    const double m01 = t ? m0[3] : m0[1], m02 = t ? m0[6] : m0[2];
+    const double m10 = t ? m0[1] : m0[3], m12 = t ? m0[7] : m0[5];
+    const double m20 = t ? m0[2] : m0[6], m21 = t ? m0[5] : m0[7];
     const double lam = sm.lam, mu = sm.mu, mtr = mu * (m00 + m11 + m22);
-    const double k[9] = {fma(lam, m00, fma(mu, m00, mtr)), fma(lam, m01, mu * m10), fma(lam, m02, mu * m20),
-                         fma(lam, m10, mu * m01), fma(lam, m11, fma(mu, m11, mtr)), fma(lam, m12, mu * m21),
-                         fma(lam, m20, mu * m02), fma(lam, m21, mu * m12), fma(lam, m22, fma(mu, m22, mtr))};
-    double* base = L.vals + chunk_vbase(L, c) + s;
-    const int stride = chunk_cap(L, c);
-    if (store) {
-#pragma unroll
-        for (int v = 0; v < 9; v++) base[(size_t)v * stride] = k[v];
-    } else {
-#pragma unroll
-        for (int v = 0; v < 9; v++) atomicAdd(base + (size_t)v * stride, k[v]);
-    }
+    out[0] = fma(lam, m00, fma(mu, m00, mtr));
+    out[1] = fma(lam, m01, mu * m10);
+    out[2] = fma(lam, m02, mu * m20);
+    out[3] = fma(lam, m10, mu * m01);
+    out[4] = fma(lam, m11, fma(mu, m11, mtr));
+    out[5] = fma(lam, m12, mu * m21);
+    out[6] = fma(lam, m20, mu * m02);
+    out[7] = fma(lam, m21, mu * m12);
+    out[8] = fma(lam, m22, fma(mu, m22, mtr));
 }
 
 // Resolves the 20 column slots of row node I of the current element and
@@ -158,7 +160,7 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
     int* view = sm.view[warp];
     const int key = lane < 20 ? sm.nodes[lane] + 1 : 0;
     int state = lane < 20 ? kUnresolved : kFound;
-    int my_c = 0, my_s = 0;
+    unsigned gid = 0;
     if (lane < 20) sm.state[warp][lane] = kUnresolved;
     int c = sm.nodes[I];
     for (int step = 0; step < kMaxChainSteps; step++) {
@@ -172,8 +174,7 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
             if (v != 0) {
                 const int j = element_lookup(sm, v & kColMask);
                 if (j >= 0) {
-                    sm.chunk[warp][j] = c;
-                    sm.slot[warp][j] = p - 2;
+                    sm.gid[warp][j] = slot_gid(L, c, p - 2);
                     sm.state[warp][j] = v < 0 ? kFoundPending : kFound;
                 }
             }
@@ -187,8 +188,7 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
         __syncwarp();
         if (state == kUnresolved && sm.state[warp][lane] != kUnresolved) {
             state = sm.state[warp][lane];
-            my_c = sm.chunk[warp][lane];
-            my_s = sm.slot[warp][lane];
+            gid = sm.gid[warp][lane];
         }
         // claim the first empty slot on the probe sequence of each absent column
         if (state == kUnresolved) {
@@ -211,8 +211,7 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
                     p0 = p;
                     continue;
                 }
-                my_c = c;
-                my_s = p - 2;
+                gid = slot_gid(L, c, p - 2);
                 break;
             }
         }
@@ -225,18 +224,46 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
         if (lane < 20 && state == kUnresolved) sm.state[warp][lane] = kUnresolved;
         __syncwarp();
     }
+    if (lane < 20) {
+        sm.state[warp][lane] = state;
+        sm.gid[warp][lane] = gid;
+        ke_block(sm, I, lane, &sm.stage[warp][lane * 9]);
+    }
     const unsigned claimed = __ballot_sync(kFull, state == kClaimed);
     if (lane == 0 && claimed) atomicAdd(L.counts + sm.nodes[I], __popc(claimed));
-    // Claimed blocks: plain stores. Found (published) blocks: atomicAdd.
-    if (state == kClaimed || (state == kFound && lane < 20)) write_block(L, sm, I, lane, my_c, my_s, state == kClaimed);
+    __syncwarp();
+    // Lane l writes entries l, l+32, ... of the row's 20 x 9 values: consecutive
+    // lanes write consecutive doubles of the same 72-byte slot block.
+    // 1. claimed blocks: plain stores, fence, publish (nothing else in between,
+    //    so slots stay pending as briefly as possible)
     if (claimed) {
+        for (int idx = lane; idx < 20 * 9; idx += 32) {
+            const int j = idx / 9;
+            if (sm.state[warp][j] == kClaimed) L.vals[(size_t)sm.gid[warp][j] * 9 + (idx - 9 * j)] = sm.stage[warp][idx];
+        }
         __threadfence();
         __syncwarp();
-        if (state == kClaimed) atomicExch(chunk_meta(L, my_c) + 2 + my_s, key);
+        if (state == kClaimed) {
+            int cc, s;
+            gid_chunk(L, gid, cc, s);
+            atomicExch(chunk_meta(L, cc) + 2 + s, key);
+        }
     }
-    // Blocks of slots another warp is still writing: wait, then add.
-    if (state == kFoundPending && wait_published(L, chunk_meta(L, my_c) + 2 + my_s))
-        write_block(L, sm, I, lane, my_c, my_s, false);
+    // 2. found (published) blocks: atomicAdd
+    for (int idx = lane; idx < 20 * 9; idx += 32) {
+        const int j = idx / 9;
+        if (sm.state[warp][j] == kFound) atomicAdd(L.vals + (size_t)sm.gid[warp][j] * 9 + (idx - 9 * j), sm.stage[warp][idx]);
+    }
+    // 3. blocks of slots another warp is still writing: wait, then add
+    if (state == kFoundPending) {
+        int cc, s;
+        gid_chunk(L, gid, cc, s);
+        if (wait_published(L, chunk_meta(L, cc) + 2 + s)) {
+            double* p = L.vals + (size_t)gid * 9;
+#pragma unroll
+            for (int v = 0; v < 9; v++) atomicAdd(p + v, sm.stage[warp][lane * 9 + v]);
+        }
+    }
     __syncwarp();
 }
 
@@ -259,7 +286,6 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
         sm.dN[g][1][n] = dy;
         sm.dN[g][2][n] = dz;
     }
-    for (int idx = tid; idx < 64 * PS; idx += kThreads) (&sm.P[0][0])[idx] = 0.0;
     if (tid < PS) sm.w[tid] = 0.0;
     int spare = -1;
     __syncthreads();
@@ -332,6 +358,11 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
             sm.w[tid] = weight3(tid / 9) * weight3((tid / 3) % 3) * weight3(tid % 3) * det;
         }
         __syncthreads();
+        // P aliases the previous element's M blocks: re-zero its padding.
+        for (int idx = tid; idx < 4 * PS + 60; idx += kThreads) {
+            if (idx < 4 * PS) (&sm.P[60][0])[idx] = 0.0;
+            else sm.P[idx - 4 * PS][27] = 0.0;
+        }
         // Physical gradients P[3n+a][g] = sum_i iJ[g][3a+i] dN[g][i][n]
         for (int idx = tid; idx < 27 * 20; idx += kThreads) {
             const int g = idx / 20, n = idx - 20 * g;
@@ -342,11 +373,11 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
         }
         __syncthreads();
         // M = (P diag(w)) P^T on the FP64 tensor cores: warp mt owns tile row mt.
-        if (warp < 8) {
-            double acc[8][2];
+        double acc[8][2];
 #pragma unroll
-            for (int nt = 0; nt < 8; nt++) acc[nt][0] = acc[nt][1] = 0.0;
-            const int fr = lane >> 2, fc = lane & 3;
+        for (int nt = 0; nt < 8; nt++) acc[nt][0] = acc[nt][1] = 0.0;
+        const int fr = lane >> 2, fc = lane & 3;
+        if (warp < 8) {
 #pragma unroll
             for (int ks = 0; ks < 7; ks++) {
                 const int k = 4 * ks + fc;
@@ -354,14 +385,17 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
 #pragma unroll
                 for (int nt = 0; nt < 8; nt++) dmma_8x8x4(acc[nt][0], acc[nt][1], a, sm.P[8 * nt + fr][k]);
             }
-            const int row = 8 * warp + fr;
+        }
+        __syncthreads();  // every warp has read P: its storage now takes the M blocks
+        if (warp < 8) {
+            const int row = 8 * warp + fr, I = row / 3, a = row - 3 * I;
             if (row < 60) {
 #pragma unroll
                 for (int nt = 0; nt < 8; nt++) {
-                    const int col = 8 * nt + 2 * fc;
-                    if (col < 60) {
-                        sm.M[row][col] = acc[nt][0];
-                        sm.M[row][col + 1] = acc[nt][1];
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int col = 8 * nt + 2 * fc + h, J = col / 3, b = col - 3 * J;
+                        if (col < 60 && I <= J) sm.Mb[pair_index(I, J)][3 * a + b] = acc[nt][h];
                     }
                 }
             }
