@@ -70,7 +70,7 @@ fem_status make_layout(const fem_mesh* m, const fem_opts* o, HostLayout& h) {
     } else {
         h.S1 = o->first_slots ? o->first_slots : 94;
         h.S2 = o->chunk_slots ? o->chunk_slots : 30;
-        if (h.S1 < 2 || h.S2 < 2 || (h.S1 + 2) % 4 || (h.S2 + 2) % 4 || h.S1 > 126 || h.S2 > 126)
+        if (h.S1 < 2 || h.S2 < 2 || (h.S1 + 2) % 4 || (h.S2 + 2) % 4 || h.S1 > 94 || h.S2 > 94)
             return FEM_ERR_BAD_ARG;
     }
     h.H1 = h.S1 + 2;

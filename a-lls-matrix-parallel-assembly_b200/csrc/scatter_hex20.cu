@@ -21,16 +21,17 @@
 // the gradients occupied. Ke blocks are formed from M per scattered row. The
 // Gauss-point shape derivatives (H20:95-128) are tabulated once per CTA.
 //
-// Scatter. Warp w serves row nodes w and w+10. It copies the row's chunk row
-// (512 bytes: next pointer + 126 hashed slots) to shared memory with one 16-byte
-// load per lane, matches every slot against a shared-memory hash of the
+// Scatter. Warp w serves row nodes w and w+10. It prefetches both rows' chunk
+// rows (384 bytes: next pointer + 94 hashed slots) into shared memory with one
+// 16-byte load per lane, matches every slot against a shared-memory hash of the
 // element's 20 nodes, and builds ballot bitmaps of the empty slots. Lane j then
 // claims the first empty slot on column node j's probe sequence with atomicCAS
 // (empty -> col|pending) if the column is absent — re-trying past slots another
 // warp has just taken — and follows / atomicCAS-links overflow chunks when the
-// probe sequence is full. Claimed blocks are stored, the warp fences and
-// publishes them; found blocks are accumulated with atomicAdd (after a bounded
-// wait for slots another warp is still writing).
+// probe sequence is full. Claimed blocks of both rows are stored, the warp
+// fences once and publishes them; found blocks are accumulated with coalesced
+// atomicAdds (after a bounded wait for slots another warp is still writing).
+// The next element's nodes and coordinates are prefetched during the scatter.
 #include "launch.h"
 
 namespace fem {
@@ -38,7 +39,7 @@ namespace {
 
 constexpr int kThreads = 320;
 constexpr int kWarps = kThreads / 32;
-constexpr int kMaxHex20Words = 128;  // chunk meta rows of at most 128 words (S <= 126, checked on the host)
+constexpr int kMaxHex20Words = 96;   // chunk meta rows of at most 96 words (S <= 94, checked on the host)
 constexpr int PS = 28;               // row stride of P (doubles): conflict-free m8n8k4 fragment loads
 constexpr int kHash = 64;            // element-node hash slots
 
@@ -84,8 +85,8 @@ struct Hex20Smem {
     double X[20][3];           // element node coordinates
     double J[27][9];           // Jacobians, then their inverses
     double w[PS];              // Gauss weight * detJ (w[27] = 0 pads the contraction)
-    alignas(16) int view[kWarps][kMaxHex20Words];  // per-warp copy of the chunk row (16-byte stores)
-    unsigned gid[kWarps][20];  // slot of each column node's entry in the row
+    alignas(16) int view[kWarps][2][kMaxHex20Words];  // per-warp copies of the two rows' chunks
+    unsigned gid[kWarps][20];  // slot of each column node's entry in the row being committed
     int state[kWarps][20];
     double stage[kWarps][20 * 9];  // the row's 20 Ke blocks, entry j*9 + v
     int hkey[kHash];           // element-node hash: node + 1 -> local index
@@ -96,6 +97,7 @@ struct Hex20Smem {
 };
 
 static_assert(offsetof(Hex20Smem, view) % 16 == 0, "int4 stores into view need 16-byte alignment");
+static_assert(kMaxHex20Words % 32 == 0 && kMaxHex20Words <= 128, "view rows: whole ballot words");
 static_assert((kMaxHex20Words * sizeof(int)) % 16 == 0, "view rows must stay 16-byte aligned");
 
 __device__ __forceinline__ unsigned hash_slot(int key) { return ((unsigned)key * 2654435761u) >> 26; }
@@ -152,21 +154,28 @@ __device__ __forceinline__ void ke_block(const Hex20Smem& sm, int I, int J, doub
     out[8] = fma(lam, m22, fma(mu, m22, mtr));
 }
 
-// Resolves the 20 column slots of row node I of the current element and
-// scatters its 20 Ke blocks (warp-cooperative; lane j owns column node j).
-__device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, int I, int warp, int lane,
-                                            int& spare) {
+// Copies the first chunk row of node n into view (one 16-byte load per lane).
+__device__ __forceinline__ void load_view(const ListLayout& L, int c, int* view, int lane) {
+    const int* meta = chunk_meta(L, c);
+    const int H = c < L.N ? L.H1 : L.H2;
+    for (int q = lane * 4; q < H; q += 128) *reinterpret_cast<int4*>(view + q) = ld_cg4(meta + q);
+}
+
+// Resolves the 20 column slots of row node I of the current element (lane j
+// owns column node j). On entry `view` holds the row's first chunk. Returns the
+// lane's state and slot; s_state / s_gid are per-warp scratch.
+__device__ __forceinline__ void resolve_row(const ListLayout& L, const Hex20Smem& sm, int I, int lane, int* view,
+                                            int* s_state, unsigned* s_gid, int& spare, int& state, unsigned& gid) {
     constexpr unsigned kFull = 0xFFFFFFFFu;
-    int* view = sm.view[warp];
     const int key = lane < 20 ? sm.nodes[lane] + 1 : 0;
-    int state = lane < 20 ? kUnresolved : kFound;
-    unsigned gid = 0;
-    if (lane < 20) sm.state[warp][lane] = kUnresolved;
+    state = lane < 20 ? kUnresolved : kFound;
+    gid = 0;
+    if (lane < 20) s_state[lane] = kUnresolved;
     int c = sm.nodes[I];
     for (int step = 0; step < kMaxChainSteps; step++) {
         int* meta = chunk_meta(L, c);
         const int H = c < L.N ? L.H1 : L.H2;
-        for (int q = lane * 4; q < H; q += 128) *reinterpret_cast<int4*>(view + q) = ld_cg4(meta + q);
+        if (step > 0) load_view(L, c, view, lane);
         __syncwarp();
         // columns already in this chunk
         for (int p = 2 + lane; p < H; p += 32) {
@@ -174,8 +183,8 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
             if (v != 0) {
                 const int j = element_lookup(sm, v & kColMask);
                 if (j >= 0) {
-                    sm.gid[warp][j] = slot_gid(L, c, p - 2);
-                    sm.state[warp][j] = v < 0 ? kFoundPending : kFound;
+                    s_gid[j] = slot_gid(L, c, p - 2);
+                    s_state[j] = v < 0 ? kFoundPending : kFound;
                 }
             }
         }
@@ -186,9 +195,9 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
             bm[k] = __ballot_sync(kFull, p >= 2 && p < H && view[p] == 0);
         }
         __syncwarp();
-        if (state == kUnresolved && sm.state[warp][lane] != kUnresolved) {
-            state = sm.state[warp][lane];
-            gid = sm.gid[warp][lane];
+        if (state == kUnresolved && s_state[lane] != kUnresolved) {
+            state = s_state[lane];
+            gid = s_gid[lane];
         }
         // claim the first empty slot on the probe sequence of each absent column
         if (state == kUnresolved) {
@@ -221,40 +230,40 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
         if (lane == 0) nc = next_chunk(L, c, spare);
         c = __shfl_sync(kFull, nc, 0);
         if (c < 0) break;  // pool overflow: status raised, unresolved columns dropped
-        if (lane < 20 && state == kUnresolved) sm.state[warp][lane] = kUnresolved;
+        if (lane < 20 && state == kUnresolved) s_state[lane] = kUnresolved;
         __syncwarp();
     }
+}
+
+// Stores the lane's claimed block (row I, column node `lane`) from registers.
+__device__ __forceinline__ void store_claimed(const ListLayout& L, const Hex20Smem& sm, int I, int lane, unsigned gid) {
+    double k[9];
+    ke_block(sm, I, lane, k);
+    double* p = L.vals + (size_t)gid * 9;
+#pragma unroll
+    for (int v = 0; v < 9; v++) p[v] = k[v];
+}
+
+__device__ __forceinline__ void publish(const ListLayout& L, unsigned gid, int key) {
+    int cc, s;
+    gid_chunk(L, gid, cc, s);
+    atomicExch(chunk_meta(L, cc) + 2 + s, key);
+}
+
+// Atomic adds of the found (published) blocks of row I: consecutive lanes add
+// consecutive doubles of the same 72-byte slot block. Pending blocks: wait, add.
+__device__ __forceinline__ void add_found(const ListLayout& L, Hex20Smem& sm, int I, int warp, int lane, int state,
+                                          unsigned gid) {
     if (lane < 20) {
         sm.state[warp][lane] = state;
         sm.gid[warp][lane] = gid;
         ke_block(sm, I, lane, &sm.stage[warp][lane * 9]);
     }
-    const unsigned claimed = __ballot_sync(kFull, state == kClaimed);
-    if (lane == 0 && claimed) atomicAdd(L.counts + sm.nodes[I], __popc(claimed));
     __syncwarp();
-    // Lane l writes entries l, l+32, ... of the row's 20 x 9 values: consecutive
-    // lanes write consecutive doubles of the same 72-byte slot block.
-    // 1. claimed blocks: plain stores, fence, publish (nothing else in between,
-    //    so slots stay pending as briefly as possible)
-    if (claimed) {
-        for (int idx = lane; idx < 20 * 9; idx += 32) {
-            const int j = idx / 9;
-            if (sm.state[warp][j] == kClaimed) L.vals[(size_t)sm.gid[warp][j] * 9 + (idx - 9 * j)] = sm.stage[warp][idx];
-        }
-        __threadfence();
-        __syncwarp();
-        if (state == kClaimed) {
-            int cc, s;
-            gid_chunk(L, gid, cc, s);
-            atomicExch(chunk_meta(L, cc) + 2 + s, key);
-        }
-    }
-    // 2. found (published) blocks: atomicAdd
     for (int idx = lane; idx < 20 * 9; idx += 32) {
         const int j = idx / 9;
         if (sm.state[warp][j] == kFound) atomicAdd(L.vals + (size_t)sm.gid[warp][j] * 9 + (idx - 9 * j), sm.stage[warp][idx]);
     }
-    // 3. blocks of slots another warp is still writing: wait, then add
     if (state == kFoundPending) {
         int cc, s;
         gid_chunk(L, gid, cc, s);
@@ -265,6 +274,36 @@ __device__ __forceinline__ void scatter_row(const ListLayout& L, Hex20Smem& sm, 
         }
     }
     __syncwarp();
+}
+
+// Scatter of row nodes I0 and I1 (I1 < 0: none) by one warp.
+__device__ __forceinline__ void scatter_rows(const ListLayout& L, Hex20Smem& sm, int I0, int I1, int warp, int lane,
+                                             int& spare) {
+    constexpr unsigned kFull = 0xFFFFFFFFu;
+    const int key = lane < 20 ? sm.nodes[lane] + 1 : 0;
+    load_view(L, sm.nodes[I0], sm.view[warp][0], lane);
+    if (I1 >= 0) load_view(L, sm.nodes[I1], sm.view[warp][1], lane);
+    int st0, st1 = kFound;
+    unsigned g0, g1 = 0;
+    resolve_row(L, sm, I0, lane, sm.view[warp][0], sm.state[warp], sm.gid[warp], spare, st0, g0);
+    if (I1 >= 0) resolve_row(L, sm, I1, lane, sm.view[warp][1], sm.state[warp], sm.gid[warp], spare, st1, g1);
+    // claimed blocks of both rows: store, one fence, publish (the slots stay
+    // pending only for the stores of this warp)
+    const unsigned c0 = __ballot_sync(kFull, st0 == kClaimed), c1 = __ballot_sync(kFull, st1 == kClaimed);
+    if (lane == 0) {
+        if (c0) atomicAdd(L.counts + sm.nodes[I0], __popc(c0));
+        if (c1) atomicAdd(L.counts + sm.nodes[I1], __popc(c1));
+    }
+    if (c0 | c1) {
+        if (st0 == kClaimed) store_claimed(L, sm, I0, lane, g0);
+        if (st1 == kClaimed) store_claimed(L, sm, I1, lane, g1);
+        __threadfence();
+        __syncwarp();
+        if (st0 == kClaimed) publish(L, g0, key);
+        if (st1 == kClaimed) publish(L, g1, key);
+    }
+    add_found(L, sm, I0, warp, lane, st0, g0);
+    if (I1 >= 0) add_found(L, sm, I1, warp, lane, st1, g1);
 }
 
 __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
@@ -288,6 +327,17 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
     }
     if (tid < PS) sm.w[tid] = 0.0;
     int spare = -1;
+    // node id and coordinates of the next element, loaded during the scatter
+    int pre_n = 0;
+    double pre_x = 0.0, pre_y = 0.0, pre_z = 0.0;
+    if (tid < 20 && blockIdx.x < m.E_count) {
+        pre_n = __ldg(m.conn + (size_t)blockIdx.x * 20 + tid);
+        if (pre_n >= 0 && pre_n < m.N) {
+            pre_x = __ldg(m.x + pre_n);
+            pre_y = __ldg(m.y + pre_n);
+            pre_z = __ldg(m.z + pre_n);
+        }
+    }
     __syncthreads();
 
     for (int e = blockIdx.x; e < m.E_count; e += gridDim.x) {
@@ -295,14 +345,14 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
         if (tid < kHash) sm.hkey[tid] = 0;
         __syncthreads();
         if (tid < 20) {
-            const int n = __ldg(m.conn + (size_t)e * 20 + tid);
+            const int n = pre_n;
             sm.nodes[tid] = n;
             if (n < 0 || n >= m.N) {
                 sm.bad = 1;
             } else {
-                sm.X[tid][0] = __ldg(m.x + n);
-                sm.X[tid][1] = __ldg(m.y + n);
-                sm.X[tid][2] = __ldg(m.z + n);
+                sm.X[tid][0] = pre_x;
+                sm.X[tid][1] = pre_y;
+                sm.X[tid][2] = pre_z;
                 // element-node hash (node ids of an element are distinct)
                 const int key = n + 1;
                 unsigned h = hash_slot(key);
@@ -323,8 +373,15 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
             sm.mu = E / (2.0 * (1.0 + nu));
         }
         __syncthreads();
+        const int e_next = e + gridDim.x;
+        if (tid < 20 && e_next < m.E_count) pre_n = __ldg(m.conn + (size_t)e_next * 20 + tid);
         if (sm.bad) {  // uniform: every thread reads the flag before anyone resets it
             if (tid == 0) raise_status(L.info, FEM_ERR_BAD_MESH);
+            if (tid < 20 && e_next < m.E_count && pre_n >= 0 && pre_n < m.N) {
+                pre_x = __ldg(m.x + pre_n);
+                pre_y = __ldg(m.y + pre_n);
+                pre_z = __ldg(m.z + pre_n);
+            }
             __syncthreads();
             continue;
         }
@@ -402,7 +459,12 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
         }
         __syncthreads();
         // Scatter: warp w serves row nodes w and w + 10.
-        for (int I = warp; I < 20; I += kWarps) scatter_row(L, sm, I, warp, lane, spare);
+        scatter_rows(L, sm, warp, warp + kWarps < 20 ? warp + kWarps : -1, warp, lane, spare);
+        if (tid < 20 && e_next < m.E_count && pre_n >= 0 && pre_n < m.N) {
+            pre_x = __ldg(m.x + pre_n);
+            pre_y = __ldg(m.y + pre_n);
+            pre_z = __ldg(m.z + pre_n);
+        }
         __syncthreads();
     }
 }

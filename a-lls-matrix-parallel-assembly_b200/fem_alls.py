@@ -21,7 +21,8 @@ from typing import Optional
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libfem_alls.so")
+# FEM_ALLS_LIB selects another build of the library (same C ABI).
+LIB_PATH = os.environ.get("FEM_ALLS_LIB") or os.path.join(HERE, "lib", "libfem_alls.so")
 
 FEM_OK = 0
 STATUS_NAMES = {0: "FEM_OK", 1: "FEM_ERR_BAD_ARG", 2: "FEM_ERR_BAD_MESH", 3: "FEM_ERR_POOL_OVERFLOW",

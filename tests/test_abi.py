@@ -49,7 +49,7 @@ def test_workspace_size_host_only(fem):
     assert fem.workspace_size(m, fem.opts(pool_factor=2.0)) > n
     h = mg.by_name("hex20_small")
     nh = fem.workspace_size(h)
-    nh2 = fem.workspace_size(h, fem.opts(first_slots=126, chunk_slots=62))
+    nh2 = fem.workspace_size(h, fem.opts(first_slots=94, chunk_slots=62))
     assert nh2 > nh
 
 
