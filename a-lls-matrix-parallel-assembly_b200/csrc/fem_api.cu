@@ -96,10 +96,12 @@ fem_status make_layout(const fem_mesh* m, const fem_opts* o, HostLayout& h) {
     off += align_up((size_t)h.N * sizeof(int));
     h.off_tiles = off;
     off += align_up((size_t)h.num_tiles * sizeof(long long));
-    h.off_elist = off;  // 2-D: visit order of the elements (perm), ranges, bucket histogram
-    if (h.dpn == 2)
-        off += align_up((size_t)h.E * sizeof(int)) + align_up(4 * sizeof(int)) +
-               align_up((size_t)2 * reorder_buckets(h.N) * sizeof(int));
+    h.off_elist = off;  // visit order of the elements (perm), ranges, bucket histogram (+ bbox)
+    {
+        const size_t nbuckets = h.dpn == 2 ? (size_t)2 * reorder_buckets(h.N) : (size_t)1 << (3 * morton_bits(h.E));
+        off += align_up((size_t)h.E * sizeof(int)) + align_up(4 * sizeof(int)) + align_up(nbuckets * sizeof(int)) +
+               align_up(6 * sizeof(unsigned long long));
+    }
     h.total = off;
     return FEM_OK;
 }
@@ -204,13 +206,17 @@ fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* wo
     if (err) return cuda_fail(err);
     if (h.E == 0) return FEM_OK;
     MeshView m = mesh_view(mesh);
+    int* perm = reinterpret_cast<int*>(b + h.off_elist);
+    int* ranges = reinterpret_cast<int*>(b + h.off_elist + align_up((size_t)h.E * sizeof(int)));
+    int* hist = reinterpret_cast<int*>(b + h.off_elist + align_up((size_t)h.E * sizeof(int)) + align_up(4 * sizeof(int)));
     if (h.kind == FEM_HEX20) {
-        err = launch_scatter_hex20(m, L, s);
+        const size_t nbuckets = (size_t)1 << (3 * morton_bits(h.E));
+        unsigned long long* bbox = reinterpret_cast<unsigned long long*>(
+            b + h.off_elist + align_up((size_t)h.E * sizeof(int)) + align_up(4 * sizeof(int)) +
+            align_up(nbuckets * sizeof(int)));
+        err = launch_reorder_3d(m, hist, ranges, perm, bbox, sm_count(), s);
+        if (!err) err = launch_scatter_hex20(m, L, perm, s);
     } else {
-        int* perm = reinterpret_cast<int*>(b + h.off_elist);
-        int* ranges = reinterpret_cast<int*>(b + h.off_elist + align_up((size_t)h.E * sizeof(int)));
-        int* hist = reinterpret_cast<int*>(b + h.off_elist + align_up((size_t)h.E * sizeof(int)) +
-                                           align_up(4 * sizeof(int)));
         err = launch_reorder(m, hist, ranges, perm, sm_count(), s);
         if (!err && h.kind != FEM_T3) err = launch_scatter_2d(m, L, 4, perm, ranges + 0, s);
         if (!err && h.kind != FEM_Q4) err = launch_scatter_2d(m, L, 3, perm, ranges + 2, s);

@@ -31,7 +31,12 @@ cudaError_t launch_scatter_2d(const MeshView& m, const ListLayout& L, int npe, c
 int reorder_buckets(int num_nodes);
 cudaError_t launch_reorder(const MeshView& m, int* hist, int* ranges, int* perm, int sms, cudaStream_t s);
 int sm_count();
-cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, cudaStream_t s);
+// perm: element visit order (spatial, from launch_reorder_3d).
+cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, const int* perm, cudaStream_t s);
+// Spatial (3-D Morton bucket) element order; hist needs 1 << (3 * morton_bits(E)) ints, bbox 6 words.
+int morton_bits(int num_elems);
+cudaError_t launch_reorder_3d(const MeshView& m, int* hist, int* ranges, int* perm, unsigned long long* bbox, int sms,
+                              cudaStream_t s);
 cudaError_t launch_consolidate(const ListLayout& L, int dpn, int* row_ptr, int* col_idx, double* values,
                                long long capacity, long long* tile_sums, int num_tiles, cudaStream_t s);
 cudaError_t launch_info_init(DevInfo* info, int pool_chunks, cudaStream_t s);

@@ -1,4 +1,4 @@
-// Element processing order for the 2-D scatter.
+// Element processing order for the scatter kernels.
 //
 // The scatter's cost is dominated by the L2 / HBM traffic of the row lists it
 // touches. Elements given in a shuffled order (the T3 and mixed benchmark
@@ -12,6 +12,13 @@
 //   k_bucket_scatter  perm[offset[key]++] = e
 // The input arrays are not modified; only the order in which the scatter
 // visits elements changes (and with it the order of the FP64 atomic adds).
+//
+// Hex20 meshes use a spatial order instead: a row node's elements (up to 8)
+// should be scattered close together in time, or its list lines are evicted
+// from L2 between their visits (in natural x-y-z order they are a whole z-layer
+// of elements apart). The key is the 3-D Morton code of the midpoint of each
+// element's corner diagonal (nodes 0 and 6), quantized on a 2^b grid over the
+// node bounding box (k_bbox), counting-sorted the same way.
 #include <algorithm>
 
 #include "launch.h"
@@ -21,6 +28,7 @@ namespace {
 
 constexpr int kBucketShift = 8;  // 256 nodes per bucket
 constexpr int kThreads = 256;
+constexpr int kMaxMortonBits = 5;  // at most 32^3 spatial buckets
 
 __device__ __forceinline__ int element_key(const MeshView& m, int e, int NB) {
     const int* c = m.conn + (size_t)e * m.stride;
@@ -93,9 +101,117 @@ __global__ void k_bucket_scatter(MeshView m, int NB, int* __restrict__ offsets, 
         perm[atomicAdd(offsets + element_key(m, e, NB), 1)] = e;
 }
 
+// Order-preserving map of a double to an unsigned 64-bit integer.
+__device__ __forceinline__ unsigned long long ordered_bits(double v) {
+    const unsigned long long u = (unsigned long long)__double_as_longlong(v);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double from_ordered_bits(unsigned long long u) {
+    return __longlong_as_double((long long)((u >> 63) ? (u & 0x7FFFFFFFFFFFFFFFull) : ~u));
+}
+
+// bbox = {min x, min y, min z, max x, max y, max z} as ordered bits.
+__global__ void k_bbox_init(unsigned long long* bbox) {
+    if (threadIdx.x < 3) bbox[threadIdx.x] = ~0ull;
+    else if (threadIdx.x < 6) bbox[threadIdx.x] = 0ull;
+}
+
+__global__ void k_bbox(MeshView m, unsigned long long* bbox) {
+    unsigned long long lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0ull, 0ull, 0ull};
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < m.N; n += gridDim.x * blockDim.x) {
+        const unsigned long long v[3] = {ordered_bits(__ldg(m.x + n)), ordered_bits(__ldg(m.y + n)),
+                                         ordered_bits(__ldg(m.z + n))};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            lo[d] = v[d] < lo[d] ? v[d] : lo[d];
+            hi[d] = v[d] > hi[d] ? v[d] : hi[d];
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long l2 = __shfl_xor_sync(0xFFFFFFFFu, lo[d], o);
+            const unsigned long long h2 = __shfl_xor_sync(0xFFFFFFFFu, hi[d], o);
+            lo[d] = l2 < lo[d] ? l2 : lo[d];
+            hi[d] = h2 > hi[d] ? h2 : hi[d];
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            atomicMin(bbox + d, lo[d]);
+            atomicMax(bbox + 3 + d, hi[d]);
+        }
+    }
+}
+
+// Spreads the low 10 bits of v to every third bit.
+__device__ __forceinline__ unsigned spread3(unsigned v) {
+    v &= 0x3FFu;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+__device__ __forceinline__ int morton_key(const MeshView& m, int e, const unsigned long long* bbox, int bits) {
+    const int* c = m.conn + (size_t)e * m.stride;
+    int n0 = __ldg(c + 0), n6 = __ldg(c + 6);
+    n0 = (n0 >= 0 && n0 < m.N) ? n0 : 0;  // bad ids are reported by the scatter
+    n6 = (n6 >= 0 && n6 < m.N) ? n6 : 0;
+    const double p[3] = {0.5 * (__ldg(m.x + n0) + __ldg(m.x + n6)), 0.5 * (__ldg(m.y + n0) + __ldg(m.y + n6)),
+                         0.5 * (__ldg(m.z + n0) + __ldg(m.z + n6))};
+    const int cells = 1 << bits;
+    unsigned q[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const double lo = from_ordered_bits(bbox[d]), hi = from_ordered_bits(bbox[3 + d]);
+        const double t = hi > lo ? (p[d] - lo) / (hi - lo) : 0.0;
+        int qi = (int)(t * cells);
+        q[d] = (unsigned)min(max(qi, 0), cells - 1);
+    }
+    return (int)(spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2));
+}
+
+__global__ void k_morton_count(MeshView m, const unsigned long long* bbox, int bits, int* __restrict__ hist) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m.E_count; e += gridDim.x * blockDim.x)
+        atomicAdd(hist + morton_key(m, e, bbox, bits), 1);
+}
+
+__global__ void k_morton_scatter(MeshView m, const unsigned long long* bbox, int bits, int* __restrict__ offsets,
+                                 int* __restrict__ perm) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m.E_count; e += gridDim.x * blockDim.x)
+        perm[atomicAdd(offsets + morton_key(m, e, bbox, bits), 1)] = e;
+}
+
 }  // namespace
 
 int reorder_buckets(int num_nodes) { return (num_nodes >> kBucketShift) + 1; }
+
+int morton_bits(int num_elems) {
+    int b = 1;
+    while (b < kMaxMortonBits && (1ll << (3 * b)) * 4 < (long long)num_elems) b++;
+    return b;
+}
+
+cudaError_t launch_reorder_3d(const MeshView& m, int* hist, int* ranges, int* perm, unsigned long long* bbox, int sms,
+                              cudaStream_t s) {
+    const int bits = morton_bits(m.E_count);
+    const int nkeys = 1 << (3 * bits);
+    cudaError_t err = cudaMemsetAsync(hist, 0, (size_t)nkeys * sizeof(int), s);
+    if (err) return err;
+    k_bbox_init<<<1, 32, 0, s>>>(bbox);
+    const long long wn = ((long long)m.N + kThreads - 1) / kThreads;
+    k_bbox<<<(int)std::min<long long>(wn > 0 ? wn : 1, (long long)sms * 4), kThreads, 0, s>>>(m, bbox);
+    const long long want = ((long long)m.E_count + kThreads - 1) / kThreads;
+    const int grid = (int)std::min<long long>(want > 0 ? want : 1, (long long)sms * 8);
+    k_morton_count<<<grid, kThreads, 0, s>>>(m, bbox, bits, hist);
+    k_bucket_scan<<<1, 1024, 0, s>>>(hist, nkeys, nkeys, 0, ranges);
+    k_morton_scatter<<<grid, kThreads, 0, s>>>(m, bbox, bits, hist, perm);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_reorder(const MeshView& m, int* hist, int* ranges, int* perm, int sms, cudaStream_t s) {
     const int NB = reorder_buckets(m.N);

@@ -5,7 +5,8 @@
 // 14.9 KB of local memory per thread and whose fixed 300-entry rows silently
 // drop overflow.
 //
-// One CTA (10 warps) per element at a time, persistent over the element range.
+// One CTA (10 warps) per element at a time, persistent over the elements, which
+// it visits in the spatial order computed by launch_reorder_3d.
 //
 // Element stiffness, in double. With the physical shape-function gradients
 // G_g (a 60-vector per Gauss point g, dof r = 3 node + dir) and
@@ -14,11 +15,11 @@
 // gives every 3x3 block of the isotropic stiffness as
 //     Ke_IJ[a][b] = lambda M[3I+a][3J+b] + mu M[3I+b][3J+a] + mu delta_ab tr(M_IJ)
 // which is algebraically the reference's per-Gauss-point block formula
-// (H20:173-191, c1 = lambda + 2 mu, c2 = lambda, c3 = mu). M is one 64x64x28
-// FP64 matrix product per element, computed on the FP64 tensor cores with
-// mma.sync.m8n8k4.f64 (8 warps x 8 tiles x 7 k-steps); only its 210 upper 3x3
-// node blocks are kept (so every Ke is exactly symmetric), in the shared memory
-// the gradients occupied. Ke blocks are formed from M per scattered row. The
+// (H20:173-191, c1 = lambda + 2 mu, c2 = lambda, c3 = mu). M is one symmetric
+// 64x64x28 FP64 matrix product per element, computed on the FP64 tensor cores
+// with mma.sync.m8n8k4.f64 (36 upper 8x8 tiles x 7 k-steps); only its 210 upper
+// 3x3 node blocks are kept (so every Ke is exactly symmetric), in the shared
+// memory the gradients occupied. Ke blocks are formed from M per scattered row. The
 // Gauss-point shape derivatives (H20:95-128) are tabulated once per CTA.
 //
 // Scatter. Warp w serves row nodes w and w+10. It prefetches both rows' chunk
@@ -47,6 +48,12 @@ constexpr int kHash = 64;            // element-node hash slots
 __constant__ signed char c_xin[20] = {-1, 1, 1, -1, -1, 1, 1, -1, 0, 1, 0, -1, 0, 1, 0, -1, -1, 1, 1, -1};
 __constant__ signed char c_etan[20] = {-1, -1, 1, 1, -1, -1, 1, 1, -1, 0, 1, 0, -1, 0, 1, 0, -1, -1, 1, 1};
 __constant__ signed char c_zetan[20] = {-1, -1, -1, -1, 1, 1, 1, 1, -1, -1, -1, -1, 1, 1, 1, 1, 0, 0, 0, 0};
+
+// The 36 upper 8x8 tiles (mt <= nt) of the 64x64 node-pair matrix.
+__constant__ unsigned char c_tile_m[36] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 1, 2, 2, 2,
+                                           2, 2, 2, 3, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 6, 6, 7};
+__constant__ unsigned char c_tile_n[36] = {0, 1, 2, 3, 4, 5, 6, 7, 1, 2, 3, 4, 5, 6, 7, 2, 3, 4,
+                                           5, 6, 7, 3, 4, 5, 6, 7, 4, 5, 6, 7, 5, 6, 7, 6, 7, 7};
 
 // Gauss abscissae / weights as the reference writes them (H20:45-46), in double.
 __device__ __forceinline__ double gauss3(int i) { return i == 0 ? -0.774596669241483 : (i == 1 ? 0.0 : 0.774596669241483); }
@@ -235,35 +242,46 @@ __device__ __forceinline__ void resolve_row(const ListLayout& L, const Hex20Smem
     }
 }
 
-// Stores the lane's claimed block (row I, column node `lane`) from registers.
-__device__ __forceinline__ void store_claimed(const ListLayout& L, const Hex20Smem& sm, int I, int lane, unsigned gid) {
-    double k[9];
-    ke_block(sm, I, lane, k);
-    double* p = L.vals + (size_t)gid * 9;
-#pragma unroll
-    for (int v = 0; v < 9; v++) p[v] = k[v];
-}
-
-__device__ __forceinline__ void publish(const ListLayout& L, unsigned gid, int key) {
-    int cc, s;
-    gid_chunk(L, gid, cc, s);
-    atomicExch(chunk_meta(L, cc) + 2 + s, key);
-}
-
-// Atomic adds of the found (published) blocks of row I: consecutive lanes add
-// consecutive doubles of the same 72-byte slot block. Pending blocks: wait, add.
-__device__ __forceinline__ void add_found(const ListLayout& L, Hex20Smem& sm, int I, int warp, int lane, int state,
-                                          unsigned gid) {
+// Stages row I's 20 Ke blocks (lane j: column node j) with their states.
+__device__ __forceinline__ void stage_row(Hex20Smem& sm, int I, int warp, int lane, int state, unsigned gid) {
     if (lane < 20) {
         sm.state[warp][lane] = state;
         sm.gid[warp][lane] = gid;
         ke_block(sm, I, lane, &sm.stage[warp][lane * 9]);
     }
     __syncwarp();
+}
+
+// Writes the staged blocks whose state is `which`: lane l handles entries
+// l, l+32, ... of the 20 x 9 values, so consecutive lanes write consecutive
+// doubles of the same 72-byte slot block (coalesced stores / atomics).
+template <bool kAtomic>
+__device__ __forceinline__ void write_staged(const ListLayout& L, const Hex20Smem& sm, int warp, int lane, int which) {
     for (int idx = lane; idx < 20 * 9; idx += 32) {
         const int j = idx / 9;
-        if (sm.state[warp][j] == kFound) atomicAdd(L.vals + (size_t)sm.gid[warp][j] * 9 + (idx - 9 * j), sm.stage[warp][idx]);
+        if (sm.state[warp][j] != which) continue;
+        double* p = L.vals + (size_t)sm.gid[warp][j] * 9 + (idx - 9 * j);
+        if (kAtomic)
+            atomicAdd(p, sm.stage[warp][idx]);
+        else
+            *p = sm.stage[warp][idx];
     }
+    __syncwarp();
+}
+
+// Publishes a claimed slot: a plain store of the column after the fence that
+// made its values visible.
+__device__ __forceinline__ void publish(const ListLayout& L, unsigned gid, int key) {
+    int cc, s;
+    gid_chunk(L, gid, cc, s);
+    __stcg(chunk_meta(L, cc) + 2 + s, key);
+}
+
+// Found (published) blocks of row I: atomicAdd. Pending blocks: wait, then add.
+__device__ __forceinline__ void add_found(const ListLayout& L, Hex20Smem& sm, int I, int warp, int lane, int state,
+                                          unsigned gid) {
+    stage_row(sm, I, warp, lane, state, gid);
+    write_staged<true>(L, sm, warp, lane, kFound);
     if (state == kFoundPending) {
         int cc, s;
         gid_chunk(L, gid, cc, s);
@@ -295,8 +313,14 @@ __device__ __forceinline__ void scatter_rows(const ListLayout& L, Hex20Smem& sm,
         if (c1) atomicAdd(L.counts + sm.nodes[I1], __popc(c1));
     }
     if (c0 | c1) {
-        if (st0 == kClaimed) store_claimed(L, sm, I0, lane, g0);
-        if (st1 == kClaimed) store_claimed(L, sm, I1, lane, g1);
+        if (c0) {
+            stage_row(sm, I0, warp, lane, st0, g0);
+            write_staged<false>(L, sm, warp, lane, kClaimed);
+        }
+        if (c1) {
+            stage_row(sm, I1, warp, lane, st1, g1);
+            write_staged<false>(L, sm, warp, lane, kClaimed);
+        }
         __threadfence();
         __syncwarp();
         if (st0 == kClaimed) publish(L, g0, key);
@@ -312,7 +336,7 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
                  : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListLayout L) {
+__global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListLayout L, const int* __restrict__ perm) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Hex20Smem& sm = *reinterpret_cast<Hex20Smem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -331,7 +355,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
     int pre_n = 0;
     double pre_x = 0.0, pre_y = 0.0, pre_z = 0.0;
     if (tid < 20 && blockIdx.x < m.E_count) {
-        pre_n = __ldg(m.conn + (size_t)blockIdx.x * 20 + tid);
+        pre_n = __ldg(m.conn + (size_t)__ldg(perm + blockIdx.x) * 20 + tid);
         if (pre_n >= 0 && pre_n < m.N) {
             pre_x = __ldg(m.x + pre_n);
             pre_y = __ldg(m.y + pre_n);
@@ -340,7 +364,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
     }
     __syncthreads();
 
-    for (int e = blockIdx.x; e < m.E_count; e += gridDim.x) {
+    for (int i = blockIdx.x; i < m.E_count; i += gridDim.x) {
+        const int e = __ldg(perm + i);
         if (tid == 0) sm.bad = 0;
         if (tid < kHash) sm.hkey[tid] = 0;
         __syncthreads();
@@ -373,11 +398,11 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
             sm.mu = E / (2.0 * (1.0 + nu));
         }
         __syncthreads();
-        const int e_next = e + gridDim.x;
-        if (tid < 20 && e_next < m.E_count) pre_n = __ldg(m.conn + (size_t)e_next * 20 + tid);
+        const int i_next = i + gridDim.x;
+        if (tid < 20 && i_next < m.E_count) pre_n = __ldg(m.conn + (size_t)__ldg(perm + i_next) * 20 + tid);
         if (sm.bad) {  // uniform: every thread reads the flag before anyone resets it
             if (tid == 0) raise_status(L.info, FEM_ERR_BAD_MESH);
-            if (tid < 20 && e_next < m.E_count && pre_n >= 0 && pre_n < m.N) {
+            if (tid < 20 && i_next < m.E_count && pre_n >= 0 && pre_n < m.N) {
                 pre_x = __ldg(m.x + pre_n);
                 pre_y = __ldg(m.y + pre_n);
                 pre_z = __ldg(m.z + pre_n);
@@ -429,30 +454,40 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
             for (int a = 0; a < 3; a++) sm.P[3 * n + a][g] = fma(iJ[3 * a], d0, fma(iJ[3 * a + 1], d1, iJ[3 * a + 2] * d2));
         }
         __syncthreads();
-        // M = (P diag(w)) P^T on the FP64 tensor cores: warp mt owns tile row mt.
-        double acc[8][2];
+        // M = (P diag(w)) P^T on the FP64 tensor cores, upper 8x8 tiles only
+        // (M is symmetric): the 36 tiles (mt <= nt) are dealt round-robin to the
+        // warps, at most 4 per warp.
+        double acc[4][2];
 #pragma unroll
-        for (int nt = 0; nt < 8; nt++) acc[nt][0] = acc[nt][1] = 0.0;
+        for (int q = 0; q < 4; q++) acc[q][0] = acc[q][1] = 0.0;
         const int fr = lane >> 2, fc = lane & 3;
-        if (warp < 8) {
 #pragma unroll
-            for (int ks = 0; ks < 7; ks++) {
-                const int k = 4 * ks + fc;
-                const double a = sm.w[k] * sm.P[8 * warp + fr][k];
+        for (int q = 0; q < 4; q++) {
+            const int t = warp + q * kWarps;
+            if (t < 36) {
+                const int mt = c_tile_m[t], nt = c_tile_n[t];
 #pragma unroll
-                for (int nt = 0; nt < 8; nt++) dmma_8x8x4(acc[nt][0], acc[nt][1], a, sm.P[8 * nt + fr][k]);
+                for (int ks = 0; ks < 7; ks++) {
+                    const int k = 4 * ks + fc;
+                    dmma_8x8x4(acc[q][0], acc[q][1], sm.w[k] * sm.P[8 * mt + fr][k], sm.P[8 * nt + fr][k]);
+                }
             }
         }
         __syncthreads();  // every warp has read P: its storage now takes the M blocks
-        if (warp < 8) {
-            const int row = 8 * warp + fr, I = row / 3, a = row - 3 * I;
-            if (row < 60) {
 #pragma unroll
-                for (int nt = 0; nt < 8; nt++) {
+        for (int q = 0; q < 4; q++) {
+            const int t = warp + q * kWarps;
+            if (t < 36) {
+                const int mt = c_tile_m[t], nt = c_tile_n[t];
 #pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        const int col = 8 * nt + 2 * fc + h, J = col / 3, b = col - 3 * J;
-                        if (col < 60 && I <= J) sm.Mb[pair_index(I, J)][3 * a + b] = acc[nt][h];
+                for (int h = 0; h < 2; h++) {
+                    const int r = 8 * mt + fr, c = 8 * nt + 2 * fc + h;
+                    // entry (r, c) stands for itself and, by symmetry, for (c, r);
+                    // in a diagonal tile only r <= c writes (its mirror is in the tile)
+                    if (r < 60 && c < 60 && (mt < nt || r <= c)) {
+                        const int I = r / 3, a = r - 3 * I, J = c / 3, b = c - 3 * J;
+                        if (I <= J) sm.Mb[pair_index(I, J)][3 * a + b] = acc[q][h];
+                        if (J <= I) sm.Mb[pair_index(J, I)][3 * b + a] = acc[q][h];
                     }
                 }
             }
@@ -460,7 +495,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
         __syncthreads();
         // Scatter: warp w serves row nodes w and w + 10.
         scatter_rows(L, sm, warp, warp + kWarps < 20 ? warp + kWarps : -1, warp, lane, spare);
-        if (tid < 20 && e_next < m.E_count && pre_n >= 0 && pre_n < m.N) {
+        if (tid < 20 && i_next < m.E_count && pre_n >= 0 && pre_n < m.N) {
             pre_x = __ldg(m.x + pre_n);
             pre_y = __ldg(m.y + pre_n);
             pre_z = __ldg(m.z + pre_n);
@@ -471,7 +506,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
 
 }  // namespace
 
-cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, cudaStream_t s) {
+cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, const int* perm, cudaStream_t s) {
     static int blocks_per_sm = 0, sms = 0;
     const size_t smem = sizeof(Hex20Smem);
     if (!blocks_per_sm) {
@@ -484,7 +519,7 @@ cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, cudaStr
     }
     long long grid = (long long)blocks_per_sm * sms;
     if (grid > m.E_count) grid = m.E_count > 0 ? m.E_count : 1;
-    k_scatter_hex20<<<(int)grid, kThreads, smem, s>>>(m, L);
+    k_scatter_hex20<<<(int)grid, kThreads, smem, s>>>(m, L, perm);
     return cudaGetLastError();
 }
 

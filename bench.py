@@ -305,9 +305,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     print(json.dumps(line), flush=True)
 
 
-# k_info_init; 2-D: k_bucket_count, k_bucket_scan, k_bucket_scatter; scatter kernel(s);
+# k_info_init; 2-D: k_bucket_count, k_bucket_scan, k_bucket_scatter; Hex20: k_bbox_init,
+# k_bbox, k_morton_count, k_bucket_scan, k_morton_scatter; scatter kernel(s);
 # k_consolidate_reset, k_scan_reduce, k_scan_tiles, k_row_ptr, k_write
-KERNELS_PER_STEP = {"q4": 10, "t3": 10, "mixed": 11, "hex20": 7}
+KERNELS_PER_STEP = {"q4": 10, "t3": 10, "mixed": 11, "hex20": 12}
 
 
 def read_profile_traffic(workload: str):
