@@ -49,6 +49,35 @@ def test_q4_values_bitwise_equal_reference_host_assembly(oracle_mod, golden, nam
     assert prec["count_gt_1e-10"] == 0 and prec["max_abs"] == 0.0
 
 
+DEVICE_NPZ = os.path.join(GOLDEN, "reference_device_ke.npz")
+
+
+@pytest.mark.parametrize("name,bound", [("t3_small", 1e-14), ("mixed_small", 1e-14), ("hex20_small", 5e-6)])
+def test_element_stiffness_matches_reference_device_functions(oracle_mod, name, bound):
+    # Per-element Ke of the reference's own device functions (computeElementStiffness
+    # T3:136 and MIX:145 in FP64, computeElementStiffnessHex20 H20:130 in FP32) on
+    # jittered meshes, generated on a B200 by make_golden.py --gpu. The error is
+    # measured against sqrt(|K_ii K_jj|); the Hex20 bound is the reference's FP32.
+    g = np.load(DEVICE_NPZ)
+    E, nu, t = g[f"{name}/material"]
+    conn, x, y = g[f"{name}/conn"], g[f"{name}/x"], g[f"{name}/y"]
+    worst = 0.0
+    for e in range(conn.shape[0]):
+        c = conn[e]
+        if name == "hex20_small":
+            k = oracle_mod.ke_hex20(x[c], y[c], g[f"{name}/z"][c], E, nu)
+            r = g[f"{name}/ke"][e].astype(np.float64)
+        elif name == "mixed_small" and g[f"{name}/types"][e] == 0:
+            k = oracle_mod.ke_q4(x[c], y[c], E, nu, t)
+            r = g[f"{name}/ke"][e]
+        else:
+            k = oracle_mod.ke_t3(x[c[:3]], y[c[:3]], E, nu, t)
+            r = g[f"{name}/ke"][e][:6, :6]
+        d = np.sqrt(np.abs(np.diag(k)))
+        worst = max(worst, float(np.max(np.abs(k - r) / np.outer(d, d))))
+    assert worst <= bound, worst
+
+
 def test_hex20_reference_lattice_has_orphan_rows(golden):
     rp = golden["hex20_ref_lattice2/row_ptr"]
     empty = int(np.sum(np.diff(rp) == 0))
