@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "launch.h"
@@ -386,6 +387,73 @@ fem_status fem_assemble_host(fem_context* ctx, const fem_mesh* hm, const fem_opt
     if (!err) err = cudaStreamSynchronize(s);
     if (err) return cuda_fail(err);
     return st;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Assembly without allocation: the workspace in a static device array
+// ---------------------------------------------------------------------------
+//
+// Some callers cannot call cudaMalloc. An application or solver framework that
+// owns the GPU's memory through its own pool allocator does not let a plug-in
+// allocate behind its back (its accounting and memory limits would be wrong),
+// and a time-stepping loop that must not stall avoids cudaMalloc and cudaFree
+// because they can synchronize the whole device. fem_assemble_static serves
+// them: it is fem_assemble with the workspace in g_static_workspace, a
+// file-scope device array of FEM_STATIC_WORKSPACE_BYTES that every GPU which
+// loads this library holds until the process exits. The caller still passes
+// the mesh arrays and the CSR output buffers.
+//
+// Set-up: the first call on a device, with that device current, looks up the
+// array's device address (cudaGetSymbolAddress) and keeps it for that device;
+// make that first call before any stream capture. In host code the name
+// g_static_workspace is only a host-side stand-in, never a device address.
+//
+// All calls on a device share the one array, which keeps the last call's
+// contents. Each assembly clears what must start at zero (info word, first
+// chunk rows, row counters) and writes every value before reading it, so
+// consecutive calls are independent; calls whose work overlaps on the GPU
+// (different streams, or different host threads) race on the array and
+// corrupt each other's results.
+
+namespace {
+
+__device__ __align__(256) unsigned char g_static_workspace[FEM_STATIC_WORKSPACE_BYTES];
+
+constexpr int kMaxStaticDevices = 64;
+std::mutex g_static_mutex;
+void* g_static_ptr[kMaxStaticDevices] = {};
+
+fem_status static_workspace(void** ptr) {
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err) return cuda_fail(err);
+    if (dev < 0 || dev >= kMaxStaticDevices) return FEM_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (!g_static_ptr[dev]) {
+        void* p = nullptr;
+        err = cudaGetSymbolAddress(&p, g_static_workspace);
+        if (err) return cuda_fail(err);
+        g_static_ptr[dev] = p;
+    }
+    *ptr = g_static_ptr[dev];
+    return FEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fem_status fem_assemble_static(const fem_mesh* mesh, const fem_opts* opts, fem_csr* out, void* stream) {
+    if (!out) return FEM_ERR_BAD_ARG;
+    size_t need = 0;
+    fem_status st = fem_alls_workspace_size(mesh, opts, &need);
+    if (st) return st;
+    if (need > (size_t)FEM_STATIC_WORKSPACE_BYTES) return FEM_ERR_WORKSPACE;  // mesh too large for the array
+    void* ws = nullptr;
+    if ((st = static_workspace(&ws))) return st;
+    return fem_assemble(mesh, opts, ws, (size_t)FEM_STATIC_WORKSPACE_BYTES, out, stream);
 }
 
 }  // extern "C"

@@ -33,7 +33,9 @@ globals().update({v: k for k, v in STATUS_NAMES.items()})
 # C ABI exports (kept in sync with include/fem_alls.h by tests/test_abi.py).
 EXPORTS = ["fem_alls_workspace_size", "fem_alls_scatter", "fem_alls_consolidate", "fem_alls_read_info",
            "fem_assemble", "fem_assemble_async", "fem_context_create", "fem_context_destroy",
-           "fem_assemble_host", "fem_status_string", "fem_last_cuda_error", "fem_abi_version"]
+           "fem_assemble_host", "fem_status_string", "fem_last_cuda_error", "fem_abi_version",
+           "fem_assemble_static"]
+STATIC_WORKSPACE_BYTES = 32 << 20  # FEM_STATIC_WORKSPACE_BYTES
 
 
 class FemMesh(C.Structure):

@@ -174,6 +174,29 @@ FEM_API void fem_context_destroy(fem_context* ctx);
 FEM_API fem_status fem_assemble_host(fem_context* ctx, const fem_mesh* host_mesh, const fem_opts* opts,
                              fem_csr* host_out, void* stream);
 
+/* ---- assembly without allocation -------------------------------------------- */
+
+/* Size of the static device workspace of fem_assemble_static (32 MiB): enough
+ * for a Q4 or T3 mesh of up to about 55,000 nodes (230x230 cells) or a Hex20
+ * mesh of 9x9x9 elements, with the default options. */
+#define FEM_STATIC_WORKSPACE_BYTES (32u << 20)
+
+/* No counterpart in the reference (its drivers cudaMalloc all device memory).
+ * For callers that cannot call cudaMalloc: a plug-in inside an application
+ * that owns the GPU's memory through its own pool allocator, or a loop that
+ * must not stall on cudaMalloc / cudaFree (they can synchronize the device).
+ * Same as fem_assemble, but the workspace is a static device array of
+ * FEM_STATIC_WORKSPACE_BYTES inside the library, which every GPU that loads
+ * the library holds until the process exits; mesh and out are still the
+ * caller's device buffers. A mesh whose fem_alls_workspace_size exceeds the
+ * array is refused with FEM_ERR_WORKSPACE before any launch. The first call on
+ * a device (with that device current) looks up the array's device address;
+ * make that first call before any stream capture. All calls on a device share
+ * the array: each call clears what must start at zero, but calls whose work
+ * overlaps on the GPU (different streams or host threads) race on it.
+ * Synchronous, like fem_assemble. */
+FEM_API fem_status fem_assemble_static(const fem_mesh* mesh, const fem_opts* opts, fem_csr* out, void* stream);
+
 /* ---- misc ------------------------------------------------------------------- */
 FEM_API const char* fem_status_string(fem_status s);
 FEM_API int32_t fem_last_cuda_error(void);   /* cudaError_t of the last FEM_ERR_CUDA (per thread) */
