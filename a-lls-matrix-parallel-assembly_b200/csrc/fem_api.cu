@@ -204,6 +204,9 @@ fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* wo
     if (!err) err = launch_info_init(L.info, h.cap2, s);
     if (!err) err = cudaMemsetAsync(b + h.off_meta1, 0, h.meta1_bytes, s);
     if (!err) err = cudaMemsetAsync(b + h.off_counts, 0, (size_t)h.N * sizeof(int), s);
+    // 2-D lists accumulate every contribution with atomic adds: their first
+    // chunks' slot values start at zero (overflow chunks are zeroed when taken).
+    if (!err && h.dpn == 2) err = cudaMemsetAsync(b + h.off_vals, 0, (size_t)h.N * h.S1 * h.B * sizeof(double), s);
     if (err) return cuda_fail(err);
     if (h.E == 0) return FEM_OK;
     MeshView m = mesh_view(mesh);

@@ -93,9 +93,12 @@ __device__ __forceinline__ void gid_chunk(const ListLayout& L, unsigned gid, int
 __device__ __forceinline__ int ld_cg(const int* p) { return __ldcg(p); }
 __device__ __forceinline__ int4 ld_cg4(const int* p) { return __ldcg(reinterpret_cast<const int4*>(p)); }
 
-// Takes one chunk from the overflow pool and zeroes its meta row. Returns the
-// chunk id, or -1 (and raises FEM_ERR_POOL_OVERFLOW) when the pool is empty.
-// The caller must __threadfence() before publishing the chunk.
+// Takes one chunk from the overflow pool and zeroes its meta row (and, with
+// kZeroVals, its slots' values, for lists whose contributions are all
+// atomic adds). Returns the chunk id, or -1 (and raises FEM_ERR_POOL_OVERFLOW)
+// when the pool is empty. The caller must __threadfence() before publishing
+// the chunk.
+template <bool kZeroVals = false>
 __device__ __forceinline__ int alloc_chunk(const ListLayout& L) {
     int k = atomicAdd(&L.info->overflow_chunks, 1);
     if (k >= L.cap2) {
@@ -104,6 +107,10 @@ __device__ __forceinline__ int alloc_chunk(const ListLayout& L) {
     }
     int* m = L.meta2 + (size_t)k * L.H2;
     for (int i = 0; i < L.H2; i += 4) *reinterpret_cast<int4*>(m + i) = make_int4(0, 0, 0, 0);
+    if (kZeroVals) {
+        double2* v = reinterpret_cast<double2*>(L.vals + (size_t)slot_gid(L, L.N + k, 0) * L.B);
+        for (int i = 0; i < L.S2 * L.B / 2; i++) v[i] = make_double2(0.0, 0.0);
+    }
     return L.N + k;
 }
 
@@ -121,11 +128,12 @@ __device__ __forceinline__ int probe_start(int key, int S) {
 // Next chunk of chunk c, allocating and atomicCAS-linking a new one if there is
 // none. Returns -1 on pool overflow (status raised). `spare` keeps a chunk that
 // lost a link race for this thread's next allocation (-1 = none).
+template <bool kZeroVals = false>
 __device__ __forceinline__ int next_chunk(const ListLayout& L, int c, int& spare) {
     int* m = chunk_meta(L, c);
     int nx = ld_cg(m + 1);
     if (nx == 0) {
-        int nc = spare >= 0 ? spare : alloc_chunk(L);
+        int nc = spare >= 0 ? spare : alloc_chunk<kZeroVals>(L);
         spare = -1;
         if (nc < 0) return -1;
         __threadfence();  // the zeroed meta row is visible before the link

@@ -3,24 +3,35 @@
 // Replaces assembleGlobalStiffnessKernelALLS
 // (ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:394-468,
 //  ALLS_T3_Unstructed_Elements_Assemble_Performance.cu:227-290,
-//  ALLS_Q4_T3_Mixed_Elements_Assembly_Performance.cu:248-312).
+//  ALLS_Q4_T3_Mixed_Elements_Assembly_Performance.cu:248-312), which runs one
+// thread per element and walks a pointer list for each of its ndof^2 entries.
 //
-// One thread per (element, row node) instead of one per element:
-//  * elements are visited in a node-local order (reorder.cu) so the lists they
-//    touch stay in L2;
-//  * the thread computes its row of Ke in registers (node-block form) and reads
-//    its row node's list one 64-byte chunk row at a time (next pointer and 14
-//    hashed slots in four 16-byte L2 loads); every column node of the element
-//    is looked up along its probe sequence and, if absent, its slot is claimed
-//    with atomicCAS (empty -> col|pending) — one slot per column and row, never
-//    a duplicate; a failed CAS re-reads the chunk before the next column;
-//  * the claimer stores its block values with plain 16-byte stores, fences, and
-//    publishes the column; found columns are accumulated with atomicAdd
-//    (red.global.add.f64), after a bounded wait if the slot is still pending.
-//    A thread publishes its own claims before it waits on anyone else's, so
-//    no wait can be circular. Claims are counted per row node for the scan.
-// The reference instead walks a pointer list per (row, col) pair and can lose a
-// contribution or insert a column twice (its head-insert race, Q4A:452-463).
+// Here one LANE serves one node block (a, b) of one element: NPE^2 lanes per
+// element (T3: 9 lanes, 3 elements per warp; Q4: 16 lanes, 2 per warp).
+//  * Every lane loads the element's nodes and coordinates (same addresses
+//    across the element's lanes, so the loads are shared) and computes its own
+//    2x2 block K_ab in FP64 (element2d.cuh).
+//  * It reads row node a's 64-byte first chunk (next pointer and 14 hashed
+//    slots) with four 16-byte L2 loads and looks for column node b in it. An
+//    absent column is claimed with atomicCAS(empty -> col) at the first empty
+//    slot of its probe sequence; a CAS that meets another column marks that
+//    slot taken in the lane's view and moves on along the sequence (slots are
+//    never freed, so a column is always found or placed at the first empty
+//    slot of its sequence, never twice). A chunk whose probe sequence is full
+//    continues in an overflow chunk (allocated from the pool with zeroed
+//    values, linked by CAS).
+//  * The values of every slot start at zero (the first chunks' values are
+//    cleared before the launch), so the claimer and every later contributor
+//    alike add their block with FP64 red.add: the claim publishes the column
+//    at once, with no pending state, no fence and no waiting on another
+//    thread. The warp transposes its blocks through shared memory so that each
+//    red instruction covers eight whole 32-byte blocks (four consecutive lanes
+//    per block) instead of 32 scattered sectors.
+//  * Claims are counted per (element, row) group with one atomic per group.
+// Elements are visited in the node-local order of reorder.cu, so the rows that
+// a warp touches are close together and stay in L2.
+// The reference's head insert can lose a contribution or insert a column
+// twice (Q4A:452-463); the claim/publish protocol above does neither.
 #include <algorithm>
 
 #include "element2d.cuh"
@@ -29,161 +40,182 @@
 namespace fem {
 namespace {
 
-enum SlotState : int { kUnresolved = 0, kFound = 1, kFoundPending = 2, kClaimed = 3 };
+enum SlotState : int { kUnresolved = 0, kFound = 1, kClaimed = 3, kSkip = 4 };
 constexpr int kMask14 = (1 << k2DSlots) - 1;
+constexpr int kThreads2D = 256;
+constexpr int kWarps2D = kThreads2D / 32;
 
 __device__ __forceinline__ unsigned rot14(unsigned m, int h) {
     return ((m >> h) | (m << (k2DSlots - h))) & kMask14;
 }
 
-template <int NPE>
-__device__ __forceinline__ void scatter_row_2d(const MeshView& m, const ListLayout& L, int e, int a, int& spare) {
-    int nodes[NPE];
-    bool bad = false;
-#pragma unroll
-    for (int a = 0; a < NPE; a++) {
-        nodes[a] = __ldg(m.conn + (size_t)e * m.stride + a);
-        bad |= (nodes[a] < 0) | (nodes[a] >= m.N);
-    }
-    if (bad) {
-        if (a == 0) raise_status(L.info, FEM_ERR_BAD_MESH);
-        return;
-    }
-    double xe[NPE], ye[NPE];
-#pragma unroll
-    for (int a = 0; a < NPE; a++) {
-        xe[a] = __ldg(m.x + nodes[a]);
-        ye[a] = __ldg(m.y + nodes[a]);
-    }
-    const double E = m.E ? __ldg(m.E + e) : m.E0;
-    const double nu = m.nu ? __ldg(m.nu + e) : m.nu0;
-    double kr[NPE][4];  // blocks K_ab of this thread's row a
-    double det;
-    if constexpr (NPE == 4) {
-        det = ke_q4_row(xe, ye, E, nu, m.t, a, kr);
-    } else {
-        det = ke_t3_row(xe, ye, E, nu, m.t, a, kr);
-    }
-    if (a == 0 && !(det > 0.0)) raise_status(L.info, FEM_ERR_DETJ);
-    int row_node = nodes[0];
-#pragma unroll
-    for (int i = 1; i < NPE; i++) row_node = a == i ? nodes[i] : row_node;
-    {
-        int state[NPE];
-        unsigned gid[NPE];
-        int* word[NPE];
-#pragma unroll
-        for (int b = 0; b < NPE; b++) {
-            state[b] = kUnresolved;
-            gid[b] = 0;
-            word[b] = nullptr;
+// Finds or claims the slot of column key `key` in the row list of node `row`.
+// Returns the slot state (kFound, kClaimed, or kSkip on pool overflow); gid is
+// the slot's global id.
+// view: the row's first chunk, loaded by the caller (possibly some time ago:
+// a stale view only costs failed CASes, never a wrong slot).
+__device__ __forceinline__ int resolve_2d(const ListLayout& L, int row, int key, const int4 (&view)[4], int& spare,
+                                          unsigned& gid) {
+    int c = row;
+    for (int step = 0; step < kMaxChainSteps; step++) {
+        int* meta = chunk_meta(L, c);
+        int4 w0 = view[0], w1 = view[1], w2 = view[2], w3 = view[3];
+        if (step > 0) {
+            w0 = ld_cg4(meta);
+            w1 = ld_cg4(meta + 4);
+            w2 = ld_cg4(meta + 8);
+            w3 = ld_cg4(meta + 12);
         }
-        // Resolve the slot of every column node of the element in row node a.
-        // A failed CAS means the register view of the chunk is stale; the chunk
-        // is then re-read before the remaining columns are resolved (a column
-        // another thread has just claimed must be found, not claimed again).
-        int c = row_node;
-        for (int step = 0; step < kMaxChainSteps; step++) {
-            int* meta = chunk_meta(L, c);
-            const int4 w0 = ld_cg4(meta), w1 = ld_cg4(meta + 4), w2 = ld_cg4(meta + 8), w3 = ld_cg4(meta + 12);
-            const int cols[k2DSlots] = {w0.z, w0.w, w1.x, w1.y, w1.z, w1.w, w2.x,
-                                        w2.y, w2.z, w2.w, w3.x, w3.y, w3.z, w3.w};
-            unsigned empty = 0, pend = 0;
+        const int cols[k2DSlots] = {w0.z, w0.w, w1.x, w1.y, w1.z, w1.w, w2.x,
+                                    w2.y, w2.z, w2.w, w3.x, w3.y, w3.z, w3.w};
+        unsigned empty = 0, match = 0;
 #pragma unroll
-            for (int s = 0; s < k2DSlots; s++) {
-                empty |= (cols[s] == 0 ? 1u : 0u) << s;
-                pend |= (cols[s] < 0 ? 1u : 0u) << s;
-            }
-            bool all = true, full = false, stale = false;
-#pragma unroll
-            for (int b = 0; b < NPE; b++) {
-                if (state[b] == kUnresolved && !stale) {
-                    const int key = nodes[b] + 1;
-                    unsigned match = 0;
-#pragma unroll
-                    for (int s = 0; s < k2DSlots; s++) match |= (((cols[s] & kColMask) == key) ? 1u : 0u) << s;
-                    const int h = probe_start(key, k2DSlots);
-                    const unsigned cand = rot14(match | empty, h);
-                    if (!cand) {
-                        full = true;  // no free slot on this chunk's probe sequence
-                    } else {
-                        int pos = h + __ffs(cand) - 1;
-                        pos -= pos >= k2DSlots ? k2DSlots : 0;
-                        if (match & (1u << pos)) {
-                            state[b] = (pend >> pos) & 1u ? kFoundPending : kFound;
-                        } else {
-                            const int old = atomicCAS(meta + 2 + pos, 0, key | kPending);
-                            if (old == 0) {
-                                state[b] = kClaimed;
-                                empty &= ~(1u << pos);
-                            } else if ((old & kColMask) == key) {
-                                state[b] = old < 0 ? kFoundPending : kFound;
-                            } else {
-                                stale = true;  // slot taken by another column: re-read the chunk
-                            }
-                        }
-                        if (state[b] != kUnresolved) {
-                            gid[b] = slot_gid(L, c, pos);
-                            word[b] = meta + 2 + pos;
-                        }
-                    }
+        for (int s = 0; s < k2DSlots; s++) {
+            empty |= (cols[s] == 0 ? 1u : 0u) << s;
+            match |= (cols[s] == key ? 1u : 0u) << s;
+        }
+        int state = kUnresolved, pos = 0;
+        if (match) {
+            pos = __ffs(match) - 1;
+            state = kFound;
+        } else {
+            const int h = probe_start(key, k2DSlots);
+            for (int tries = 0; tries < k2DSlots; tries++) {
+                const unsigned cand = rot14(empty, h);
+                if (!cand) break;  // probe sequence full in this chunk: go on in the next one
+                pos = h + __ffs(cand) - 1;
+                pos -= pos >= k2DSlots ? k2DSlots : 0;
+                const int old = atomicCAS(meta + 2 + pos, 0, key);
+                if (old == 0) {
+                    state = kClaimed;
+                    break;
                 }
-                all &= state[b] != kUnresolved;
+                if (old == key) {
+                    state = kFound;
+                    break;
+                }
+                empty &= ~(1u << pos);  // taken by another column meanwhile
             }
-            if (all) break;
-            if (stale || !full) continue;  // same chunk, fresh view
-            c = next_chunk(L, c, spare);
-            if (c < 0) break;  // pool overflow: status raised, the rest of the row is dropped
         }
-        // Claimed slots: store values, fence, publish — before any atomic, so the
-        // fence waits only for these stores and the slots stay pending briefly.
-        int nclaimed = 0;
-#pragma unroll
-        for (int b = 0; b < NPE; b++) nclaimed += state[b] == kClaimed;
-        if (nclaimed) {
-            atomicAdd(L.counts + row_node, nclaimed);
-#pragma unroll
-            for (int b = 0; b < NPE; b++) {
-                if (state[b] != kClaimed) continue;
-                double* p = L.vals + (size_t)gid[b] * 4;
-                reinterpret_cast<double2*>(p)[0] = make_double2(kr[b][0], kr[b][1]);
-                reinterpret_cast<double2*>(p)[1] = make_double2(kr[b][2], kr[b][3]);
-            }
-            __threadfence();
-#pragma unroll
-            for (int b = 0; b < NPE; b++)
-                if (state[b] == kClaimed) atomicExch(word[b], nodes[b] + 1);
+        if (state != kUnresolved) {
+            gid = slot_gid(L, c, pos);
+            return state;
         }
-        // Found (published) slots: atomicAdd.
-#pragma unroll
-        for (int b = 0; b < NPE; b++) {
-            if (state[b] != kFound) continue;
-            double* p = L.vals + (size_t)gid[b] * 4;
-#pragma unroll
-            for (int v = 0; v < 4; v++) atomicAdd(p + v, kr[b][v]);
-        }
-        // Columns another thread is still writing: wait for them, then add.
-#pragma unroll
-        for (int b = 0; b < NPE; b++) {
-            if (state[b] != kFoundPending) continue;
-            if (!wait_published(L, word[b])) continue;
-            double* p = L.vals + (size_t)gid[b] * 4;
-#pragma unroll
-            for (int v = 0; v < 4; v++) atomicAdd(p + v, kr[b][v]);
-        }
+        c = next_chunk<true>(L, c, spare);
+        if (c < 0) return kSkip;  // pool overflow: status raised, the block is dropped
     }
+    raise_status(L.info, FEM_ERR_TIMEOUT);
+    return kSkip;
+}
+
+// Element id of work item `i` of this lane (valid: inside the range).
+__device__ __forceinline__ int element_of(const int* perm, int begin, int count, long long i, bool ok, bool& valid) {
+    valid = ok && i < count;
+    return valid ? __ldg(perm + begin + i) : 0;
 }
 
 template <int NPE>
-__global__ void __launch_bounds__(256, NPE == 3 ? 3 : 2) k_scatter_2d(MeshView m, ListLayout L, const int* __restrict__ perm,
-                                                   const int* __restrict__ range) {
+__global__ void __launch_bounds__(kThreads2D, NPE == 3 ? 4 : 2)
+    k_scatter_2d(MeshView m, ListLayout L, const int* __restrict__ perm, const int* __restrict__ range) {
+    constexpr int G = NPE * NPE;   // lanes per element
+    constexpr int EPW = 32 / G;    // elements per warp
+    constexpr unsigned kFull = 0xFFFFFFFFu;
+    __shared__ double s_val[kWarps2D][32][4];
+    __shared__ unsigned s_gid[kWarps2D][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int eslot = lane / G, sub = lane - eslot * G;
+    const int a = sub / NPE, b = sub - (sub / NPE) * NPE;
+    const bool lane_used = eslot < EPW;
+    const unsigned row_group = ((1u << NPE) - 1u) << (eslot * G + a * NPE);
     const int begin = range[0], count = range[1] - range[0];
-    const long long work = (long long)count * NPE;
+    const long long warp_id = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long stride = (((long long)gridDim.x * blockDim.x) >> 5) * EPW;
     int spare = -1;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < work;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t / NPE), a = (int)(t - (long long)i * NPE);
-        scatter_row_2d<NPE>(m, L, __ldg(perm + begin + i), a, spare);
+
+    // Software pipeline over this warp's work items k = 0, 1, 2, ...:
+    // iteration k works on element k (nodes, coordinates and material loaded
+    // during iteration k-1) while element k+1's node ids and element k+2's id
+    // are in flight.
+    long long base = warp_id * EPW;
+    bool valid, valid1, valid2;
+    int e = element_of(perm, begin, count, base + eslot, lane_used, valid);
+    int e1 = element_of(perm, begin, count, base + stride + eslot, lane_used, valid1);
+    int nodes[NPE], nodes1[NPE];
+#pragma unroll
+    for (int k = 0; k < NPE; k++) {
+        nodes[k] = valid ? __ldg(m.conn + (size_t)e * m.stride + k) : 0;
+        nodes1[k] = valid1 ? __ldg(m.conn + (size_t)e1 * m.stride + k) : 0;
+    }
+    int e2 = element_of(perm, begin, count, base + 2 * stride + eslot, lane_used, valid2);
+    double xe[NPE], ye[NPE], Ee = 0.0, nue = 0.0;
+    auto load_element = [&]() {
+        bool bad = false;
+#pragma unroll
+        for (int k = 0; k < NPE; k++) bad |= (nodes[k] < 0) | (nodes[k] >= m.N);
+        if (valid && bad) {
+            if (sub == 0) raise_status(L.info, FEM_ERR_BAD_MESH);
+            valid = false;
+        }
+#pragma unroll
+        for (int k = 0; k < NPE; k++) {
+            xe[k] = valid ? __ldg(m.x + nodes[k]) : 0.0;
+            ye[k] = valid ? __ldg(m.y + nodes[k]) : 0.0;
+        }
+        Ee = !valid ? 0.0 : (m.E ? __ldg(m.E + e) : m.E0);
+        nue = !valid ? 0.0 : (m.nu ? __ldg(m.nu + e) : m.nu0);
+    };
+    load_element();
+
+    for (; base < count; base += stride) {
+        int row = nodes[0], col = nodes[0];
+#pragma unroll
+        for (int k = 1; k < NPE; k++) {
+            row = a == k ? nodes[k] : row;
+            col = b == k ? nodes[k] : col;
+        }
+        int4 view[4] = {make_int4(0, 0, 0, 0), make_int4(0, 0, 0, 0), make_int4(0, 0, 0, 0), make_int4(0, 0, 0, 0)};
+        if (valid) {
+            const int* meta = chunk_meta(L, row);
+#pragma unroll
+            for (int q = 0; q < 4; q++) view[q] = ld_cg4(meta + 4 * q);
+        }
+        double kv[4] = {0.0, 0.0, 0.0, 0.0};
+        int state = kSkip;
+        unsigned gid = 0;
+        if (valid) {
+            const double det = ke_block_2d<NPE>(xe, ye, Ee, nue, m.t, a, b, kv);
+            if (sub == 0 && !(det > 0.0)) raise_status(L.info, FEM_ERR_DETJ);
+            state = resolve_2d(L, row, col + 1, view, spare, gid);
+        }
+        // claims of each (element, row) group: one counter atomic per group
+        const unsigned claimed = __ballot_sync(kFull, state == kClaimed);
+        if (valid && b == 0 && (claimed & row_group)) atomicAdd(L.counts + row, __popc(claimed & row_group));
+        // every block (claimed or found) is added to its zero-initialised slot
+        // with red.add, four consecutive lanes per block
+        s_gid[warp][lane] = state != kSkip ? gid : 0xFFFFFFFFu;
+        s_val[warp][lane][0] = kv[0];
+        s_val[warp][lane][1] = kv[1];
+        s_val[warp][lane][2] = kv[2];
+        s_val[warp][lane][3] = kv[3];
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int src = 8 * r + (lane >> 2), v = lane & 3;
+            const unsigned g = s_gid[warp][src];
+            if (g != 0xFFFFFFFFu) atomicAdd(L.vals + (size_t)g * 4 + v, s_val[warp][src][v]);
+        }
+        __syncwarp();
+        // advance the pipeline
+        e = e1;
+        valid = valid1;
+#pragma unroll
+        for (int k = 0; k < NPE; k++) nodes[k] = nodes1[k];
+        e1 = e2;
+        valid1 = valid2;
+#pragma unroll
+        for (int k = 0; k < NPE; k++) nodes1[k] = valid1 ? __ldg(m.conn + (size_t)e1 * m.stride + k) : 0;
+        e2 = element_of(perm, begin, count, base + 3 * stride + eslot, lane_used, valid2);
+        load_element();
     }
 }
 
@@ -191,13 +223,25 @@ __global__ void __launch_bounds__(256, NPE == 3 ? 3 : 2) k_scatter_2d(MeshView m
 
 cudaError_t launch_scatter_2d(const MeshView& m, const ListLayout& L, int npe, const int* perm, const int* range,
                               cudaStream_t s) {
-    const int threads = 256;
-    const long long want = ((long long)m.E_count * npe + threads - 1) / threads;
-    const int grid = (int)std::min<long long>(want > 0 ? want : 1, (long long)sm_count() * 8);
+    // A persistent grid: every warp runs the pipeline over many elements.
+    static int resident[2] = {0, 0};
+    const int t = npe == 4 ? 0 : 1;
+    if (!resident[t]) {
+        int per_sm = 0;
+        cudaError_t err = npe == 4
+                              ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scatter_2d<4>, kThreads2D, 0)
+                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scatter_2d<3>, kThreads2D, 0);
+        if (err) return err;
+        resident[t] = std::max(per_sm, 1) * sm_count();
+    }
+    const int epw = npe == 4 ? 2 : 3;
+    const long long warps = ((long long)m.E_count + epw - 1) / epw;
+    const long long want = (warps + kWarps2D - 1) / kWarps2D;
+    const int grid = (int)std::min<long long>(want > 0 ? want : 1, (long long)resident[t]);
     if (npe == 4)
-        k_scatter_2d<4><<<grid, threads, 0, s>>>(m, L, perm, range);
+        k_scatter_2d<4><<<grid, kThreads2D, 0, s>>>(m, L, perm, range);
     else
-        k_scatter_2d<3><<<grid, threads, 0, s>>>(m, L, perm, range);
+        k_scatter_2d<3><<<grid, kThreads2D, 0, s>>>(m, L, perm, range);
     return cudaGetLastError();
 }
 
