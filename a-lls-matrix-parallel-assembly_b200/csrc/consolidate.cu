@@ -23,12 +23,12 @@
 #include <algorithm>
 
 #include "launch.h"
+#include "scan.cuh"
 
 namespace fem {
 namespace {
 
 constexpr unsigned long long kEmptyKey = ~0ull;
-constexpr int kScanThreads = 256;
 constexpr int kScanItems = kScanTile / kScanThreads;  // 16 nodes per thread
 
 __device__ __forceinline__ unsigned long long shfl_xor_u64(unsigned long long v, int m) {
@@ -36,35 +36,6 @@ __device__ __forceinline__ unsigned long long shfl_xor_u64(unsigned long long v,
     lo = __shfl_xor_sync(0xFFFFFFFFu, lo, m);
     hi = __shfl_xor_sync(0xFFFFFFFFu, hi, m);
     return ((unsigned long long)hi << 32) | lo;
-}
-
-// Block-wide exclusive scan of one long long per thread (kScanThreads threads).
-__device__ __forceinline__ long long block_exclusive_scan(long long v, long long* s_warp, long long& total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    long long inc = v;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const long long o = __shfl_up_sync(0xFFFFFFFFu, inc, d);
-        if (lane >= d) inc += o;
-    }
-    if (lane == 31) s_warp[warp] = inc;
-    __syncthreads();
-    if (warp == 0) {
-        long long w = lane < kScanThreads / 32 ? s_warp[lane] : 0;
-        long long wi = w;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const long long o = __shfl_up_sync(0xFFFFFFFFu, wi, d);
-            if (lane >= d) wi += o;
-        }
-        if (lane < kScanThreads / 32) s_warp[lane] = wi - w;
-        if (lane == kScanThreads / 32 - 1) s_warp[kScanThreads / 32] = wi;
-    }
-    __syncthreads();
-    total = s_warp[kScanThreads / 32];
-    const long long out = s_warp[warp] + inc - v;
-    __syncthreads();  // s_warp may be reused by the caller's next scan
-    return out;
 }
 
 // Tile sums of dpn^2 * counts.

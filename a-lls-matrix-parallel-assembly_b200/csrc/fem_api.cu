@@ -274,6 +274,119 @@ fem_status fem_assemble(const fem_mesh* mesh, const fem_opts* opts, void* worksp
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Element-colouring baseline
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct ColourHostLayout {
+    size_t off_info, off_cnt, off_off, off_inc, off_colour, off_perm, off_hist, off_ranges, off_tiles, total;
+};
+
+ColourHostLayout colour_layout(const fem_mesh* m) {
+    ColourHostLayout h{};
+    const size_t N = (size_t)m->num_nodes, E = (size_t)m->num_elems;
+    const size_t tiles = (N + kScanTile - 1) / kScanTile;
+    size_t off = 0;
+    h.off_info = off;
+    off += align_up(sizeof(ColourInfo));
+    h.off_cnt = off;
+    off += align_up(N * sizeof(int));
+    h.off_off = off;
+    off += align_up((N + 1) * sizeof(int));
+    h.off_inc = off;
+    off += align_up(E * (size_t)m->conn_stride * sizeof(int));
+    h.off_colour = off;
+    off += align_up(E * sizeof(int));
+    h.off_perm = off;
+    off += align_up(E * sizeof(int));
+    h.off_hist = off;
+    off += align_up(2 * kMaxColours * sizeof(int));
+    h.off_ranges = off;
+    off += align_up((2 * kMaxColours + 1) * sizeof(int));
+    h.off_tiles = off;
+    off += align_up(tiles * sizeof(long long));
+    h.total = off;
+    return h;
+}
+
+ColourLayout colour_device_layout(const ColourHostLayout& h, const void* ws) {
+    unsigned char* b = static_cast<unsigned char*>(const_cast<void*>(ws));
+    ColourLayout C;
+    C.info = reinterpret_cast<ColourInfo*>(b + h.off_info);
+    C.cnt = reinterpret_cast<int*>(b + h.off_cnt);
+    C.off = reinterpret_cast<int*>(b + h.off_off);
+    C.inc = reinterpret_cast<int*>(b + h.off_inc);
+    C.colour = reinterpret_cast<int*>(b + h.off_colour);
+    C.perm = reinterpret_cast<int*>(b + h.off_perm);
+    C.hist = reinterpret_cast<int*>(b + h.off_hist);
+    C.ranges = reinterpret_cast<int*>(b + h.off_ranges);
+    C.tiles = reinterpret_cast<long long*>(b + h.off_tiles);
+    return C;
+}
+
+}  // namespace
+
+extern "C" {
+
+fem_status fem_colour_workspace_size(const fem_mesh* mesh, size_t* bytes) {
+    if (!bytes) return FEM_ERR_BAD_ARG;
+    fem_status st = check_mesh(mesh);
+    if (st) return st;
+    *bytes = colour_layout(mesh).total;
+    return FEM_OK;
+}
+
+fem_status fem_colour_prepare(const fem_mesh* mesh, void* workspace, size_t workspace_bytes, int32_t* num_colours,
+                              int32_t* colour_of_element, void* stream) {
+    fem_status st = check_mesh(mesh);
+    if (st) return st;
+    const ColourHostLayout h = colour_layout(mesh);
+    if (!workspace || workspace_bytes < h.total || reinterpret_cast<uintptr_t>(workspace) % kAlign || !num_colours)
+        return !num_colours ? FEM_ERR_BAD_ARG : FEM_ERR_WORKSPACE;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const ColourLayout C = colour_device_layout(h, workspace);
+    int nc = 0, bits = 0;
+    cudaError_t err = launch_colour_prepare(mesh_view(mesh), C, sm_count(), s, &nc, &bits);
+    if (!err && colour_of_element && mesh->num_elems > 0)
+        err = launch_colour_export(C, mesh->num_elems, colour_of_element, sm_count(), s);
+    if (!err && colour_of_element) err = cudaStreamSynchronize(s);
+    if (err) return cuda_fail(err);
+    *num_colours = nc;
+    return decode_bits(bits);
+}
+
+fem_status fem_colour_assemble(const fem_mesh* mesh, const void* workspace, size_t workspace_bytes,
+                               int32_t num_colours, const int32_t* row_ptr, const int32_t* col_idx, double* values,
+                               int64_t nnz, void* stream) {
+    fem_status st = check_mesh(mesh);
+    if (st) return st;
+    if (mesh->kind == FEM_HEX20) return FEM_ERR_BAD_ARG;  // 2-D element kinds only
+    const ColourHostLayout h = colour_layout(mesh);
+    if (!workspace || workspace_bytes < h.total || reinterpret_cast<uintptr_t>(workspace) % kAlign)
+        return FEM_ERR_WORKSPACE;
+    if (num_colours < 0 || num_colours > kMaxColours || nnz < 0 || !row_ptr || (nnz > 0 && (!col_idx || !values)))
+        return FEM_ERR_BAD_ARG;
+    if (mesh->num_elems == 0 || nnz == 0) return FEM_OK;
+    cudaError_t err = launch_colour_assemble(mesh_view(mesh), colour_device_layout(h, workspace), num_colours, row_ptr,
+                                             col_idx, values, nnz, sm_count(), static_cast<cudaStream_t>(stream));
+    return err ? cuda_fail(err) : FEM_OK;
+}
+
+fem_status fem_colour_read_info(const void* workspace, int32_t* num_colours, void* stream) {
+    if (!workspace) return FEM_ERR_BAD_ARG;
+    ColourInfo h{};
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t err = cudaMemcpyAsync(&h, workspace, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (!err) err = cudaStreamSynchronize(s);
+    if (err) return cuda_fail(err);
+    if (num_colours) *num_colours = h.num_colours;
+    return decode_bits(h.status_bits);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
 // Host-buffer entry point
 // ---------------------------------------------------------------------------
 

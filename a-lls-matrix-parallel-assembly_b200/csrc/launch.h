@@ -41,5 +41,39 @@ cudaError_t launch_consolidate(const ListLayout& L, int dpn, int* row_ptr, int* 
                                long long capacity, long long* tile_sums, int num_tiles, cudaStream_t s);
 cudaError_t launch_info_init(DevInfo* info, int pool_chunks, cudaStream_t s);
 
+// ---- element-colouring baseline (colour.cu) ----
+constexpr int kMaxColours = 64;         // colours per mesh (a 64-bit mask of neighbour colours)
+constexpr int kMaxColourRounds = 4096;  // bound on Jones-Plassmann rounds
+
+struct ColourInfo {
+    int num_colours;
+    int status_bits;  // 1 << FEM_ERR_*
+    int uncoloured;   // elements left after the last round
+    int pad[13];
+};
+static_assert(sizeof(ColourInfo) == 64, "ColourInfo size");
+
+// Device buffers of the colouring path (inside the caller's workspace).
+struct ColourLayout {
+    ColourInfo* info;
+    int* cnt;        // [N] incidence counts, then fill cursors
+    int* off;        // [N + 1] node -> element offsets
+    int* inc;        // [sum of nodes per element] incidence lists
+    int* colour;     // [E] round << 8 | colour, -1 = uncoloured
+    int* perm;       // [E] elements grouped by (colour, type)
+    int* hist;       // [2 * kMaxColours] counts, then cursors
+    int* ranges;     // [2 * kMaxColours + 1] offsets of each (colour, type) group in perm
+    long long* tiles;  // [ceil(N / kScanTile)] scan partials
+};
+
+// Incidence, colouring rounds (host loop, one sync per round) and grouping.
+cudaError_t launch_colour_prepare(const MeshView& m, const ColourLayout& C, int sms, cudaStream_t s, int* num_colours,
+                                  int* status_bits);
+// out[e] = colour of element e.
+cudaError_t launch_colour_export(const ColourLayout& C, int E, int* out, int sms, cudaStream_t s);
+// values = 0, then one launch per (colour, type) group. Asynchronous.
+cudaError_t launch_colour_assemble(const MeshView& m, const ColourLayout& C, int num_colours, const int* row_ptr,
+                                   const int* col_idx, double* values, long long nnz, int sms, cudaStream_t s);
+
 
 }  // namespace fem

@@ -34,7 +34,8 @@ globals().update({v: k for k, v in STATUS_NAMES.items()})
 EXPORTS = ["fem_alls_workspace_size", "fem_alls_scatter", "fem_alls_consolidate", "fem_alls_read_info",
            "fem_assemble", "fem_assemble_async", "fem_context_create", "fem_context_destroy",
            "fem_assemble_host", "fem_status_string", "fem_last_cuda_error", "fem_abi_version",
-           "fem_assemble_static"]
+           "fem_assemble_static", "fem_colour_workspace_size", "fem_colour_prepare", "fem_colour_assemble",
+           "fem_colour_read_info"]
 STATIC_WORKSPACE_BYTES = 32 << 20  # FEM_STATIC_WORKSPACE_BYTES
 
 
@@ -95,6 +96,10 @@ def load() -> C.CDLL:
         L.fem_context_destroy.argtypes = [vp]
         L.fem_context_destroy.restype = None
         L.fem_assemble_host.argtypes = [vp, p(FemMesh), p(FemOpts), p(FemCsr), vp]
+        L.fem_colour_workspace_size.argtypes = [p(FemMesh), p(C.c_size_t)]
+        L.fem_colour_prepare.argtypes = [p(FemMesh), vp, C.c_size_t, p(C.c_int32), vp, vp]
+        L.fem_colour_assemble.argtypes = [p(FemMesh), vp, C.c_size_t, C.c_int32, vp, vp, vp, C.c_int64, vp]
+        L.fem_colour_read_info.argtypes = [vp, p(C.c_int32), vp]
         L.fem_status_string.argtypes = [C.c_int32]
         L.fem_status_string.restype = C.c_char_p
         for f in EXPORTS:
@@ -263,3 +268,46 @@ class HostContext:
         out = FemCsr(mesh.num_dofs, 0, 0, cap, _ptr(row_ptr), _ptr(col_idx), _ptr(values))
         st = self.lib.fem_assemble_host(self.ctx, C.byref(m), C.byref(o) if o else None, C.byref(out), stream)
         return st, int(out.nnz)
+
+
+class Colouring:
+    """The element-colouring baseline through the C ABI (fem_colour_*): device
+    colouring of the elements, then one launch per colour adding element blocks
+    into a given CSR pattern without atomics (the reference's coloured path,
+    ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:504-572,648-747, rebuilt)."""
+
+    def __init__(self, mesh, device="cuda", dev_arrays=None):
+        import torch
+        self.torch = torch
+        self.mesh = mesh
+        self.dev = dev_arrays if dev_arrays is not None else device_arrays(mesh, device)
+        self.cm = fem_mesh_struct(mesh, self.dev)
+        self.lib = load()
+        n = C.c_size_t(0)
+        check(self.lib.fem_colour_workspace_size(C.byref(self.cm), C.byref(n)), "fem_colour_workspace_size")
+        self.ws_bytes = n.value
+        self.ws = torch.empty(self.ws_bytes + 256, dtype=torch.uint8, device=device)
+        self.ws_ptr = (self.ws.data_ptr() + 255) // 256 * 256
+        self.colours = torch.empty(max(mesh.num_elems, 1), dtype=torch.int32, device=device)
+        self.num_colours = 0
+
+    def _stream(self):
+        return self.torch.cuda.current_stream().cuda_stream
+
+    def prepare(self, allow=(FEM_OK,)) -> int:
+        nc = C.c_int32(0)
+        st = self.lib.fem_colour_prepare(C.byref(self.cm), self.ws_ptr, self.ws_bytes, C.byref(nc),
+                                         _ptr(self.colours), self._stream())
+        check(st, "fem_colour_prepare", allow)
+        self.num_colours = nc.value
+        return self.num_colours
+
+    def assemble(self, row_ptr, col_idx, values, nnz: int, allow=(FEM_OK,)):
+        check(self.lib.fem_colour_assemble(C.byref(self.cm), self.ws_ptr, self.ws_bytes, self.num_colours,
+                                           _ptr(row_ptr), _ptr(col_idx), _ptr(values), nnz, self._stream()),
+              "fem_colour_assemble", allow)
+
+    def read_info(self) -> tuple:
+        nc = C.c_int32(0)
+        st = self.lib.fem_colour_read_info(self.ws_ptr, C.byref(nc), self._stream())
+        return st, nc.value

@@ -160,6 +160,42 @@ FEM_API fem_status fem_assemble(const fem_mesh* mesh, const fem_opts* opts, void
 FEM_API fem_status fem_assemble_async(const fem_mesh* mesh, const fem_opts* opts, void* workspace,
                               size_t workspace_bytes, fem_csr* out, void* stream);
 
+/* ---- element-colouring baseline ----------------------------------------------
+ * The comparison baseline of the A-LLS path: elements are coloured so that no
+ * two elements of one colour share a node, then each colour is assembled
+ * without atomics into a given CSR pattern. Replaces the reference's host
+ * colorElements (ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:648-747,
+ * ALLS_T3_Unstructed_Elements_Assemble_Performance.cu:484-523,
+ * ALLS_Q4_T3_Mixed_Elements_Assembly_Performance.cu:514-553) and its coloured
+ * kernels (assembleGlobalStiffnessKernelColoredNoAtomic, Q4A:504-572;
+ * assembleGlobalStiffnessKernelColored, T3:316-363, MIX:341-390), whose
+ * colours all run at once and so race. */
+
+/* Bytes of device workspace the colouring path needs for this mesh. */
+FEM_API fem_status fem_colour_workspace_size(const fem_mesh* mesh, size_t* bytes);
+
+/* Colours the elements on the device (Jones-Plassmann rounds, each element
+ * taking the smallest colour none of its node-sharing neighbours has; at most
+ * 64 colours, else FEM_ERR_RANGE) and groups them by colour in the workspace.
+ * colour_of_element: optional device int32 [num_elems] that receives each
+ * element's colour. Synchronous (one host sync per colouring round). */
+FEM_API fem_status fem_colour_prepare(const fem_mesh* mesh, void* workspace, size_t workspace_bytes,
+                                      int32_t* num_colours, int32_t* colour_of_element, void* stream);
+
+/* Assembles the FP64 values of a 2-D mesh (Q4, T3, mixed) into the CSR pattern
+ * row_ptr / col_idx (as fem_assemble returns it; nnz entries) after
+ * fem_colour_prepare on the same workspace: values are zeroed, then one launch
+ * per colour adds every element block at its binary-searched position with
+ * plain loads and stores. Asynchronous; fem_colour_read_info reports a block
+ * missing from the pattern (FEM_ERR_INTERNAL) or a non-positive detJ. */
+FEM_API fem_status fem_colour_assemble(const fem_mesh* mesh, const void* workspace, size_t workspace_bytes,
+                                       int32_t num_colours, const int32_t* row_ptr, const int32_t* col_idx,
+                                       double* values, int64_t nnz, void* stream);
+
+/* Number of colours and the most severe status of the colouring workspace
+ * (synchronizes the stream). */
+FEM_API fem_status fem_colour_read_info(const void* workspace, int32_t* num_colours, void* stream);
+
 /* ---- host-buffer entry point ------------------------------------------------ */
 
 typedef struct fem_context fem_context;
