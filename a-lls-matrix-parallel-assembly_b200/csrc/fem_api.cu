@@ -274,6 +274,36 @@ fem_status fem_assemble(const fem_mesh* mesh, const fem_opts* opts, void* worksp
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Element stiffness on its own
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+fem_status fem_element_stiffness_size(const fem_mesh* mesh, int64_t* doubles_per_element) {
+    fem_status st = check_mesh(mesh);
+    if (st) return st;
+    if (!doubles_per_element) return FEM_ERR_BAD_ARG;
+    *doubles_per_element = mesh->kind == FEM_HEX20 ? kPackedHex20
+                           : mesh->kind == FEM_T3  ? kPacked2D_T3
+                                                   : kPacked2D_Q4;
+    return FEM_OK;
+}
+
+fem_status fem_element_stiffness(const fem_mesh* mesh, const fem_opts* opts, double* ke_out, int32_t* status,
+                                 void* stream) {
+    fem_status st = check_mesh(mesh);
+    if (st) return st;
+    if (!status || (mesh->num_elems > 0 && !ke_out)) return FEM_ERR_BAD_ARG;
+    if (opts && opts->precision != FEM_PREC_FP64) return FEM_ERR_BAD_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t err = cudaMemsetAsync(status, 0, sizeof(int32_t), s);
+    if (!err) err = launch_element_stiffness(mesh_view(mesh), mesh->kind, ke_out, status, s);
+    return err ? cuda_fail(err) : FEM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
 // Element-colouring baseline
 // ---------------------------------------------------------------------------
 

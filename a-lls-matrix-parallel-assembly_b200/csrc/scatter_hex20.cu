@@ -17,10 +17,11 @@
 // which is algebraically the reference's per-Gauss-point block formula
 // (H20:173-191, c1 = lambda + 2 mu, c2 = lambda, c3 = mu). M is one symmetric
 // 64x64x28 FP64 matrix product per element, computed on the FP64 tensor cores
-// with mma.sync.m8n8k4.f64 (36 upper 8x8 tiles x 7 k-steps); only its 210 upper
-// 3x3 node blocks are kept (so every Ke is exactly symmetric), in the shared
-// memory the gradients occupied. Ke blocks are formed from M per scattered row. The
-// Gauss-point shape derivatives (H20:95-128) are tabulated once per CTA.
+// with mma.sync.m8n8k4.f64 (36 upper 8x8 tiles x 7 k-steps); each upper entry
+// is written to both of its places in M (so every Ke is exactly symmetric), in
+// the shared memory the gradients occupied. Ke blocks are formed from M per
+// scattered row. The Gauss-point shape derivatives (H20:95-128) are tabulated
+// once per CTA.
 //
 // Scatter. Warp w serves row nodes w and w+10. It prefetches both rows' chunk
 // rows (384 bytes: next pointer + 94 hashed slots) into shared memory with one
@@ -29,10 +30,12 @@
 // claims the first empty slot on column node j's probe sequence with atomicCAS
 // (empty -> col|pending) if the column is absent — re-trying past slots another
 // warp has just taken — and follows / atomicCAS-links overflow chunks when the
-// probe sequence is full. Claimed blocks of both rows are stored, the warp
-// fences once and publishes them; found blocks are accumulated with coalesced
-// atomicAdds (after a bounded wait for slots another warp is still writing).
-// The next element's nodes and coordinates are prefetched during the scatter.
+// probe sequence is full. Each row's 20 blocks are staged once and written in
+// one coalesced pass: plain stores into the slots the warp claimed, FP64
+// atomicAdds into published ones. The warp then fences once and publishes its
+// claims of both rows; blocks whose slot another warp was still writing are
+// added after a bounded wait. The next element's nodes and coordinates are
+// prefetched during the compute and the scatter.
 #include "launch.h"
 
 namespace fem {
@@ -42,6 +45,7 @@ constexpr int kThreads = 320;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxHex20Words = 96;   // chunk meta rows of at most 96 words (S <= 94, checked on the host)
 constexpr int PS = 28;               // row stride of P (doubles): conflict-free m8n8k4 fragment loads
+constexpr int MP = 61;               // row stride of M (doubles, odd: few bank conflicts on block reads)
 constexpr int kHash = 64;            // element-node hash slots
 
 // Natural coordinates of the 20 nodes in the reference order (H20:97-99).
@@ -87,7 +91,7 @@ struct Hex20Smem {
     double dN[27][3][20];      // shape derivatives at the Gauss points
     union {
         double P[64][PS];      // P[3n+a][g] = G_g[n][a]; rows 60..63 and column 27 zeroed per element
-        double Mb[210][9];     // upper 3x3 node blocks of the node-pair matrix: Mb[pair(I,J)][3a+b]
+        double M[60][MP];      // the node-pair matrix M = P diag(w) P^T (exactly symmetric)
     };
     double X[20][3];           // element node coordinates
     double J[27][9];           // Jacobians, then their inverses
@@ -139,16 +143,11 @@ __device__ __forceinline__ int first_empty_from(const unsigned (&bm)[4], int nw,
 
 // Block Ke_IJ into out[0..9) (row-major 3x3):
 //   Ke_IJ[a][b] = lambda M[3I+a][3J+b] + mu M[3I+b][3J+a] + mu delta_ab tr(M_IJ)
-__device__ __forceinline__ int pair_index(int I, int J) { return I * 20 - I * (I - 1) / 2 + (J - I); }
-
 __device__ __forceinline__ void ke_block(const Hex20Smem& sm, int I, int J, double* out) {
-    // M is symmetric: block (I, J) with I > J is the transpose of block (J, I).
-    const bool t = I > J;
-    const double* m0 = sm.Mb[t ? pair_index(J, I) : pair_index(I, J)];
-    const double m00 = m0[0], m11 = m0[4], m22 = m0[8];
-    const double m01 = t ? m0[3] : m0[1], m02 = t ? m0[6] : m0[2];
-    const double m10 = t ? m0[1] : m0[3], m12 = t ? m0[7] : m0[5];
-    const double m20 = t ? m0[2] : m0[6], m21 = t ? m0[5] : m0[7];
+    const double* r0 = &sm.M[3 * I][3 * J];
+    const double m00 = r0[0], m01 = r0[1], m02 = r0[2];
+    const double m10 = r0[MP], m11 = r0[MP + 1], m12 = r0[MP + 2];
+    const double m20 = r0[2 * MP], m21 = r0[2 * MP + 1], m22 = r0[2 * MP + 2];
     const double lam = sm.lam, mu = sm.mu, mtr = mu * (m00 + m11 + m22);
     out[0] = fma(lam, m00, fma(mu, m00, mtr));
     out[1] = fma(lam, m01, mu * m10);
@@ -242,29 +241,31 @@ __device__ __forceinline__ void resolve_row(const ListLayout& L, const Hex20Smem
     }
 }
 
-// Stages row I's 20 Ke blocks (lane j: column node j) with their states.
-__device__ __forceinline__ void stage_row(Hex20Smem& sm, int I, int warp, int lane, int state, unsigned gid) {
+// Stages row I's 20 Ke blocks (lane j: column node j) with their states, then
+// writes them in one pass: lane l handles entries l, l+32, ... of the 20 x 9
+// values, so consecutive lanes write consecutive doubles of the same 72-byte
+// slot block. Claimed slots (ours, not yet published) take plain stores,
+// published ones FP64 red.add; pending ones are left for later.
+__device__ __forceinline__ void write_row(const ListLayout& L, Hex20Smem& sm, int I, int warp, int lane, int state,
+                                          unsigned gid) {
     if (lane < 20) {
         sm.state[warp][lane] = state;
         sm.gid[warp][lane] = gid;
         ke_block(sm, I, lane, &sm.stage[warp][lane * 9]);
     }
     __syncwarp();
-}
-
-// Writes the staged blocks whose state is `which`: lane l handles entries
-// l, l+32, ... of the 20 x 9 values, so consecutive lanes write consecutive
-// doubles of the same 72-byte slot block (coalesced stores / atomics).
-template <bool kAtomic>
-__device__ __forceinline__ void write_staged(const ListLayout& L, const Hex20Smem& sm, int warp, int lane, int which) {
-    for (int idx = lane; idx < 20 * 9; idx += 32) {
-        const int j = idx / 9;
-        if (sm.state[warp][j] != which) continue;
-        double* p = L.vals + (size_t)sm.gid[warp][j] * 9 + (idx - 9 * j);
-        if (kAtomic)
-            atomicAdd(p, sm.stage[warp][idx]);
-        else
-            *p = sm.stage[warp][idx];
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        const int idx = lane + 32 * k;
+        if (idx < 20 * 9) {
+            const int j = (idx * 57) >> 9;  // idx / 9 for idx < 180
+            const int st = sm.state[warp][j];
+            double* p = L.vals + (size_t)sm.gid[warp][j] * 9 + (idx - 9 * j);
+            if (st == kClaimed)
+                *p = sm.stage[warp][idx];
+            else if (st == kFound)
+                atomicAdd(p, sm.stage[warp][idx]);
+        }
     }
     __syncwarp();
 }
@@ -277,21 +278,18 @@ __device__ __forceinline__ void publish(const ListLayout& L, unsigned gid, int k
     __stcg(chunk_meta(L, cc) + 2 + s, key);
 }
 
-// Found (published) blocks of row I: atomicAdd. Pending blocks: wait, then add.
-__device__ __forceinline__ void add_found(const ListLayout& L, Hex20Smem& sm, int I, int warp, int lane, int state,
-                                          unsigned gid) {
-    stage_row(sm, I, warp, lane, state, gid);
-    write_staged<true>(L, sm, warp, lane, kFound);
-    if (state == kFoundPending) {
-        int cc, s;
-        gid_chunk(L, gid, cc, s);
-        if (wait_published(L, chunk_meta(L, cc) + 2 + s)) {
-            double* p = L.vals + (size_t)gid * 9;
+// A block whose slot another warp had claimed but not yet published: wait
+// (bounded), then add it.
+__device__ __forceinline__ void add_pending(const ListLayout& L, const Hex20Smem& sm, int I, int lane, unsigned gid) {
+    int cc, s;
+    gid_chunk(L, gid, cc, s);
+    if (wait_published(L, chunk_meta(L, cc) + 2 + s)) {
+        double v[9];
+        ke_block(sm, I, lane, v);
+        double* p = L.vals + (size_t)gid * 9;
 #pragma unroll
-            for (int v = 0; v < 9; v++) atomicAdd(p + v, sm.stage[warp][lane * 9 + v]);
-        }
+        for (int k = 0; k < 9; k++) atomicAdd(p + k, v[k]);
     }
-    __syncwarp();
 }
 
 // Scatter of row nodes I0 and I1 (I1 < 0: none) by one warp.
@@ -305,29 +303,24 @@ __device__ __forceinline__ void scatter_rows(const ListLayout& L, Hex20Smem& sm,
     unsigned g0, g1 = 0;
     resolve_row(L, sm, I0, lane, sm.view[warp][0], sm.state[warp], sm.gid[warp], spare, st0, g0);
     if (I1 >= 0) resolve_row(L, sm, I1, lane, sm.view[warp][1], sm.state[warp], sm.gid[warp], spare, st1, g1);
-    // claimed blocks of both rows: store, one fence, publish (the slots stay
-    // pending only for the stores of this warp)
     const unsigned c0 = __ballot_sync(kFull, st0 == kClaimed), c1 = __ballot_sync(kFull, st1 == kClaimed);
     if (lane == 0) {
         if (c0) atomicAdd(L.counts + sm.nodes[I0], __popc(c0));
         if (c1) atomicAdd(L.counts + sm.nodes[I1], __popc(c1));
     }
+    // claimed blocks stored, found blocks added; one fence, then the claims of
+    // both rows are published (their slots stay pending only this long)
+    write_row(L, sm, I0, warp, lane, st0, g0);
+    if (I1 >= 0) write_row(L, sm, I1, warp, lane, st1, g1);
     if (c0 | c1) {
-        if (c0) {
-            stage_row(sm, I0, warp, lane, st0, g0);
-            write_staged<false>(L, sm, warp, lane, kClaimed);
-        }
-        if (c1) {
-            stage_row(sm, I1, warp, lane, st1, g1);
-            write_staged<false>(L, sm, warp, lane, kClaimed);
-        }
         __threadfence();
         __syncwarp();
         if (st0 == kClaimed) publish(L, g0, key);
         if (st1 == kClaimed) publish(L, g1, key);
     }
-    add_found(L, sm, I0, warp, lane, st0, g0);
-    if (I1 >= 0) add_found(L, sm, I1, warp, lane, st1, g1);
+    if (st0 == kFoundPending) add_pending(L, sm, I0, lane, g0);
+    if (st1 == kFoundPending) add_pending(L, sm, I1, lane, g1);
+    __syncwarp();
 }
 
 __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
@@ -473,7 +466,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
                 }
             }
         }
-        __syncthreads();  // every warp has read P: its storage now takes the M blocks
+        __syncthreads();  // every warp has read P: its storage now takes M
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const int t = warp + q * kWarps;
@@ -485,21 +478,21 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
                     // entry (r, c) stands for itself and, by symmetry, for (c, r);
                     // in a diagonal tile only r <= c writes (its mirror is in the tile)
                     if (r < 60 && c < 60 && (mt < nt || r <= c)) {
-                        const int I = r / 3, a = r - 3 * I, J = c / 3, b = c - 3 * J;
-                        if (I <= J) sm.Mb[pair_index(I, J)][3 * a + b] = acc[q][h];
-                        if (J <= I) sm.Mb[pair_index(J, I)][3 * b + a] = acc[q][h];
+                        sm.M[r][c] = acc[q][h];
+                        sm.M[c][r] = acc[q][h];
                     }
                 }
             }
         }
         __syncthreads();
-        // Scatter: warp w serves row nodes w and w + 10.
-        scatter_rows(L, sm, warp, warp + kWarps < 20 ? warp + kWarps : -1, warp, lane, spare);
+        // next element's coordinates: in flight during the scatter
         if (tid < 20 && i_next < m.E_count && pre_n >= 0 && pre_n < m.N) {
             pre_x = __ldg(m.x + pre_n);
             pre_y = __ldg(m.y + pre_n);
             pre_z = __ldg(m.z + pre_n);
         }
+        // Scatter: warp w serves row nodes w and w + 10.
+        scatter_rows(L, sm, warp, warp + kWarps < 20 ? warp + kWarps : -1, warp, lane, spare);
         __syncthreads();
     }
 }

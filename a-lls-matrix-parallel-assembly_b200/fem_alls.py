@@ -35,7 +35,7 @@ EXPORTS = ["fem_alls_workspace_size", "fem_alls_scatter", "fem_alls_consolidate"
            "fem_assemble", "fem_assemble_async", "fem_context_create", "fem_context_destroy",
            "fem_assemble_host", "fem_status_string", "fem_last_cuda_error", "fem_abi_version",
            "fem_assemble_static", "fem_colour_workspace_size", "fem_colour_prepare", "fem_colour_assemble",
-           "fem_colour_read_info"]
+           "fem_colour_read_info", "fem_element_stiffness_size", "fem_element_stiffness"]
 STATIC_WORKSPACE_BYTES = 32 << 20  # FEM_STATIC_WORKSPACE_BYTES
 
 
@@ -100,6 +100,8 @@ def load() -> C.CDLL:
         L.fem_colour_prepare.argtypes = [p(FemMesh), vp, C.c_size_t, p(C.c_int32), vp, vp]
         L.fem_colour_assemble.argtypes = [p(FemMesh), vp, C.c_size_t, C.c_int32, vp, vp, vp, C.c_int64, vp]
         L.fem_colour_read_info.argtypes = [vp, p(C.c_int32), vp]
+        L.fem_element_stiffness_size.argtypes = [p(FemMesh), p(C.c_int64)]
+        L.fem_element_stiffness.argtypes = [p(FemMesh), p(FemOpts), vp, vp, vp]
         L.fem_status_string.argtypes = [C.c_int32]
         L.fem_status_string.restype = C.c_char_p
         for f in EXPORTS:
@@ -311,3 +313,34 @@ class Colouring:
         nc = C.c_int32(0)
         st = self.lib.fem_colour_read_info(self.ws_ptr, C.byref(nc), self._stream())
         return st, nc.value
+
+
+def element_stiffness(mesh, o: Optional[FemOpts] = None, device="cuda", dev_arrays=None, out=None):
+    """Packed symmetric element stiffness of every element (fem_element_stiffness):
+    returns (ke [num_elems, doubles_per_element] tensor, status bits)."""
+    import torch
+    dev = dev_arrays if dev_arrays is not None else device_arrays(mesh, device)
+    cm = fem_mesh_struct(mesh, dev)
+    lib = load()
+    n = C.c_int64(0)
+    check(lib.fem_element_stiffness_size(C.byref(cm), C.byref(n)), "fem_element_stiffness_size")
+    if out is None:
+        out = torch.empty((max(mesh.num_elems, 1), n.value), dtype=torch.float64, device=device)
+    status = torch.zeros(1, dtype=torch.int32, device=device)
+    check(lib.fem_element_stiffness(C.byref(cm), C.byref(o) if o else None, _ptr(out), _ptr(status),
+                                    torch.cuda.current_stream().cuda_stream), "fem_element_stiffness")
+    return out[: mesh.num_elems], int(status.item())
+
+
+def unpack_element_stiffness(packed: np.ndarray, npe: int, dpn: int) -> np.ndarray:
+    """Full ndof x ndof Ke of one element from its packed upper node blocks."""
+    nd = npe * dpn
+    ke = np.zeros((nd, nd))
+    k = 0
+    for a in range(npe):
+        for b in range(a, npe):
+            blk = packed[k * dpn * dpn:(k + 1) * dpn * dpn].reshape(dpn, dpn)
+            ke[a * dpn:(a + 1) * dpn, b * dpn:(b + 1) * dpn] = blk
+            ke[b * dpn:(b + 1) * dpn, a * dpn:(a + 1) * dpn] = blk.T
+            k += 1
+    return ke

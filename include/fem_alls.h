@@ -160,6 +160,30 @@ FEM_API fem_status fem_assemble(const fem_mesh* mesh, const fem_opts* opts, void
 FEM_API fem_status fem_assemble_async(const fem_mesh* mesh, const fem_opts* opts, void* workspace,
                               size_t workspace_bytes, fem_csr* out, void* stream);
 
+/* ---- element stiffness on its own -------------------------------------------
+ * Replaces the reference's device element functions computeElementStiffness
+ * (ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:178-212,
+ * ALLS_T3_Unstructed_Elements_Assemble_Performance.cu:136-206,
+ * ALLS_Q4_T3_Mixed_Elements_Assembly_Performance.cu:145-227) and
+ * computeElementStiffnessHex20 (ALLS_Hex20_3D_Assembly_Performance.cu:130-195)
+ * as a batched call over a whole mesh (the reference calls them inside its
+ * assembly kernels only). Output, per element in natural order, the packed
+ * symmetric form: the upper node blocks (a <= b, row-major over the pairs),
+ * each dof_per_node^2 entries row-major, entry (i, j) of block (a, b) being
+ * Ke[a*dpn + i][b*dpn + j] in the element's node order. Doubles per element:
+ * Q4 40 (10 blocks), T3 24 (6), mixed 40 (a T3's last 4 blocks are zero),
+ * Hex20 1890 (210 blocks). */
+
+/* Doubles per element of fem_element_stiffness's output for this mesh. */
+FEM_API fem_status fem_element_stiffness_size(const fem_mesh* mesh, int64_t* doubles_per_element);
+
+/* ke_out: device [num_elems * doubles_per_element]. status: a device int32
+ * that is zeroed and then receives (1 << FEM_ERR_*) bits (BAD_MESH: the
+ * element's output is zero; DETJ). Asynchronous. opts->precision must be
+ * FEM_PREC_FP64. */
+FEM_API fem_status fem_element_stiffness(const fem_mesh* mesh, const fem_opts* opts, double* ke_out,
+                                         int32_t* status, void* stream);
+
 /* ---- element-colouring baseline ----------------------------------------------
  * The comparison baseline of the A-LLS path: elements are coloured so that no
  * two elements of one colour share a node, then each colour is assembled
