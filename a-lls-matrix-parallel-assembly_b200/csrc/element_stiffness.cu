@@ -11,8 +11,8 @@
 //
 // 2-D (k_ke_2d): one lane per node block, as the A-LLS scatter computes it.
 //
-// Hex20 (k_hex20_ke): one CTA (10 warps) per element at a time, persistent:
-//   Jacobians at the 27 Gauss points (243 threads), their inverses and
+// Hex20 (k_hex20_ke): one CTA (4 warps) per element at a time, persistent:
+//   Jacobians at the 27 Gauss points (243 entries), their inverses and
 //   w_g = weight * detJ_g (27 threads; a non-positive detJ raises
 //   FEM_ERR_DETJ), physical gradients P[3n+a][g] (540 items), then
 //   M = P diag(w) P^T on the FP64 tensor cores with mma.sync.m8n8k4.f64
@@ -20,7 +20,9 @@
 //   entry of M is written to its upper 3x3 node block (so Ke is exactly
 //   symmetric), and the 210 Ke blocks
 //       Ke_IJ[a][b] = lambda M_IJ[a][b] + mu M_IJ[b][a] + mu delta_ab tr(M_IJ)
-//   are written with coalesced stores. The Gauss-point shape derivatives
+//   are written with coalesced stores. With FEM_PREC_TC_F16X3 the contraction
+//   runs on the FP16 tensor cores instead (split operands, FP32 accumulation;
+//   tc_prepare / tc_contract in hex20.cuh). The Gauss-point shape derivatives
 //   (H20:95-128) are tabulated once per CTA; the next element's nodes and
 //   coordinates are loaded while the current one is computed.
 #include <algorithm>
@@ -33,8 +35,9 @@ namespace {
 
 using namespace hex20;
 
-constexpr int kThreads = 320;
+constexpr int kThreads = 128;  // small CTAs: several elements' phases overlap on an SM
 constexpr int kWarps = kThreads / 32;
+constexpr int kTilesPerWarp = (36 + kWarps - 1) / kWarps;
 constexpr int PS = 28;  // row stride of P (doubles): conflict-free m8n8k4 fragment loads
 
 // The 36 upper 8x8 tiles (mt <= nt) of the 64x64 node-pair matrix.
@@ -52,8 +55,10 @@ struct KeSmem {
     double X[20][3];  // element node coordinates
     double J[27][9];  // Jacobians, then their inverses
     double w[PS];     // Gauss weight * detJ (w[27] = 0 pads the contraction)
+    TcScratch tc;     // FP16 split operands of the tensor-core form
     double lam, mu;
     int bad;
+    unsigned long long dnmax_bits;  // largest |dN| of the table (bits of a positive double)
 };
 static_assert(offsetof(KeSmem, Mb) % 16 == 0, "16-byte copies out of Mb");
 
@@ -63,12 +68,18 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
                  : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(kThreads, 3) k_hex20_ke(MeshView m, double* __restrict__ ke_out,
+// kTc: the node-pair contraction on the FP16 tensor cores (tc_prepare /
+// tc_contract of hex20.cuh) instead of the FP64 ones.
+template <bool kTc>
+__global__ void __launch_bounds__(kThreads, 5) k_hex20_ke(MeshView m, double* __restrict__ ke_out,
                                                           int* __restrict__ status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     KeSmem& sm = *reinterpret_cast<KeSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
+    if (tid == 0) sm.dnmax_bits = 0ull;
+    __syncthreads();
+    double dnmax = 0.0;
     for (int idx = tid; idx < 27 * 20; idx += kThreads) {
         const int g = idx / 20, n = idx % 20;
         double dx, dy, dz;
@@ -76,7 +87,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_hex20_ke(MeshView m, double* __
         sm.dN[g][0][n] = dx;
         sm.dN[g][1][n] = dy;
         sm.dN[g][2][n] = dz;
+        dnmax = fmax(dnmax, fmax(fabs(dx), fmax(fabs(dy), fabs(dz))));
     }
+    if (kTc) atomicMax(&sm.dnmax_bits, (unsigned long long)__double_as_longlong(dnmax));
     if (tid < PS) sm.w[tid] = 0.0;
     // node id and coordinates of the next element, loaded a step ahead
     int pre_n = 0;
@@ -94,7 +107,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_hex20_ke(MeshView m, double* __
 
     for (int e = first; e < end; e += gridDim.x) {
         double* out = ke_out + (size_t)e * kPackedHex20;
-        if (tid == 0) sm.bad = 0;
+        if (tid == 0) {
+            sm.bad = 0;
+            if (kTc) sm.tc.bound_bits = 0ull;
+        }
         __syncthreads();
         if (tid < 20) {
             if (pre_n < 0 || pre_n >= m.N) {
@@ -128,8 +144,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_hex20_ke(MeshView m, double* __
             continue;
         }
         // Jacobians: J[g][3i+j] = sum_n dN[g][i][n] X[n][j]
-        if (tid < 243) {
-            const int g = tid / 9, r = tid % 9, i = r / 3, j = r % 3;
+        for (int idx = tid; idx < 243; idx += kThreads) {
+            const int g = idx / 9, r = idx % 9, i = r / 3, j = r % 3;
             double acc = 0.0;
 #pragma unroll
             for (int n = 0; n < 20; n++) acc = fma(sm.dN[g][i][n], sm.X[n][j], acc);
@@ -155,6 +171,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_hex20_ke(MeshView m, double* __
 #pragma unroll
             for (int k = 0; k < 9; k++) J[k] = iJ[k];
             sm.w[tid] = weight3(tid / 9) * weight3((tid / 3) % 3) * weight3(tid % 3) * det;
+            if (kTc)
+                hex20::tc_gauss_point(sm.tc, tid, J, sm.w[tid], __longlong_as_double((long long)sm.dnmax_bits));
         }
         __syncthreads();
         // P aliases the previous element's M blocks: re-zero its padding.
@@ -171,15 +189,24 @@ __global__ void __launch_bounds__(kThreads, 3) k_hex20_ke(MeshView m, double* __
             for (int a = 0; a < 3; a++) sm.P[3 * n + a][g] = fma(iJ[3 * a], d0, fma(iJ[3 * a + 1], d1, iJ[3 * a + 2] * d2));
         }
         __syncthreads();
+        if (kTc) {
+            tc_prepare<kThreads>(&sm.P[0][0], PS, sm.w, sm.tc, tid);
+            // P is no longer read: its storage takes the M blocks
+            tc_contract<kWarps>(sm.tc, warp, lane, [&](int r, int c, double v) {
+                const int I = r / 3, a = r - 3 * I, J = c / 3, b = c - 3 * J;
+                sm.Mb[pair_index(I, J)][3 * a + b] = v;
+                if (I == J) sm.Mb[pair_index(I, I)][3 * b + a] = v;
+            });
+        } else {
         // M = (P diag(w)) P^T on the FP64 tensor cores, upper 8x8 tiles only
         // (M is symmetric): the 36 tiles (mt <= nt) are dealt round-robin to the
-        // warps, at most 4 per warp.
-        double acc[4][2];
+        // warps.
+        double acc[kTilesPerWarp][2];
 #pragma unroll
-        for (int q = 0; q < 4; q++) acc[q][0] = acc[q][1] = 0.0;
+        for (int q = 0; q < kTilesPerWarp; q++) acc[q][0] = acc[q][1] = 0.0;
         const int fr = lane >> 2, fc = lane & 3;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
+        for (int q = 0; q < kTilesPerWarp; q++) {
             const int t = warp + q * kWarps;
             if (t < 36) {
                 const int mt = c_tile_m[t], nt = c_tile_n[t];
@@ -192,7 +219,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_hex20_ke(MeshView m, double* __
         }
         __syncthreads();  // every warp has read P: its storage now takes the M blocks
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
+        for (int q = 0; q < kTilesPerWarp; q++) {
             const int t = warp + q * kWarps;
             if (t < 36) {
                 const int mt = c_tile_m[t], nt = c_tile_n[t];
@@ -208,6 +235,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_hex20_ke(MeshView m, double* __
                     }
                 }
             }
+        }
         }
         __syncthreads();
         // Ke upper blocks, consecutive threads on consecutive entries
@@ -285,24 +313,32 @@ __global__ void __launch_bounds__(kThreads2D) k_ke_2d(MeshView m, double* __rest
     }
 }
 
+template <bool kTc>
+cudaError_t launch_hex20_ke(const MeshView& m, double* ke_out, int* status, cudaStream_t s) {
+    static int blocks_per_sm = 0;
+    const size_t smem = sizeof(KeSmem);
+    if (!blocks_per_sm) {
+        cudaError_t err = cudaFuncSetAttribute(k_hex20_ke<kTc>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (err) return err;
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_hex20_ke<kTc>, kThreads, smem);
+        if (err) return err;
+        if (blocks_per_sm < 1) blocks_per_sm = 1;
+    }
+    const long long grid = std::min<long long>((long long)blocks_per_sm * sm_count(), m.E_count);
+    k_hex20_ke<kTc><<<(int)grid, kThreads, smem, s>>>(m, ke_out, status);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
-cudaError_t launch_element_stiffness(const MeshView& m, int kind, double* ke_out, int* status, cudaStream_t s) {
+cudaError_t launch_element_stiffness(const MeshView& m, int kind, int precision, double* ke_out, int* status,
+                                     cudaStream_t s) {
     if (m.E_count <= 0) return cudaSuccess;
     if (kind == FEM_HEX20) {
-        static int blocks_per_sm = 0;
-        const size_t smem = sizeof(KeSmem);
-        if (!blocks_per_sm) {
-            cudaError_t err = cudaFuncSetAttribute(k_hex20_ke, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (err) return err;
-            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_hex20_ke, kThreads, smem);
-            if (err) return err;
-            if (blocks_per_sm < 1) blocks_per_sm = 1;
-        }
-        const long long grid = std::min<long long>((long long)blocks_per_sm * sm_count(), m.E_count);
-        k_hex20_ke<<<(int)grid, kThreads, smem, s>>>(m, ke_out, status);
+        return precision == FEM_PREC_TC_F16X3 ? launch_hex20_ke<true>(m, ke_out, status, s)
+                                              : launch_hex20_ke<false>(m, ke_out, status, s);
     } else {
-        const long long warps = ((long long)m.E_count + 1) / 2;  // 2 Q4 / 3 T3 elements per warp
+        const long long warps = ((long long)m.E_count + 1) / 2;  // two elements per warp
         const int grid = (int)std::min<long long>((warps * 32 + kThreads2D - 1) / kThreads2D, (long long)sm_count() * 8);
         k_ke_2d<<<grid > 0 ? grid : 1, kThreads2D, 0, s>>>(m, ke_out, status);
     }

@@ -196,7 +196,8 @@ fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* wo
     fem_status st = make_layout(mesh, opts, h);
     if (st) return st;
     if ((st = check_ws(h, workspace, workspace_bytes))) return st;
-    if (opts && opts->precision != FEM_PREC_FP64) return FEM_ERR_BAD_ARG;
+    const int precision = opts ? opts->precision : FEM_PREC_FP64;
+    if (precision != FEM_PREC_FP64 && !(precision == FEM_PREC_TC_F16X3 && h.kind == FEM_HEX20)) return FEM_ERR_BAD_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     ListLayout L = device_layout(h, workspace);
     unsigned char* b = static_cast<unsigned char*>(workspace);
@@ -219,7 +220,7 @@ fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* wo
             b + h.off_elist + align_up((size_t)h.E * sizeof(int)) + align_up(4 * sizeof(int)) +
             align_up(nbuckets * sizeof(int)));
         err = launch_reorder_3d(m, hist, ranges, perm, bbox, sm_count(), s);
-        if (!err) err = launch_scatter_hex20(m, L, perm, s);
+        if (!err) err = launch_scatter_hex20(m, L, precision, perm, s);
     } else {
         err = launch_reorder(m, hist, ranges, perm, sm_count(), s);
         if (!err && h.kind != FEM_T3) err = launch_scatter_2d(m, L, 4, perm, ranges + 0, s);
@@ -294,10 +295,12 @@ fem_status fem_element_stiffness(const fem_mesh* mesh, const fem_opts* opts, dou
     fem_status st = check_mesh(mesh);
     if (st) return st;
     if (!status || (mesh->num_elems > 0 && !ke_out)) return FEM_ERR_BAD_ARG;
-    if (opts && opts->precision != FEM_PREC_FP64) return FEM_ERR_BAD_ARG;
+    const int precision = opts ? opts->precision : FEM_PREC_FP64;
+    if (precision != FEM_PREC_FP64 && !(precision == FEM_PREC_TC_F16X3 && mesh->kind == FEM_HEX20))
+        return FEM_ERR_BAD_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t err = cudaMemsetAsync(status, 0, sizeof(int32_t), s);
-    if (!err) err = launch_element_stiffness(mesh_view(mesh), mesh->kind, ke_out, status, s);
+    if (!err) err = launch_element_stiffness(mesh_view(mesh), mesh->kind, precision, ke_out, status, s);
     return err ? cuda_fail(err) : FEM_OK;
 }
 

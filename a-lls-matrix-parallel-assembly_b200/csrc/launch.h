@@ -36,9 +36,11 @@ constexpr int kPackedHex20 = 210 * 9;  // 210 upper 3x3 node blocks
 constexpr int kPacked2D_Q4 = 10 * 4;   // 10 upper 2x2 node blocks (also the mixed-mesh stride)
 constexpr int kPacked2D_T3 = 6 * 4;
 // Element stiffness of every element, natural order; status gets 1 << FEM_ERR_* bits.
-cudaError_t launch_element_stiffness(const MeshView& m, int kind, double* ke_out, int* status, cudaStream_t s);
-// perm: element visit order (spatial, from launch_reorder_3d).
-cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, const int* perm, cudaStream_t s);
+cudaError_t launch_element_stiffness(const MeshView& m, int kind, int precision, double* ke_out, int* status,
+                                     cudaStream_t s);
+// perm: element visit order (spatial, from launch_reorder_3d); precision FEM_PREC_*.
+cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm,
+                                 cudaStream_t s);
 // Spatial (3-D Morton bucket) element order; hist needs 1 << (3 * morton_bits(E)) ints, bbox 6 words.
 int morton_bits(int num_elems);
 cudaError_t launch_reorder_3d(const MeshView& m, int* hist, int* ranges, int* perm, unsigned long long* bbox, int sms,

@@ -8,20 +8,15 @@
 // One CTA (10 warps) per element at a time, persistent over the elements, which
 // it visits in the spatial order computed by launch_reorder_3d.
 //
-// Element stiffness, in double. With the physical shape-function gradients
-// G_g (a 60-vector per Gauss point g, dof r = 3 node + dir) and
-// w_g = gauss weight * detJ_g, the node-pair matrix
-//     M = sum_g w_g G_g G_g^T          (60 x 60, contraction length 27)
-// gives every 3x3 block of the isotropic stiffness as
-//     Ke_IJ[a][b] = lambda M[3I+a][3J+b] + mu M[3I+b][3J+a] + mu delta_ab tr(M_IJ)
-// which is algebraically the reference's per-Gauss-point block formula
-// (H20:173-191, c1 = lambda + 2 mu, c2 = lambda, c3 = mu). M is one symmetric
-// 64x64x28 FP64 matrix product per element, computed on the FP64 tensor cores
-// with mma.sync.m8n8k4.f64 (36 upper 8x8 tiles x 7 k-steps); each upper entry
-// is written to both of its places in M (so every Ke is exactly symmetric), in
-// the shared memory the gradients occupied. Ke blocks are formed from M per
-// scattered row. The Gauss-point shape derivatives (H20:95-128) are tabulated
-// once per CTA.
+// Element stiffness (the node-pair matrix M of hex20.cuh), in double: M is one
+// symmetric 64x64x28 FP64 matrix product per element, computed on the FP64
+// tensor cores with mma.sync.m8n8k4.f64 (36 upper 8x8 tiles x 7 k-steps), or
+// with FEM_PREC_TC_F16X3 on the FP16 tensor cores from split operands
+// (tc_prepare / tc_contract); each upper entry is written to both of its
+// places in M (so every Ke is exactly symmetric), in the shared memory the
+// gradients occupied. Ke blocks are formed from M per scattered row. The
+// Gauss-point shape derivatives (ALLS_Hex20_3D_Assembly_Performance.cu:95-128)
+// are tabulated once per CTA.
 //
 // Scatter. Warp w serves row nodes w and w+10. It prefetches both rows' chunk
 // rows (384 bytes: next pointer + 94 hashed slots) into shared memory with one
@@ -36,10 +31,12 @@
 // claims of both rows; blocks whose slot another warp was still writing are
 // added after a bounded wait. The next element's nodes and coordinates are
 // prefetched during the compute and the scatter.
-#include "launch.h"
+#include "hex20.cuh"
 
 namespace fem {
 namespace {
+
+using hex20::TcScratch;
 
 constexpr int kThreads = 320;
 constexpr int kWarps = kThreads / 32;
@@ -48,42 +45,11 @@ constexpr int PS = 28;               // row stride of P (doubles): conflict-free
 constexpr int MP = 61;               // row stride of M (doubles, odd: few bank conflicts on block reads)
 constexpr int kHash = 64;            // element-node hash slots
 
-// Natural coordinates of the 20 nodes in the reference order (H20:97-99).
-__constant__ signed char c_xin[20] = {-1, 1, 1, -1, -1, 1, 1, -1, 0, 1, 0, -1, 0, 1, 0, -1, -1, 1, 1, -1};
-__constant__ signed char c_etan[20] = {-1, -1, 1, 1, -1, -1, 1, 1, -1, 0, 1, 0, -1, 0, 1, 0, -1, -1, 1, 1};
-__constant__ signed char c_zetan[20] = {-1, -1, -1, -1, 1, 1, 1, 1, -1, -1, -1, -1, 1, 1, 1, 1, 0, 0, 0, 0};
-
 // The 36 upper 8x8 tiles (mt <= nt) of the 64x64 node-pair matrix.
 __constant__ unsigned char c_tile_m[36] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 1, 2, 2, 2,
                                            2, 2, 2, 3, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 6, 6, 7};
 __constant__ unsigned char c_tile_n[36] = {0, 1, 2, 3, 4, 5, 6, 7, 1, 2, 3, 4, 5, 6, 7, 2, 3, 4,
                                            5, 6, 7, 3, 4, 5, 6, 7, 4, 5, 6, 7, 5, 6, 7, 6, 7, 7};
-
-// Gauss abscissae / weights as the reference writes them (H20:45-46), in double.
-__device__ __forceinline__ double gauss3(int i) { return i == 0 ? -0.774596669241483 : (i == 1 ? 0.0 : 0.774596669241483); }
-__device__ __forceinline__ double weight3(int i) { return i == 1 ? 0.888888888888889 : 0.555555555555556; }
-
-// dN_n/d(xi, eta, zeta) at one point (formulas of H20:95-128).
-__device__ void hex20_dshape_node(int n, double xi, double eta, double zeta, double& dx, double& dy, double& dz) {
-    const double a = c_xin[n], b = c_etan[n], c = c_zetan[n];
-    if (n < 8) {
-        dx = 0.125 * a * (1.0 + b * eta) * (1.0 + c * zeta) * (2.0 * a * xi + b * eta + c * zeta - 1.0);
-        dy = 0.125 * b * (1.0 + a * xi) * (1.0 + c * zeta) * (a * xi + 2.0 * b * eta + c * zeta - 1.0);
-        dz = 0.125 * c * (1.0 + a * xi) * (1.0 + b * eta) * (a * xi + b * eta + 2.0 * c * zeta - 1.0);
-    } else if (n == 8 || n == 10 || n == 12 || n == 14) {
-        dx = -0.5 * xi * (1.0 + b * eta) * (1.0 + c * zeta);
-        dy = 0.25 * b * (1.0 - xi * xi) * (1.0 + c * zeta);
-        dz = 0.25 * c * (1.0 - xi * xi) * (1.0 + b * eta);
-    } else if (n < 16) {
-        dx = 0.25 * a * (1.0 - eta * eta) * (1.0 + c * zeta);
-        dy = -0.5 * eta * (1.0 + a * xi) * (1.0 + c * zeta);
-        dz = 0.25 * c * (1.0 + a * xi) * (1.0 - eta * eta);
-    } else {
-        dx = 0.25 * a * (1.0 + b * eta) * (1.0 - zeta * zeta);
-        dy = 0.25 * b * (1.0 + a * xi) * (1.0 - zeta * zeta);
-        dz = -0.5 * zeta * (1.0 + a * xi) * (1.0 + b * eta);
-    }
-}
 
 enum SlotState : int { kUnresolved = 0, kFound = 1, kFoundPending = 2, kClaimed = 3 };
 
@@ -99,12 +65,16 @@ struct Hex20Smem {
     alignas(16) int view[kWarps][2][kMaxHex20Words];  // per-warp copies of the two rows' chunks
     unsigned gid[kWarps][20];  // slot of each column node's entry in the row being committed
     int state[kWarps][20];
-    double stage[kWarps][20 * 9];  // the row's 20 Ke blocks, entry j*9 + v
+    union {
+        double stage[kWarps][20 * 9];  // the row's 20 Ke blocks, entry j*9 + v
+        TcScratch tc;                  // FP16 split operands while M is computed (tensor-core form)
+    };
     int hkey[kHash];           // element-node hash: node + 1 -> local index
     int hval[kHash];
     int nodes[20];
     double lam, mu;
     int bad;
+    unsigned long long dnmax_bits;  // largest |dN| of the table (bits of a positive double)
 };
 
 static_assert(offsetof(Hex20Smem, view) % 16 == 0, "int4 stores into view need 16-byte alignment");
@@ -329,19 +299,26 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
                  : "d"(a), "d"(b));
 }
 
+// kTc: the node-pair contraction on the FP16 tensor cores (hex20.cuh).
+template <bool kTc>
 __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListLayout L, const int* __restrict__ perm) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Hex20Smem& sm = *reinterpret_cast<Hex20Smem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
+    if (tid == 0) sm.dnmax_bits = 0ull;
+    __syncthreads();
+    double dnmax = 0.0;
     for (int idx = tid; idx < 27 * 20; idx += kThreads) {
         const int g = idx / 20, n = idx % 20;
         double dx, dy, dz;
-        hex20_dshape_node(n, gauss3(g / 9), gauss3((g / 3) % 3), gauss3(g % 3), dx, dy, dz);
+        hex20::dshape_node(n, hex20::gauss3(g / 9), hex20::gauss3((g / 3) % 3), hex20::gauss3(g % 3), dx, dy, dz);
         sm.dN[g][0][n] = dx;
         sm.dN[g][1][n] = dy;
         sm.dN[g][2][n] = dz;
+        dnmax = fmax(dnmax, fmax(fabs(dx), fmax(fabs(dy), fabs(dz))));
     }
+    if (kTc) atomicMax(&sm.dnmax_bits, (unsigned long long)__double_as_longlong(dnmax));
     if (tid < PS) sm.w[tid] = 0.0;
     int spare = -1;
     // node id and coordinates of the next element, loaded during the scatter
@@ -359,7 +336,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
 
     for (int i = blockIdx.x; i < m.E_count; i += gridDim.x) {
         const int e = __ldg(perm + i);
-        if (tid == 0) sm.bad = 0;
+        if (tid == 0) {
+            sm.bad = 0;
+            if (kTc) sm.tc.bound_bits = 0ull;
+        }
         if (tid < kHash) sm.hkey[tid] = 0;
         __syncthreads();
         if (tid < 20) {
@@ -430,7 +410,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
             iJ[8] = (J[0] * J[4] - J[1] * J[3]) * r;
 #pragma unroll
             for (int k = 0; k < 9; k++) J[k] = iJ[k];
-            sm.w[tid] = weight3(tid / 9) * weight3((tid / 3) % 3) * weight3(tid % 3) * det;
+            sm.w[tid] = hex20::weight3(tid / 9) * hex20::weight3((tid / 3) % 3) * hex20::weight3(tid % 3) * det;
+            if (kTc)
+                hex20::tc_gauss_point(sm.tc, tid, J, sm.w[tid], __longlong_as_double((long long)sm.dnmax_bits));
         }
         __syncthreads();
         // P aliases the previous element's M blocks: re-zero its padding.
@@ -447,6 +429,14 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
             for (int a = 0; a < 3; a++) sm.P[3 * n + a][g] = fma(iJ[3 * a], d0, fma(iJ[3 * a + 1], d1, iJ[3 * a + 2] * d2));
         }
         __syncthreads();
+        if (kTc) {
+            hex20::tc_prepare<kThreads>(&sm.P[0][0], PS, sm.w, sm.tc, tid);
+            // P is no longer read: its storage takes M
+            hex20::tc_contract<kWarps>(sm.tc, warp, lane, [&](int r, int c, double v) {
+                sm.M[r][c] = v;
+                sm.M[c][r] = v;
+            });
+        } else {
         // M = (P diag(w)) P^T on the FP64 tensor cores, upper 8x8 tiles only
         // (M is symmetric): the 36 tiles (mt <= nt) are dealt round-robin to the
         // warps, at most 4 per warp.
@@ -484,6 +474,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
                 }
             }
         }
+        }
         __syncthreads();
         // next element's coordinates: in flight during the scatter
         if (tid < 20 && i_next < m.E_count && pre_n >= 0 && pre_n < m.N) {
@@ -499,21 +490,28 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
 
 }  // namespace
 
-cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, const int* perm, cudaStream_t s) {
-    static int blocks_per_sm = 0, sms = 0;
+template <bool kTc>
+cudaError_t launch_scatter_hex20_t(const MeshView& m, const ListLayout& L, const int* perm, cudaStream_t s) {
+    static int blocks_per_sm = 0;
     const size_t smem = sizeof(Hex20Smem);
     if (!blocks_per_sm) {
-        cudaError_t err = cudaFuncSetAttribute(k_scatter_hex20, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t err =
+            cudaFuncSetAttribute(k_scatter_hex20<kTc>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (err) return err;
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_scatter_hex20, kThreads, smem);
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_scatter_hex20<kTc>, kThreads, smem);
         if (err) return err;
-        sms = sm_count();
         if (blocks_per_sm < 1) blocks_per_sm = 1;
     }
-    long long grid = (long long)blocks_per_sm * sms;
+    long long grid = (long long)blocks_per_sm * sm_count();
     if (grid > m.E_count) grid = m.E_count > 0 ? m.E_count : 1;
-    k_scatter_hex20<<<(int)grid, kThreads, smem, s>>>(m, L, perm);
+    k_scatter_hex20<kTc><<<(int)grid, kThreads, smem, s>>>(m, L, perm);
     return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm,
+                                 cudaStream_t s) {
+    return precision == FEM_PREC_TC_F16X3 ? launch_scatter_hex20_t<true>(m, L, perm, s)
+                                          : launch_scatter_hex20_t<false>(m, L, perm, s);
 }
 
 }  // namespace fem

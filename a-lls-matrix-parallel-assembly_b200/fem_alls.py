@@ -111,8 +111,11 @@ def load() -> C.CDLL:
     return _lib
 
 
-def opts(first_slots: int = 0, chunk_slots: int = 0, pool_factor: float = 0.0) -> FemOpts:
-    return FemOpts(0, first_slots, chunk_slots, 0, pool_factor)
+FEM_PREC_FP64, FEM_PREC_TC_F16X3 = 0, 1
+
+
+def opts(first_slots: int = 0, chunk_slots: int = 0, pool_factor: float = 0.0, precision: int = 0) -> FemOpts:
+    return FemOpts(precision, first_slots, chunk_slots, 0, pool_factor)
 
 
 def _ptr(t) -> Optional[int]:

@@ -76,7 +76,11 @@ typedef int32_t fem_status;
 #define FEM_MIXED_2D 3  /* Q4 and T3 in one mesh; conn_stride 4, elem_type per element */
 
 /* ---- precision of the element stiffness --------------------------------- */
-#define FEM_PREC_FP64 0  /* plain FP64 element stiffness (the oracle path) */
+#define FEM_PREC_FP64 0      /* plain FP64 element stiffness (the oracle path) */
+#define FEM_PREC_TC_F16X3 1  /* Hex20 only: the node-pair contraction of Ke on the FP16 tensor
+                                cores with split operands (A = A_hi + A_lo, three products,
+                                FP32 accumulation); Jacobians, detJ, inverses and the global
+                                accumulation stay FP64. Value error stated by the tests. */
 
 typedef struct fem_mesh {
     int32_t kind;          /* FEM_Q4, FEM_T3, FEM_HEX20, FEM_MIXED_2D */
@@ -179,8 +183,8 @@ FEM_API fem_status fem_element_stiffness_size(const fem_mesh* mesh, int64_t* dou
 
 /* ke_out: device [num_elems * doubles_per_element]. status: a device int32
  * that is zeroed and then receives (1 << FEM_ERR_*) bits (BAD_MESH: the
- * element's output is zero; DETJ). Asynchronous. opts->precision must be
- * FEM_PREC_FP64. */
+ * element's output is zero; DETJ). Asynchronous. opts->precision:
+ * FEM_PREC_FP64, or FEM_PREC_TC_F16X3 for a Hex20 mesh. */
 FEM_API fem_status fem_element_stiffness(const fem_mesh* mesh, const fem_opts* opts, double* ke_out,
                                          int32_t* status, void* stream);
 

@@ -47,3 +47,31 @@ def test_element_stiffness_reports_bad_node(fem, cuda_device):
     ke, status = fem.element_stiffness(m)
     assert status & (1 << 2)
     assert np.all(ke[1].cpu().numpy() == 0.0)
+
+
+# The tensor-core form (FEM_PREC_TC_F16X3): FP16 split operands, FP32
+# accumulation of the node-pair contraction, FP64 everywhere else. Its error is
+# measured against the FP64 oracle on the element's scale and stated here.
+TC_ELEMENT_TOL = 2e-6
+
+
+def test_tensor_core_element_stiffness_error(fem, oracle_mod, cuda_device):
+    import meshgen as mg
+    m = mg.by_name("hex20_small")
+    ke, status = fem.element_stiffness(m, fem.opts(precision=1))
+    assert status == 0
+    ke = ke.cpu().numpy()
+    worst = 0.0
+    for e in range(m.num_elems):
+        ref, npe, dpn = _oracle_ke(oracle_mod, m, e)
+        got = fem.unpack_element_stiffness(ke[e], npe, dpn)
+        err = np.max(np.abs(got - ref)) / np.max(np.abs(np.diag(ref)))
+        worst = max(worst, err)
+    print(f"tensor-core Ke: max error {worst:.3e} of the element's largest diagonal entry")
+    assert worst <= TC_ELEMENT_TOL
+
+
+def test_tensor_core_form_rejected_for_2d(fem, cuda_device):
+    import meshgen as mg
+    with pytest.raises(fem.FemError):
+        fem.element_stiffness(mg.by_name("t3_small"), fem.opts(precision=1))

@@ -192,3 +192,23 @@ def test_host_entry_point(fem, oracle_mod, cuda_device):
     np.testing.assert_array_equal(ci, oci)
     np.testing.assert_allclose(v, ov, rtol=1e-12, atol=1e-12 * np.abs(ov).max())
     ctx.close()
+
+
+# Full assembly with the tensor-core Ke form (FEM_PREC_TC_F16X3): the pattern
+# is the same bit for bit; values (FP64 global accumulation of the per-element
+# FP16-split contraction) agree with the FP64 oracle within TC_RTOL on the
+# row/column scale max(|K_ij|, sqrt(|K_ii K_jj|)).
+TC_RTOL = 2e-6
+
+
+@pytest.mark.parametrize("name", ["hex20_small"])
+def test_tensor_core_form_assembly(fem, oracle_mod, cuda_device, name):
+    import meshgen as mg
+    m = mg.by_name(name)
+    rp, ci, v, info = fem.assemble(m, fem.opts(precision=1))
+    orp, oci, ov = oracle_mod.assemble(m)
+    np.testing.assert_array_equal(rp, orp)
+    np.testing.assert_array_equal(ci, oci)
+    rel, scaled = value_errors(orp, oci, ov, v)
+    print(f"{name} tensor-core form: max scaled error {scaled:.3e}, max per-entry relative {rel:.3e}")
+    assert scaled <= TC_RTOL
