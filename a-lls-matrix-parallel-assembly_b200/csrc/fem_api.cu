@@ -307,6 +307,122 @@ fem_status fem_element_stiffness(const fem_mesh* mesh, const fem_opts* opts, dou
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Value-only re-assembly through a scatter map
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct MapHostLayout {
+    int G;  // map entries per element
+    size_t off_info, off_pos, off_perm, off_ranges, off_hist, off_bbox, total;
+};
+
+MapHostLayout map_layout(const fem_mesh* m) {
+    MapHostLayout h{};
+    const size_t E = (size_t)m->num_elems;
+    const int npe = m->kind == FEM_HEX20 ? 20 : (m->kind == FEM_T3 ? 3 : 4);
+    h.G = npe * npe;
+    const size_t nbuckets = m->kind == FEM_HEX20 ? (size_t)1 << (3 * morton_bits(m->num_elems))
+                                                 : (size_t)2 * reorder_buckets(m->num_nodes);
+    size_t off = 0;
+    h.off_info = off;
+    off += align_up(sizeof(DevInfo));
+    h.off_pos = off;
+    off += align_up(E * h.G * sizeof(int));
+    h.off_perm = off;
+    off += align_up(E * sizeof(int));
+    h.off_ranges = off;
+    off += align_up(4 * sizeof(int));
+    h.off_hist = off;
+    off += align_up(nbuckets * sizeof(int));
+    h.off_bbox = off;
+    off += align_up(6 * sizeof(unsigned long long));
+    h.total = off;
+    return h;
+}
+
+fem_status check_map(const fem_mesh* mesh, const void* map, size_t map_bytes, MapHostLayout& h) {
+    fem_status st = check_mesh(mesh);
+    if (st) return st;
+    h = map_layout(mesh);
+    if (!map || map_bytes < h.total || reinterpret_cast<uintptr_t>(map) % kAlign) return FEM_ERR_WORKSPACE;
+    return FEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fem_status fem_scatter_map_size(const fem_mesh* mesh, size_t* bytes) {
+    fem_status st = check_mesh(mesh);
+    if (st) return st;
+    if (!bytes) return FEM_ERR_BAD_ARG;
+    *bytes = map_layout(mesh).total;
+    return FEM_OK;
+}
+
+fem_status fem_scatter_map_build(const fem_mesh* mesh, const int32_t* row_ptr, const int32_t* col_idx, void* map,
+                                 size_t map_bytes, void* stream) {
+    MapHostLayout h;
+    fem_status st = check_map(mesh, map, map_bytes, h);
+    if (st) return st;
+    if (!row_ptr || (mesh->num_elems > 0 && !col_idx)) return FEM_ERR_BAD_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned char* b = static_cast<unsigned char*>(map);
+    DevInfo* info = reinterpret_cast<DevInfo*>(b + h.off_info);
+    const MeshView m = mesh_view(mesh);
+    int* perm = reinterpret_cast<int*>(b + h.off_perm);
+    int* ranges = reinterpret_cast<int*>(b + h.off_ranges);
+    int* hist = reinterpret_cast<int*>(b + h.off_hist);
+    cudaError_t err = cudaMemsetAsync(info, 0, sizeof(DevInfo), s);
+    if (!err && mesh->num_elems > 0) {
+        err = launch_build_map(m, mesh->kind, row_ptr, col_idx, reinterpret_cast<int*>(b + h.off_pos),
+                               &info->status_bits, s);
+        // the element visit order of the A-LLS scatter, for the locality of the adds
+        if (!err && mesh->kind == FEM_HEX20)
+            err = launch_reorder_3d(m, hist, ranges, perm, reinterpret_cast<unsigned long long*>(b + h.off_bbox),
+                                    sm_count(), s);
+        else if (!err)
+            err = launch_reorder(m, hist, ranges, perm, sm_count(), s);
+    }
+    return err ? cuda_fail(err) : FEM_OK;
+}
+
+fem_status fem_reassemble_values(const fem_mesh* mesh, const fem_opts* opts, const void* map, size_t map_bytes,
+                                 const int32_t* row_ptr, double* values, int64_t nnz, void* stream) {
+    MapHostLayout h;
+    fem_status st = check_map(mesh, map, map_bytes, h);
+    if (st) return st;
+    const int precision = opts ? opts->precision : FEM_PREC_FP64;
+    if (precision != FEM_PREC_FP64 && !(precision == FEM_PREC_TC_F16X3 && mesh->kind == FEM_HEX20))
+        return FEM_ERR_BAD_ARG;
+    if (!row_ptr || nnz < 0 || (nnz > 0 && !values)) return FEM_ERR_BAD_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned char* b = static_cast<unsigned char*>(const_cast<void*>(map));
+    DevInfo* info = reinterpret_cast<DevInfo*>(b + h.off_info);
+    const int* pos = reinterpret_cast<const int*>(b + h.off_pos);
+    const int* perm = reinterpret_cast<const int*>(b + h.off_perm);
+    const int* ranges = reinterpret_cast<const int*>(b + h.off_ranges);
+    cudaError_t err = cudaMemsetAsync(&info->status_bits, 0, sizeof(int), s);
+    if (!err && nnz > 0) err = cudaMemsetAsync(values, 0, (size_t)nnz * sizeof(double), s);
+    if (!err && mesh->num_elems > 0) {
+        const MeshView m = mesh_view(mesh);
+        if (mesh->kind == FEM_HEX20)
+            err = launch_reassemble_hex20(m, precision, perm, MapTarget{pos, row_ptr, values}, info, s);
+        else
+            err = launch_reassemble_2d(m, pos, h.G, perm, ranges, row_ptr, values, &info->status_bits, s);
+    }
+    return err ? cuda_fail(err) : FEM_OK;
+}
+
+fem_status fem_scatter_map_read_info(const void* map, void* stream) {
+    fem_info info;
+    return fem_alls_read_info(map, &info, stream);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
 // Element-colouring baseline
 // ---------------------------------------------------------------------------
 

@@ -38,6 +38,23 @@ constexpr int kPacked2D_T3 = 6 * 4;
 // Element stiffness of every element, natural order; status gets 1 << FEM_ERR_* bits.
 cudaError_t launch_element_stiffness(const MeshView& m, int kind, int precision, double* ke_out, int* status,
                                      cudaStream_t s);
+// Target of a value-only re-assembly: CSR positions of every element block.
+struct MapTarget {
+    const int* map;      // [E * npe^2] position of block (a, b) of element e at e * npe^2 + a * npe + b
+    const int* row_ptr;  // CSR row pointers of the pattern the map was built for
+    double* values;      // CSR values (zeroed by the caller)
+};
+
+// Scatter map of a mesh into a CSR pattern; status gets 1 << FEM_ERR_* bits.
+cudaError_t launch_build_map(const MeshView& m, int kind, const int* row_ptr, const int* col_idx, int* map,
+                             int* status, cudaStream_t s);
+// Value-only re-assembly (atomics into values): 2-D kinds over perm ranges
+// {q4 begin, q4 end, t3 begin, t3 end}; Hex20 over perm (status bits in info).
+cudaError_t launch_reassemble_2d(const MeshView& m, const int* map, int G, const int* perm, const int* ranges,
+                                 const int* row_ptr, double* values, int* status, cudaStream_t s);
+cudaError_t launch_reassemble_hex20(const MeshView& m, int precision, const int* perm, const MapTarget& t,
+                                    DevInfo* info, cudaStream_t s);
+
 // perm: element visit order (spatial, from launch_reorder_3d); precision FEM_PREC_*.
 cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm,
                                  cudaStream_t s);

@@ -293,6 +293,26 @@ __device__ __forceinline__ void scatter_rows(const ListLayout& L, Hex20Smem& sm,
     __syncwarp();
 }
 
+// Value-only re-assembly (reassemble.cu): row nodes I0 and I1 of element e,
+// lane j adds block (I, j) at the CSR positions of the scatter map.
+__device__ __forceinline__ void map_rows(const MapTarget& t, const Hex20Smem& sm, int e, int I0, int I1, int lane) {
+    if (lane >= 20) return;
+    for (int r = 0; r < 2; r++) {
+        const int I = r == 0 ? I0 : I1;
+        if (I < 0) continue;
+        const int p = __ldg(t.map + (size_t)e * 400 + I * 20 + lane);
+        if (p < 0) continue;
+        const int r0 = 3 * sm.nodes[I];
+        const int len = __ldg(t.row_ptr + r0 + 1) - __ldg(t.row_ptr + r0);
+        double v[9];
+        ke_block(sm, I, lane, v);
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) atomicAdd(t.values + p + i * len + j, v[3 * i + j]);
+    }
+}
+
 __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                  : "+d"(c0), "+d"(c1)
@@ -300,8 +320,11 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
 }
 
 // kTc: the node-pair contraction on the FP16 tensor cores (hex20.cuh).
-template <bool kTc>
-__global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListLayout L, const int* __restrict__ perm) {
+// kMap: value-only re-assembly into a CSR pattern through a scatter map
+// instead of the A-LLS list scatter.
+template <bool kTc, bool kMap>
+__global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListLayout L, const int* __restrict__ perm,
+                                                               MapTarget target) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Hex20Smem& sm = *reinterpret_cast<Hex20Smem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -483,35 +506,48 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
             pre_z = __ldg(m.z + pre_n);
         }
         // Scatter: warp w serves row nodes w and w + 10.
-        scatter_rows(L, sm, warp, warp + kWarps < 20 ? warp + kWarps : -1, warp, lane, spare);
+        if (kMap)
+            map_rows(target, sm, e, warp, warp + kWarps < 20 ? warp + kWarps : -1, lane);
+        else
+            scatter_rows(L, sm, warp, warp + kWarps < 20 ? warp + kWarps : -1, warp, lane, spare);
         __syncthreads();
     }
 }
 
 }  // namespace
 
-template <bool kTc>
-cudaError_t launch_scatter_hex20_t(const MeshView& m, const ListLayout& L, const int* perm, cudaStream_t s) {
+template <bool kTc, bool kMap>
+cudaError_t launch_scatter_hex20_t(const MeshView& m, const ListLayout& L, const int* perm, const MapTarget& t,
+                                   cudaStream_t s) {
     static int blocks_per_sm = 0;
     const size_t smem = sizeof(Hex20Smem);
     if (!blocks_per_sm) {
         cudaError_t err =
-            cudaFuncSetAttribute(k_scatter_hex20<kTc>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaFuncSetAttribute(k_scatter_hex20<kTc, kMap>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (err) return err;
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_scatter_hex20<kTc>, kThreads, smem);
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_scatter_hex20<kTc, kMap>, kThreads, smem);
         if (err) return err;
         if (blocks_per_sm < 1) blocks_per_sm = 1;
     }
     long long grid = (long long)blocks_per_sm * sm_count();
     if (grid > m.E_count) grid = m.E_count > 0 ? m.E_count : 1;
-    k_scatter_hex20<kTc><<<(int)grid, kThreads, smem, s>>>(m, L, perm);
+    k_scatter_hex20<kTc, kMap><<<(int)grid, kThreads, smem, s>>>(m, L, perm, t);
     return cudaGetLastError();
 }
 
 cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm,
                                  cudaStream_t s) {
-    return precision == FEM_PREC_TC_F16X3 ? launch_scatter_hex20_t<true>(m, L, perm, s)
-                                          : launch_scatter_hex20_t<false>(m, L, perm, s);
+    const MapTarget none{};
+    return precision == FEM_PREC_TC_F16X3 ? launch_scatter_hex20_t<true, false>(m, L, perm, none, s)
+                                          : launch_scatter_hex20_t<false, false>(m, L, perm, none, s);
+}
+
+cudaError_t launch_reassemble_hex20(const MeshView& m, int precision, const int* perm, const MapTarget& t,
+                                    DevInfo* info, cudaStream_t s) {
+    ListLayout L{};
+    L.info = info;  // status bits (BAD_MESH, DETJ) of the element stiffness
+    return precision == FEM_PREC_TC_F16X3 ? launch_scatter_hex20_t<true, true>(m, L, perm, t, s)
+                                          : launch_scatter_hex20_t<false, true>(m, L, perm, t, s);
 }
 
 }  // namespace fem

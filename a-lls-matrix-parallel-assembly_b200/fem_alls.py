@@ -35,7 +35,8 @@ EXPORTS = ["fem_alls_workspace_size", "fem_alls_scatter", "fem_alls_consolidate"
            "fem_assemble", "fem_assemble_async", "fem_context_create", "fem_context_destroy",
            "fem_assemble_host", "fem_status_string", "fem_last_cuda_error", "fem_abi_version",
            "fem_assemble_static", "fem_colour_workspace_size", "fem_colour_prepare", "fem_colour_assemble",
-           "fem_colour_read_info", "fem_element_stiffness_size", "fem_element_stiffness"]
+           "fem_colour_read_info", "fem_element_stiffness_size", "fem_element_stiffness",
+           "fem_scatter_map_size", "fem_scatter_map_build", "fem_reassemble_values", "fem_scatter_map_read_info"]
 STATIC_WORKSPACE_BYTES = 32 << 20  # FEM_STATIC_WORKSPACE_BYTES
 
 
@@ -102,6 +103,10 @@ def load() -> C.CDLL:
         L.fem_colour_read_info.argtypes = [vp, p(C.c_int32), vp]
         L.fem_element_stiffness_size.argtypes = [p(FemMesh), p(C.c_int64)]
         L.fem_element_stiffness.argtypes = [p(FemMesh), p(FemOpts), vp, vp, vp]
+        L.fem_scatter_map_size.argtypes = [p(FemMesh), p(C.c_size_t)]
+        L.fem_scatter_map_build.argtypes = [p(FemMesh), vp, vp, vp, C.c_size_t, vp]
+        L.fem_reassemble_values.argtypes = [p(FemMesh), p(FemOpts), vp, C.c_size_t, vp, vp, C.c_int64, vp]
+        L.fem_scatter_map_read_info.argtypes = [vp, vp]
         L.fem_status_string.argtypes = [C.c_int32]
         L.fem_status_string.restype = C.c_char_p
         for f in EXPORTS:
@@ -347,3 +352,37 @@ def unpack_element_stiffness(packed: np.ndarray, npe: int, dpn: int) -> np.ndarr
             ke[b * dpn:(b + 1) * dpn, a * dpn:(a + 1) * dpn] = blk.T
             k += 1
     return ke
+
+
+class Reassembler:
+    """Value-only re-assembly (fem_scatter_map_* / fem_reassemble_values) into
+    the CSR pattern of an Assembler's last assembly."""
+
+    def __init__(self, asm: "Assembler"):
+        import torch
+        self.torch = torch
+        self.asm = asm
+        self.lib = load()
+        n = C.c_size_t(0)
+        check(self.lib.fem_scatter_map_size(C.byref(asm.cm), C.byref(n)), "fem_scatter_map_size")
+        self.map_bytes = n.value
+        self.buf = torch.empty(self.map_bytes + 256, dtype=torch.uint8, device=asm.row_ptr.device)
+        self.map_ptr = (self.buf.data_ptr() + 255) // 256 * 256
+
+    def _stream(self):
+        return self.torch.cuda.current_stream().cuda_stream
+
+    def build(self, nnz: int):
+        self.nnz = nnz
+        check(self.lib.fem_scatter_map_build(C.byref(self.asm.cm), _ptr(self.asm.row_ptr), _ptr(self.asm.col_idx),
+                                             self.map_ptr, self.map_bytes, self._stream()), "fem_scatter_map_build")
+        check(self.lib.fem_scatter_map_read_info(self.map_ptr, self._stream()), "scatter map")
+
+    def reassemble(self, values, o: Optional[FemOpts] = None):
+        """values: device float64 tensor of nnz entries (overwritten)."""
+        check(self.lib.fem_reassemble_values(C.byref(self.asm.cm), C.byref(o) if o else None, self.map_ptr,
+                                             self.map_bytes, _ptr(self.asm.row_ptr), _ptr(values), self.nnz,
+                                             self._stream()), "fem_reassemble_values")
+
+    def read_info(self) -> int:
+        return self.lib.fem_scatter_map_read_info(self.map_ptr, self._stream())

@@ -188,6 +188,39 @@ FEM_API fem_status fem_element_stiffness_size(const fem_mesh* mesh, int64_t* dou
 FEM_API fem_status fem_element_stiffness(const fem_mesh* mesh, const fem_opts* opts, double* ke_out,
                                          int32_t* status, void* stream);
 
+/* ---- value-only re-assembly through a scatter map ----------------------------
+ * For a mesh whose connectivity is unchanged between assemblies (new
+ * coordinates, E or nu: nonlinear and time-stepping solvers). The reference
+ * has no such path: every assembly repeats the list build and the host pattern
+ * (ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:394-501,605-645). A scatter map,
+ * built once from the CSR pattern of a full assembly, holds the CSR position
+ * of every element node block; re-assembly then adds each element's blocks at
+ * those positions with FP64 atomics, with no list, no pattern build and no
+ * sort. The map buffer also holds the element visit order and a status word. */
+
+/* Bytes of the scatter-map buffer (device, 256-byte aligned) for this mesh:
+ * 4 * num_elems * npe^2 (npe 4 for Q4 and mixed, 3 for T3, 20 for Hex20) plus
+ * num_elems ints and a few KB. */
+FEM_API fem_status fem_scatter_map_size(const fem_mesh* mesh, size_t* bytes);
+
+/* Builds the map from row_ptr / col_idx as fem_assemble returned them for this
+ * mesh's connectivity. A block missing from the pattern raises
+ * FEM_ERR_INTERNAL, a bad node id FEM_ERR_BAD_MESH (fem_scatter_map_read_info).
+ * Asynchronous. */
+FEM_API fem_status fem_scatter_map_build(const fem_mesh* mesh, const int32_t* row_ptr, const int32_t* col_idx,
+                                         void* map, size_t map_bytes, void* stream);
+
+/* values[0, nnz) = the assembled FP64 values of the mesh's current
+ * coordinates and materials, in the pattern the map was built for (zeroed,
+ * then every element block added). opts->precision as fem_alls_scatter.
+ * Values are not bitwise reproducible run to run (atomic order). Asynchronous. */
+FEM_API fem_status fem_reassemble_values(const fem_mesh* mesh, const fem_opts* opts, const void* map,
+                                         size_t map_bytes, const int32_t* row_ptr, double* values, int64_t nnz,
+                                         void* stream);
+
+/* Most severe status of the last map build or re-assembly (synchronizes). */
+FEM_API fem_status fem_scatter_map_read_info(const void* map, void* stream);
+
 /* ---- element-colouring baseline ----------------------------------------------
  * The comparison baseline of the A-LLS path: elements are coloured so that no
  * two elements of one colour share a node, then each colour is assembled
