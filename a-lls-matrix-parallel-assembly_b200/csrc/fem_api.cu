@@ -307,6 +307,96 @@ fem_status fem_element_stiffness(const fem_mesh* mesh, const fem_opts* opts, dou
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Batched assembly
+// ---------------------------------------------------------------------------
+
+namespace {
+
+int batch_slots(int n, int concurrency) {
+    int k = concurrency > 0 ? concurrency : 4;
+    k = std::min(k, kMaxBatchConcurrency);
+    return std::max(1, std::min(k, n));
+}
+
+// Workspace offset of each slot (bytes), sized for the largest mesh of the slot.
+fem_status batch_layout(const fem_mesh* meshes, int n, const fem_opts* opts, int slots, std::vector<int>& slot_of,
+                        std::vector<size_t>& slot_off, size_t& total) {
+    slot_of = batch_schedule(meshes, n, slots);
+    std::vector<size_t> need(slots, 0);
+    for (int i = 0; i < n; i++) {
+        size_t b = 0;
+        fem_status st = fem_alls_workspace_size(&meshes[i], opts, &b);
+        if (st) return st;
+        need[slot_of[i]] = std::max(need[slot_of[i]], b);
+    }
+    slot_off.assign(slots, 0);
+    total = 0;
+    for (int k = 0; k < slots; k++) {
+        slot_off[k] = total;
+        total += align_up(need[k]);
+    }
+    return FEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fem_status fem_batched_workspace_size(const fem_mesh* meshes, int32_t n, const fem_opts* opts, int32_t concurrency,
+                                      size_t* bytes) {
+    if (!meshes || n <= 0 || !bytes) return FEM_ERR_BAD_ARG;
+    std::vector<int> slot_of;
+    std::vector<size_t> slot_off;
+    return batch_layout(meshes, n, opts, batch_slots(n, concurrency), slot_of, slot_off, *bytes);
+}
+
+fem_status fem_assemble_batched(const fem_mesh* meshes, int32_t n, const fem_opts* opts, int32_t concurrency,
+                                void* workspace, size_t workspace_bytes, fem_csr* outs, fem_info* infos,
+                                unsigned long long* stamps, void* stream) {
+    if (!meshes || n <= 0 || !outs || !infos) return FEM_ERR_BAD_ARG;
+    const int slots = batch_slots(n, concurrency);
+    std::vector<int> slot_of;
+    std::vector<size_t> slot_off;
+    size_t total = 0;
+    fem_status st = batch_layout(meshes, n, opts, slots, slot_of, slot_off, total);
+    if (st) return st;
+    if (!workspace || workspace_bytes < total || reinterpret_cast<uintptr_t>(workspace) % kAlign)
+        return FEM_ERR_WORKSPACE;
+    for (int i = 0; i < n; i++)
+        if (!outs[i].row_ptr || outs[i].capacity < 0 || (outs[i].capacity > 0 && (!outs[i].col_idx || !outs[i].values)))
+            return FEM_ERR_BAD_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t err = stamps ? launch_stamp(stamps, s) : cudaSuccess;
+    cudaStream_t ss[kMaxBatchConcurrency];
+    if (!err) err = batch_fork(slots, s, ss);
+    if (err) return cuda_fail(err);
+    // each slot: its meshes smallest first (the slots were filled largest first
+    // for balance; within a slot the shortest jobs go first, which lowers the
+    // meshes' completion times without changing the slot's total)
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return batch_cost(meshes[a]) < batch_cost(meshes[b]); });
+    unsigned char* base = static_cast<unsigned char*>(workspace);
+    for (int i : order) {
+        const int k = slot_of[i];
+        void* ws = base + slot_off[k];
+        const size_t wsb = (k + 1 < slots ? slot_off[k + 1] : total) - slot_off[k];
+        if ((st = fem_alls_scatter(&meshes[i], opts, ws, wsb, ss[k]))) return st;
+        if ((st = fem_alls_consolidate(&meshes[i], opts, ws, wsb, outs[i].row_ptr, outs[i].col_idx, outs[i].values,
+                                       outs[i].capacity, ss[k])))
+            return st;
+        err = launch_finish(static_cast<const DevInfo*>(ws), infos + i, stamps ? stamps + 1 + i : nullptr, ss[k]);
+        if (err) return cuda_fail(err);
+        outs[i].n_rows = meshes[i].num_nodes * kind_dpn(meshes[i].kind);
+    }
+    err = batch_join(slots, s);
+    return err ? cuda_fail(err) : FEM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
 // Value-only re-assembly through a scatter map
 // ---------------------------------------------------------------------------
 

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "fem_internal.cuh"
 
 namespace fem {
@@ -65,6 +67,18 @@ cudaError_t launch_reorder_3d(const MeshView& m, int* hist, int* ranges, int* pe
 cudaError_t launch_consolidate(const ListLayout& L, int dpn, int* row_ptr, int* col_idx, double* values,
                                long long capacity, long long* tile_sums, int num_tiles, cudaStream_t s);
 cudaError_t launch_info_init(DevInfo* info, int pool_chunks, cudaStream_t s);
+
+// ---- batched assembly (batched.cu) ----
+constexpr int kMaxBatchConcurrency = 16;
+// Estimated work of a mesh (elements weighted by kind) and the slot of each
+// mesh (largest first onto the least loaded slot).
+double batch_cost(const fem_mesh& m);
+std::vector<int> batch_schedule(const fem_mesh* meshes, int n, int slots);
+// The slots' library streams wait for the caller's stream / the caller's stream waits for them.
+cudaError_t batch_fork(int slots, cudaStream_t s, cudaStream_t* out_streams);
+cudaError_t batch_join(int slots, cudaStream_t s);
+cudaError_t launch_stamp(unsigned long long* out, cudaStream_t s);
+cudaError_t launch_finish(const DevInfo* info, fem_info* dst, unsigned long long* stamp, cudaStream_t s);
 
 // ---- element-colouring baseline (colour.cu) ----
 constexpr int kMaxColours = 64;         // colours per mesh (a 64-bit mask of neighbour colours)

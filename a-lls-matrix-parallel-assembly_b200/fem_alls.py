@@ -36,7 +36,8 @@ EXPORTS = ["fem_alls_workspace_size", "fem_alls_scatter", "fem_alls_consolidate"
            "fem_assemble_host", "fem_status_string", "fem_last_cuda_error", "fem_abi_version",
            "fem_assemble_static", "fem_colour_workspace_size", "fem_colour_prepare", "fem_colour_assemble",
            "fem_colour_read_info", "fem_element_stiffness_size", "fem_element_stiffness",
-           "fem_scatter_map_size", "fem_scatter_map_build", "fem_reassemble_values", "fem_scatter_map_read_info"]
+           "fem_scatter_map_size", "fem_scatter_map_build", "fem_reassemble_values", "fem_scatter_map_read_info",
+           "fem_batched_workspace_size", "fem_assemble_batched"]
 STATIC_WORKSPACE_BYTES = 32 << 20  # FEM_STATIC_WORKSPACE_BYTES
 
 
@@ -107,6 +108,9 @@ def load() -> C.CDLL:
         L.fem_scatter_map_build.argtypes = [p(FemMesh), vp, vp, vp, C.c_size_t, vp]
         L.fem_reassemble_values.argtypes = [p(FemMesh), p(FemOpts), vp, C.c_size_t, vp, vp, C.c_int64, vp]
         L.fem_scatter_map_read_info.argtypes = [vp, vp]
+        L.fem_batched_workspace_size.argtypes = [p(FemMesh), C.c_int32, p(FemOpts), C.c_int32, p(C.c_size_t)]
+        L.fem_assemble_batched.argtypes = [p(FemMesh), C.c_int32, p(FemOpts), C.c_int32, vp, C.c_size_t, p(FemCsr),
+                                           vp, vp, vp]
         L.fem_status_string.argtypes = [C.c_int32]
         L.fem_status_string.restype = C.c_char_p
         for f in EXPORTS:
@@ -386,3 +390,92 @@ class Reassembler:
 
     def read_info(self) -> int:
         return self.lib.fem_scatter_map_read_info(self.map_ptr, self._stream())
+
+
+class Batch:
+    """Batched assembly of many meshes (fem_assemble_batched) with device-resident
+    inputs, workspace and outputs. sizes() runs a counting pass (capacity 0) to
+    size the CSR outputs; run() assembles; results(i) returns mesh i's CSR."""
+
+    def __init__(self, meshes, o: Optional[FemOpts] = None, concurrency: int = 4, device="cuda"):
+        import torch
+        self.torch = torch
+        self.meshes = meshes
+        self.opts = o
+        self.concurrency = concurrency
+        self.device = device
+        self.lib = load()
+        self.dev = [device_arrays(m, device) for m in meshes]
+        n = len(meshes)
+        self.cm = (FemMesh * n)(*[fem_mesh_struct(m, d) for m, d in zip(meshes, self.dev)])
+        need = 0
+        for k in sorted({1, concurrency}):   # the workspace serves every concurrency up to this one
+            b = C.c_size_t(0)
+            check(self.lib.fem_batched_workspace_size(self.cm, n, C.byref(o) if o else None, k, C.byref(b)),
+                  "fem_batched_workspace_size")
+            need = max(need, b.value)
+        self.ws_bytes = need
+        self.ws = torch.empty(self.ws_bytes + 256, dtype=torch.uint8, device=device)
+        self.ws_ptr = (self.ws.data_ptr() + 255) // 256 * 256
+        self.row_ptr = [torch.empty(m.num_dofs + 1, dtype=torch.int32, device=device) for m in meshes]
+        self.col_idx = [None] * n
+        self.values = [None] * n
+        self.infos = torch.zeros((n, C.sizeof(FemInfo) // 8), dtype=torch.int64, device=device)
+        self.stamps = torch.zeros(n + 1, dtype=torch.int64, device=device)
+        self.outs = (FemCsr * n)()
+        self._set_outs(capacity=False)
+
+    def _set_outs(self, capacity: bool):
+        for i, m in enumerate(self.meshes):
+            cap = int(self.col_idx[i].numel()) if capacity and self.col_idx[i] is not None else 0
+            self.outs[i] = FemCsr(m.num_dofs, 0, 0, cap, _ptr(self.row_ptr[i]),
+                                  _ptr(self.col_idx[i]) if cap else None, _ptr(self.values[i]) if cap else None)
+
+    def workspace_bytes(self, concurrency: int) -> int:
+        b = C.c_size_t(0)
+        check(self.lib.fem_batched_workspace_size(self.cm, len(self.meshes), C.byref(self.opts) if self.opts else None,
+                                                  concurrency, C.byref(b)), "fem_batched_workspace_size")
+        return b.value
+
+    def _launch(self, concurrency: Optional[int] = None):
+        k = self.concurrency if concurrency is None else concurrency
+        check(self.lib.fem_assemble_batched(self.cm, len(self.meshes), C.byref(self.opts) if self.opts else None,
+                                            k, self.ws_ptr, self.ws_bytes, self.outs,
+                                            _ptr(self.infos), _ptr(self.stamps),
+                                            self.torch.cuda.current_stream().cuda_stream), "fem_assemble_batched")
+
+    def info(self, i: int) -> dict:
+        raw = self.infos[i].cpu().numpy().tobytes()
+        return FemInfo.from_buffer_copy(raw).as_dict()
+
+    def sizes(self):
+        """Counting pass: nnz of every mesh; allocates the CSR outputs."""
+        self._set_outs(capacity=False)
+        self._launch()
+        self.torch.cuda.synchronize()
+        nnz = []
+        for i in range(len(self.meshes)):
+            inf = self.info(i)
+            nz = int(inf["nnz"])
+            nnz.append(nz)
+            self.col_idx[i] = self.torch.empty(max(nz, 1), dtype=self.torch.int32, device=self.device)
+            self.values[i] = self.torch.empty(max(nz, 1), dtype=self.torch.float64, device=self.device)
+        self._set_outs(capacity=True)
+        return nnz
+
+    def run(self, concurrency: Optional[int] = None):
+        self._launch(concurrency)
+
+    def statuses(self) -> list:
+        raw = self.infos.cpu().numpy()
+        return [int(FemInfo.from_buffer_copy(r.tobytes()).status_bits) for r in raw]
+
+    def latencies_ms(self):
+        """Per-mesh completion time after the batch start (GPU global timer), ms."""
+        st = self.stamps.cpu().numpy()
+        return (st[1:] - st[0]) / 1e6
+
+    def result(self, i: int):
+        nz = int(self.info(i)["nnz"])
+        return (self.row_ptr[i].cpu().numpy(), self.col_idx[i][:nz].cpu().numpy(),
+                self.values[i][:nz].cpu().numpy())

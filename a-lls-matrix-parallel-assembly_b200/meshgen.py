@@ -384,6 +384,35 @@ def min_detj(mesh: Mesh) -> float:
     return min(a, b)
 
 
+def batch_meshes(n: int = 256, *, seed: int = 5, emin: int = 1000, emax: int = 200_000,
+                 kinds=("q4", "t3", "mixed", "hex20")) -> list:
+    """The batched configuration: n independent meshes, kind drawn uniformly
+    from `kinds`, element count log-uniform over [emin, emax] (the grid is the
+    nearest box of that many elements), jitter and material distributions of
+    each kind's own generator, one seed per mesh."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        kind = kinds[int(rng.integers(len(kinds)))]
+        target = float(np.exp(rng.uniform(np.log(emin), np.log(emax))))
+        s = int(rng.integers(1 << 30))
+        if kind == "q4":
+            nx = max(1, int(round(np.sqrt(target))))
+            m = q4_grid(nx, nx, seed=s)
+        elif kind == "t3":
+            nx = max(1, int(round(np.sqrt(target / 2))))
+            m = t3_grid(nx, nx, seed=s)
+        elif kind == "mixed":
+            nx = max(1, int(round(np.sqrt(target / 1.5))))
+            m = mixed_grid(nx, nx, seed=s)
+        else:
+            nx = max(1, int(round(np.cbrt(target))))
+            m = hex20_grid(nx, seed=s)
+        m.name = f"batch{i}_{m.name}"
+        out.append(m)
+    return out
+
+
 def by_name(name: str) -> Mesh:
     """The benchmark meshes by short name ('q4', 't3', 'mixed', 'hex20') and a few
     small variants used in tests ('q4_small', ...)."""

@@ -41,6 +41,8 @@ WORKLOADS = {
     "t3": ("t3_1000x1000", "T3 1000x1000 grid, random diagonals, jitter 0.2h, shuffled, E~LogNormal(0,0.5), nu=0.3"),
     "mixed": ("mixed_1500x1500", "Q4+T3 1500x1500 grid (p_Q4=0.5), jitter 0.15h, shuffled, E~LogNormal(0,0.5), nu~U[0.2,0.4]"),
     "hex20": ("hex20_64x64x64", "Hex20 64^3 compact serendipity mesh, jitter 0.05h, E=1, nu=0.3, 3x3x3 Gauss"),
+    "batched": ("batched_256", "256 independent meshes, kind uniform over {Q4, T3, mixed, Hex20}, elements "
+                "log-uniform over 1k-200k, each kind's jitter and material distributions"),
 }
 # A smaller instance of each workload's generator, for the CPU legs.
 CPU_SAMPLES = {"q4": ("q4", {}), "t3": ("t3", {"nx": 400, "ny": 400}),
@@ -177,11 +179,111 @@ def cpu_baseline(workload: str, use_reference: bool, workers: int) -> dict:
 # GPU leg
 # ---------------------------------------------------------------------------
 
+def run_batched(args, rank: int, world: int, local_rank: int):
+    """The batched configuration: 256 meshes assembled by fem_assemble_batched
+    (one call per step, graph-captured), concurrency picked by timing 1/4/8
+    slots; concurrency 1 is the sequential baseline (the same per-mesh launches
+    one after another on one stream). value = elements/s of the whole batch."""
+    import torch
+    import fem_alls as fem
+    import meshgen as mg
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    name, desc = WORKLOADS["batched"]
+    t0 = time.perf_counter()
+    meshes = mg.batch_meshes(256, seed=5 + rank)
+    gen_s = time.perf_counter() - t0
+    elems = sum(m.num_elems for m in meshes)
+    slots = (1, 4, 8)
+    b = fem.Batch(meshes, concurrency=max(slots), device=dev)
+    nnz = b.sizes()
+    flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, steps):
+        ts = []
+        for _ in range(steps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            z = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            z.record(stream)
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(z))
+        return ts
+
+    per_k = {}
+    for k in slots:
+        for _ in range(args.warmup):
+            b.run(k)
+        torch.cuda.synchronize()
+        ts = timed(lambda: b.run(k), args.steps)
+        lat = b.latencies_ms()
+        per_k[k] = {"ms": statistics.mean(ts), "p50_ms": float(np.percentile(lat, 50)),
+                    "p99_ms": float(np.percentile(lat, 99))}
+    best = min((k for k in slots if k > 1), key=lambda k: per_k[k]["ms"])
+    # the chosen concurrency captured in a CUDA graph and replayed
+    side = torch.cuda.Stream()
+    side.wait_stream(stream)
+    with torch.cuda.stream(side):
+        b.run(best)
+    stream.wait_stream(side)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        b.run(best)
+    for _ in range(args.warmup):
+        g.replay()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    with ClockSampler(local_rank) as clk:
+        ts = timed(g.replay, args.steps)
+    st = b.statuses()
+    bad = [i for i, v in enumerate(st) if v & ~(1 << 4)]
+    if bad:
+        raise RuntimeError(f"batched assembly: status bits {st[bad[0]]} on mesh {bad[0]}")
+    lat = b.latencies_ms()
+    tot = torch.tensor([sum(ts)], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(tot, op=torch.distributed.ReduceOp.MAX)
+    ms = float(tot.item()) / args.steps
+    if rank != 0:
+        return
+    seq = per_k[1]
+    line = {
+        "metric": "elements/s (device FP64 A-LLS assembly: element stiffness, list scatter, CSR pattern + values)",
+        "value": world * elems / (ms / 1e3), "unit": "elements/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded mesh generator)",
+        "config": {"workload": name, "description": desc, "meshes": len(meshes), "elements": elems,
+                   "nnz": int(sum(nnz)), "kinds": {k: sum(1 for m in meshes if m.kind == k) for k in range(4)},
+                   "l2": "2x L2 buffer zeroed between steps, outside the per-step events",
+                   "parallelism": f"replicas{world}", "mesh_generation_s": gen_s},
+        "meshes_per_s": world * len(meshes) / (ms / 1e3),
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "what": "per-mesh completion after the batch start (GPU global timer), graph replay"},
+        "concurrency": {"chosen": best, "timed": {str(k): v for k, v in per_k.items()}},
+        "sequential": {"ms": seq["ms"], "meshes_per_s": len(meshes) / (seq["ms"] / 1e3),
+                       "p50_ms": seq["p50_ms"], "p99_ms": seq["p99_ms"],
+                       "what": "the 256 meshes' launches one after another on one stream (concurrency 1)"},
+        "speedup_vs_sequential": seq["ms"] / ms,
+        "clocks": clk.summary(),
+        "gpu_launches": None,
+        "api": "fem_assemble_batched, captured in one CUDA graph",
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import torch
     import fem_alls as fem
     import build
     build.build()
+    if args.workload == "batched":
+        run_batched(args, rank, world, local_rank)
+        return
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     name, desc = WORKLOADS[args.workload]

@@ -188,6 +188,30 @@ FEM_API fem_status fem_element_stiffness_size(const fem_mesh* mesh, int64_t* dou
 FEM_API fem_status fem_element_stiffness(const fem_mesh* mesh, const fem_opts* opts, double* ke_out,
                                          int32_t* status, void* stream);
 
+/* ---- batched assembly -------------------------------------------------------
+ * Many independent meshes (any element kinds, uneven sizes) in one
+ * stream-ordered call; the reference assembles one mesh per program run
+ * (its drivers' main, e.g. ALLS_Q4_T3_Mixed_Elements_Assembly_Performance.cu:742-854).
+ * The meshes are dealt (largest first, to the least loaded) to `concurrency`
+ * workspace slots (0 = 4, at most 16); each slot assembles its meshes one after
+ * another, smallest first, on a library stream that forks from and joins
+ * `stream`, so slots run side by side and the whole call can be captured into a
+ * CUDA graph (make one uncaptured call first: it creates the library streams). */
+
+/* Bytes of workspace for this batch (the slots are sized for their largest mesh). */
+FEM_API fem_status fem_batched_workspace_size(const fem_mesh* meshes, int32_t n, const fem_opts* opts,
+                                              int32_t concurrency, size_t* bytes);
+
+/* Assembles meshes[0..n) into outs[0..n) (caller's device buffers, as for
+ * fem_alls_consolidate: a mesh whose capacity is below its nnz gets only
+ * row_ptr and FEM_ERR_CAPACITY in its info). infos: DEVICE array [n] that
+ * receives each mesh's fem_info (nnz, status bits, ...). stamps: optional
+ * DEVICE array [n + 1] of GPU global-timer nanoseconds: stamps[0] at the start,
+ * stamps[1 + i] when mesh i is done. outs[i].n_rows is set. Asynchronous. */
+FEM_API fem_status fem_assemble_batched(const fem_mesh* meshes, int32_t n, const fem_opts* opts,
+                                        int32_t concurrency, void* workspace, size_t workspace_bytes,
+                                        fem_csr* outs, fem_info* infos, unsigned long long* stamps, void* stream);
+
 /* ---- value-only re-assembly through a scatter map ----------------------------
  * For a mesh whose connectivity is unchanged between assemblies (new
  * coordinates, E or nu: nonlinear and time-stepping solvers). The reference
