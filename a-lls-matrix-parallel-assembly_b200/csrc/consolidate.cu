@@ -19,7 +19,9 @@
 //                  consecutive entries. Rows longer than the group's sort
 //                  capacity take an exact slow path.
 // Every dof row of node n holds {c*dpn + b : c in adj(n)} in increasing order,
-// which is the reference's pattern.
+// which is the reference's pattern. The same pass can write the node-block
+// (BSR) form instead: one block row per node, the sorted column nodes and
+// their dpn x dpn blocks.
 #include <algorithm>
 
 #include "launch.h"
@@ -58,7 +60,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int* __restr
 // Exclusive scan of the tile sums in place (one CTA), nnz, last row_ptr entry.
 __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(long long* __restrict__ tile_sums, int num_tiles,
                                                              DevInfo* info, int* __restrict__ row_ptr_end,
-                                                             long long capacity) {
+                                                             long long capacity, int end_div) {
     __shared__ long long s_warp[kScanThreads / 32 + 1];
     long long carry = 0;
     for (int base = 0; base < num_tiles; base += kScanThreads) {
@@ -71,14 +73,15 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(long long* __restri
     }
     if (threadIdx.x == 0) {
         info->nnz = carry;
-        *row_ptr_end = (int)carry;
+        *row_ptr_end = (int)(carry / end_div);
         if (carry > 0x7FFFFFFFll) raise_status(info, FEM_ERR_RANGE);
         if (carry > capacity) raise_status(info, FEM_ERR_CAPACITY);
     }
 }
 
 // row_ptr of every dof row: node n's rows start at dpn^2 * (exclusive count sum).
-template <int DPN>
+// kBsr: one block row per node, block_row_ptr[n] = exclusive count sum.
+template <int DPN, bool kBsr>
 __global__ void __launch_bounds__(kScanThreads) k_row_ptr(const int* __restrict__ counts, int N,
                                                           const long long* __restrict__ tile_offsets,
                                                           int* __restrict__ row_ptr) {
@@ -99,8 +102,12 @@ __global__ void __launch_bounds__(kScanThreads) k_row_ptr(const int* __restrict_
     for (int i = 0; i < kScanItems; i++) {
         const long long n = base + i;
         if (n < N) {
+            if (kBsr) {
+                row_ptr[n] = (int)(off / B);
+            } else {
 #pragma unroll
-            for (int a = 0; a < DPN; a++) row_ptr[n * DPN + a] = (int)(off + (long long)a * DPN * c[i]);
+                for (int a = 0; a < DPN; a++) row_ptr[n * DPN + a] = (int)(off + (long long)a * DPN * c[i]);
+            }
         }
         off += (long long)B * c[i];
     }
@@ -217,7 +224,49 @@ __device__ void long_row_write(const ListLayout& L, int n, int u, long long base
     }
 }
 
-template <int DPN, int G, int KPL>
+// Long-row slow path of the block (BSR) output: block k of the node's block row.
+template <int DPN, int G>
+__device__ void long_row_write_bsr(const ListLayout& L, int n, int u, long long base, int glane, unsigned mask,
+                                   int* __restrict__ col_idx, double* __restrict__ values) {
+    constexpr int B = DPN * DPN;
+    int last = -1;
+    for (int k = 0; k < u; k++) {
+        const int col = long_row_next_col<G>(L, n, last, glane, mask);
+        last = col;
+        double sum[B];
+#pragma unroll
+        for (int v = 0; v < B; v++) sum[v] = 0.0;
+        int c = n;
+        for (int step = 0; step < kMaxChainSteps; step++) {
+            const int* meta = chunk_meta(L, c);
+            const int cap = chunk_cap(L, c);
+            const int next = __ldg(meta + 1);
+            for (int s = glane; s < cap; s += G) {
+                if ((__ldg(meta + 2 + s) & kColMask) - 1 == col) {
+                    const double* p = L.vals + (size_t)slot_gid(L, c, s) * B;
+#pragma unroll
+                    for (int v = 0; v < B; v++) sum[v] += __ldg(p + v);
+                }
+            }
+            if (next == 0) break;
+            c = next - 1;
+        }
+#pragma unroll
+        for (int v = 0; v < B; v++) {
+#pragma unroll
+            for (int d = G / 2; d > 0; d >>= 1) sum[v] += __shfl_xor_sync(mask, sum[v], d);
+        }
+        if (glane == 0) {
+            col_idx[base + k] = col;
+#pragma unroll
+            for (int v = 0; v < B; v++) values[(base + k) * B + v] = sum[v];
+        }
+    }
+}
+
+// kBsr: block (BSR) output, one block row per node: block_col_idx = column
+// node, block values dpn x dpn row-major; row_ptr is then the block row pointer.
+template <int DPN, int G, int KPL, bool kBsr>
 __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int* __restrict__ row_ptr,
                                                          int* __restrict__ col_idx, double* __restrict__ values,
                                                          long long capacity) {
@@ -237,8 +286,13 @@ __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int
         int u = 0;
         long long base = 0;
         if (valid) {
-            base = __ldg(row_ptr + (size_t)n * DPN);
-            u = (__ldg(row_ptr + (size_t)n * DPN + 1) - (int)base) / DPN;
+            if (kBsr) {
+                base = __ldg(row_ptr + n);
+                u = __ldg(row_ptr + n + 1) - (int)base;
+            } else {
+                base = __ldg(row_ptr + (size_t)n * DPN);
+                u = (__ldg(row_ptr + (size_t)n * DPN + 1) - (int)base) / DPN;
+            }
         }
         // 1. gather the non-empty slots of the node's chunk chain
         int T = 0;
@@ -278,8 +332,18 @@ __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int
 #pragma unroll
         for (int i = 0; i < KPL; i++) s_keys[grp][glane * KPL + i] = keys[i];
         __syncwarp();
-        // 3. write the dpn rows of the node
-        if (valid) {
+        // 3. write the dpn rows of the node (or its block row)
+        if (valid && kBsr) {
+            if (long_row) {
+                long_row_write_bsr<DPN, G>(L, n, u, base, glane, gmask, col_idx, values);
+            } else {
+                for (int k = glane; k < Ts; k += G) col_idx[base + k] = (int)(s_keys[grp][k] >> 32);
+                for (int idx = glane; idx < Ts * B; idx += G) {
+                    const int k = idx / B, v = idx - k * B;
+                    values[base * B + idx] = __ldg(L.vals + (size_t)(unsigned)s_keys[grp][k] * B + v);
+                }
+            }
+        } else if (valid) {
             if (long_row) {
                 long_row_write<DPN, G>(L, n, u, base, glane, gmask, col_idx, values);
             } else {
@@ -324,19 +388,21 @@ __global__ void k_consolidate_reset(DevInfo* info) {
     info->max_row_entries = 0;
 }
 
-template <int DPN, int G, int KPL>
+template <int DPN, int G, int KPL, bool kBsr>
 cudaError_t launch_all(const ListLayout& L, int* row_ptr, int* col_idx, double* values, long long capacity,
                        long long* tile_sums, int num_tiles, cudaStream_t s) {
+    // capacity is in scalar entries (BSR: blocks * dpn^2)
     k_consolidate_reset<<<1, 1, 0, s>>>(L.info);
     k_scan_reduce<DPN * DPN><<<num_tiles, kScanThreads, 0, s>>>(L.counts, L.N, tile_sums);
-    k_scan_tiles<<<1, kScanThreads, 0, s>>>(tile_sums, num_tiles, L.info, row_ptr + (size_t)L.N * DPN, capacity);
-    k_row_ptr<DPN><<<num_tiles, kScanThreads, 0, s>>>(L.counts, L.N, tile_sums, row_ptr);
+    k_scan_tiles<<<1, kScanThreads, 0, s>>>(tile_sums, num_tiles, L.info, row_ptr + (size_t)L.N * (kBsr ? 1 : DPN),
+                                            capacity, kBsr ? DPN * DPN : 1);
+    k_row_ptr<DPN, kBsr><<<num_tiles, kScanThreads, 0, s>>>(L.counts, L.N, tile_sums, row_ptr);
     if (capacity > 0) {
         constexpr int NPB = kBlockThreads / G;
         const long long batches = ((long long)L.N + NPB - 1) / NPB;
         const long long grid = std::min<long long>(batches, (long long)sm_count() * 8);
-        k_write<DPN, G, KPL><<<(int)(grid > 0 ? grid : 1), kBlockThreads, 0, s>>>(L, row_ptr, col_idx, values,
-                                                                                capacity);
+        k_write<DPN, G, KPL, kBsr><<<(int)(grid > 0 ? grid : 1), kBlockThreads, 0, s>>>(L, row_ptr, col_idx, values,
+                                                                                      capacity);
     }
     return cudaGetLastError();
 }
@@ -345,8 +411,17 @@ cudaError_t launch_all(const ListLayout& L, int* row_ptr, int* col_idx, double* 
 
 cudaError_t launch_consolidate(const ListLayout& L, int dpn, int* row_ptr, int* col_idx, double* values,
                                long long capacity, long long* tile_sums, int num_tiles, cudaStream_t s) {
-    if (dpn == 3) return launch_all<3, 32, 4>(L, row_ptr, col_idx, values, capacity, tile_sums, num_tiles, s);
-    return launch_all<2, 8, 2>(L, row_ptr, col_idx, values, capacity, tile_sums, num_tiles, s);
+    if (dpn == 3) return launch_all<3, 32, 4, false>(L, row_ptr, col_idx, values, capacity, tile_sums, num_tiles, s);
+    return launch_all<2, 8, 2, false>(L, row_ptr, col_idx, values, capacity, tile_sums, num_tiles, s);
+}
+
+cudaError_t launch_consolidate_bsr(const ListLayout& L, int dpn, int* block_row_ptr, int* block_col_idx,
+                                   double* block_values, long long capacity_blocks, long long* tile_sums,
+                                   int num_tiles, cudaStream_t s) {
+    const long long cap = capacity_blocks * dpn * dpn;
+    if (dpn == 3)
+        return launch_all<3, 32, 4, true>(L, block_row_ptr, block_col_idx, block_values, cap, tile_sums, num_tiles, s);
+    return launch_all<2, 8, 2, true>(L, block_row_ptr, block_col_idx, block_values, cap, tile_sums, num_tiles, s);
 }
 
 cudaError_t launch_info_init(DevInfo* info, int pool_chunks, cudaStream_t s) {

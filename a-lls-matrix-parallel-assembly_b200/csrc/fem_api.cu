@@ -243,6 +243,23 @@ fem_status fem_alls_consolidate(const fem_mesh* mesh, const fem_opts* opts, void
     return err ? cuda_fail(err) : FEM_OK;
 }
 
+fem_status fem_alls_consolidate_bsr(const fem_mesh* mesh, const fem_opts* opts, void* workspace,
+                                    size_t workspace_bytes, int32_t* block_row_ptr, int32_t* block_col_idx,
+                                    double* block_values, int64_t capacity_blocks, void* stream) {
+    HostLayout h;
+    fem_status st = make_layout(mesh, opts, h);
+    if (st) return st;
+    if ((st = check_ws(h, workspace, workspace_bytes))) return st;
+    if (!block_row_ptr || capacity_blocks < 0 || (capacity_blocks > 0 && (!block_col_idx || !block_values)))
+        return FEM_ERR_BAD_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    ListLayout L = device_layout(h, workspace);
+    long long* tiles = reinterpret_cast<long long*>(static_cast<unsigned char*>(workspace) + h.off_tiles);
+    cudaError_t err = launch_consolidate_bsr(L, h.dpn, block_row_ptr, block_col_idx, block_values, capacity_blocks,
+                                             tiles, h.num_tiles, s);
+    return err ? cuda_fail(err) : FEM_OK;
+}
+
 fem_status fem_alls_read_info(const void* workspace, fem_info* info, void* stream) {
     if (!workspace || !info) return FEM_ERR_BAD_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);

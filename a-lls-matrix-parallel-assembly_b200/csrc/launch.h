@@ -66,6 +66,10 @@ cudaError_t launch_reorder_3d(const MeshView& m, int* hist, int* ranges, int* pe
                               cudaStream_t s);
 cudaError_t launch_consolidate(const ListLayout& L, int dpn, int* row_ptr, int* col_idx, double* values,
                                long long capacity, long long* tile_sums, int num_tiles, cudaStream_t s);
+// Node-block (BSR) form of the consolidation; capacity in blocks.
+cudaError_t launch_consolidate_bsr(const ListLayout& L, int dpn, int* block_row_ptr, int* block_col_idx,
+                                   double* block_values, long long capacity_blocks, long long* tile_sums,
+                                   int num_tiles, cudaStream_t s);
 cudaError_t launch_info_init(DevInfo* info, int pool_chunks, cudaStream_t s);
 
 // ---- batched assembly (batched.cu) ----

@@ -37,7 +37,7 @@ EXPORTS = ["fem_alls_workspace_size", "fem_alls_scatter", "fem_alls_consolidate"
            "fem_assemble_static", "fem_colour_workspace_size", "fem_colour_prepare", "fem_colour_assemble",
            "fem_colour_read_info", "fem_element_stiffness_size", "fem_element_stiffness",
            "fem_scatter_map_size", "fem_scatter_map_build", "fem_reassemble_values", "fem_scatter_map_read_info",
-           "fem_batched_workspace_size", "fem_assemble_batched"]
+           "fem_batched_workspace_size", "fem_assemble_batched", "fem_alls_consolidate_bsr"]
 STATIC_WORKSPACE_BYTES = 32 << 20  # FEM_STATIC_WORKSPACE_BYTES
 
 
@@ -111,6 +111,7 @@ def load() -> C.CDLL:
         L.fem_batched_workspace_size.argtypes = [p(FemMesh), C.c_int32, p(FemOpts), C.c_int32, p(C.c_size_t)]
         L.fem_assemble_batched.argtypes = [p(FemMesh), C.c_int32, p(FemOpts), C.c_int32, vp, C.c_size_t, p(FemCsr),
                                            vp, vp, vp]
+        L.fem_alls_consolidate_bsr.argtypes = [p(FemMesh), p(FemOpts), vp, C.c_size_t, vp, vp, vp, C.c_int64, vp]
         L.fem_status_string.argtypes = [C.c_int32]
         L.fem_status_string.restype = C.c_char_p
         for f in EXPORTS:
@@ -220,6 +221,20 @@ class Assembler:
                                             _ptr(self.row_ptr), _ptr(self.col_idx) if cap else None,
                                             _ptr(self.values) if cap else None, cap, self._stream()),
               "fem_alls_consolidate")
+
+    def consolidate_bsr(self):
+        """Node-block (BSR) form of the last scatter: (block_row_ptr, block_col_idx, block_values) tensors."""
+        torch = self.torch
+        st, info = self.read_info()
+        nb = int(info.nnz) // (self.mesh.dpn ** 2) if info.nnz else 0
+        brp = torch.empty(self.mesh.num_nodes + 1, dtype=torch.int32, device=self.row_ptr.device)
+        bci = torch.empty(max(nb, 1), dtype=torch.int32, device=self.row_ptr.device)
+        bv = torch.empty(max(nb, 1) * self.mesh.dpn ** 2, dtype=torch.float64, device=self.row_ptr.device)
+        check(self.lib.fem_alls_consolidate_bsr(C.byref(self.cm), C.byref(self.opts), self.ws_ptr, self.ws_bytes,
+                                                _ptr(brp), _ptr(bci), _ptr(bv), nb, self._stream()),
+              "fem_alls_consolidate_bsr")
+        check(self.read_info()[0], "bsr consolidation")
+        return brp, bci[:nb], bv[: nb * self.mesh.dpn ** 2]
 
     def read_info(self) -> tuple:
         info = FemInfo()

@@ -151,6 +151,19 @@ FEM_API fem_status fem_alls_consolidate(const fem_mesh* mesh, const fem_opts* op
                                 size_t workspace_bytes, int32_t* row_ptr, int32_t* col_idx,
                                 double* values, int64_t capacity, void* stream);
 
+/* The node-block (BSR) form of fem_alls_consolidate, for solvers that work on
+ * dof_per_node^2 blocks (no counterpart in the reference, whose output is
+ * scalar CSR only): one block row per node, block_row_ptr [num_nodes + 1],
+ * block_col_idx [nnz / dpn^2] (column nodes, sorted within each block row),
+ * block_values [nnz] (each block dpn x dpn row-major: entry (i, j) of block
+ * (n, m) is K[n*dpn + i][m*dpn + j]). It holds exactly the entries of the CSR
+ * form; the info word's nnz stays in scalar entries. If capacity_blocks is
+ * below the block count nothing but block_row_ptr is written and the info gets
+ * FEM_ERR_CAPACITY. Asynchronous. */
+FEM_API fem_status fem_alls_consolidate_bsr(const fem_mesh* mesh, const fem_opts* opts, void* workspace,
+                                            size_t workspace_bytes, int32_t* block_row_ptr, int32_t* block_col_idx,
+                                            double* block_values, int64_t capacity_blocks, void* stream);
+
 /* Copies the device info word of the last assembly to the host (synchronizes
  * the stream) and returns the most severe status it holds. */
 FEM_API fem_status fem_alls_read_info(const void* workspace, fem_info* info, void* stream);
