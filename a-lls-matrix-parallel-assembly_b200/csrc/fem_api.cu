@@ -324,6 +324,37 @@ fem_status fem_element_stiffness(const fem_mesh* mesh, const fem_opts* opts, dou
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Load vector and boundary conditions
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+fem_status fem_assemble_body_force(const fem_mesh* mesh, const double* body_force, const double* b0, double* f,
+                                   int32_t* status, void* stream) {
+    fem_status st = check_mesh(mesh);
+    if (st) return st;
+    if (!f || !status || (!body_force && !b0)) return FEM_ERR_BAD_ARG;
+    const int dim = mesh->kind == FEM_HEX20 ? 3 : 2;
+    double b[3] = {0.0, 0.0, 0.0};
+    if (!body_force)
+        for (int d = 0; d < dim; d++) b[d] = b0[d];
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t err = cudaMemsetAsync(status, 0, sizeof(int32_t), s);
+    if (!err) err = launch_body_force(mesh_view(mesh), mesh->kind, body_force, b, f, status, s);
+    return err ? cuda_fail(err) : FEM_OK;
+}
+
+fem_status fem_apply_dirichlet(int32_t n_rows, const int32_t* row_ptr, const int32_t* col_idx, double* values,
+                               double* f, const uint8_t* fixed, const double* u, void* stream) {
+    if (n_rows < 0 || (n_rows > 0 && (!row_ptr || !col_idx || !values || !fixed || !u))) return FEM_ERR_BAD_ARG;
+    cudaError_t err =
+        launch_dirichlet(n_rows, row_ptr, col_idx, values, f, fixed, u, static_cast<cudaStream_t>(stream));
+    return err ? cuda_fail(err) : FEM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
 // Batched assembly
 // ---------------------------------------------------------------------------
 

@@ -72,6 +72,14 @@ cudaError_t launch_consolidate_bsr(const ListLayout& L, int dpn, int* block_row_
                                    int num_tiles, cudaStream_t s);
 cudaError_t launch_info_init(DevInfo* info, int pool_chunks, cudaStream_t s);
 
+// ---- load vector and boundary conditions (loads.cu) ----
+// f += body-force load vector (b: device [E * dim] or NULL for the uniform b0[dim], host values).
+cudaError_t launch_body_force(const MeshView& m, int kind, const double* b, const double* b0, double* f, int* status,
+                              cudaStream_t s);
+// Symmetric elimination of fixed dofs in place on a CSR matrix (and f).
+cudaError_t launch_dirichlet(int n_rows, const int* row_ptr, const int* col_idx, double* values, double* f,
+                             const unsigned char* fixed, const double* u, cudaStream_t s);
+
 // ---- batched assembly (batched.cu) ----
 constexpr int kMaxBatchConcurrency = 16;
 // Estimated work of a mesh (elements weighted by kind) and the slot of each

@@ -37,7 +37,8 @@ EXPORTS = ["fem_alls_workspace_size", "fem_alls_scatter", "fem_alls_consolidate"
            "fem_assemble_static", "fem_colour_workspace_size", "fem_colour_prepare", "fem_colour_assemble",
            "fem_colour_read_info", "fem_element_stiffness_size", "fem_element_stiffness",
            "fem_scatter_map_size", "fem_scatter_map_build", "fem_reassemble_values", "fem_scatter_map_read_info",
-           "fem_batched_workspace_size", "fem_assemble_batched", "fem_alls_consolidate_bsr"]
+           "fem_batched_workspace_size", "fem_assemble_batched", "fem_alls_consolidate_bsr",
+           "fem_assemble_body_force", "fem_apply_dirichlet"]
 STATIC_WORKSPACE_BYTES = 32 << 20  # FEM_STATIC_WORKSPACE_BYTES
 
 
@@ -112,6 +113,8 @@ def load() -> C.CDLL:
         L.fem_assemble_batched.argtypes = [p(FemMesh), C.c_int32, p(FemOpts), C.c_int32, vp, C.c_size_t, p(FemCsr),
                                            vp, vp, vp]
         L.fem_alls_consolidate_bsr.argtypes = [p(FemMesh), p(FemOpts), vp, C.c_size_t, vp, vp, vp, C.c_int64, vp]
+        L.fem_assemble_body_force.argtypes = [p(FemMesh), vp, vp, vp, vp, vp]
+        L.fem_apply_dirichlet.argtypes = [C.c_int32, vp, vp, vp, vp, vp, vp, vp]
         L.fem_status_string.argtypes = [C.c_int32]
         L.fem_status_string.restype = C.c_char_p
         for f in EXPORTS:
@@ -494,3 +497,32 @@ class Batch:
         nz = int(self.info(i)["nnz"])
         return (self.row_ptr[i].cpu().numpy(), self.col_idx[i][:nz].cpu().numpy(),
                 self.values[i][:nz].cpu().numpy())
+
+
+def body_force(mesh, b, dev_arrays=None, device="cuda"):
+    """Load vector of a body force (fem_assemble_body_force). b: a per-element
+    [num_elems, dim] numpy array, or a uniform length-dim sequence. Returns
+    (f tensor [ndof], status bits)."""
+    import torch
+    dev = dev_arrays if dev_arrays is not None else device_arrays(mesh, device)
+    cm = fem_mesh_struct(mesh, dev)
+    f = torch.zeros(mesh.num_dofs, dtype=torch.float64, device=device)
+    status = torch.zeros(1, dtype=torch.int32, device=device)
+    b = np.asarray(b, np.float64)
+    if b.ndim == 2:
+        bd = torch.from_numpy(np.ascontiguousarray(b)).to(device)
+        args = (_ptr(bd), None)
+    else:
+        b0 = np.ascontiguousarray(b)
+        args = (None, b0.ctypes.data)
+    check(load().fem_assemble_body_force(C.byref(cm), args[0], args[1], _ptr(f), _ptr(status),
+                                         torch.cuda.current_stream().cuda_stream), "fem_assemble_body_force")
+    return f, int(status.item())
+
+
+def apply_dirichlet(row_ptr, col_idx, values, f, fixed, u):
+    """Symmetric elimination of the fixed dofs in place (fem_apply_dirichlet); all device tensors."""
+    import torch
+    check(load().fem_apply_dirichlet(int(row_ptr.numel() - 1), _ptr(row_ptr), _ptr(col_idx), _ptr(values),
+                                     _ptr(f) if f is not None else None, _ptr(fixed), _ptr(u),
+                                     torch.cuda.current_stream().cuda_stream), "fem_apply_dirichlet")

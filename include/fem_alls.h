@@ -201,6 +201,29 @@ FEM_API fem_status fem_element_stiffness_size(const fem_mesh* mesh, int64_t* dou
 FEM_API fem_status fem_element_stiffness(const fem_mesh* mesh, const fem_opts* opts, double* ke_out,
                                          int32_t* status, void* stream);
 
+/* ---- load vector and boundary conditions -------------------------------------
+ * The steps after the assembled matrix (no counterpart in the reference, which
+ * stops at the stiffness values). */
+
+/* f[ndof] += the body-force load vector: for every element node a, the
+ * integral of N_a b over the element (T3 one point, Q4 2x2, Hex20 3x3x3 Gauss;
+ * 2-D kinds per area times the thickness). body_force: DEVICE [num_elems * dim]
+ * force per volume (per area in 2-D), or NULL for the uniform b0 (HOST [dim]).
+ * status: a device int32, zeroed, then (1 << FEM_ERR_*) bits (BAD_MESH: the
+ * element is skipped; DETJ). FP64 atomics, asynchronous. */
+FEM_API fem_status fem_assemble_body_force(const fem_mesh* mesh, const double* body_force, const double* b0,
+                                           double* f, int32_t* status, void* stream);
+
+/* Dirichlet conditions by symmetric elimination, in place on a CSR matrix and
+ * its right-hand side (all DEVICE arrays): for every entry K_jc of a free row j
+ * and a fixed column c, f_j -= K_jc u_c and K_jc = 0; a fixed row i keeps only
+ * K_ii = 1 and gets f_i = u_i. fixed [n_rows] (nonzero = prescribed), u
+ * [n_rows] (prescribed values, read where fixed). f may be NULL (matrix only).
+ * The pattern is unchanged and the matrix stays symmetric. Asynchronous. */
+FEM_API fem_status fem_apply_dirichlet(int32_t n_rows, const int32_t* row_ptr, const int32_t* col_idx,
+                                       double* values, double* f, const uint8_t* fixed, const double* u,
+                                       void* stream);
+
 /* ---- batched assembly -------------------------------------------------------
  * Many independent meshes (any element kinds, uneven sizes) in one
  * stream-ordered call; the reference assembles one mesh per program run
