@@ -284,6 +284,17 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if args.workload == "batched":
         run_batched(args, rank, world, local_rank)
         return
+    if args.ke_only:
+        torch.cuda.set_device(local_rank)
+        dev = torch.device("cuda", local_rank)
+        mesh = make_mesh("hex20", args.size)
+        flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device=dev)
+        line = {"workload": mesh.name, "elements": mesh.num_elems,
+                "ke_form": ke_form(fem, torch, mesh, fem.device_arrays(mesh, dev), args, flush,
+                                   torch.cuda.current_stream())}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     name, desc = WORKLOADS[args.workload]
@@ -380,6 +391,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if not args.no_colour and mesh.kind != 2:
         colour = colour_baseline(fem, torch, asm, mesh, nnz, args, flush, stream)
     reasm = None if args.no_reassembly else reassembly(fem, torch, asm, mesh, nnz, args, flush, stream)
+    kef = ke_form(fem, torch, mesh, asm.dev, args, flush, stream) if mesh.kind == 2 and not args.no_ke else None
 
     if rank != 0:
         return
@@ -432,9 +444,48 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         line["colour_baseline"] = colour
     if reasm:
         line["reassembly"] = reasm
+    if kef:
+        line["ke_form"] = kef
     if not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args.workload, use_reference=False, workers=1)
     print(json.dumps(line), flush=True)
+
+
+def ke_form(fem, torch, mesh, dev_arrays, args, flush, stream) -> dict:
+    """The Hex20 element stiffness on its own (fem_element_stiffness), plain
+    FP64 (FP64 tensor cores) and the FP16-split tensor-core form, timed alike;
+    the tensor-core values are compared with the FP64 ones per element, on the
+    scale of the element's largest diagonal entry."""
+    out = {}
+    kes = {}
+    for prec, name in ((0, "fp64"), (1, "tc_f16x3")):
+        o = fem.opts(precision=prec)
+        ke, st = fem.element_stiffness(mesh, o, dev_arrays=dev_arrays)
+        fem.check(0 if st == 0 else 1, f"element stiffness {name}")
+        for _ in range(args.warmup):
+            fem.element_stiffness(mesh, o, dev_arrays=dev_arrays, out=ke)
+        ts = []
+        for _ in range(args.steps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fem.element_stiffness(mesh, o, dev_arrays=dev_arrays, out=ke)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        out[name + "_ms"] = statistics.mean(ts)
+        kes[name] = ke
+    # diagonal entries of the packed upper blocks: block (I, I) entries 0, 4, 8
+    diag_idx = [9 * (i * 20 - i * (i - 1) // 2) + v for i in range(20) for v in (0, 4, 8)]
+    d = kes["fp64"][:, diag_idx].abs().max(dim=1).values
+    err = ((kes["tc_f16x3"] - kes["fp64"]).abs().max(dim=1).values / d).max()
+    flops = 2 * 60 * 60 * 27 * mesh.num_elems  # the node-pair contraction
+    out.update({"speedup_tc_vs_fp64": out["fp64_ms"] / out["tc_f16x3_ms"], "max_err_tc_vs_fp64": float(err),
+                "err_scale": "per element, max |difference| / the element's largest diagonal entry",
+                "contraction_gflop": flops / 1e9, "bytes_written": int(kes["fp64"].numel() * 8),
+                "what": "fem_element_stiffness: packed symmetric Ke (210 3x3 blocks, 15.1 KB) of every element"})
+    return out
 
 
 def reassembly(fem, torch, asm, mesh, nnz, args, flush, stream) -> dict:
@@ -571,6 +622,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-colour", action="store_true", help="skip the element-colouring baseline leg")
     ap.add_argument("--no-reassembly", action="store_true", help="skip the value-only re-assembly leg")
+    ap.add_argument("--no-ke", action="store_true", help="skip the Hex20 element-stiffness (Ke form) leg")
+    ap.add_argument("--ke-only", action="store_true",
+                    help="Hex20: time only the element-stiffness kernels (FP64 and tensor-core forms)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
