@@ -12,9 +12,9 @@
 // symmetric 64x64x28 FP64 matrix product per element, computed on the FP64
 // tensor cores with mma.sync.m8n8k4.f64 (36 upper 8x8 tiles x 7 k-steps), or
 // with FEM_PREC_TC_F16X3 on the FP16 tensor cores from split operands
-// (tc_prepare / tc_contract); each upper entry is written to both of its
-// places in M (so every Ke is exactly symmetric), in the shared memory the
-// gradients occupied. Ke blocks are formed from M per scattered row. The
+// (tc_prepare / tc_contract); only the 210 upper 3x3 node blocks of M are kept
+// (so every Ke is exactly symmetric), in the shared memory the gradients
+// occupied. Ke blocks are formed from M per scattered row. The
 // Gauss-point shape derivatives (ALLS_Hex20_3D_Assembly_Performance.cu:95-128)
 // are tabulated once per CTA.
 //
@@ -42,7 +42,6 @@ constexpr int kThreads = 320;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxHex20Words = 96;   // chunk meta rows of at most 96 words (S <= 94, checked on the host)
 constexpr int PS = 28;               // row stride of P (doubles): conflict-free m8n8k4 fragment loads
-constexpr int MP = 61;               // row stride of M (doubles, odd: few bank conflicts on block reads)
 constexpr int kHash = 64;            // element-node hash slots
 
 // The 36 upper 8x8 tiles (mt <= nt) of the 64x64 node-pair matrix.
@@ -57,7 +56,7 @@ struct Hex20Smem {
     double dN[27][3][20];      // shape derivatives at the Gauss points
     union {
         double P[64][PS];      // P[3n+a][g] = G_g[n][a]; rows 60..63 and column 27 zeroed per element
-        double M[60][MP];      // the node-pair matrix M = P diag(w) P^T (exactly symmetric)
+        double Mb[210][9];     // upper 3x3 node blocks of M: Mb[pair(I, J)][3a + b] = M[3I+a][3J+b], I <= J
     };
     double X[20][3];           // element node coordinates
     double J[27][9];           // Jacobians, then their inverses
@@ -114,10 +113,12 @@ __device__ __forceinline__ int first_empty_from(const unsigned (&bm)[4], int nw,
 // Block Ke_IJ into out[0..9) (row-major 3x3):
 //   Ke_IJ[a][b] = lambda M[3I+a][3J+b] + mu M[3I+b][3J+a] + mu delta_ab tr(M_IJ)
 __device__ __forceinline__ void ke_block(const Hex20Smem& sm, int I, int J, double* out) {
-    const double* r0 = &sm.M[3 * I][3 * J];
-    const double m00 = r0[0], m01 = r0[1], m02 = r0[2];
-    const double m10 = r0[MP], m11 = r0[MP + 1], m12 = r0[MP + 2];
-    const double m20 = r0[2 * MP], m21 = r0[2 * MP + 1], m22 = r0[2 * MP + 2];
+    const bool t = I > J;
+    const double* m0 = sm.Mb[t ? hex20::pair_index(J, I) : hex20::pair_index(I, J)];
+    const double m00 = m0[0], m11 = m0[4], m22 = m0[8];
+    const double m01 = t ? m0[3] : m0[1], m02 = t ? m0[6] : m0[2];
+    const double m10 = t ? m0[1] : m0[3], m12 = t ? m0[7] : m0[5];
+    const double m20 = t ? m0[2] : m0[6], m21 = t ? m0[5] : m0[7];
     const double lam = sm.lam, mu = sm.mu, mtr = mu * (m00 + m11 + m22);
     out[0] = fma(lam, m00, fma(mu, m00, mtr));
     out[1] = fma(lam, m01, mu * m10);
@@ -456,8 +457,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
             hex20::tc_prepare<kThreads>(&sm.P[0][0], PS, sm.w, sm.tc, tid);
             // P is no longer read: its storage takes M
             hex20::tc_contract<kWarps>(sm.tc, warp, lane, [&](int r, int c, double v) {
-                sm.M[r][c] = v;
-                sm.M[c][r] = v;
+{ const int I_ = r / 3, a_ = r - 3 * I_, J_ = c / 3, b_ = c - 3 * J_;
+                        if (I_ <= J_) sm.Mb[hex20::pair_index(I_, J_)][3 * a_ + b_] = v;
+                        if (J_ <= I_) sm.Mb[hex20::pair_index(J_, I_)][3 * b_ + a_] = v; }
             });
         } else {
         // M = (P diag(w)) P^T on the FP64 tensor cores, upper 8x8 tiles only
@@ -491,8 +493,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
                     // entry (r, c) stands for itself and, by symmetry, for (c, r);
                     // in a diagonal tile only r <= c writes (its mirror is in the tile)
                     if (r < 60 && c < 60 && (mt < nt || r <= c)) {
-                        sm.M[r][c] = acc[q][h];
-                        sm.M[c][r] = acc[q][h];
+{ const int I_ = r / 3, a_ = r - 3 * I_, J_ = c / 3, b_ = c - 3 * J_;
+                        if (I_ <= J_) sm.Mb[hex20::pair_index(I_, J_)][3 * a_ + b_] = acc[q][h];
+                        if (J_ <= I_) sm.Mb[hex20::pair_index(J_, I_)][3 * b_ + a_] = acc[q][h]; }
                     }
                 }
             }
