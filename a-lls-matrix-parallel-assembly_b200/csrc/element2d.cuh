@@ -7,174 +7,17 @@
 // (xa, ya), (xb, yb) and D = [[d11 d12 0][d12 d11 0][0 0 d33]] the 2x2 block is
 //     K_ab = w * [ d11 xa xb + d33 ya yb    d12 xa yb + d33 ya xb ]
 //                [ d12 ya xb + d33 xa yb    d11 ya yb + d33 xa xb ]
-// which is what these functions accumulate (8 FMAs per block per Gauss point,
-// upper blocks only; K_ba = K_ab^T). D uses each element's own E and nu.
+// which is what ke_block_2d accumulates (8 FMAs per block per Gauss point;
+// K_ba = K_ab^T). D uses each element's own E and nu.
 #pragma once
 
 namespace fem {
-
-// Number of upper-triangle node blocks (a <= b) of an element with n nodes.
-template <int NPE>
-struct Blocks2D {
-    static constexpr int kCount = NPE * (NPE + 1) / 2;
-    // Block index of (a, b) with a <= b.
-    static __host__ __device__ constexpr int idx(int a, int b) { return a * NPE - a * (a - 1) / 2 + (b - a); }
-};
 
 __device__ __forceinline__ void plane_stress_d(double E, double nu, double& d11, double& d12, double& d33) {
     double f = E / (1.0 - nu * nu);
     d11 = f;
     d12 = f * nu;
     d33 = f * (1.0 - nu) / 2.0;
-}
-
-template <int NPE>
-__device__ __forceinline__ void accumulate_blocks_2d(const double (&gx)[NPE], const double (&gy)[NPE], double w,
-                                                     double d11, double d12, double d33,
-                                                     double (&kb)[Blocks2D<NPE>::kCount][4]) {
-#pragma unroll
-    for (int a = 0; a < NPE; a++) {
-        double wxa = w * gx[a], wya = w * gy[a];
-#pragma unroll
-        for (int b = a; b < NPE; b++) {
-            double* k = kb[Blocks2D<NPE>::idx(a, b)];
-            k[0] = fma(d11 * wxa, gx[b], fma(d33 * wya, gy[b], k[0]));
-            k[1] = fma(d12 * wxa, gy[b], fma(d33 * wya, gx[b], k[1]));
-            k[2] = fma(d12 * wya, gx[b], fma(d33 * wxa, gy[b], k[2]));
-            k[3] = fma(d11 * wya, gy[b], fma(d33 * wxa, gx[b], k[3]));
-        }
-    }
-}
-
-// Q4, 2x2 Gauss with the reference's abscissa (Q4A:85). Returns the minimum detJ.
-__device__ __forceinline__ double ke_q4_blocks(const double (&x)[4], const double (&y)[4], double E, double nu,
-                                               double t, double (&kb)[Blocks2D<4>::kCount][4]) {
-    constexpr double g = 0.577350269189626;
-    double d11, d12, d33;
-    plane_stress_d(E, nu, d11, d12, d33);
-#pragma unroll
-    for (int i = 0; i < Blocks2D<4>::kCount; i++) kb[i][0] = kb[i][1] = kb[i][2] = kb[i][3] = 0.0;
-    double min_det = 1e300;
-#pragma unroll
-    for (int gi = 0; gi < 2; gi++) {
-#pragma unroll
-        for (int gj = 0; gj < 2; gj++) {
-            const double xi = gi ? g : -g, eta = gj ? g : -g;
-            const double dxi[4] = {-0.25 * (1.0 - eta), 0.25 * (1.0 - eta), 0.25 * (1.0 + eta), -0.25 * (1.0 + eta)};
-            const double deta[4] = {-0.25 * (1.0 - xi), -0.25 * (1.0 + xi), 0.25 * (1.0 + xi), 0.25 * (1.0 - xi)};
-            double j0 = 0.0, j1 = 0.0, j2 = 0.0, j3 = 0.0;
-#pragma unroll
-            for (int a = 0; a < 4; a++) {
-                j0 = fma(dxi[a], x[a], j0);
-                j1 = fma(dxi[a], y[a], j1);
-                j2 = fma(deta[a], x[a], j2);
-                j3 = fma(deta[a], y[a], j3);
-            }
-            double det = j0 * j3 - j1 * j2;
-            min_det = fmin(min_det, det);
-            double i0 = j3 / det, i1 = -j1 / det, i2 = -j2 / det, i3 = j0 / det;
-            double gx[4], gy[4];
-#pragma unroll
-            for (int a = 0; a < 4; a++) {
-                gx[a] = fma(i0, dxi[a], i1 * deta[a]);
-                gy[a] = fma(i2, dxi[a], i3 * deta[a]);
-            }
-            accumulate_blocks_2d<4>(gx, gy, det * t, d11, d12, d33, kb);
-        }
-    }
-    return min_det;
-}
-
-// T3 constant-strain triangle (T3:131-134,177-205). Returns detJ.
-__device__ __forceinline__ double ke_t3_blocks(const double (&x)[3], const double (&y)[3], double E, double nu,
-                                               double t, double (&kb)[Blocks2D<3>::kCount][4]) {
-    double d11, d12, d33;
-    plane_stress_d(E, nu, d11, d12, d33);
-#pragma unroll
-    for (int i = 0; i < Blocks2D<3>::kCount; i++) kb[i][0] = kb[i][1] = kb[i][2] = kb[i][3] = 0.0;
-    // dN/dxi = (-1, 1, 0), dN/deta = (-1, 0, 1)
-    double j0 = x[1] - x[0], j1 = y[1] - y[0], j2 = x[2] - x[0], j3 = y[2] - y[0];
-    double det = j0 * j3 - j1 * j2;
-    double i0 = j3 / det, i1 = -j1 / det, i2 = -j2 / det, i3 = j0 / det;
-    double gx[3] = {-i0 - i1, i0, i1};
-    double gy[3] = {-i2 - i3, i2, i3};
-    accumulate_blocks_2d<3>(gx, gy, 0.5 * det * t, d11, d12, d33, kb);
-    return det;
-}
-
-// Row a of Ke only: blocks K_ab for all b (used when one thread serves one row).
-template <int NPE>
-__device__ __forceinline__ void accumulate_row_2d(const double (&gx)[NPE], const double (&gy)[NPE], int a, double w,
-                                                  double d11, double d12, double d33, double (&kr)[NPE][4]) {
-    double xa = gx[0], ya = gy[0];
-#pragma unroll
-    for (int i = 1; i < NPE; i++) {
-        xa = a == i ? gx[i] : xa;
-        ya = a == i ? gy[i] : ya;
-    }
-    const double wxa = w * xa, wya = w * ya;
-#pragma unroll
-    for (int b = 0; b < NPE; b++) {
-        kr[b][0] = fma(d11 * wxa, gx[b], fma(d33 * wya, gy[b], kr[b][0]));
-        kr[b][1] = fma(d12 * wxa, gy[b], fma(d33 * wya, gx[b], kr[b][1]));
-        kr[b][2] = fma(d12 * wya, gx[b], fma(d33 * wxa, gy[b], kr[b][2]));
-        kr[b][3] = fma(d11 * wya, gy[b], fma(d33 * wxa, gx[b], kr[b][3]));
-    }
-}
-
-// Row a of a Q4 Ke (2x2 Gauss). Returns the minimum detJ.
-__device__ __forceinline__ double ke_q4_row(const double (&x)[4], const double (&y)[4], double E, double nu, double t,
-                                            int a, double (&kr)[4][4]) {
-    constexpr double g = 0.577350269189626;
-    double d11, d12, d33;
-    plane_stress_d(E, nu, d11, d12, d33);
-#pragma unroll
-    for (int b = 0; b < 4; b++) kr[b][0] = kr[b][1] = kr[b][2] = kr[b][3] = 0.0;
-    double min_det = 1e300;
-#pragma unroll
-    for (int gi = 0; gi < 2; gi++) {
-#pragma unroll
-        for (int gj = 0; gj < 2; gj++) {
-            const double xi = gi ? g : -g, eta = gj ? g : -g;
-            const double dxi[4] = {-0.25 * (1.0 - eta), 0.25 * (1.0 - eta), 0.25 * (1.0 + eta), -0.25 * (1.0 + eta)};
-            const double deta[4] = {-0.25 * (1.0 - xi), -0.25 * (1.0 + xi), 0.25 * (1.0 + xi), 0.25 * (1.0 - xi)};
-            double j0 = 0.0, j1 = 0.0, j2 = 0.0, j3 = 0.0;
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                j0 = fma(dxi[k], x[k], j0);
-                j1 = fma(dxi[k], y[k], j1);
-                j2 = fma(deta[k], x[k], j2);
-                j3 = fma(deta[k], y[k], j3);
-            }
-            const double det = j0 * j3 - j1 * j2;
-            min_det = fmin(min_det, det);
-            const double i0 = j3 / det, i1 = -j1 / det, i2 = -j2 / det, i3 = j0 / det;
-            double gx[4], gy[4];
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                gx[k] = fma(i0, dxi[k], i1 * deta[k]);
-                gy[k] = fma(i2, dxi[k], i3 * deta[k]);
-            }
-            accumulate_row_2d<4>(gx, gy, a, det * t, d11, d12, d33, kr);
-        }
-    }
-    return min_det;
-}
-
-// Row a of a T3 Ke. Returns detJ.
-__device__ __forceinline__ double ke_t3_row(const double (&x)[3], const double (&y)[3], double E, double nu, double t,
-                                            int a, double (&kr)[3][4]) {
-    double d11, d12, d33;
-    plane_stress_d(E, nu, d11, d12, d33);
-#pragma unroll
-    for (int b = 0; b < 3; b++) kr[b][0] = kr[b][1] = kr[b][2] = kr[b][3] = 0.0;
-    const double j0 = x[1] - x[0], j1 = y[1] - y[0], j2 = x[2] - x[0], j3 = y[2] - y[0];
-    const double det = j0 * j3 - j1 * j2;
-    const double i0 = j3 / det, i1 = -j1 / det, i2 = -j2 / det, i3 = j0 / det;
-    const double gx[3] = {-i0 - i1, i0, i1};
-    const double gy[3] = {-i2 - i3, i2, i3};
-    accumulate_row_2d<3>(gx, gy, a, 0.5 * det * t, d11, d12, d33, kr);
-    return det;
 }
 
 // One block K_ab (entries a_dof * 2 + b_dof) of a T3 or Q4 element, computed
@@ -243,12 +86,6 @@ __device__ __forceinline__ double ke_block_2d(const double (&x)[NPE], const doub
         }
         return min_det;
     }
-}
-
-// Entry v (= a_dof * 2 + b_dof) of block (a, b) from the upper blocks.
-template <int NPE>
-__device__ __forceinline__ double block_entry(const double (&kb)[Blocks2D<NPE>::kCount][4], int a, int b, int v) {
-    return a <= b ? kb[Blocks2D<NPE>::idx(a, b)][v] : kb[Blocks2D<NPE>::idx(b, a)][((v & 1) << 1) | (v >> 1)];
 }
 
 }  // namespace fem
