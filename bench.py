@@ -76,6 +76,17 @@ def algorithmic_bytes(mesh, nnz: int) -> dict:
     return {"in": b_in, "out": b_out, "list": b_list, "total": b_in + b_out + b_list}
 
 
+def job_ms(local_ms: float, world: int, device) -> float:
+    """Time of the whole job: the maximum over the ranks of each rank's device
+    time (weak scaling: every rank did the same amount of work)."""
+    if world <= 1:
+        return float(local_ms)
+    import torch
+    t = torch.tensor([float(local_ms)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -245,10 +256,7 @@ def run_batched(args, rank: int, world: int, local_rank: int):
     if bad:
         raise RuntimeError(f"batched assembly: status bits {st[bad[0]]} on mesh {bad[0]}")
     lat = b.latencies_ms()
-    tot = torch.tensor([sum(ts)], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(tot, op=torch.distributed.ReduceOp.MAX)
-    ms = float(tot.item()) / args.steps
+    ms = job_ms(sum(ts), world, dev) / args.steps
     if rank != 0:
         return
     seq = per_k[1]
@@ -344,12 +352,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     consolidate_ms = statistics.mean(s.elapsed_time(e) for s, e in zip(mids, stops))
     st, info = asm.read_info()
     fem.check(st, "timed assembly")
-    total_ms = sum(times)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    total_ms = float(t.item())
-    ms = total_ms / args.steps
+    ms = job_ms(sum(times), world, dev) / args.steps
     clocks = clk.summary()
 
     # end to end through the host-buffer entry point
@@ -377,10 +380,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             b.synchronize()
             e_times.append(a.elapsed_time(b))
         ctx.close()
-        te = torch.tensor([sum(e_times)], dtype=torch.float64, device=dev)
-        if world > 1:
-            torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-        e_ms = float(te.item()) / args.steps
+        e_ms = job_ms(sum(e_times), world, dev) / args.steps
         h2d = sum(v.nbytes for v in harr.values())
         d2h = rp.nbytes + ci.nbytes + vv.nbytes
         e2e = {"value": world * mesh.num_elems / (e_ms / 1e3), "unit": "elements/s", "ms_per_step": e_ms,
