@@ -546,7 +546,7 @@ fem_status fem_reassemble_values(const fem_mesh* mesh, const fem_opts* opts, con
     if (!err && mesh->num_elems > 0) {
         const MeshView m = mesh_view(mesh);
         if (mesh->kind == FEM_HEX20)
-            err = launch_reassemble_hex20(m, precision, perm, MapTarget{pos, row_ptr, values}, info, s);
+            err = launch_reassemble_hex20(m, precision, perm, MapTarget{pos, row_ptr, values, nullptr}, info, s);
         else
             err = launch_reassemble_2d(m, pos, h.G, perm, ranges, row_ptr, values, &info->status_bits, s);
     }
@@ -567,7 +567,7 @@ fem_status fem_scatter_map_read_info(const void* map, void* stream) {
 namespace {
 
 struct ColourHostLayout {
-    size_t off_info, off_cnt, off_off, off_inc, off_colour, off_perm, off_hist, off_ranges, off_tiles, total;
+    size_t off_info, off_kinfo, off_cnt, off_off, off_inc, off_colour, off_perm, off_hist, off_ranges, off_tiles, total;
 };
 
 ColourHostLayout colour_layout(const fem_mesh* m) {
@@ -577,6 +577,8 @@ ColourHostLayout colour_layout(const fem_mesh* m) {
     size_t off = 0;
     h.off_info = off;
     off += align_up(sizeof(ColourInfo));
+    h.off_kinfo = off;  // status of the Hex20 element kernel in the coloured assembly
+    off += align_up(sizeof(DevInfo));
     h.off_cnt = off;
     off += align_up(N * sizeof(int));
     h.off_off = off;
@@ -634,7 +636,8 @@ fem_status fem_colour_prepare(const fem_mesh* mesh, void* workspace, size_t work
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const ColourLayout C = colour_device_layout(h, workspace);
     int nc = 0, bits = 0;
-    cudaError_t err = launch_colour_prepare(mesh_view(mesh), C, sm_count(), s, &nc, &bits);
+    cudaError_t err = cudaMemsetAsync(static_cast<unsigned char*>(workspace) + h.off_kinfo, 0, sizeof(DevInfo), s);
+    if (!err) err = launch_colour_prepare(mesh_view(mesh), C, sm_count(), s, &nc, &bits);
     if (!err && colour_of_element && mesh->num_elems > 0)
         err = launch_colour_export(C, mesh->num_elems, colour_of_element, sm_count(), s);
     if (!err && colour_of_element) err = cudaStreamSynchronize(s);
@@ -648,27 +651,44 @@ fem_status fem_colour_assemble(const fem_mesh* mesh, const void* workspace, size
                                int64_t nnz, void* stream) {
     fem_status st = check_mesh(mesh);
     if (st) return st;
-    if (mesh->kind == FEM_HEX20) return FEM_ERR_BAD_ARG;  // 2-D element kinds only
     const ColourHostLayout h = colour_layout(mesh);
     if (!workspace || workspace_bytes < h.total || reinterpret_cast<uintptr_t>(workspace) % kAlign)
         return FEM_ERR_WORKSPACE;
     if (num_colours < 0 || num_colours > kMaxColours || nnz < 0 || !row_ptr || (nnz > 0 && (!col_idx || !values)))
         return FEM_ERR_BAD_ARG;
     if (mesh->num_elems == 0 || nnz == 0) return FEM_OK;
-    cudaError_t err = launch_colour_assemble(mesh_view(mesh), colour_device_layout(h, workspace), num_colours, row_ptr,
-                                             col_idx, values, nnz, sm_count(), static_cast<cudaStream_t>(stream));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const ColourLayout C = colour_device_layout(h, workspace);
+    cudaError_t err = cudaSuccess;
+    if (mesh->kind == FEM_HEX20) {
+        // the Hex20 element kernel, one launch per colour, plain adds; its
+        // status bits go to the workspace's element-kernel info word
+        DevInfo* info = reinterpret_cast<DevInfo*>(static_cast<unsigned char*>(const_cast<void*>(workspace)) +
+                                                   h.off_kinfo);
+        err = cudaMemsetAsync(info, 0, sizeof(DevInfo), s);
+        if (!err) err = cudaMemsetAsync(values, 0, (size_t)nnz * sizeof(double), s);
+        for (int c = 0; c < num_colours && !err; c++)
+            err = launch_colour_hex20(mesh_view(mesh), C.perm, C.ranges + 2 * c,
+                                      MapTarget{nullptr, row_ptr, values, col_idx}, info, s);
+    } else {
+        err = launch_colour_assemble(mesh_view(mesh), C, num_colours, row_ptr, col_idx, values, nnz, sm_count(), s);
+    }
     return err ? cuda_fail(err) : FEM_OK;
 }
 
 fem_status fem_colour_read_info(const void* workspace, int32_t* num_colours, void* stream) {
     if (!workspace) return FEM_ERR_BAD_ARG;
     ColourInfo h{};
+    DevInfo k{};
+    const unsigned char* b = static_cast<const unsigned char*>(workspace);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    cudaError_t err = cudaMemcpyAsync(&h, workspace, sizeof(h), cudaMemcpyDeviceToHost, s);
+    cudaError_t err = cudaMemcpyAsync(&h, b, sizeof(h), cudaMemcpyDeviceToHost, s);
+    // the element-kernel info word follows the colouring one (first region, 256-byte aligned)
+    if (!err) err = cudaMemcpyAsync(&k, b + align_up(sizeof(ColourInfo)), sizeof(k), cudaMemcpyDeviceToHost, s);
     if (!err) err = cudaStreamSynchronize(s);
     if (err) return cuda_fail(err);
     if (num_colours) *num_colours = h.num_colours;
-    return decode_bits(h.status_bits);
+    return decode_bits(h.status_bits | k.status_bits);
 }
 
 }  // extern "C"

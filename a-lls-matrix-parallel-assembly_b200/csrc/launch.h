@@ -45,6 +45,7 @@ struct MapTarget {
     const int* map;      // [E * npe^2] position of block (a, b) of element e at e * npe^2 + a * npe + b
     const int* row_ptr;  // CSR row pointers of the pattern the map was built for
     double* values;      // CSR values (zeroed by the caller)
+    const int* col_idx;  // CSR columns (the colouring baseline searches them)
 };
 
 // Scatter map of a mesh into a CSR pattern; status gets 1 << FEM_ERR_* bits.
@@ -56,6 +57,10 @@ cudaError_t launch_reassemble_2d(const MeshView& m, const int* map, int G, const
                                  const int* row_ptr, double* values, int* status, cudaStream_t s);
 cudaError_t launch_reassemble_hex20(const MeshView& m, int precision, const int* perm, const MapTarget& t,
                                     DevInfo* info, cudaStream_t s);
+// Colouring baseline for Hex20: elements perm[range[0], range[1]) (one colour),
+// plain adds at binary-searched CSR positions (t.map unused); status bits in info.
+cudaError_t launch_colour_hex20(const MeshView& m, const int* perm, const int* range, const MapTarget& t,
+                                DevInfo* info, cudaStream_t s);
 
 // perm: element visit order (spatial, from launch_reorder_3d); precision FEM_PREC_*.
 cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm,

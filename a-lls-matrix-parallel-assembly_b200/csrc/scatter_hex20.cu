@@ -51,6 +51,7 @@ __constant__ unsigned char c_tile_n[36] = {0, 1, 2, 3, 4, 5, 6, 7, 1, 2, 3, 4, 5
                                            5, 6, 7, 3, 4, 5, 6, 7, 4, 5, 6, 7, 5, 6, 7, 6, 7, 7};
 
 enum SlotState : int { kUnresolved = 0, kFound = 1, kFoundPending = 2, kClaimed = 3 };
+enum OutMode : int { kOutLists = 0, kOutMap = 1, kOutColour = 2 };
 
 struct Hex20Smem {
     double dN[27][3][20];      // shape derivatives at the Gauss points
@@ -296,6 +297,41 @@ __device__ __forceinline__ void scatter_rows(const ListLayout& L, Hex20Smem& sm,
 
 // Value-only re-assembly (reassemble.cu): row nodes I0 and I1 of element e,
 // lane j adds block (I, j) at the CSR positions of the scatter map.
+// Colouring baseline (colour.cu): row nodes I0 and I1, lane j adds block
+// (I, j) at its binary-searched CSR position with plain loads and stores (no
+// two elements of a colour share a node, so no two lanes write one entry).
+__device__ __forceinline__ void colour_rows(const MapTarget& t, const Hex20Smem& sm, int I0, int I1, int lane,
+                                            DevInfo* info) {
+    if (lane >= 20) return;
+    for (int r = 0; r < 2; r++) {
+        const int I = r == 0 ? I0 : I1;
+        if (I < 0) continue;
+        const int r0 = 3 * sm.nodes[I], col = 3 * sm.nodes[lane];
+        int lo = __ldg(t.row_ptr + r0), hi = __ldg(t.row_ptr + r0 + 1) - 1, p = -1;
+        const int len = hi + 1 - lo;
+        while (lo <= hi) {
+            const int mid = (lo + hi) >> 1;
+            const int c = __ldg(t.col_idx + mid);
+            if (c == col) {
+                p = mid;
+                break;
+            }
+            if (c < col) lo = mid + 1;
+            else hi = mid - 1;
+        }
+        if (p < 0) {
+            raise_status(info, FEM_ERR_INTERNAL);  // the pattern lacks the block
+            continue;
+        }
+        double v[9];
+        ke_block(sm, I, lane, v);
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) t.values[p + i * len + j] += v[3 * i + j];
+    }
+}
+
 __device__ __forceinline__ void map_rows(const MapTarget& t, const Hex20Smem& sm, int e, int I0, int I1, int lane) {
     if (lane >= 20) return;
     for (int r = 0; r < 2; r++) {
@@ -321,11 +357,12 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
 }
 
 // kTc: the node-pair contraction on the FP16 tensor cores (hex20.cuh).
-// kMap: value-only re-assembly into a CSR pattern through a scatter map
-// instead of the A-LLS list scatter.
-template <bool kTc, bool kMap>
+// kOut: kOutLists = the A-LLS list scatter; kOutMap = value-only re-assembly
+// into a CSR pattern through a scatter map (atomic adds); kOutColour = the
+// colouring baseline (plain adds, elements perm[range[0], range[1]) of one colour).
+template <bool kTc, int kOut>
 __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListLayout L, const int* __restrict__ perm,
-                                                               MapTarget target) {
+                                                               MapTarget target, const int* __restrict__ range) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Hex20Smem& sm = *reinterpret_cast<Hex20Smem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -348,8 +385,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
     // node id and coordinates of the next element, loaded during the scatter
     int pre_n = 0;
     double pre_x = 0.0, pre_y = 0.0, pre_z = 0.0;
-    if (tid < 20 && blockIdx.x < m.E_count) {
-        pre_n = __ldg(m.conn + (size_t)__ldg(perm + blockIdx.x) * 20 + tid);
+    const int i_begin = range ? range[0] : 0, i_end = range ? range[1] : m.E_count;
+    if (tid < 20 && i_begin + (int)blockIdx.x < i_end) {
+        pre_n = __ldg(m.conn + (size_t)__ldg(perm + i_begin + blockIdx.x) * 20 + tid);
         if (pre_n >= 0 && pre_n < m.N) {
             pre_x = __ldg(m.x + pre_n);
             pre_y = __ldg(m.y + pre_n);
@@ -358,7 +396,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
     }
     __syncthreads();
 
-    for (int i = blockIdx.x; i < m.E_count; i += gridDim.x) {
+    for (int i = i_begin + blockIdx.x; i < i_end; i += gridDim.x) {
         const int e = __ldg(perm + i);
         if (tid == 0) {
             sm.bad = 0;
@@ -396,10 +434,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
         }
         __syncthreads();
         const int i_next = i + gridDim.x;
-        if (tid < 20 && i_next < m.E_count) pre_n = __ldg(m.conn + (size_t)__ldg(perm + i_next) * 20 + tid);
+        if (tid < 20 && i_next < i_end) pre_n = __ldg(m.conn + (size_t)__ldg(perm + i_next) * 20 + tid);
         if (sm.bad) {  // uniform: every thread reads the flag before anyone resets it
             if (tid == 0) raise_status(L.info, FEM_ERR_BAD_MESH);
-            if (tid < 20 && i_next < m.E_count && pre_n >= 0 && pre_n < m.N) {
+            if (tid < 20 && i_next < i_end && pre_n >= 0 && pre_n < m.N) {
                 pre_x = __ldg(m.x + pre_n);
                 pre_y = __ldg(m.y + pre_n);
                 pre_z = __ldg(m.z + pre_n);
@@ -503,14 +541,16 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
         }
         __syncthreads();
         // next element's coordinates: in flight during the scatter
-        if (tid < 20 && i_next < m.E_count && pre_n >= 0 && pre_n < m.N) {
+        if (tid < 20 && i_next < i_end && pre_n >= 0 && pre_n < m.N) {
             pre_x = __ldg(m.x + pre_n);
             pre_y = __ldg(m.y + pre_n);
             pre_z = __ldg(m.z + pre_n);
         }
         // Scatter: warp w serves row nodes w and w + 10.
-        if (kMap)
+        if (kOut == kOutMap)
             map_rows(target, sm, e, warp, warp + kWarps < 20 ? warp + kWarps : -1, lane);
+        else if (kOut == kOutColour)
+            colour_rows(target, sm, warp, warp + kWarps < 20 ? warp + kWarps : -1, lane, L.info);
         else
             scatter_rows(L, sm, warp, warp + kWarps < 20 ? warp + kWarps : -1, warp, lane, spare);
         __syncthreads();
@@ -519,38 +559,45 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
 
 }  // namespace
 
-template <bool kTc, bool kMap>
+template <bool kTc, int kOut>
 cudaError_t launch_scatter_hex20_t(const MeshView& m, const ListLayout& L, const int* perm, const MapTarget& t,
-                                   cudaStream_t s) {
+                                   const int* range, cudaStream_t s) {
     static int blocks_per_sm = 0;
     const size_t smem = sizeof(Hex20Smem);
     if (!blocks_per_sm) {
         cudaError_t err =
-            cudaFuncSetAttribute(k_scatter_hex20<kTc, kMap>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaFuncSetAttribute(k_scatter_hex20<kTc, kOut>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (err) return err;
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_scatter_hex20<kTc, kMap>, kThreads, smem);
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_scatter_hex20<kTc, kOut>, kThreads, smem);
         if (err) return err;
         if (blocks_per_sm < 1) blocks_per_sm = 1;
     }
     long long grid = (long long)blocks_per_sm * sm_count();
     if (grid > m.E_count) grid = m.E_count > 0 ? m.E_count : 1;
-    k_scatter_hex20<kTc, kMap><<<(int)grid, kThreads, smem, s>>>(m, L, perm, t);
+    k_scatter_hex20<kTc, kOut><<<(int)grid, kThreads, smem, s>>>(m, L, perm, t, range);
     return cudaGetLastError();
 }
 
 cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm,
                                  cudaStream_t s) {
     const MapTarget none{};
-    return precision == FEM_PREC_TC_F16X3 ? launch_scatter_hex20_t<true, false>(m, L, perm, none, s)
-                                          : launch_scatter_hex20_t<false, false>(m, L, perm, none, s);
+    return precision == FEM_PREC_TC_F16X3 ? launch_scatter_hex20_t<true, kOutLists>(m, L, perm, none, nullptr, s)
+                                          : launch_scatter_hex20_t<false, kOutLists>(m, L, perm, none, nullptr, s);
 }
 
 cudaError_t launch_reassemble_hex20(const MeshView& m, int precision, const int* perm, const MapTarget& t,
                                     DevInfo* info, cudaStream_t s) {
     ListLayout L{};
     L.info = info;  // status bits (BAD_MESH, DETJ) of the element stiffness
-    return precision == FEM_PREC_TC_F16X3 ? launch_scatter_hex20_t<true, true>(m, L, perm, t, s)
-                                          : launch_scatter_hex20_t<false, true>(m, L, perm, t, s);
+    return precision == FEM_PREC_TC_F16X3 ? launch_scatter_hex20_t<true, kOutMap>(m, L, perm, t, nullptr, s)
+                                          : launch_scatter_hex20_t<false, kOutMap>(m, L, perm, t, nullptr, s);
+}
+
+cudaError_t launch_colour_hex20(const MeshView& m, const int* perm, const int* range, const MapTarget& t,
+                                DevInfo* info, cudaStream_t s) {
+    ListLayout L{};
+    L.info = info;
+    return launch_scatter_hex20_t<false, kOutColour>(m, L, perm, t, range, s);
 }
 
 }  // namespace fem

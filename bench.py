@@ -388,7 +388,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                "api": "fem_assemble_host (pinned host buffers, copies inside the call)"}
 
     colour = None
-    if not args.no_colour and mesh.kind != 2:
+    if not args.no_colour:
         colour = colour_baseline(fem, torch, asm, mesh, nnz, args, flush, stream)
     reasm = None if args.no_reassembly else reassembly(fem, torch, asm, mesh, nnz, args, flush, stream)
     kef = ke_form(fem, torch, mesh, asm.dev, args, flush, stream) if mesh.kind == 2 and not args.no_ke else None
@@ -563,7 +563,8 @@ def colour_baseline(fem, torch, asm, mesh, nnz, args, flush, stream) -> dict:
             "value": mesh.num_elems / (ms / 1e3), "unit": "elements/s (values into the A-LLS pattern; colouring "
             "and pattern excluded, as the reference times its coloured kernel)",
             "max_scaled_diff_vs_alls": diff,
-            "kernels": "k_colour_assemble_2d, one launch per colour and element type"}
+            "kernels": ("k_scatter_hex20 (colour form)" if mesh.kind == 2 else "k_colour_assemble_2d") +
+                       ", one launch per colour and element type"}
 
 
 # k_info_init; 2-D: k_bucket_count, k_bucket_scan, k_bucket_scatter; Hex20: k_bbox_init,

@@ -303,12 +303,14 @@ FEM_API fem_status fem_colour_workspace_size(const fem_mesh* mesh, size_t* bytes
 FEM_API fem_status fem_colour_prepare(const fem_mesh* mesh, void* workspace, size_t workspace_bytes,
                                       int32_t* num_colours, int32_t* colour_of_element, void* stream);
 
-/* Assembles the FP64 values of a 2-D mesh (Q4, T3, mixed) into the CSR pattern
+/* Assembles the FP64 values of the mesh (any kind) into the CSR pattern
  * row_ptr / col_idx (as fem_assemble returns it; nnz entries) after
  * fem_colour_prepare on the same workspace: values are zeroed, then one launch
- * per colour adds every element block at its binary-searched position with
- * plain loads and stores. Asynchronous; fem_colour_read_info reports a block
- * missing from the pattern (FEM_ERR_INTERNAL) or a non-positive detJ. */
+ * per colour (2-D: one lane per element block; Hex20: the Hex20 element
+ * kernel, one CTA per element) adds every element block at its
+ * binary-searched position with plain loads and stores. Asynchronous;
+ * fem_colour_read_info reports a block missing from the pattern
+ * (FEM_ERR_INTERNAL) or a non-positive detJ. */
 FEM_API fem_status fem_colour_assemble(const fem_mesh* mesh, const void* workspace, size_t workspace_bytes,
                                        int32_t num_colours, const int32_t* row_ptr, const int32_t* col_idx,
                                        double* values, int64_t nnz, void* stream);
