@@ -68,9 +68,11 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
                  : "d"(a), "d"(b));
 }
 
-// kTc: the node-pair contraction on the FP16 tensor cores (tc_prepare /
-// tc_contract of hex20.cuh) instead of the FP64 ones.
-template <bool kTc>
+// kPrec: the node-pair contraction on the FP64 tensor cores (FEM_PREC_FP64),
+// on the FP16 tensor cores (FEM_PREC_TC_F16X3: tc_prepare / tc_contract of
+// hex20.cuh), or as plain FP64 dot products on the CUDA cores
+// (FEM_PREC_FP64_SIMT, the reference's arithmetic without tensor cores).
+template <int kPrec>
 __global__ void __launch_bounds__(kThreads, 5) k_hex20_ke(MeshView m, double* __restrict__ ke_out,
                                                           int* __restrict__ status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -89,7 +91,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_hex20_ke(MeshView m, double* __
         sm.dN[g][2][n] = dz;
         dnmax = fmax(dnmax, fmax(fabs(dx), fmax(fabs(dy), fabs(dz))));
     }
-    if (kTc) atomicMax(&sm.dnmax_bits, (unsigned long long)__double_as_longlong(dnmax));
+    if (kPrec == FEM_PREC_TC_F16X3) atomicMax(&sm.dnmax_bits, (unsigned long long)__double_as_longlong(dnmax));
     if (tid < PS) sm.w[tid] = 0.0;
     // node id and coordinates of the next element, loaded a step ahead
     int pre_n = 0;
@@ -109,7 +111,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_hex20_ke(MeshView m, double* __
         double* out = ke_out + (size_t)e * kPackedHex20;
         if (tid == 0) {
             sm.bad = 0;
-            if (kTc) sm.tc.bound_bits = 0ull;
+            if (kPrec == FEM_PREC_TC_F16X3) sm.tc.bound_bits = 0ull;
         }
         __syncthreads();
         if (tid < 20) {
@@ -171,7 +173,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_hex20_ke(MeshView m, double* __
 #pragma unroll
             for (int k = 0; k < 9; k++) J[k] = iJ[k];
             sm.w[tid] = weight3(tid / 9) * weight3((tid / 3) % 3) * weight3(tid % 3) * det;
-            if (kTc)
+            if (kPrec == FEM_PREC_TC_F16X3)
                 hex20::tc_gauss_point(sm.tc, tid, J, sm.w[tid], __longlong_as_double((long long)sm.dnmax_bits));
         }
         __syncthreads();
@@ -189,7 +191,40 @@ __global__ void __launch_bounds__(kThreads, 5) k_hex20_ke(MeshView m, double* __
             for (int a = 0; a < 3; a++) sm.P[3 * n + a][g] = fma(iJ[3 * a], d0, fma(iJ[3 * a + 1], d1, iJ[3 * a + 2] * d2));
         }
         __syncthreads();
-        if (kTc) {
+        if (kPrec == FEM_PREC_FP64_SIMT) {
+            // every upper entry (r <= c < 60) of M as a plain FP64 dot product
+            // over the 27 Gauss points; kept in registers until every thread
+            // has read P, whose storage then takes the M blocks
+            constexpr int kUpper = 60 * 61 / 2, kPer = (kUpper + kThreads - 1) / kThreads;
+            double mv[kPer];
+            int rc[kPer];
+#pragma unroll
+            for (int k = 0; k < kPer; k++) {
+                const int idx = tid + k * kThreads;
+                rc[k] = -1;
+                mv[k] = 0.0;
+                if (idx < kUpper) {
+                    // row r of the upper triangle starts at r * 60 - r (r - 1) / 2
+                    int r = (int)((121.0f - sqrtf(14641.0f - 8.0f * (float)idx)) * 0.5f);
+                    while (r > 0 && r * 60 - r * (r - 1) / 2 > idx) r--;
+                    while ((r + 1) * 60 - (r + 1) * r / 2 <= idx) r++;
+                    const int c = r + (idx - (r * 60 - r * (r - 1) / 2));
+                    double acc = 0.0;
+                    for (int g = 0; g < 27; g++) acc = fma(sm.w[g] * sm.P[r][g], sm.P[c][g], acc);
+                    mv[k] = acc;
+                    rc[k] = r * 64 + c;
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < kPer; k++) {
+                if (rc[k] < 0) continue;
+                const int r = rc[k] >> 6, c = rc[k] & 63;
+                const int I = r / 3, a = r - 3 * I, J = c / 3, b = c - 3 * J;
+                sm.Mb[pair_index(I, J)][3 * a + b] = mv[k];
+                if (I == J) sm.Mb[pair_index(I, I)][3 * b + a] = mv[k];
+            }
+        } else if (kPrec == FEM_PREC_TC_F16X3) {
             tc_prepare<kThreads>(&sm.P[0][0], PS, sm.w, sm.tc, tid);
             // P is no longer read: its storage takes the M blocks
             tc_contract<kWarps>(sm.tc, warp, lane, [&](int r, int c, double v) {
@@ -313,19 +348,19 @@ __global__ void __launch_bounds__(kThreads2D) k_ke_2d(MeshView m, double* __rest
     }
 }
 
-template <bool kTc>
+template <int kPrec>
 cudaError_t launch_hex20_ke(const MeshView& m, double* ke_out, int* status, cudaStream_t s) {
     static int blocks_per_sm = 0;
     const size_t smem = sizeof(KeSmem);
     if (!blocks_per_sm) {
-        cudaError_t err = cudaFuncSetAttribute(k_hex20_ke<kTc>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t err = cudaFuncSetAttribute(k_hex20_ke<kPrec>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (err) return err;
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_hex20_ke<kTc>, kThreads, smem);
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_hex20_ke<kPrec>, kThreads, smem);
         if (err) return err;
         if (blocks_per_sm < 1) blocks_per_sm = 1;
     }
     const long long grid = std::min<long long>((long long)blocks_per_sm * sm_count(), m.E_count);
-    k_hex20_ke<kTc><<<(int)grid, kThreads, smem, s>>>(m, ke_out, status);
+    k_hex20_ke<kPrec><<<(int)grid, kThreads, smem, s>>>(m, ke_out, status);
     return cudaGetLastError();
 }
 
@@ -335,8 +370,9 @@ cudaError_t launch_element_stiffness(const MeshView& m, int kind, int precision,
                                      cudaStream_t s) {
     if (m.E_count <= 0) return cudaSuccess;
     if (kind == FEM_HEX20) {
-        return precision == FEM_PREC_TC_F16X3 ? launch_hex20_ke<true>(m, ke_out, status, s)
-                                              : launch_hex20_ke<false>(m, ke_out, status, s);
+        if (precision == FEM_PREC_TC_F16X3) return launch_hex20_ke<FEM_PREC_TC_F16X3>(m, ke_out, status, s);
+        if (precision == FEM_PREC_FP64_SIMT) return launch_hex20_ke<FEM_PREC_FP64_SIMT>(m, ke_out, status, s);
+        return launch_hex20_ke<FEM_PREC_FP64>(m, ke_out, status, s);
     } else {
         const long long warps = ((long long)m.E_count + 1) / 2;  // two elements per warp
         const int grid = (int)std::min<long long>((warps * 32 + kThreads2D - 1) / kThreads2D, (long long)sm_count() * 8);

@@ -313,7 +313,8 @@ fem_status fem_element_stiffness(const fem_mesh* mesh, const fem_opts* opts, dou
     if (st) return st;
     if (!status || (mesh->num_elems > 0 && !ke_out)) return FEM_ERR_BAD_ARG;
     const int precision = opts ? opts->precision : FEM_PREC_FP64;
-    if (precision != FEM_PREC_FP64 && !(precision == FEM_PREC_TC_F16X3 && mesh->kind == FEM_HEX20))
+    if (precision != FEM_PREC_FP64 &&
+        !((precision == FEM_PREC_TC_F16X3 || precision == FEM_PREC_FP64_SIMT) && mesh->kind == FEM_HEX20))
         return FEM_ERR_BAD_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t err = cudaMemsetAsync(status, 0, sizeof(int32_t), s);

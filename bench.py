@@ -452,13 +452,14 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
 
 def ke_form(fem, torch, mesh, dev_arrays, args, flush, stream) -> dict:
-    """The Hex20 element stiffness on its own (fem_element_stiffness), plain
-    FP64 (FP64 tensor cores) and the FP16-split tensor-core form, timed alike;
+    """The Hex20 element stiffness on its own (fem_element_stiffness) in its
+    three forms (FP64 tensor cores, FP16-split tensor cores, plain FP64 on the
+    CUDA cores), timed alike;
     the tensor-core values are compared with the FP64 ones per element, on the
     scale of the element's largest diagonal entry."""
     out = {}
     kes = {}
-    for prec, name in ((0, "fp64"), (1, "tc_f16x3")):
+    for prec, name in ((0, "fp64"), (1, "tc_f16x3"), (2, "fp64_simt")):
         o = fem.opts(precision=prec)
         ke, st = fem.element_stiffness(mesh, o, dev_arrays=dev_arrays)
         fem.check(0 if st == 0 else 1, f"element stiffness {name}")
@@ -481,7 +482,11 @@ def ke_form(fem, torch, mesh, dev_arrays, args, flush, stream) -> dict:
     d = kes["fp64"][:, diag_idx].abs().max(dim=1).values
     err = ((kes["tc_f16x3"] - kes["fp64"]).abs().max(dim=1).values / d).max()
     flops = 2 * 60 * 60 * 27 * mesh.num_elems  # the node-pair contraction
-    out.update({"speedup_tc_vs_fp64": out["fp64_ms"] / out["tc_f16x3_ms"], "max_err_tc_vs_fp64": float(err),
+    out.update({"speedup_tc_vs_fp64": out["fp64_ms"] / out["tc_f16x3_ms"],
+                "speedup_tc_vs_fp64_simt": out["fp64_simt_ms"] / out["tc_f16x3_ms"],
+                "forms": "fp64: contraction on the FP64 tensor cores (the library's default); tc_f16x3: FP16 split "
+                         "operands on the FP16 tensor cores; fp64_simt: plain FP64 dot products on the CUDA cores",
+                "max_err_tc_vs_fp64": float(err),
                 "err_scale": "per element, max |difference| / the element's largest diagonal entry",
                 "contraction_gflop": flops / 1e9, "bytes_written": int(kes["fp64"].numel() * 8),
                 "what": "fem_element_stiffness: packed symmetric Ke (210 3x3 blocks, 15.1 KB) of every element"})

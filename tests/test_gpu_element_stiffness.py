@@ -75,3 +75,19 @@ def test_tensor_core_form_rejected_for_2d(fem, cuda_device):
     import meshgen as mg
     with pytest.raises(fem.FemError):
         fem.element_stiffness(mg.by_name("t3_small"), fem.opts(precision=1))
+
+
+def test_plain_fp64_simt_form_matches_oracle(fem, oracle_mod, cuda_device):
+    # FEM_PREC_FP64_SIMT: the same Ke with the contraction as plain FP64 dot
+    # products (no tensor cores), the comparison point of the tensor-core forms
+    import meshgen as mg
+    m = mg.by_name("hex20_small")
+    ke, status = fem.element_stiffness(m, fem.opts(precision=2))
+    assert status == 0
+    ke = ke.cpu().numpy()
+    for e in range(m.num_elems):
+        ref, npe, dpn = _oracle_ke(oracle_mod, m, e)
+        got = fem.unpack_element_stiffness(ke[e], npe, dpn)
+        assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(np.diag(ref)))
+    with pytest.raises(fem.FemError):   # not an assembly precision
+        fem.assemble(m, fem.opts(precision=2))
