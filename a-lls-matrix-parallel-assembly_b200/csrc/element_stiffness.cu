@@ -9,7 +9,8 @@
 // which build a full Ke per thread (the Hex20 one a 60x60 FP32 array in 14.9 KB
 // of local memory).
 //
-// 2-D (k_ke_2d): one lane per node block, as the A-LLS scatter computes it.
+// 2-D (k_ke_2d): one lane per node block, as the A-LLS scatter computes it
+// (FP64, or FP32 blocks with FEM_PREC_FP32).
 //
 // Hex20 (k_hex20_ke): one CTA (4 warps) per element at a time, persistent:
 //   Jacobians at the 27 Gauss points (243 entries), their inverses and
@@ -292,6 +293,7 @@ constexpr int kThreads2D = 256;
 // One lane per upper node block (a <= b) of one 2-D element; a Q4 element
 // takes 10 lanes, a T3 element 6 (its 4 block slots past the sixth are zeroed
 // in a mixed mesh, whose stride is the Q4 one).
+template <typename T>
 __global__ void __launch_bounds__(kThreads2D) k_ke_2d(MeshView m, double* __restrict__ ke_out,
                                                       int* __restrict__ status) {
     constexpr int kLanes = 16;  // two elements per warp, up to 10 blocks each
@@ -332,7 +334,7 @@ __global__ void __launch_bounds__(kThreads2D) k_ke_2d(MeshView m, double* __rest
                 xe[k] = __ldg(m.x + nodes[k]);
                 ye[k] = __ldg(m.y + nodes[k]);
             }
-            const double det = ke_block_2d<4>(xe, ye, E, nu, m.t, a, b, kv);
+            const double det = ke_block_2d<4, T>(xe, ye, E, nu, m.t, a, b, kv);
             if (sub == 0 && !(det > 0.0)) atomicOr(status, 1 << FEM_ERR_DETJ);
         } else {
             double xe[3], ye[3];
@@ -340,7 +342,7 @@ __global__ void __launch_bounds__(kThreads2D) k_ke_2d(MeshView m, double* __rest
                 xe[k] = __ldg(m.x + nodes[k]);
                 ye[k] = __ldg(m.y + nodes[k]);
             }
-            const double det = ke_block_2d<3>(xe, ye, E, nu, m.t, a, b, kv);
+            const double det = ke_block_2d<3, T>(xe, ye, E, nu, m.t, a, b, kv);
             if (sub == 0 && !(det > 0.0)) atomicOr(status, 1 << FEM_ERR_DETJ);
         }
         reinterpret_cast<double2*>(out)[0] = make_double2(kv[0], kv[1]);
@@ -370,13 +372,16 @@ cudaError_t launch_element_stiffness(const MeshView& m, int kind, int precision,
                                      cudaStream_t s) {
     if (m.E_count <= 0) return cudaSuccess;
     if (kind == FEM_HEX20) {
-        if (precision == FEM_PREC_TC_F16X3) return launch_hex20_ke<FEM_PREC_TC_F16X3>(m, ke_out, status, s);
+        if (precision == FEM_PREC_TC_F16X3) return launch_hex20_ke_tcgen05(m, ke_out, status, s);
         if (precision == FEM_PREC_FP64_SIMT) return launch_hex20_ke<FEM_PREC_FP64_SIMT>(m, ke_out, status, s);
         return launch_hex20_ke<FEM_PREC_FP64>(m, ke_out, status, s);
     } else {
         const long long warps = ((long long)m.E_count + 1) / 2;  // two elements per warp
         const int grid = (int)std::min<long long>((warps * 32 + kThreads2D - 1) / kThreads2D, (long long)sm_count() * 8);
-        k_ke_2d<<<grid > 0 ? grid : 1, kThreads2D, 0, s>>>(m, ke_out, status);
+        if (precision == FEM_PREC_FP32)
+            k_ke_2d<float><<<grid > 0 ? grid : 1, kThreads2D, 0, s>>>(m, ke_out, status);
+        else
+            k_ke_2d<double><<<grid > 0 ? grid : 1, kThreads2D, 0, s>>>(m, ke_out, status);
     }
     return cudaGetLastError();
 }

@@ -157,6 +157,15 @@ fem_status decode_bits(int bits) {
     return FEM_OK;
 }
 
+// Precisions of the assembly entry points: FP64 for every kind; the FP16
+// tensor-core contraction for Hex20; FP32 blocks for the 2-D kinds.
+bool assembly_precision_ok(int precision, int kind) {
+    if (precision == FEM_PREC_FP64) return true;
+    if (precision == FEM_PREC_TC_F16X3) return kind == FEM_HEX20;
+    if (precision == FEM_PREC_FP32) return kind == FEM_Q4 || kind == FEM_T3 || kind == FEM_MIXED_2D;
+    return false;
+}
+
 }  // namespace
 
 extern "C" {
@@ -197,7 +206,7 @@ fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* wo
     if (st) return st;
     if ((st = check_ws(h, workspace, workspace_bytes))) return st;
     const int precision = opts ? opts->precision : FEM_PREC_FP64;
-    if (precision != FEM_PREC_FP64 && !(precision == FEM_PREC_TC_F16X3 && h.kind == FEM_HEX20)) return FEM_ERR_BAD_ARG;
+    if (!assembly_precision_ok(precision, h.kind)) return FEM_ERR_BAD_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     ListLayout L = device_layout(h, workspace);
     unsigned char* b = static_cast<unsigned char*>(workspace);
@@ -223,8 +232,8 @@ fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* wo
         if (!err) err = launch_scatter_hex20(m, L, precision, perm, s);
     } else {
         err = launch_reorder(m, hist, ranges, perm, sm_count(), s);
-        if (!err && h.kind != FEM_T3) err = launch_scatter_2d(m, L, 4, perm, ranges + 0, s);
-        if (!err && h.kind != FEM_Q4) err = launch_scatter_2d(m, L, 3, perm, ranges + 2, s);
+        if (!err && h.kind != FEM_T3) err = launch_scatter_2d(m, L, 4, precision, perm, ranges + 0, s);
+        if (!err && h.kind != FEM_Q4) err = launch_scatter_2d(m, L, 3, precision, perm, ranges + 2, s);
     }
     return err ? cuda_fail(err) : FEM_OK;
 }
@@ -313,8 +322,8 @@ fem_status fem_element_stiffness(const fem_mesh* mesh, const fem_opts* opts, dou
     if (st) return st;
     if (!status || (mesh->num_elems > 0 && !ke_out)) return FEM_ERR_BAD_ARG;
     const int precision = opts ? opts->precision : FEM_PREC_FP64;
-    if (precision != FEM_PREC_FP64 &&
-        !((precision == FEM_PREC_TC_F16X3 || precision == FEM_PREC_FP64_SIMT) && mesh->kind == FEM_HEX20))
+    if (!assembly_precision_ok(precision, mesh->kind) &&
+        !(precision == FEM_PREC_FP64_SIMT && mesh->kind == FEM_HEX20))
         return FEM_ERR_BAD_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t err = cudaMemsetAsync(status, 0, sizeof(int32_t), s);
@@ -533,7 +542,7 @@ fem_status fem_reassemble_values(const fem_mesh* mesh, const fem_opts* opts, con
     fem_status st = check_map(mesh, map, map_bytes, h);
     if (st) return st;
     const int precision = opts ? opts->precision : FEM_PREC_FP64;
-    if (precision != FEM_PREC_FP64 && !(precision == FEM_PREC_TC_F16X3 && mesh->kind == FEM_HEX20))
+    if (!assembly_precision_ok(precision, mesh->kind))
         return FEM_ERR_BAD_ARG;
     if (!row_ptr || nnz < 0 || (nnz > 0 && !values)) return FEM_ERR_BAD_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -549,7 +558,7 @@ fem_status fem_reassemble_values(const fem_mesh* mesh, const fem_opts* opts, con
         if (mesh->kind == FEM_HEX20)
             err = launch_reassemble_hex20(m, precision, perm, MapTarget{pos, row_ptr, values, nullptr}, info, s);
         else
-            err = launch_reassemble_2d(m, pos, h.G, perm, ranges, row_ptr, values, &info->status_bits, s);
+            err = launch_reassemble_2d(m, precision, pos, h.G, perm, ranges, row_ptr, values, &info->status_bits, s);
     }
     return err ? cuda_fail(err) : FEM_OK;
 }

@@ -26,9 +26,10 @@ struct MeshView {
 // 2-D chunk rows are 16 int32 words (14 slots + fill + next).
 constexpr int k2DSlots = 14;
 
-// perm: element visit order; range: device ints {begin, end} into perm.
-cudaError_t launch_scatter_2d(const MeshView& m, const ListLayout& L, int npe, const int* perm, const int* range,
-                              cudaStream_t s);
+// perm: element visit order; range: device ints {begin, end} into perm;
+// precision FEM_PREC_FP64 or FEM_PREC_FP32 (the arithmetic of the Ke blocks).
+cudaError_t launch_scatter_2d(const MeshView& m, const ListLayout& L, int npe, int precision, const int* perm,
+                              const int* range, cudaStream_t s);
 // Node-local element order (perm) and the element ranges {q4 begin, q4 end, t3 begin, t3 end}.
 int reorder_buckets(int num_nodes);
 cudaError_t launch_reorder(const MeshView& m, int* hist, int* ranges, int* perm, int sms, cudaStream_t s);
@@ -40,6 +41,9 @@ constexpr int kPacked2D_T3 = 6 * 4;
 // Element stiffness of every element, natural order; status gets 1 << FEM_ERR_* bits.
 cudaError_t launch_element_stiffness(const MeshView& m, int kind, int precision, double* ke_out, int* status,
                                      cudaStream_t s);
+// Hex20 element stiffness with the contraction on the tcgen05 tensor cores
+// (FEM_PREC_TC_F16X3), two elements per CTA step.
+cudaError_t launch_hex20_ke_tcgen05(const MeshView& m, double* ke_out, int* status, cudaStream_t s);
 // Target of a value-only re-assembly: CSR positions of every element block.
 struct MapTarget {
     const int* map;      // [E * npe^2] position of block (a, b) of element e at e * npe^2 + a * npe + b
@@ -53,8 +57,8 @@ cudaError_t launch_build_map(const MeshView& m, int kind, const int* row_ptr, co
                              int* status, cudaStream_t s);
 // Value-only re-assembly (atomics into values): 2-D kinds over perm ranges
 // {q4 begin, q4 end, t3 begin, t3 end}; Hex20 over perm (status bits in info).
-cudaError_t launch_reassemble_2d(const MeshView& m, const int* map, int G, const int* perm, const int* ranges,
-                                 const int* row_ptr, double* values, int* status, cudaStream_t s);
+cudaError_t launch_reassemble_2d(const MeshView& m, int precision, const int* map, int G, const int* perm,
+                                 const int* ranges, const int* row_ptr, double* values, int* status, cudaStream_t s);
 cudaError_t launch_reassemble_hex20(const MeshView& m, int precision, const int* perm, const MapTarget& t,
                                     DevInfo* info, cudaStream_t s);
 // Colouring baseline for Hex20: elements perm[range[0], range[1]) (one colour),

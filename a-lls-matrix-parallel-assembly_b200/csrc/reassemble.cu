@@ -72,7 +72,7 @@ __global__ void k_build_map(MeshView m, int dpn, int npe_max, const int* __restr
 
 // 2-D value-only assembly: one lane per element block (NPE^2 lanes per
 // element), elements perm[range[0], range[1]), FP64 red.add into the values.
-template <int NPE>
+template <int NPE, typename T>
 __global__ void __launch_bounds__(kThreads) k_reassemble_2d(MeshView m, const int* __restrict__ map, int G,
                                                             const int* __restrict__ perm, const int* __restrict__ range,
                                                             const int* __restrict__ row_ptr,
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(kThreads) k_reassemble_2d(MeshView m, const in
         const double E = m.E ? __ldg(m.E + e) : m.E0;
         const double nu = m.nu ? __ldg(m.nu + e) : m.nu0;
         double kv[4];
-        const double det = ke_block_2d<NPE>(xe, ye, E, nu, m.t, a, b, kv);
+        const double det = ke_block_2d<NPE, T>(xe, ye, E, nu, m.t, a, b, kv);
         if (sub == 0 && !(det > 0.0)) atomicOr(status, 1 << FEM_ERR_DETJ);
         int row = nodes[0];
 #pragma unroll
@@ -126,17 +126,26 @@ cudaError_t launch_build_map(const MeshView& m, int kind, const int* row_ptr, co
     return cudaGetLastError();
 }
 
-cudaError_t launch_reassemble_2d(const MeshView& m, const int* map, int G, const int* perm, const int* ranges,
-                                 const int* row_ptr, double* values, int* status, cudaStream_t s) {
+template <typename T>
+void reassemble_2d_t(const MeshView& m, const int* map, int G, const int* perm, const int* ranges, const int* row_ptr,
+                     double* values, int* status, cudaStream_t s) {
     const bool has_q4 = m.types || m.stride == 4, has_t3 = m.types || m.stride == 3;
     const long long warps = ((long long)m.E_count + 1) / 2;
     const int grid = (int)std::min<long long>((warps * 32 + kThreads - 1) / kThreads, (long long)sm_count() * 8);
     if (has_q4)
-        k_reassemble_2d<4><<<grid > 0 ? grid : 1, kThreads, 0, s>>>(m, map, G, perm, ranges + 0, row_ptr, values,
-                                                                   status);
+        k_reassemble_2d<4, T><<<grid > 0 ? grid : 1, kThreads, 0, s>>>(m, map, G, perm, ranges + 0, row_ptr, values,
+                                                                      status);
     if (has_t3)
-        k_reassemble_2d<3><<<grid > 0 ? grid : 1, kThreads, 0, s>>>(m, map, G, perm, ranges + 2, row_ptr, values,
-                                                                   status);
+        k_reassemble_2d<3, T><<<grid > 0 ? grid : 1, kThreads, 0, s>>>(m, map, G, perm, ranges + 2, row_ptr, values,
+                                                                      status);
+}
+
+cudaError_t launch_reassemble_2d(const MeshView& m, int precision, const int* map, int G, const int* perm,
+                                 const int* ranges, const int* row_ptr, double* values, int* status, cudaStream_t s) {
+    if (precision == FEM_PREC_FP32)
+        reassemble_2d_t<float>(m, map, G, perm, ranges, row_ptr, values, status, s);
+    else
+        reassemble_2d_t<double>(m, map, G, perm, ranges, row_ptr, values, status, s);
     return cudaGetLastError();
 }
 

@@ -114,7 +114,7 @@ __device__ __forceinline__ int element_of(const int* perm, int begin, int count,
     return valid ? __ldg(perm + begin + i) : 0;
 }
 
-template <int NPE>
+template <int NPE, typename T>
 __global__ void __launch_bounds__(kThreads2D, NPE == 3 ? 4 : 2)
     k_scatter_2d(MeshView m, ListLayout L, const int* __restrict__ perm, const int* __restrict__ range) {
     constexpr int G = NPE * NPE;   // lanes per element
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(kThreads2D, NPE == 3 ? 4 : 2)
         int state = kSkip;
         unsigned gid = 0;
         if (valid) {
-            const double det = ke_block_2d<NPE>(xe, ye, Ee, nue, m.t, a, b, kv);
+            const double det = ke_block_2d<NPE, T>(xe, ye, Ee, nue, m.t, a, b, kv);
             if (sub == 0 && !(det > 0.0)) raise_status(L.info, FEM_ERR_DETJ);
             state = resolve_2d(L, row, col + 1, view, spare, gid);
         }
@@ -221,28 +221,33 @@ __global__ void __launch_bounds__(kThreads2D, NPE == 3 ? 4 : 2)
 
 }  // namespace
 
-cudaError_t launch_scatter_2d(const MeshView& m, const ListLayout& L, int npe, const int* perm, const int* range,
-                              cudaStream_t s) {
+template <int NPE, typename T>
+cudaError_t launch_scatter_2d_t(const MeshView& m, const ListLayout& L, const int* perm, const int* range,
+                                cudaStream_t s) {
     // A persistent grid: every warp runs the pipeline over many elements.
-    static int resident[2] = {0, 0};
-    const int t = npe == 4 ? 0 : 1;
-    if (!resident[t]) {
+    static int resident = 0;
+    if (!resident) {
         int per_sm = 0;
-        cudaError_t err = npe == 4
-                              ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scatter_2d<4>, kThreads2D, 0)
-                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scatter_2d<3>, kThreads2D, 0);
+        const cudaError_t err =
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scatter_2d<NPE, T>, kThreads2D, 0);
         if (err) return err;
-        resident[t] = std::max(per_sm, 1) * sm_count();
+        resident = std::max(per_sm, 1) * sm_count();
     }
-    const int epw = npe == 4 ? 2 : 3;
+    constexpr int epw = 32 / (NPE * NPE);
     const long long warps = ((long long)m.E_count + epw - 1) / epw;
     const long long want = (warps + kWarps2D - 1) / kWarps2D;
-    const int grid = (int)std::min<long long>(want > 0 ? want : 1, (long long)resident[t]);
-    if (npe == 4)
-        k_scatter_2d<4><<<grid, kThreads2D, 0, s>>>(m, L, perm, range);
-    else
-        k_scatter_2d<3><<<grid, kThreads2D, 0, s>>>(m, L, perm, range);
+    const int grid = (int)std::min<long long>(want > 0 ? want : 1, (long long)resident);
+    k_scatter_2d<NPE, T><<<grid, kThreads2D, 0, s>>>(m, L, perm, range);
     return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_2d(const MeshView& m, const ListLayout& L, int npe, int precision, const int* perm,
+                              const int* range, cudaStream_t s) {
+    if (precision == FEM_PREC_FP32)
+        return npe == 4 ? launch_scatter_2d_t<4, float>(m, L, perm, range, s)
+                        : launch_scatter_2d_t<3, float>(m, L, perm, range, s);
+    return npe == 4 ? launch_scatter_2d_t<4, double>(m, L, perm, range, s)
+                    : launch_scatter_2d_t<3, double>(m, L, perm, range, s);
 }
 
 }  // namespace fem

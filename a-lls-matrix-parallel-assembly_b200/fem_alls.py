@@ -124,7 +124,7 @@ def load() -> C.CDLL:
     return _lib
 
 
-FEM_PREC_FP64, FEM_PREC_TC_F16X3, FEM_PREC_FP64_SIMT = 0, 1, 2
+FEM_PREC_FP64, FEM_PREC_TC_F16X3, FEM_PREC_FP64_SIMT, FEM_PREC_FP32 = 0, 1, 2, 3
 
 
 def opts(first_slots: int = 0, chunk_slots: int = 0, pool_factor: float = 0.0, precision: int = 0) -> FemOpts:

@@ -392,6 +392,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         colour = colour_baseline(fem, torch, asm, mesh, nnz, args, flush, stream)
     reasm = None if args.no_reassembly else reassembly(fem, torch, asm, mesh, nnz, args, flush, stream)
     kef = ke_form(fem, torch, mesh, asm.dev, args, flush, stream) if mesh.kind == 2 and not args.no_ke else None
+    f32 = fp32_form(fem, torch, asm, mesh, nnz, args, flush, stream) if mesh.kind != 2 and not args.no_ke else None
 
     if rank != 0:
         return
@@ -446,6 +447,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         line["reassembly"] = reasm
     if kef:
         line["ke_form"] = kef
+    if f32:
+        line["fp32_form"] = f32
     if not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args.workload, use_reference=False, workers=1)
     print(json.dumps(line), flush=True)
@@ -491,6 +494,52 @@ def ke_form(fem, torch, mesh, dev_arrays, args, flush, stream) -> dict:
                 "contraction_gflop": flops / 1e9, "bytes_written": int(kes["fp64"].numel() * 8),
                 "what": "fem_element_stiffness: packed symmetric Ke (210 3x3 blocks, 15.1 KB) of every element"})
     return out
+
+
+def row_col_scale(torch, rp, ci, v, n):
+    """max(|K_ij|, sqrt(|K_ii K_jj|)) of every entry of a CSR matrix."""
+    rows = torch.repeat_interleave(torch.arange(n, device=rp.device), (rp[1:] - rp[:-1]).long())
+    diag = torch.zeros(n, dtype=torch.float64, device=rp.device)
+    on = rows == ci.long()
+    diag[rows[on]] = v[on].abs()
+    scale = torch.maximum(v.abs(), torch.sqrt(diag[rows] * diag[ci.long()]))
+    return torch.where(scale > 0, scale, torch.ones_like(scale))
+
+
+def fp32_form(fem, torch, asm, mesh, nnz, args, flush, stream) -> dict:
+    """The whole A-LLS assembly with the FP32 Ke blocks of the 2-D kinds
+    (FEM_PREC_FP32), timed like the FP64 step; its values are compared with
+    the FP64 assembly's on the row/column scale."""
+    v64 = asm.values[:nnz].clone()
+    o64 = asm.opts
+    asm.opts = fem.opts(precision=fem.FEM_PREC_FP32)
+    try:
+        for _ in range(args.warmup):
+            asm.assemble_async()
+        ts = []
+        for _ in range(args.steps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            asm.scatter()
+            asm.consolidate()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        st, _ = asm.read_info()
+        fem.check(st, "FP32-form assembly")
+        scale = row_col_scale(torch, asm.row_ptr, asm.col_idx[:nnz], v64, mesh.num_dofs)
+        err = float(((asm.values[:nnz] - v64).abs() / scale).max()) if nnz else 0.0
+    finally:
+        asm.opts = o64
+        asm.assemble()                         # leave the FP64 values in place
+    ms = statistics.mean(ts)
+    return {"value": mesh.num_elems / (ms / 1e3), "unit": "elements/s", "ms_per_step": ms,
+            "max_scaled_err_vs_fp64": err,
+            "err_scale": "max |difference| / max(|K_ij|, sqrt(|K_ii K_jj|)) over the CSR entries",
+            "what": "fem_alls_scatter + fem_alls_consolidate with FEM_PREC_FP32 (Ke blocks in FP32 from "
+                    "coordinates relative to the element's first node, FP64 accumulation)"}
 
 
 def reassembly(fem, torch, asm, mesh, nnz, args, flush, stream) -> dict:
@@ -557,13 +606,8 @@ def colour_baseline(fem, torch, asm, mesh, nnz, args, flush, stream) -> dict:
     ms = statistics.mean(ts)
     # agreement with the A-LLS values of the same pattern, on the row/column scale
     v_alls = asm.values[:nnz]
-    n = mesh.num_dofs
-    rows = torch.repeat_interleave(torch.arange(n, device=rp.device), (rp[1:] - rp[:-1]).long())
-    diag = torch.zeros(n, dtype=torch.float64, device=rp.device)
-    on = rows == ci.long()
-    diag[rows[on]] = v_alls[on].abs()
-    scale = torch.maximum(v_alls.abs(), torch.sqrt(diag[rows] * diag[ci.long()]))
-    diff = float(((vals - v_alls).abs() / torch.where(scale > 0, scale, torch.ones_like(scale))).max())
+    scale = row_col_scale(torch, rp, ci[:nnz], v_alls, mesh.num_dofs)
+    diff = float(((vals - v_alls).abs() / scale).max())
     return {"num_colours": nc, "prepare_ms": prep_ms, "assemble_ms": ms,
             "value": mesh.num_elems / (ms / 1e3), "unit": "elements/s (values into the A-LLS pattern; colouring "
             "and pattern excluded, as the reference times its coloured kernel)",
@@ -628,7 +672,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-colour", action="store_true", help="skip the element-colouring baseline leg")
     ap.add_argument("--no-reassembly", action="store_true", help="skip the value-only re-assembly leg")
-    ap.add_argument("--no-ke", action="store_true", help="skip the Hex20 element-stiffness (Ke form) leg")
+    ap.add_argument("--no-ke", action="store_true", help="skip the precision-form leg (Hex20: element-stiffness forms; 2-D: the FP32-form assembly)")
     ap.add_argument("--ke-only", action="store_true",
                     help="Hex20: time only the element-stiffness kernels (FP64 and tensor-core forms)")
     args = ap.parse_args()

@@ -84,6 +84,10 @@ typedef int32_t fem_status;
 #define FEM_PREC_FP64_SIMT 2 /* fem_element_stiffness only, Hex20: the contraction as plain FP64
                                 dot products on the CUDA cores (the reference's arithmetic, no
                                 tensor cores), for comparing the tensor-core forms against */
+#define FEM_PREC_FP32 3      /* Q4, T3 and mixed meshes: each Ke block computed in FP32 from
+                                node coordinates taken relative to the element's first node
+                                (differenced in FP64); the global accumulation stays FP64.
+                                Value error stated by the tests. */
 
 typedef struct fem_mesh {
     int32_t kind;          /* FEM_Q4, FEM_T3, FEM_HEX20, FEM_MIXED_2D */
@@ -200,7 +204,8 @@ FEM_API fem_status fem_element_stiffness_size(const fem_mesh* mesh, int64_t* dou
 /* ke_out: device [num_elems * doubles_per_element]. status: a device int32
  * that is zeroed and then receives (1 << FEM_ERR_*) bits (BAD_MESH: the
  * element's output is zero; DETJ). Asynchronous. opts->precision:
- * FEM_PREC_FP64, or for a Hex20 mesh FEM_PREC_TC_F16X3 or FEM_PREC_FP64_SIMT. */
+ * FEM_PREC_FP64; for a Hex20 mesh also FEM_PREC_TC_F16X3 or FEM_PREC_FP64_SIMT;
+ * for a 2-D mesh also FEM_PREC_FP32. */
 FEM_API fem_status fem_element_stiffness(const fem_mesh* mesh, const fem_opts* opts, double* ke_out,
                                          int32_t* status, void* stream);
 

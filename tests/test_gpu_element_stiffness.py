@@ -91,3 +91,26 @@ def test_plain_fp64_simt_form_matches_oracle(fem, oracle_mod, cuda_device):
         assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(np.diag(ref)))
     with pytest.raises(fem.FemError):   # not an assembly precision
         fem.assemble(m, fem.opts(precision=2))
+
+
+# The FP32 form of the 2-D kinds (FEM_PREC_FP32): each block in FP32 from
+# node coordinates relative to the element's first node.
+FP32_ELEMENT_TOL = 1e-5
+
+
+@pytest.mark.parametrize("name", ["q4_small", "t3_small", "mixed_small"])
+def test_fp32_element_stiffness_error(fem, oracle_mod, cuda_device, name):
+    import meshgen as mg
+    m = mg.by_name(name)
+    ke, status = fem.element_stiffness(m, fem.opts(precision=fem.FEM_PREC_FP32))
+    assert status == 0
+    ke = ke.cpu().numpy()
+    worst = 0.0
+    for e in range(min(m.num_elems, 200)):
+        ref, npe, dpn = _oracle_ke(oracle_mod, m, e)
+        got = fem.unpack_element_stiffness(ke[e], npe, dpn)
+        worst = max(worst, np.max(np.abs(got - ref)) / np.max(np.abs(np.diag(ref))))
+    print(f"{name} FP32 Ke: max error {worst:.3e} of the element's largest diagonal entry")
+    assert worst <= FP32_ELEMENT_TOL
+    with pytest.raises(fem.FemError):
+        fem.element_stiffness(mg.by_name("hex20_small"), fem.opts(precision=fem.FEM_PREC_FP32))

@@ -212,3 +212,29 @@ def test_tensor_core_form_assembly(fem, oracle_mod, cuda_device, name):
     rel, scaled = value_errors(orp, oci, ov, v)
     print(f"{name} tensor-core form: max scaled error {scaled:.3e}, max per-entry relative {rel:.3e}")
     assert scaled <= TC_RTOL
+
+
+# Full assembly with the FP32 Ke form of the 2-D kinds (FEM_PREC_FP32): the
+# pattern is the same bit for bit; the FP32 blocks accumulated in FP64 agree
+# with the FP64 oracle within FP32_RTOL on the row/column scale.
+FP32_RTOL = 1e-5
+
+
+@pytest.mark.parametrize("name", ["q4_small", "t3_small", "mixed_small", "t3"])
+def test_fp32_form_assembly(fem, oracle_mod, cuda_device, name):
+    import meshgen as mg
+    m = mg.by_name(name)
+    rp, ci, v, info = fem.assemble(m, fem.opts(precision=fem.FEM_PREC_FP32))
+    orp, oci, ov = oracle_mod.assemble(m)
+    np.testing.assert_array_equal(rp, orp)
+    np.testing.assert_array_equal(ci, oci)
+    rel, scaled = value_errors(orp, oci, ov, v)
+    print(f"{name} FP32 form: max scaled error {scaled:.3e}, max per-entry relative {rel:.3e}")
+    assert scaled <= FP32_RTOL
+    assert info["list_entries"] == oci.shape[0] // 4
+
+
+def test_fp32_form_rejected_for_hex20(fem, cuda_device):
+    import meshgen as mg
+    with pytest.raises(fem.FemError):
+        fem.assemble(mg.by_name("hex20_small"), fem.opts(precision=fem.FEM_PREC_FP32))

@@ -56,3 +56,23 @@ def test_reassembly_after_moving_nodes(fem, oracle_mod, cuda_device, name):
     rel, scaled = value_errors(orp2, oci2, ov2, vals.cpu().numpy())
     print(f"{name}: re-assembly max scaled error {scaled:.2e}")
     assert scaled <= RTOL, scaled
+
+
+@pytest.mark.parametrize("name", ["t3_small", "mixed_small"])
+def test_fp32_reassembly(fem, oracle_mod, cuda_device, name):
+    # value-only re-assembly with the FP32 blocks of the 2-D kinds
+    import torch
+    import meshgen as mg
+    m = mg.by_name(name)
+    asm = fem.Assembler(m)
+    rp, ci, v, info = asm.assemble()
+    nnz = int(info.nnz)
+    re = fem.Reassembler(asm)
+    re.build(nnz)
+    vals = torch.empty(nnz, dtype=torch.float64, device=rp.device)
+    re.reassemble(vals, fem.opts(precision=fem.FEM_PREC_FP32))
+    assert re.read_info() == 0
+    orp, oci, ov = oracle_mod.assemble(m)
+    rel, scaled = value_errors(orp, oci, ov, vals.cpu().numpy())
+    print(f"{name}: FP32 re-assembly max scaled error {scaled:.2e}")
+    assert scaled <= 1e-5, scaled
