@@ -114,3 +114,61 @@ def test_fp32_element_stiffness_error(fem, oracle_mod, cuda_device, name):
     assert worst <= FP32_ELEMENT_TOL
     with pytest.raises(fem.FemError):
         fem.element_stiffness(mg.by_name("hex20_small"), fem.opts(precision=fem.FEM_PREC_FP32))
+
+
+def _tc_error(fem, oracle_mod, m, ke):
+    worst = 0.0
+    for e in range(m.num_elems):
+        ref, npe, dpn = _oracle_ke(oracle_mod, m, e)
+        got = fem.unpack_element_stiffness(ke[e], npe, dpn)
+        worst = max(worst, np.max(np.abs(got - ref)) / np.max(np.abs(np.diag(ref))))
+    return worst
+
+
+def test_tensor_core_odd_count_and_unaligned_output(fem, oracle_mod, cuda_device):
+    # The tensor-core kernel takes elements in pairs: an odd count leaves the
+    # last pair half empty. An output that is not 16-byte aligned is written
+    # with plain stores instead of the bulk copy; the neighbouring doubles
+    # must stay untouched.
+    import torch
+    import meshgen as mg
+    m = mg.by_name("hex20_small")
+    k = m.num_elems - 1 if m.num_elems % 2 == 0 else m.num_elems
+    m.conn = m.conn[:k].copy()
+    if m.E is not None:
+        m.E = m.E[:k]
+    if m.nu is not None:
+        m.nu = m.nu[:k]
+    assert k % 2 == 1
+    ke, status = fem.element_stiffness(m, fem.opts(precision=1))
+    assert status == 0
+    assert _tc_error(fem, oracle_mod, m, ke.cpu().numpy()) <= TC_ELEMENT_TOL
+    n = ke.shape[1]
+    buf = torch.full((k * n + 2,), 7.0, dtype=torch.float64, device=ke.device)
+    out = buf[1:1 + k * n].view(k, n)                     # 8 bytes past a 16-byte boundary
+    ke2, status = fem.element_stiffness(m, fem.opts(precision=1), out=out)
+    assert status == 0
+    assert torch.equal(ke2, ke)
+    assert buf[0].item() == 7.0 and buf[-1].item() == 7.0
+
+
+def test_tensor_core_inverted_element(fem, oracle_mod, cuda_device):
+    # An element with negative Gauss-point weights (detJ < 0): FEM_ERR_DETJ is
+    # raised and its Ke still follows the signed weights (B = A diag(sgn w)).
+    import meshgen as mg
+    m = mg.hex20_grid(2, seed=3)
+    m.conn = m.conn.copy()
+    c = m.conn[1]
+    # mirror the element in zeta: swap its bottom and top faces (and the edge nodes)
+    m.conn[1] = c[[4, 5, 6, 7, 0, 1, 2, 3, 12, 13, 14, 15, 8, 9, 10, 11, 16, 17, 18, 19]]
+    ke, status = fem.element_stiffness(m, fem.opts(precision=1))
+    assert status & (1 << fem.FEM_ERR_DETJ)
+    ke64, status64 = fem.element_stiffness(m)
+    assert status64 & (1 << fem.FEM_ERR_DETJ)
+    ke, ke64 = ke.cpu().numpy(), ke64.cpu().numpy()
+    for e in range(m.num_elems):
+        ref, npe, dpn = _oracle_ke(oracle_mod, m, e)
+        got = fem.unpack_element_stiffness(ke[e], npe, dpn)
+        assert np.max(np.abs(got - ref)) <= TC_ELEMENT_TOL * np.max(np.abs(np.diag(ref))), e
+        got64 = fem.unpack_element_stiffness(ke64[e], npe, dpn)
+        assert np.max(np.abs(got64 - ref)) <= 1e-12 * np.max(np.abs(np.diag(ref))), e
