@@ -207,6 +207,8 @@ fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* wo
     if ((st = check_ws(h, workspace, workspace_bytes))) return st;
     const int precision = opts ? opts->precision : FEM_PREC_FP64;
     if (!assembly_precision_ok(precision, h.kind)) return FEM_ERR_BAD_ARG;
+    const int ctas = opts ? opts->ctas_per_sm : 0;
+    if (ctas < 0) return FEM_ERR_BAD_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     ListLayout L = device_layout(h, workspace);
     unsigned char* b = static_cast<unsigned char*>(workspace);
@@ -229,11 +231,11 @@ fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* wo
             b + h.off_elist + align_up((size_t)h.E * sizeof(int)) + align_up(4 * sizeof(int)) +
             align_up(nbuckets * sizeof(int)));
         err = launch_reorder_3d(m, hist, ranges, perm, bbox, sm_count(), s);
-        if (!err) err = launch_scatter_hex20(m, L, precision, perm, s);
+        if (!err) err = launch_scatter_hex20(m, L, precision, perm, ctas, s);
     } else {
         err = launch_reorder(m, hist, ranges, perm, sm_count(), s);
-        if (!err && h.kind != FEM_T3) err = launch_scatter_2d(m, L, 4, precision, perm, ranges + 0, s);
-        if (!err && h.kind != FEM_Q4) err = launch_scatter_2d(m, L, 3, precision, perm, ranges + 2, s);
+        if (!err && h.kind != FEM_T3) err = launch_scatter_2d(m, L, 4, precision, perm, ranges + 0, ctas, s);
+        if (!err && h.kind != FEM_Q4) err = launch_scatter_2d(m, L, 3, precision, perm, ranges + 2, ctas, s);
     }
     return err ? cuda_fail(err) : FEM_OK;
 }
@@ -449,6 +451,156 @@ fem_status fem_assemble_batched(const fem_mesh* meshes, int32_t n, const fem_opt
         outs[i].n_rows = meshes[i].num_nodes * kind_dpn(meshes[i].kind);
     }
     err = batch_join(slots, s);
+    return err ? cuda_fail(err) : FEM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Autotuner
+// ---------------------------------------------------------------------------
+
+namespace {
+
+// Candidate options for one mesh: the scatter grid (all resident CTAs, or
+// 1..3 per SM) and, for Hex20, the list shape (first chunk 94 / 62 / 46
+// slots, overflow chunks of 30; a pool of one overflow chunk per node for the
+// smaller first chunks, whose corner-node rows spill).
+std::vector<fem_opts> tune_candidates(const fem_mesh* m, const fem_opts* base) {
+    fem_opts b{};
+    if (base) b = *base;
+    std::vector<fem_opts> out;
+    const int ctas[] = {0, 1, 2, 3};
+    if (m->kind == FEM_HEX20) {
+        const int first[] = {94, 62, 46};
+        for (int f : first)
+            for (int c : ctas) {
+                fem_opts o = b;
+                o.first_slots = f;
+                o.chunk_slots = 30;
+                if (f < 94) o.pool_factor = std::max(o.pool_factor, 1.0);
+                o.ctas_per_sm = c;
+                out.push_back(o);
+            }
+    } else {
+        for (int c : ctas) {
+            fem_opts o = b;
+            o.first_slots = o.chunk_slots = 0;
+            o.ctas_per_sm = c;
+            out.push_back(o);
+        }
+    }
+    return out;
+}
+
+// Mean milliseconds of `repeats` calls of fn() on stream s (CUDA events).
+template <typename Fn>
+fem_status time_calls(cudaStream_t s, int repeats, Fn fn, float& ms) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaError_t err = cudaEventCreate(&a);
+    if (!err) err = cudaEventCreate(&b);
+    fem_status st = FEM_OK;
+    if (!err) err = cudaEventRecord(a, s);
+    for (int r = 0; r < repeats && !err && !st; r++) st = fn();
+    if (!err && !st) err = cudaEventRecord(b, s);
+    if (!err && !st) err = cudaEventSynchronize(b);
+    if (!err && !st) err = cudaEventElapsedTime(&ms, a, b);
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (err) return cuda_fail(err);
+    if (!st) ms /= (float)repeats;
+    return st;
+}
+
+fem_status not_capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const cudaError_t err = cudaStreamIsCapturing(s, &cs);
+    if (err) return cuda_fail(err);
+    return cs == cudaStreamCaptureStatusNone ? FEM_OK : FEM_ERR_BAD_ARG;
+}
+
+}  // namespace
+
+extern "C" {
+
+fem_status fem_autotune_workspace_size(const fem_mesh* mesh, const fem_opts* opts, size_t* bytes) {
+    fem_status st = check_mesh(mesh);
+    if (st) return st;
+    if (!bytes) return FEM_ERR_BAD_ARG;
+    *bytes = 0;
+    for (const fem_opts& o : tune_candidates(mesh, opts)) {
+        size_t b = 0;
+        if ((st = fem_alls_workspace_size(mesh, &o, &b))) return st;
+        *bytes = std::max(*bytes, b);
+    }
+    return FEM_OK;
+}
+
+fem_status fem_autotune(const fem_mesh* mesh, const fem_opts* opts, void* workspace, size_t workspace_bytes,
+                        fem_csr* out, int32_t repeats, fem_opts* best, float* best_ms, void* stream) {
+    if (!out || !best || repeats < 1) return FEM_ERR_BAD_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    fem_status st = not_capturing(s);
+    if (st) return st;
+    if ((st = check_mesh(mesh))) return st;
+    bool found = false;
+    float best_t = 0.0f;
+    for (const fem_opts& o : tune_candidates(mesh, opts)) {
+        size_t need = 0;
+        if ((st = fem_alls_workspace_size(mesh, &o, &need))) return st;
+        if (need > workspace_bytes) continue;
+        // one untimed run: its status decides whether the candidate counts
+        fem_csr c = *out;
+        st = fem_assemble(mesh, &o, workspace, workspace_bytes, &c, stream);
+        if (st == FEM_ERR_POOL_OVERFLOW) continue;
+        if (st && st != FEM_ERR_DETJ) return st;
+        float ms = 0.0f;
+        st = time_calls(s, repeats, [&] { return fem_assemble_async(mesh, &o, workspace, workspace_bytes, &c, stream); },
+                        ms);
+        if (st) return st;
+        if (!found || ms < best_t) {
+            found = true;
+            best_t = ms;
+            *best = o;
+        }
+    }
+    if (!found) return FEM_ERR_WORKSPACE;
+    if (best_ms) *best_ms = best_t;
+    // leave the chosen options' assembly in out
+    return fem_assemble(mesh, best, workspace, workspace_bytes, out, stream);
+}
+
+fem_status fem_autotune_batched(const fem_mesh* meshes, int32_t n, const fem_opts* opts, void* workspace,
+                                size_t workspace_bytes, fem_csr* outs, fem_info* infos, int32_t repeats,
+                                int32_t* best_concurrency, float* best_ms, void* stream) {
+    if (!meshes || n <= 0 || !outs || !infos || !best_concurrency || repeats < 1) return FEM_ERR_BAD_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    fem_status st = not_capturing(s);
+    if (st) return st;
+    bool found = false;
+    float best_t = 0.0f;
+    for (int k = 1; k <= kMaxBatchConcurrency && k <= std::max(1, (int)n); k *= 2) {
+        size_t need = 0;
+        if ((st = fem_batched_workspace_size(meshes, n, opts, k, &need))) return st;
+        if (need > workspace_bytes) continue;
+        auto run = [&] {
+            return fem_assemble_batched(meshes, n, opts, k, workspace, workspace_bytes, outs, infos, nullptr, stream);
+        };
+        if ((st = run())) return st;  // untimed (creates the slot streams)
+        float ms = 0.0f;
+        if ((st = time_calls(s, repeats, run, ms))) return st;
+        if (!found || ms < best_t) {
+            found = true;
+            best_t = ms;
+            *best_concurrency = k;
+        }
+    }
+    if (!found) return FEM_ERR_WORKSPACE;
+    if (best_ms) *best_ms = best_t;
+    st = fem_assemble_batched(meshes, n, opts, *best_concurrency, workspace, workspace_bytes, outs, infos, nullptr,
+                              stream);
+    if (st) return st;
+    const cudaError_t err = cudaStreamSynchronize(s);
     return err ? cuda_fail(err) : FEM_OK;
 }
 

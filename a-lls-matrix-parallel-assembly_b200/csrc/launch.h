@@ -28,8 +28,9 @@ constexpr int k2DSlots = 14;
 
 // perm: element visit order; range: device ints {begin, end} into perm;
 // precision FEM_PREC_FP64 or FEM_PREC_FP32 (the arithmetic of the Ke blocks).
+// ctas_per_sm: cap on the persistent grid's resident CTAs per SM (0 = all that fit).
 cudaError_t launch_scatter_2d(const MeshView& m, const ListLayout& L, int npe, int precision, const int* perm,
-                              const int* range, cudaStream_t s);
+                              const int* range, int ctas_per_sm, cudaStream_t s);
 // Node-local element order (perm) and the element ranges {q4 begin, q4 end, t3 begin, t3 end}.
 int reorder_buckets(int num_nodes);
 cudaError_t launch_reorder(const MeshView& m, int* hist, int* ranges, int* perm, int sms, cudaStream_t s);
@@ -67,7 +68,7 @@ cudaError_t launch_colour_hex20(const MeshView& m, const int* perm, const int* r
                                 DevInfo* info, cudaStream_t s);
 
 // perm: element visit order (spatial, from launch_reorder_3d); precision FEM_PREC_*.
-cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm,
+cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm, int ctas_per_sm,
                                  cudaStream_t s);
 // Spatial (3-D Morton bucket) element order; hist needs 1 << (3 * morton_bits(E)) ints, bbox 6 words.
 int morton_bits(int num_elems);

@@ -223,31 +223,31 @@ __global__ void __launch_bounds__(kThreads2D, NPE == 3 ? 4 : 2)
 
 template <int NPE, typename T>
 cudaError_t launch_scatter_2d_t(const MeshView& m, const ListLayout& L, const int* perm, const int* range,
-                                cudaStream_t s) {
+                                int ctas_per_sm, cudaStream_t s) {
     // A persistent grid: every warp runs the pipeline over many elements.
-    static int resident = 0;
-    if (!resident) {
-        int per_sm = 0;
+    static int per_sm = 0;
+    if (!per_sm) {
         const cudaError_t err =
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scatter_2d<NPE, T>, kThreads2D, 0);
         if (err) return err;
-        resident = std::max(per_sm, 1) * sm_count();
+        per_sm = std::max(per_sm, 1);
     }
+    const int use = ctas_per_sm > 0 ? std::min(ctas_per_sm, per_sm) : per_sm;
     constexpr int epw = 32 / (NPE * NPE);
     const long long warps = ((long long)m.E_count + epw - 1) / epw;
     const long long want = (warps + kWarps2D - 1) / kWarps2D;
-    const int grid = (int)std::min<long long>(want > 0 ? want : 1, (long long)resident);
+    const int grid = (int)std::min<long long>(want > 0 ? want : 1, (long long)use * sm_count());
     k_scatter_2d<NPE, T><<<grid, kThreads2D, 0, s>>>(m, L, perm, range);
     return cudaGetLastError();
 }
 
 cudaError_t launch_scatter_2d(const MeshView& m, const ListLayout& L, int npe, int precision, const int* perm,
-                              const int* range, cudaStream_t s) {
+                              const int* range, int ctas_per_sm, cudaStream_t s) {
     if (precision == FEM_PREC_FP32)
-        return npe == 4 ? launch_scatter_2d_t<4, float>(m, L, perm, range, s)
-                        : launch_scatter_2d_t<3, float>(m, L, perm, range, s);
-    return npe == 4 ? launch_scatter_2d_t<4, double>(m, L, perm, range, s)
-                    : launch_scatter_2d_t<3, double>(m, L, perm, range, s);
+        return npe == 4 ? launch_scatter_2d_t<4, float>(m, L, perm, range, ctas_per_sm, s)
+                        : launch_scatter_2d_t<3, float>(m, L, perm, range, ctas_per_sm, s);
+    return npe == 4 ? launch_scatter_2d_t<4, double>(m, L, perm, range, ctas_per_sm, s)
+                    : launch_scatter_2d_t<3, double>(m, L, perm, range, ctas_per_sm, s);
 }
 
 }  // namespace fem

@@ -561,7 +561,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
 
 template <bool kTc, int kOut>
 cudaError_t launch_scatter_hex20_t(const MeshView& m, const ListLayout& L, const int* perm, const MapTarget& t,
-                                   const int* range, cudaStream_t s) {
+                                   const int* range, cudaStream_t s, int ctas_per_sm = 0) {
     static int blocks_per_sm = 0;
     const size_t smem = sizeof(Hex20Smem);
     if (!blocks_per_sm) {
@@ -572,17 +572,19 @@ cudaError_t launch_scatter_hex20_t(const MeshView& m, const ListLayout& L, const
         if (err) return err;
         if (blocks_per_sm < 1) blocks_per_sm = 1;
     }
-    long long grid = (long long)blocks_per_sm * sm_count();
+    const int use = ctas_per_sm > 0 ? std::min(ctas_per_sm, blocks_per_sm) : blocks_per_sm;
+    long long grid = (long long)use * sm_count();
     if (grid > m.E_count) grid = m.E_count > 0 ? m.E_count : 1;
     k_scatter_hex20<kTc, kOut><<<(int)grid, kThreads, smem, s>>>(m, L, perm, t, range);
     return cudaGetLastError();
 }
 
-cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm,
+cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm, int ctas_per_sm,
                                  cudaStream_t s) {
     const MapTarget none{};
-    return precision == FEM_PREC_TC_F16X3 ? launch_scatter_hex20_t<true, kOutLists>(m, L, perm, none, nullptr, s)
-                                          : launch_scatter_hex20_t<false, kOutLists>(m, L, perm, none, nullptr, s);
+    return precision == FEM_PREC_TC_F16X3
+               ? launch_scatter_hex20_t<true, kOutLists>(m, L, perm, none, nullptr, s, ctas_per_sm)
+               : launch_scatter_hex20_t<false, kOutLists>(m, L, perm, none, nullptr, s, ctas_per_sm);
 }
 
 cudaError_t launch_reassemble_hex20(const MeshView& m, int precision, const int* perm, const MapTarget& t,

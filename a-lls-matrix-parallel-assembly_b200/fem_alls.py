@@ -38,6 +38,7 @@ EXPORTS = ["fem_alls_workspace_size", "fem_alls_scatter", "fem_alls_consolidate"
            "fem_colour_read_info", "fem_element_stiffness_size", "fem_element_stiffness",
            "fem_scatter_map_size", "fem_scatter_map_build", "fem_reassemble_values", "fem_scatter_map_read_info",
            "fem_batched_workspace_size", "fem_assemble_batched", "fem_alls_consolidate_bsr",
+           "fem_autotune_workspace_size", "fem_autotune", "fem_autotune_batched",
            "fem_assemble_body_force", "fem_apply_dirichlet"]
 STATIC_WORKSPACE_BYTES = 32 << 20  # FEM_STATIC_WORKSPACE_BYTES
 
@@ -51,7 +52,7 @@ class FemMesh(C.Structure):
 
 class FemOpts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("first_slots", C.c_int32), ("chunk_slots", C.c_int32),
-                ("flags", C.c_int32), ("pool_factor", C.c_double)]
+                ("ctas_per_sm", C.c_int32), ("pool_factor", C.c_double)]
 
 
 class FemCsr(C.Structure):
@@ -115,6 +116,11 @@ def load() -> C.CDLL:
         L.fem_alls_consolidate_bsr.argtypes = [p(FemMesh), p(FemOpts), vp, C.c_size_t, vp, vp, vp, C.c_int64, vp]
         L.fem_assemble_body_force.argtypes = [p(FemMesh), vp, vp, vp, vp, vp]
         L.fem_apply_dirichlet.argtypes = [C.c_int32, vp, vp, vp, vp, vp, vp, vp]
+        L.fem_autotune_workspace_size.argtypes = [p(FemMesh), p(FemOpts), p(C.c_size_t)]
+        L.fem_autotune.argtypes = [p(FemMesh), p(FemOpts), vp, C.c_size_t, p(FemCsr), C.c_int32, p(FemOpts),
+                                   p(C.c_float), vp]
+        L.fem_autotune_batched.argtypes = [p(FemMesh), C.c_int32, p(FemOpts), vp, C.c_size_t, p(FemCsr), vp,
+                                           C.c_int32, p(C.c_int32), p(C.c_float), vp]
         L.fem_status_string.argtypes = [C.c_int32]
         L.fem_status_string.restype = C.c_char_p
         for f in EXPORTS:
@@ -127,8 +133,9 @@ def load() -> C.CDLL:
 FEM_PREC_FP64, FEM_PREC_TC_F16X3, FEM_PREC_FP64_SIMT, FEM_PREC_FP32 = 0, 1, 2, 3
 
 
-def opts(first_slots: int = 0, chunk_slots: int = 0, pool_factor: float = 0.0, precision: int = 0) -> FemOpts:
-    return FemOpts(precision, first_slots, chunk_slots, 0, pool_factor)
+def opts(first_slots: int = 0, chunk_slots: int = 0, pool_factor: float = 0.0, precision: int = 0,
+         ctas_per_sm: int = 0) -> FemOpts:
+    return FemOpts(precision, first_slots, chunk_slots, ctas_per_sm, pool_factor)
 
 
 def _ptr(t) -> Optional[int]:
@@ -243,6 +250,29 @@ class Assembler:
         info = FemInfo()
         st = self.lib.fem_alls_read_info(self.ws_ptr, C.byref(info), self._stream())
         return st, info
+
+    def autotune(self, repeats: int = 3) -> tuple:
+        """fem_autotune on this mesh: picks the fastest scatter grid / list shape,
+        adopts it (self.opts, a workspace that fits it) and leaves its assembly in
+        the outputs. Returns (opts, mean ms per assembly)."""
+        torch = self.torch
+        if self.capacity == 0:
+            self.assemble()                      # sizes the outputs
+        n = C.c_size_t(0)
+        check(self.lib.fem_autotune_workspace_size(C.byref(self.cm), C.byref(self.opts), C.byref(n)),
+              "fem_autotune_workspace_size")
+        if n.value > self.ws_bytes:
+            self.ws = torch.empty(n.value + 256, dtype=torch.uint8, device=self.row_ptr.device)
+            self.ws_ptr = (self.ws.data_ptr() + 255) // 256 * 256
+            self.ws_bytes = n.value
+        out = FemCsr(self.n_rows, 0, 0, self.capacity, _ptr(self.row_ptr), _ptr(self.col_idx), _ptr(self.values))
+        best = FemOpts()
+        ms = C.c_float(0.0)
+        st = self.lib.fem_autotune(C.byref(self.cm), C.byref(self.opts), self.ws_ptr, self.ws_bytes, C.byref(out),
+                                   repeats, C.byref(best), C.byref(ms), self._stream())
+        check(st if st != FEM_ERR_DETJ else FEM_OK, "fem_autotune")
+        self.opts = best
+        return best, ms.value
 
     def assemble_async(self):
         """scatter + consolidate into the reserved capacity, no host sync."""
@@ -483,6 +513,19 @@ class Batch:
 
     def run(self, concurrency: Optional[int] = None):
         self._launch(concurrency)
+
+    def autotune(self, repeats: int = 2) -> tuple:
+        """fem_autotune_batched: the fastest concurrency that fits this batch's
+        workspace (sized for concurrency at construction); adopts it. Returns
+        (concurrency, mean ms per batch)."""
+        best = C.c_int32(0)
+        ms = C.c_float(0.0)
+        check(self.lib.fem_autotune_batched(self.cm, len(self.meshes), C.byref(self.opts) if self.opts else None,
+                                            self.ws_ptr, self.ws_bytes, self.outs, _ptr(self.infos), repeats,
+                                            C.byref(best), C.byref(ms), self.torch.cuda.current_stream().cuda_stream),
+              "fem_autotune_batched")
+        self.concurrency = best.value
+        return best.value, ms.value
 
     def statuses(self) -> list:
         raw = self.infos.cpu().numpy()

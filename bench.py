@@ -192,9 +192,10 @@ def cpu_baseline(workload: str, use_reference: bool, workers: int) -> dict:
 
 def run_batched(args, rank: int, world: int, local_rank: int):
     """The batched configuration: 256 meshes assembled by fem_assemble_batched
-    (one call per step, graph-captured), concurrency picked by timing 1/4/8
-    slots; concurrency 1 is the sequential baseline (the same per-mesh launches
-    one after another on one stream). value = elements/s of the whole batch."""
+    (one call per step, graph-captured), concurrency picked by the library's
+    autotuner (fem_autotune_batched: 1/2/4/8/16 slots timed on this batch);
+    concurrency 1 is the sequential baseline (the same per-mesh launches one
+    after another on one stream). value = elements/s of the whole batch."""
     import torch
     import fem_alls as fem
     import meshgen as mg
@@ -205,9 +206,12 @@ def run_batched(args, rank: int, world: int, local_rank: int):
     meshes = mg.batch_meshes(256, seed=5 + rank)
     gen_s = time.perf_counter() - t0
     elems = sum(m.num_elems for m in meshes)
-    slots = (1, 4, 8)
-    b = fem.Batch(meshes, concurrency=max(slots), device=dev)
+    b = fem.Batch(meshes, concurrency=16, device=dev)
     nnz = b.sizes()
+    t0 = time.perf_counter()
+    best, tune_ms = b.autotune(repeats=1)
+    tune_s = time.perf_counter() - t0
+    slots = (1, best) if best != 1 else (1,)
     flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
 
@@ -233,7 +237,6 @@ def run_batched(args, rank: int, world: int, local_rank: int):
         lat = b.latencies_ms()
         per_k[k] = {"ms": statistics.mean(ts), "p50_ms": float(np.percentile(lat, 50)),
                     "p99_ms": float(np.percentile(lat, 99))}
-    best = min((k for k in slots if k > 1), key=lambda k: per_k[k]["ms"])
     # the chosen concurrency captured in a CUDA graph and replayed
     side = torch.cuda.Stream()
     side.wait_stream(stream)
@@ -272,7 +275,9 @@ def run_batched(args, rank: int, world: int, local_rank: int):
         "meshes_per_s": world * len(meshes) / (ms / 1e3),
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "what": "per-mesh completion after the batch start (GPU global timer), graph replay"},
-        "concurrency": {"chosen": best, "timed": {str(k): v for k, v in per_k.items()}},
+        "concurrency": {"chosen": best, "timed": {str(k): v for k, v in per_k.items()},
+                        "autotune": {"api": "fem_autotune_batched (1, 2, 4, 8, 16 slots)", "best_ms": tune_ms,
+                                     "tuning_s": tune_s}},
         "sequential": {"ms": seq["ms"], "meshes_per_s": len(meshes) / (seq["ms"] / 1e3),
                        "p50_ms": seq["p50_ms"], "p99_ms": seq["p99_ms"],
                        "what": "the 256 meshes' launches one after another on one stream (concurrency 1)"},
@@ -393,6 +398,15 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     reasm = None if args.no_reassembly else reassembly(fem, torch, asm, mesh, nnz, args, flush, stream)
     kef = ke_form(fem, torch, mesh, asm.dev, args, flush, stream) if mesh.kind == 2 and not args.no_ke else None
     f32 = fp32_form(fem, torch, asm, mesh, nnz, args, flush, stream) if mesh.kind != 2 and not args.no_ke else None
+    tuned = None
+    if not args.no_autotune:
+        t0 = time.perf_counter()
+        best, best_ms = asm.autotune(repeats=3)
+        tuned = {"api": "fem_autotune (scatter grid CTAs/SM; Hex20 also first/overflow chunk slots)",
+                 "best": {"ctas_per_sm": best.ctas_per_sm, "first_slots": best.first_slots,
+                          "chunk_slots": best.chunk_slots, "pool_factor": best.pool_factor},
+                 "best_ms": best_ms, "default_ms": ms, "tuning_s": time.perf_counter() - t0,
+                 "note": "timed back to back without the L2 flush; the headline uses the default options"}
 
     if rank != 0:
         return
@@ -449,6 +463,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         line["ke_form"] = kef
     if f32:
         line["fp32_form"] = f32
+    if tuned:
+        line["autotune"] = tuned
     if not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args.workload, use_reference=False, workers=1)
     print(json.dumps(line), flush=True)
@@ -672,6 +688,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-colour", action="store_true", help="skip the element-colouring baseline leg")
     ap.add_argument("--no-reassembly", action="store_true", help="skip the value-only re-assembly leg")
+    ap.add_argument("--no-autotune", action="store_true", help="skip the autotuner leg")
     ap.add_argument("--no-ke", action="store_true", help="skip the precision-form leg (Hex20: element-stiffness forms; 2-D: the FP32-form assembly)")
     ap.add_argument("--ke-only", action="store_true",
                     help="Hex20: time only the element-stiffness kernels (FP64 and tensor-core forms)")

@@ -110,7 +110,8 @@ typedef struct fem_opts {
     int32_t precision;     /* FEM_PREC_FP64 */
     int32_t first_slots;   /* list slots in each node's first chunk; 0 = default */
     int32_t chunk_slots;   /* list slots per overflow chunk; 0 = default */
-    int32_t flags;         /* reserved, 0 */
+    int32_t ctas_per_sm;   /* resident CTAs per SM of the scatter kernel's persistent grid
+                              (capped at what fits); 0 = all that fit */
     double pool_factor;    /* overflow chunks per node in the pool; 0 = default */
 } fem_opts;
 
@@ -255,6 +256,35 @@ FEM_API fem_status fem_batched_workspace_size(const fem_mesh* meshes, int32_t n,
 FEM_API fem_status fem_assemble_batched(const fem_mesh* meshes, int32_t n, const fem_opts* opts,
                                         int32_t concurrency, void* workspace, size_t workspace_bytes,
                                         fem_csr* outs, fem_info* infos, unsigned long long* stamps, void* stream);
+
+/* ---- autotuner ------------------------------------------------------------------
+ * Times candidate launch and list shapes on the caller's own mesh or batch and
+ * returns the fastest (no counterpart in the reference, whose launch shape is
+ * fixed at 256 threads per block and one element per thread,
+ * ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:815-818). Each candidate runs once
+ * untimed, then `repeats` times between two CUDA events on `stream`; both calls
+ * synchronize the stream and must not be captured. */
+
+/* Bytes of workspace that every candidate of fem_autotune fits in. */
+FEM_API fem_status fem_autotune_workspace_size(const fem_mesh* mesh, const fem_opts* opts, size_t* bytes);
+
+/* One mesh: the scatter grid (opts.ctas_per_sm: all that fit, 1, 2 or 3) and,
+ * for Hex20, the list shape (first_slots 94, 62 or 46 with chunk_slots 30; pool
+ * factor at least 1 for the smaller first chunks). The precision of opts is
+ * kept. out: as for fem_assemble, with capacity >= nnz; on return it holds the
+ * assembly with the chosen options (status as fem_assemble's). *best: the
+ * fastest options; *best_ms (may be NULL): their mean time per assembly.
+ * Candidates that overflow the pool or do not fit the workspace are skipped. */
+FEM_API fem_status fem_autotune(const fem_mesh* mesh, const fem_opts* opts, void* workspace, size_t workspace_bytes,
+                                fem_csr* out, int32_t repeats, fem_opts* best, float* best_ms, void* stream);
+
+/* A batch: the concurrency of fem_assemble_batched (1, 2, 4, 8, 16 slots, at
+ * most n; candidates whose workspace exceeds workspace_bytes are skipped).
+ * outs / infos as for fem_assemble_batched; on return they hold the batch
+ * assembled with *best_concurrency. */
+FEM_API fem_status fem_autotune_batched(const fem_mesh* meshes, int32_t n, const fem_opts* opts, void* workspace,
+                                        size_t workspace_bytes, fem_csr* outs, fem_info* infos, int32_t repeats,
+                                        int32_t* best_concurrency, float* best_ms, void* stream);
 
 /* ---- value-only re-assembly through a scatter map ----------------------------
  * For a mesh whose connectivity is unchanged between assemblies (new
