@@ -8,8 +8,8 @@
 // split into two FP16 parts A = A_hi + A_lo, and
 //     M = A diag(sgn w) A^T / s^2 ~ (A_lo B_hi^T + A_hi B_lo^T + A_hi B_hi^T) / s^2
 // with B = A diag(sgn w) (B = A unless some w_g < 0), summed in FP32 on the
-// tensor cores. Jacobians, their inverses and determinants, the Ke block
-// formula and the output stay FP64. It replaces the reference's per-thread
+// tensor cores. Jacobians, their inverses and determinants stay FP64; the Ke
+// block formula is applied in FP32 to the FP32 products and the output is FP64. It replaces the reference's per-thread
 // FP32 computeElementStiffnessHex20 (ALLS_Hex20_3D_Assembly_Performance.cu:130-195).
 //
 // One 4-warp CTA takes two elements at a time (persistent over element pairs):
@@ -58,10 +58,9 @@ struct KeTcSmem {
         uint4 op[4][kRows * 4];
         double ke[2][kPackedHex20];  // the pair's packed Ke, staged for the bulk copy
     };
-    double dNt[20][27][3];  // dN_n / dxi_i at Gauss point g
+    double dNt[20][27][4];  // dN_n / dxi_i at Gauss point g (i = 3: padding for 16-byte loads)
     double X[2][20][3];
-    double iJ[2][27][12];   // Jacobian (row-major 3x3), then its inverse with row a at [4a, 4a + 3)
-    double sqw[2][32];      // sqrt |w_g|
+    double iJ[2][27][12];   // Jacobian (row-major 3x3), then sqrt|w_g| times its inverse, row a at [4a, 4a + 3)
     double lam[2], mu[2];
     unsigned long long bound_bits[2];  // bound on s-free |P| sqrt|w| (bits of a positive double)
     unsigned long long dnmax_bits;
@@ -189,14 +188,16 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
 
     uint32_t parity = 0;
     bool timed_out = false;
+    // per-pair flags and bounds, reset again after each pair's last reader
+    // (state in step 4, bounds and signs in step 7)
+    if (tid < 2) {
+        sm.state[tid] = 0;
+        sm.bound_bits[tid] = 0ull;
+        sm.negmask[tid] = 0u;
+    }
+    __syncthreads();
     for (long long p = blockIdx.x; p < npairs; p += gridDim.x) {
         // 1. the pair's nodes and materials
-        if (tid < 2) {
-            sm.state[tid] = 0;
-            sm.bound_bits[tid] = 0ull;
-            sm.negmask[tid] = 0u;
-        }
-        __syncthreads();
         if (tid < 40) {
             const int e = tid / 20, k = tid % 20;
             sm.X[e][k][0] = pre_state == 0 ? pre_x : 0.0;
@@ -253,14 +254,13 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
                 iJ[8] = (J[0] * J[4] - J[1] * J[3]) * r;
                 w = weight3(g / 9) * weight3((g / 3) % 3) * weight3(g % 3) * det;
             }
+            const double sq = sqrt(fabs(w));
 #pragma unroll
             for (int a = 0; a < 3; a++) {
-                Jg[4 * a] = iJ[3 * a];
-                Jg[4 * a + 1] = iJ[3 * a + 1];
-                Jg[4 * a + 2] = iJ[3 * a + 2];
+                Jg[4 * a] = iJ[3 * a] * sq;
+                Jg[4 * a + 1] = iJ[3 * a + 1] * sq;
+                Jg[4 * a + 2] = iJ[3 * a + 2] * sq;
             }
-            const double sq = sqrt(fabs(w));
-            sm.sqw[e][g] = sq;
             double rn = 0.0;
 #pragma unroll
             for (int a = 0; a < 3; a++) rn = fmax(rn, fabs(iJ[3 * a]) + fabs(iJ[3 * a + 1]) + fabs(iJ[3 * a + 2]));
@@ -272,6 +272,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
         if (tid == 0 && bulk_out) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
         __syncthreads();
         // 4. operands: thread t writes row t of A (and of B when a weight is negative)
+        if (tid < 2) sm.state[tid] = 0;  // last read in step 3; next written in step 1
         const bool signed_b = (sm.negmask[0] | sm.negmask[1]) != 0u;
         {
             const int e = tid >> 6, i = tid & 63, l = i & 31;
@@ -293,15 +294,18 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
                         const int g = 8 * kc + 2 * q + h;
                         v[h] = 0.0f;
                         if (g < 27 && real) {
-                            const double* iJ = &sm.iJ[e][g][4 * a];
-                            const double P = fma(iJ[0], sm.dNt[n][g][0], fma(iJ[1], sm.dNt[n][g][1], iJ[2] * sm.dNt[n][g][2]));
-                            v[h] = (float)(s * P * sm.sqw[e][g]);
+                            // sqrt|w_g| P[(n,a)][g] = (sqrt|w_g| iJ_g row a) . dN_g[.][n]
+                            const double2 j01 = *reinterpret_cast<const double2*>(&sm.iJ[e][g][4 * a]);
+                            const double2 d01 = *reinterpret_cast<const double2*>(&sm.dNt[n][g][0]);
+                            const double P = fma(j01.x, d01.x, fma(j01.y, d01.y, sm.iJ[e][g][4 * a + 2] * sm.dNt[n][g][2]));
+                            v[h] = (float)(s * P);
                         }
                     }
-                    const __half h0 = __float2half_rn(v[0]), h1 = __float2half_rn(v[1]);
-                    const __half l0 = __float2half_rn(v[0] - __half2float(h0)), l1 = __float2half_rn(v[1] - __half2float(h1));
-                    hw[q] = pack_half2(h0, h1);
-                    lw[q] = pack_half2(l0, l1);
+                    const __half2 hi = __float22half2_rn(make_float2(v[0], v[1]));
+                    const float2 hf = __half22float2(hi);
+                    const __half2 lo = __float22half2_rn(make_float2(v[0] - hf.x, v[1] - hf.y));  // exact differences
+                    hw[q] = pack_half2(__low2half(hi), __high2half(hi));
+                    lw[q] = pack_half2(__low2half(lo), __high2half(lo));
                     // B = A diag(sgn w): flip the sign bits of the negative-weight points
                     const int g0 = 8 * kc + 2 * q;
                     const unsigned flip = ((neg >> g0) & 1u ? 0x8000u : 0u) | ((neg >> (g0 + 1)) & 1u ? 0x80000000u : 0u);
@@ -355,7 +359,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
             int ex = 0;
             if (bound > 0.0) frexp(bound, &ex);
             const double inv_s2 = ldexp(1.0, 2 * ex);
-            const double lam = sm.lam[e], mu = sm.mu[e];
+            const float lam = (float)sm.lam[e], mu = (float)sm.mu[e];
             double* out = sm.ke[e] + 9 * (I * 20 - I * (I - 1) / 2 - I) + 3 * a;  // + 9 J: block (I, J)
 #pragma unroll
             for (int J = 0; J < 20; J++) {
@@ -368,27 +372,31 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
                 const float t1 = __shfl_sync(0xFFFFFFFFu, send1, src1);  // M[(I,a+1),(J,a)]
                 const float t2 = __shfl_sync(0xFFFFFFFFu, send2, src2);  // M[(I,a+2),(J,a)]
                 const float d1 = __shfl_sync(0xFFFFFFFFu, dg, src1), d2 = __shfl_sync(0xFFFFFFFFu, dg, src2);
+                const float mtr = mu * (dg + d1 + d2);
+                // M[(I,b),(J,a)] for b = 0, 1, 2
+                const float T0 = a == 0 ? dg : (a == 1 ? t2 : t1);
+                const float T1 = a == 0 ? t1 : (a == 1 ? dg : t2);
+                const float T2 = a == 0 ? t2 : (a == 1 ? t1 : dg);
+                // Ke_IJ[a][b] = lam M[(I,a),(J,b)] + mu M[(I,b),(J,a)] + mu delta_ab tr(M_IJ), FP32 on the
+                // FP32 products, then scaled back by 1 / s^2 in FP64
+                const float k0 = fmaf(lam, o0, fmaf(mu, T0, a == 0 ? mtr : 0.0f));
+                const float k1 = fmaf(lam, o1, fmaf(mu, T1, a == 1 ? mtr : 0.0f));
+                const float k2 = fmaf(lam, o2, fmaf(mu, T2, a == 2 ? mtr : 0.0f));
                 if (real && J >= I) {
-                    const double tr = (double)dg + (double)d1 + (double)d2;
-                    // M[(I,b),(J,a)] for b = 0, 1, 2
-                    const double T0 = a == 0 ? dg : (a == 1 ? t2 : t1);
-                    const double T1 = a == 0 ? t1 : (a == 1 ? dg : t2);
-                    const double T2 = a == 0 ? t2 : (a == 1 ? t1 : dg);
-                    double k0 = fma(lam, (double)o0, mu * T0), k1 = fma(lam, (double)o1, mu * T1),
-                           k2 = fma(lam, (double)o2, mu * T2);
-                    if (a == 0) k0 = fma(mu, tr, k0);
-                    if (a == 1) k1 = fma(mu, tr, k1);
-                    if (a == 2) k2 = fma(mu, tr, k2);
-                    out[9 * J] = k0 * inv_s2;
-                    out[9 * J + 1] = k1 * inv_s2;
-                    out[9 * J + 2] = k2 * inv_s2;
+                    out[9 * J] = (double)k0 * inv_s2;
+                    out[9 * J + 1] = (double)k1 * inv_s2;
+                    out[9 * J + 2] = (double)k2 * inv_s2;
                 }
             }
         }
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
-        // 7. copy the pair's Ke out
+        // 7. copy the pair's Ke out (the bounds and signs were last read above)
+        if (tid < 2) {
+            sm.bound_bits[tid] = 0ull;
+            sm.negmask[tid] = 0u;
+        }
         const int nvalid = 2 * p + 1 < m.E_count ? 2 : 1;
         double* dst = ke_out + (size_t)(2 * p) * kPackedHex20;
         if (bulk_out) {
