@@ -21,9 +21,9 @@
 //   entry of M is written to its upper 3x3 node block (so Ke is exactly
 //   symmetric), and the 210 Ke blocks
 //       Ke_IJ[a][b] = lambda M_IJ[a][b] + mu M_IJ[b][a] + mu delta_ab tr(M_IJ)
-//   are written with coalesced stores. With FEM_PREC_TC_F16X3 the contraction
-//   runs on the FP16 tensor cores instead (split operands, FP32 accumulation;
-//   tc_prepare / tc_contract in hex20.cuh). The Gauss-point shape derivatives
+//   are written with coalesced stores. With FEM_PREC_FP64_SIMT the contraction
+//   is plain FP64 dot products instead; FEM_PREC_TC_F16X3 runs the tcgen05
+//   kernel of ke_tcgen05.cu. The Gauss-point shape derivatives
 //   (H20:95-128) are tabulated once per CTA; the next element's nodes and
 //   coordinates are loaded while the current one is computed.
 #include <algorithm>
@@ -56,10 +56,8 @@ struct KeSmem {
     double X[20][3];  // element node coordinates
     double J[27][9];  // Jacobians, then their inverses
     double w[PS];     // Gauss weight * detJ (w[27] = 0 pads the contraction)
-    TcScratch tc;     // FP16 split operands of the tensor-core form
     double lam, mu;
     int bad;
-    unsigned long long dnmax_bits;  // largest |dN| of the table (bits of a positive double)
 };
 static_assert(offsetof(KeSmem, Mb) % 16 == 0, "16-byte copies out of Mb");
 
@@ -69,10 +67,9 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
                  : "d"(a), "d"(b));
 }
 
-// kPrec: the node-pair contraction on the FP64 tensor cores (FEM_PREC_FP64),
-// on the FP16 tensor cores (FEM_PREC_TC_F16X3: tc_prepare / tc_contract of
-// hex20.cuh), or as plain FP64 dot products on the CUDA cores
-// (FEM_PREC_FP64_SIMT, the reference's arithmetic without tensor cores).
+// kPrec: the node-pair contraction on the FP64 tensor cores (FEM_PREC_FP64)
+// or as plain FP64 dot products on the CUDA cores (FEM_PREC_FP64_SIMT, the
+// reference's arithmetic without tensor cores).
 template <int kPrec>
 __global__ void __launch_bounds__(kThreads, 5) k_hex20_ke(MeshView m, double* __restrict__ ke_out,
                                                           int* __restrict__ status) {
@@ -80,9 +77,6 @@ __global__ void __launch_bounds__(kThreads, 5) k_hex20_ke(MeshView m, double* __
     KeSmem& sm = *reinterpret_cast<KeSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
-    if (tid == 0) sm.dnmax_bits = 0ull;
-    __syncthreads();
-    double dnmax = 0.0;
     for (int idx = tid; idx < 27 * 20; idx += kThreads) {
         const int g = idx / 20, n = idx % 20;
         double dx, dy, dz;
@@ -90,9 +84,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_hex20_ke(MeshView m, double* __
         sm.dN[g][0][n] = dx;
         sm.dN[g][1][n] = dy;
         sm.dN[g][2][n] = dz;
-        dnmax = fmax(dnmax, fmax(fabs(dx), fmax(fabs(dy), fabs(dz))));
     }
-    if (kPrec == FEM_PREC_TC_F16X3) atomicMax(&sm.dnmax_bits, (unsigned long long)__double_as_longlong(dnmax));
     if (tid < PS) sm.w[tid] = 0.0;
     // node id and coordinates of the next element, loaded a step ahead
     int pre_n = 0;
@@ -110,10 +102,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_hex20_ke(MeshView m, double* __
 
     for (int e = first; e < end; e += gridDim.x) {
         double* out = ke_out + (size_t)e * kPackedHex20;
-        if (tid == 0) {
-            sm.bad = 0;
-            if (kPrec == FEM_PREC_TC_F16X3) sm.tc.bound_bits = 0ull;
-        }
+        if (tid == 0) sm.bad = 0;
         __syncthreads();
         if (tid < 20) {
             if (pre_n < 0 || pre_n >= m.N) {
@@ -174,8 +163,6 @@ __global__ void __launch_bounds__(kThreads, 5) k_hex20_ke(MeshView m, double* __
 #pragma unroll
             for (int k = 0; k < 9; k++) J[k] = iJ[k];
             sm.w[tid] = weight3(tid / 9) * weight3((tid / 3) % 3) * weight3(tid % 3) * det;
-            if (kPrec == FEM_PREC_TC_F16X3)
-                hex20::tc_gauss_point(sm.tc, tid, J, sm.w[tid], __longlong_as_double((long long)sm.dnmax_bits));
         }
         __syncthreads();
         // P aliases the previous element's M blocks: re-zero its padding.
@@ -225,14 +212,6 @@ __global__ void __launch_bounds__(kThreads, 5) k_hex20_ke(MeshView m, double* __
                 sm.Mb[pair_index(I, J)][3 * a + b] = mv[k];
                 if (I == J) sm.Mb[pair_index(I, I)][3 * b + a] = mv[k];
             }
-        } else if (kPrec == FEM_PREC_TC_F16X3) {
-            tc_prepare<kThreads>(&sm.P[0][0], PS, sm.w, sm.tc, tid);
-            // P is no longer read: its storage takes the M blocks
-            tc_contract<kWarps>(sm.tc, warp, lane, [&](int r, int c, double v) {
-                const int I = r / 3, a = r - 3 * I, J = c / 3, b = c - 3 * J;
-                sm.Mb[pair_index(I, J)][3 * a + b] = v;
-                if (I == J) sm.Mb[pair_index(I, I)][3 * b + a] = v;
-            });
         } else {
         // M = (P diag(w)) P^T on the FP64 tensor cores, upper 8x8 tiles only
         // (M is symmetric): the 36 tiles (mt <= nt) are dealt round-robin to the
