@@ -21,7 +21,10 @@
 // Every dof row of node n holds {c*dpn + b : c in adj(n)} in increasing order,
 // which is the reference's pattern. The same pass can write the node-block
 // (BSR) form instead: one block row per node, the sorted column nodes and
-// their dpn x dpn blocks.
+// their dpn x dpn blocks; or the upper triangle only (columns >= row, the
+// symmetric storage a Cholesky or symmetric solver reads): k_count_upper
+// counts each node's columns >= the node, the scan and row pointers use those
+// counts, and k_write keeps the tail of each sorted row.
 #include <algorithm>
 
 #include "launch.h"
@@ -113,6 +116,99 @@ __global__ void __launch_bounds__(kScanThreads) k_row_ptr(const int* __restrict_
     }
 }
 
+template <int G>
+__device__ __forceinline__ unsigned group_mask(int grp_in_warp) {
+    return G == 32 ? 0xFFFFFFFFu : (((1u << G) - 1u) << (grp_in_warp * G));
+}
+
+// Upper-triangle CSR: entries of node n's dof rows when u of its column nodes
+// are >= n (the node itself among them): row a holds (dpn - a) entries of the
+// diagonal block and dpn of each of the u - 1 later blocks.
+template <int DPN>
+__device__ __forceinline__ long long upper_row_len(int u, int a) {
+    return u > 0 ? (long long)(u - 1) * DPN + (DPN - a) : 0;
+}
+template <int DPN>
+__device__ __forceinline__ long long upper_node_entries(int u) {
+    return u > 0 ? (long long)(u - 1) * DPN * DPN + DPN * (DPN + 1) / 2 : 0;
+}
+
+// Columns >= n in node n's list (a group of G lanes per node).
+template <int G>
+__global__ void __launch_bounds__(kBlockThreads) k_count_upper(ListLayout L, int* __restrict__ ucounts) {
+    constexpr int NPB = kBlockThreads / G;
+    const int tid = threadIdx.x, grp = tid / G, glane = tid % G;
+    const unsigned gmask = group_mask<G>((tid & 31) / G);
+    for (long long nb = (long long)blockIdx.x * NPB; nb < L.N; nb += (long long)gridDim.x * NPB) {
+        const int n = (int)(nb + grp);
+        int cnt = 0;
+        if (n < L.N) {
+            int c = n;
+            for (int step = 0; step < kMaxChainSteps; step++) {
+                const int* meta = chunk_meta(L, c);
+                const int cap = chunk_cap(L, c);
+                const int next = __ldg(meta + 1);
+                for (int s = glane; s < cap; s += G) {
+                    const int col = (__ldg(meta + 2 + s) & kColMask) - 1;
+                    cnt += col >= n;
+                }
+                if (next == 0) break;
+                c = next - 1;
+            }
+        }
+#pragma unroll
+        for (int d = G / 2; d > 0; d >>= 1) cnt += __shfl_xor_sync(gmask, cnt, d);
+        if (n < L.N && glane == 0) ucounts[n] = cnt;
+    }
+}
+
+template <int DPN>
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce_upper(const int* __restrict__ ucounts, int N,
+                                                                    long long* __restrict__ tile_sums) {
+    __shared__ long long s_warp[kScanThreads / 32 + 1];
+    const long long base = (long long)blockIdx.x * kScanTile;
+    long long sum = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        const long long n = base + (long long)i * kScanThreads + threadIdx.x;
+        if (n < N) sum += upper_node_entries<DPN>(__ldg(ucounts + n));
+    }
+    long long total;
+    block_exclusive_scan(sum, s_warp, total);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+template <int DPN>
+__global__ void __launch_bounds__(kScanThreads) k_row_ptr_upper(const int* __restrict__ ucounts, int N,
+                                                                const long long* __restrict__ tile_offsets,
+                                                                int* __restrict__ row_ptr) {
+    __shared__ long long s_warp[kScanThreads / 32 + 1];
+    const long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+    int c[kScanItems];
+    long long sum = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        const long long n = base + i;
+        c[i] = n < N ? __ldg(ucounts + n) : 0;
+        sum += upper_node_entries<DPN>(c[i]);
+    }
+    long long total;
+    long long off = tile_offsets[blockIdx.x] + block_exclusive_scan(sum, s_warp, total);
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        const long long n = base + i;
+        if (n < N) {
+            long long r = off;
+#pragma unroll
+            for (int a = 0; a < DPN; a++) {
+                row_ptr[n * DPN + a] = (int)r;
+                r += upper_row_len<DPN>(c[i], a);
+            }
+        }
+        off += upper_node_entries<DPN>(c[i]);
+    }
+}
+
 // Ascending bitonic sort of G*KPL keys held as keys[i] at position lane*KPL + i
 // of a G-lane group. Every lane of the warp must call it.
 template <int G, int KPL>
@@ -150,11 +246,6 @@ __device__ __forceinline__ void group_sort(unsigned long long (&keys)[KPL], int 
             }
         }
     }
-}
-
-template <int G>
-__device__ __forceinline__ unsigned group_mask(int grp_in_warp) {
-    return G == 32 ? 0xFFFFFFFFu : (((1u << G) - 1u) << (grp_in_warp * G));
 }
 
 // Slow path for a row with more entries than a group can sort at once (a node
@@ -264,12 +355,65 @@ __device__ void long_row_write_bsr(const ListLayout& L, int n, int u, long long 
     }
 }
 
-// kBsr: block (BSR) output, one block row per node: block_col_idx = column
-// node, block values dpn x dpn row-major; row_ptr is then the block row pointer.
-template <int DPN, int G, int KPL, bool kBsr>
+// Long-row slow path of the upper-triangle output: the node's u column nodes
+// >= n in increasing order (the first is n itself).
+template <int DPN, int G>
+__device__ void long_row_write_upper(const ListLayout& L, int n, int u, const int* __restrict__ row_ptr, int glane,
+                                     unsigned mask, int* __restrict__ col_idx, double* __restrict__ values) {
+    constexpr int B = DPN * DPN;
+    int last = n - 1;
+    for (int k = 0; k < u; k++) {
+        const int col = long_row_next_col<G>(L, n, last, glane, mask);
+        last = col;
+        double sum[B];
+#pragma unroll
+        for (int v = 0; v < B; v++) sum[v] = 0.0;
+        int c = n;
+        for (int step = 0; step < kMaxChainSteps; step++) {
+            const int* meta = chunk_meta(L, c);
+            const int cap = chunk_cap(L, c);
+            const int next = __ldg(meta + 1);
+            for (int s = glane; s < cap; s += G) {
+                if ((__ldg(meta + 2 + s) & kColMask) - 1 == col) {
+                    const double* p = L.vals + (size_t)slot_gid(L, c, s) * B;
+#pragma unroll
+                    for (int v = 0; v < B; v++) sum[v] += __ldg(p + v);
+                }
+            }
+            if (next == 0) break;
+            c = next - 1;
+        }
+#pragma unroll
+        for (int v = 0; v < B; v++) {
+#pragma unroll
+            for (int d = G / 2; d > 0; d >>= 1) sum[v] += __shfl_xor_sync(mask, sum[v], d);
+        }
+        if (glane == 0) {
+#pragma unroll
+            for (int a = 0; a < DPN; a++) {
+                const long long rbase = __ldg(row_ptr + (size_t)n * DPN + a);
+#pragma unroll
+                for (int b = 0; b < DPN; b++) {
+                    if (k == 0 && b < a) continue;  // below the diagonal
+                    const long long pos = k == 0 ? rbase + (b - a) : rbase + (DPN - a) + (long long)(k - 1) * DPN + b;
+                    col_idx[pos] = col * DPN + b;
+                    values[pos] = sum[a * DPN + b];
+                }
+            }
+        }
+    }
+}
+
+enum : int { kOutCsr = 0, kOutBsr = 1, kOutUpper = 2 };
+
+// kMode kOutBsr: block (BSR) output, one block row per node: block_col_idx =
+// column node, block values dpn x dpn row-major; row_ptr is then the block row
+// pointer. kOutUpper: the upper triangle in CSR (ucounts: columns >= n).
+template <int DPN, int G, int KPL, int kMode>
 __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int* __restrict__ row_ptr,
                                                          int* __restrict__ col_idx, double* __restrict__ values,
-                                                         long long capacity) {
+                                                         long long capacity, const int* __restrict__ ucounts) {
+    constexpr bool kBsr = kMode == kOutBsr;
     constexpr int NPB = kBlockThreads / G;  // nodes per batch
     constexpr int NK = G * KPL;             // sort capacity per node
     constexpr int B = DPN * DPN;
@@ -286,7 +430,9 @@ __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int
         int u = 0;
         long long base = 0;
         if (valid) {
-            if (kBsr) {
+            if (kMode == kOutUpper) {
+                u = __ldg(ucounts + n);  // columns >= n (the full row count is in L.counts)
+            } else if (kBsr) {
                 base = __ldg(row_ptr + n);
                 u = __ldg(row_ptr + n + 1) - (int)base;
             } else {
@@ -314,12 +460,13 @@ __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int
                 if (next == 0) break;
                 c = next - 1;
             }
-            if (glane == 0 && T != u) raise_status(L.info, FEM_ERR_INTERNAL);
+            const int expect = kMode == kOutUpper ? __ldg(L.counts + n) : u;
+            if (glane == 0 && (T != expect || u > T)) raise_status(L.info, FEM_ERR_INTERNAL);
         }
         t_sum += T;
         t_max = max(t_max, T);
         const bool long_row = T > NK;
-        const int Ts = long_row ? 0 : min(T, u);
+        const int Ts = long_row ? 0 : min(T, kMode == kOutUpper ? T : u);
         __syncwarp();
         // 2. sort
         unsigned long long keys[KPL];
@@ -332,8 +479,32 @@ __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int
 #pragma unroll
         for (int i = 0; i < KPL; i++) s_keys[grp][glane * KPL + i] = keys[i];
         __syncwarp();
-        // 3. write the dpn rows of the node (or its block row)
-        if (valid && kBsr) {
+        // 3. write the dpn rows of the node (or its block row, or its upper rows)
+        if (valid && kMode == kOutUpper) {
+            if (long_row) {
+                long_row_write_upper<DPN, G>(L, n, u, row_ptr, glane, gmask, col_idx, values);
+            } else if (u > 0 && u <= Ts) {
+                const int k0 = Ts - u;  // the sorted row's first column >= n (n itself)
+                for (int a = 0; a < DPN; a++) {
+                    const long long rbase = __ldg(row_ptr + (size_t)n * DPN + a);
+                    const int len = (u - 1) * DPN + (DPN - a);
+                    for (int r = glane; r < len; r += G) {
+                        int k, b;
+                        if (r < DPN - a) {
+                            k = k0;
+                            b = a + r;
+                        } else {
+                            const int q = r - (DPN - a);
+                            k = k0 + 1 + q / DPN;
+                            b = q - (q / DPN) * DPN;
+                        }
+                        const unsigned long long key = s_keys[grp][k];
+                        col_idx[rbase + r] = (int)(key >> 32) * DPN + b;
+                        values[rbase + r] = __ldg(L.vals + (size_t)(unsigned)key * B + a * DPN + b);
+                    }
+                }
+            }
+        } else if (valid && kBsr) {
             if (long_row) {
                 long_row_write_bsr<DPN, G>(L, n, u, base, glane, gmask, col_idx, values);
             } else {
@@ -391,6 +562,7 @@ __global__ void k_consolidate_reset(DevInfo* info) {
 template <int DPN, int G, int KPL, bool kBsr>
 cudaError_t launch_all(const ListLayout& L, int* row_ptr, int* col_idx, double* values, long long capacity,
                        long long* tile_sums, int num_tiles, cudaStream_t s) {
+    constexpr int kMode = kBsr ? kOutBsr : kOutCsr;
     // capacity is in scalar entries (BSR: blocks * dpn^2)
     k_consolidate_reset<<<1, 1, 0, s>>>(L.info);
     k_scan_reduce<DPN * DPN><<<num_tiles, kScanThreads, 0, s>>>(L.counts, L.N, tile_sums);
@@ -401,9 +573,25 @@ cudaError_t launch_all(const ListLayout& L, int* row_ptr, int* col_idx, double* 
         constexpr int NPB = kBlockThreads / G;
         const long long batches = ((long long)L.N + NPB - 1) / NPB;
         const long long grid = std::min<long long>(batches, (long long)sm_count() * 8);
-        k_write<DPN, G, KPL, kBsr><<<(int)(grid > 0 ? grid : 1), kBlockThreads, 0, s>>>(L, row_ptr, col_idx, values,
-                                                                                      capacity);
+        k_write<DPN, G, KPL, kMode><<<(int)(grid > 0 ? grid : 1), kBlockThreads, 0, s>>>(L, row_ptr, col_idx, values,
+                                                                                       capacity, nullptr);
     }
+    return cudaGetLastError();
+}
+
+template <int DPN, int G, int KPL>
+cudaError_t launch_upper(const ListLayout& L, int* ucounts, int* row_ptr, int* col_idx, double* values,
+                         long long capacity, long long* tile_sums, int num_tiles, cudaStream_t s) {
+    constexpr int NPB = kBlockThreads / G;
+    const long long batches = ((long long)L.N + NPB - 1) / NPB;
+    const int grid = (int)std::max<long long>(1, std::min<long long>(batches, (long long)sm_count() * 8));
+    k_consolidate_reset<<<1, 1, 0, s>>>(L.info);
+    k_count_upper<G><<<grid, kBlockThreads, 0, s>>>(L, ucounts);
+    k_scan_reduce_upper<DPN><<<num_tiles, kScanThreads, 0, s>>>(ucounts, L.N, tile_sums);
+    k_scan_tiles<<<1, kScanThreads, 0, s>>>(tile_sums, num_tiles, L.info, row_ptr + (size_t)L.N * DPN, capacity, 1);
+    k_row_ptr_upper<DPN><<<num_tiles, kScanThreads, 0, s>>>(ucounts, L.N, tile_sums, row_ptr);
+    if (capacity > 0)
+        k_write<DPN, G, KPL, kOutUpper><<<grid, kBlockThreads, 0, s>>>(L, row_ptr, col_idx, values, capacity, ucounts);
     return cudaGetLastError();
 }
 
@@ -413,6 +601,13 @@ cudaError_t launch_consolidate(const ListLayout& L, int dpn, int* row_ptr, int* 
                                long long capacity, long long* tile_sums, int num_tiles, cudaStream_t s) {
     if (dpn == 3) return launch_all<3, 32, 4, false>(L, row_ptr, col_idx, values, capacity, tile_sums, num_tiles, s);
     return launch_all<2, 8, 2, false>(L, row_ptr, col_idx, values, capacity, tile_sums, num_tiles, s);
+}
+
+cudaError_t launch_consolidate_upper(const ListLayout& L, int dpn, int* ucounts, int* row_ptr, int* col_idx,
+                                     double* values, long long capacity, long long* tile_sums, int num_tiles,
+                                     cudaStream_t s) {
+    if (dpn == 3) return launch_upper<3, 32, 4>(L, ucounts, row_ptr, col_idx, values, capacity, tile_sums, num_tiles, s);
+    return launch_upper<2, 8, 2>(L, ucounts, row_ptr, col_idx, values, capacity, tile_sums, num_tiles, s);
 }
 
 cudaError_t launch_consolidate_bsr(const ListLayout& L, int dpn, int* block_row_ptr, int* block_col_idx,

@@ -95,6 +95,8 @@ fem_status make_layout(const fem_mesh* m, const fem_opts* o, HostLayout& h) {
     off += align_up((size_t)slots * h.B * sizeof(double));
     h.off_counts = off;
     off += align_up((size_t)h.N * sizeof(int));
+    h.off_ucounts = off;  // upper-triangle column counts (fem_alls_consolidate_upper)
+    off += align_up((size_t)h.N * sizeof(int));
     h.off_tiles = off;
     off += align_up((size_t)h.num_tiles * sizeof(long long));
     h.off_elist = off;  // visit order of the elements (perm), ranges, bucket histogram (+ bbox)
@@ -268,6 +270,24 @@ fem_status fem_alls_consolidate_bsr(const fem_mesh* mesh, const fem_opts* opts, 
     long long* tiles = reinterpret_cast<long long*>(static_cast<unsigned char*>(workspace) + h.off_tiles);
     cudaError_t err = launch_consolidate_bsr(L, h.dpn, block_row_ptr, block_col_idx, block_values, capacity_blocks,
                                              tiles, h.num_tiles, s);
+    return err ? cuda_fail(err) : FEM_OK;
+}
+
+fem_status fem_alls_consolidate_upper(const fem_mesh* mesh, const fem_opts* opts, void* workspace,
+                                      size_t workspace_bytes, int32_t* row_ptr, int32_t* col_idx, double* values,
+                                      int64_t capacity, void* stream) {
+    HostLayout h;
+    fem_status st = make_layout(mesh, opts, h);
+    if (st) return st;
+    if ((st = check_ws(h, workspace, workspace_bytes))) return st;
+    if (!row_ptr || capacity < 0 || (capacity > 0 && (!col_idx || !values))) return FEM_ERR_BAD_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    ListLayout L = device_layout(h, workspace);
+    unsigned char* b = static_cast<unsigned char*>(workspace);
+    long long* tiles = reinterpret_cast<long long*>(b + h.off_tiles);
+    int* ucounts = reinterpret_cast<int*>(b + h.off_ucounts);
+    cudaError_t err =
+        launch_consolidate_upper(L, h.dpn, ucounts, row_ptr, col_idx, values, capacity, tiles, h.num_tiles, s);
     return err ? cuda_fail(err) : FEM_OK;
 }
 

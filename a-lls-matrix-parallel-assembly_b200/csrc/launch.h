@@ -77,6 +77,10 @@ cudaError_t launch_reorder_3d(const MeshView& m, int* hist, int* ranges, int* pe
 cudaError_t launch_consolidate(const ListLayout& L, int dpn, int* row_ptr, int* col_idx, double* values,
                                long long capacity, long long* tile_sums, int num_tiles, cudaStream_t s);
 // Node-block (BSR) form of the consolidation; capacity in blocks.
+// Upper triangle (columns >= row, diagonal included) in CSR; ucounts: N ints of scratch.
+cudaError_t launch_consolidate_upper(const ListLayout& L, int dpn, int* ucounts, int* row_ptr, int* col_idx,
+                                     double* values, long long capacity, long long* tile_sums, int num_tiles,
+                                     cudaStream_t s);
 cudaError_t launch_consolidate_bsr(const ListLayout& L, int dpn, int* block_row_ptr, int* block_col_idx,
                                    double* block_values, long long capacity_blocks, long long* tile_sums,
                                    int num_tiles, cudaStream_t s);

@@ -38,7 +38,7 @@ EXPORTS = ["fem_alls_workspace_size", "fem_alls_scatter", "fem_alls_consolidate"
            "fem_colour_read_info", "fem_element_stiffness_size", "fem_element_stiffness",
            "fem_scatter_map_size", "fem_scatter_map_build", "fem_reassemble_values", "fem_scatter_map_read_info",
            "fem_batched_workspace_size", "fem_assemble_batched", "fem_alls_consolidate_bsr",
-           "fem_autotune_workspace_size", "fem_autotune", "fem_autotune_batched",
+           "fem_autotune_workspace_size", "fem_autotune", "fem_autotune_batched", "fem_alls_consolidate_upper",
            "fem_assemble_body_force", "fem_apply_dirichlet"]
 STATIC_WORKSPACE_BYTES = 32 << 20  # FEM_STATIC_WORKSPACE_BYTES
 
@@ -114,6 +114,7 @@ def load() -> C.CDLL:
         L.fem_assemble_batched.argtypes = [p(FemMesh), C.c_int32, p(FemOpts), C.c_int32, vp, C.c_size_t, p(FemCsr),
                                            vp, vp, vp]
         L.fem_alls_consolidate_bsr.argtypes = [p(FemMesh), p(FemOpts), vp, C.c_size_t, vp, vp, vp, C.c_int64, vp]
+        L.fem_alls_consolidate_upper.argtypes = [p(FemMesh), p(FemOpts), vp, C.c_size_t, vp, vp, vp, C.c_int64, vp]
         L.fem_assemble_body_force.argtypes = [p(FemMesh), vp, vp, vp, vp, vp]
         L.fem_apply_dirichlet.argtypes = [C.c_int32, vp, vp, vp, vp, vp, vp, vp]
         L.fem_autotune_workspace_size.argtypes = [p(FemMesh), p(FemOpts), p(C.c_size_t)]
@@ -245,6 +246,26 @@ class Assembler:
               "fem_alls_consolidate_bsr")
         check(self.read_info()[0], "bsr consolidation")
         return brp, bci[:nb], bv[: nb * self.mesh.dpn ** 2]
+
+    def consolidate_upper(self, capacity: Optional[int] = None):
+        """Upper-triangle CSR of the last scatter (fem_alls_consolidate_upper):
+        (row_ptr, col_idx, values) tensors. Sizes its outputs with a counting
+        pass when capacity is None."""
+        torch = self.torch
+        dev = self.row_ptr.device
+        rp = torch.empty(self.n_rows + 1, dtype=torch.int32, device=dev)
+        if capacity is None:
+            check(self.lib.fem_alls_consolidate_upper(C.byref(self.cm), C.byref(self.opts), self.ws_ptr, self.ws_bytes,
+                                                      _ptr(rp), None, None, 0, self._stream()),
+                  "fem_alls_consolidate_upper")
+            st, info = self.read_info()
+            capacity = int(info.nnz)
+        ci = torch.empty(max(capacity, 1), dtype=torch.int32, device=dev)
+        v = torch.empty(max(capacity, 1), dtype=torch.float64, device=dev)
+        check(self.lib.fem_alls_consolidate_upper(C.byref(self.cm), C.byref(self.opts), self.ws_ptr, self.ws_bytes,
+                                                  _ptr(rp), _ptr(ci), _ptr(v), capacity, self._stream()),
+              "fem_alls_consolidate_upper")
+        return rp, ci, v
 
     def read_info(self) -> tuple:
         info = FemInfo()

@@ -396,6 +396,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if not args.no_colour:
         colour = colour_baseline(fem, torch, asm, mesh, nnz, args, flush, stream)
     reasm = None if args.no_reassembly else reassembly(fem, torch, asm, mesh, nnz, args, flush, stream)
+    upper = None if args.no_reassembly else upper_output(fem, torch, asm, mesh, nnz, args, flush, stream)
     kef = ke_form(fem, torch, mesh, asm.dev, args, flush, stream) if mesh.kind == 2 and not args.no_ke else None
     f32 = fp32_form(fem, torch, asm, mesh, nnz, args, flush, stream) if mesh.kind != 2 and not args.no_ke else None
     tuned = None
@@ -459,6 +460,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         line["colour_baseline"] = colour
     if reasm:
         line["reassembly"] = reasm
+    if upper:
+        line["upper_output"] = upper
     if kef:
         line["ke_form"] = kef
     if f32:
@@ -556,6 +559,35 @@ def fp32_form(fem, torch, asm, mesh, nnz, args, flush, stream) -> dict:
             "err_scale": "max |difference| / max(|K_ij|, sqrt(|K_ii K_jj|)) over the CSR entries",
             "what": "fem_alls_scatter + fem_alls_consolidate with FEM_PREC_FP32 (Ke blocks in FP32 from "
                     "coordinates relative to the element's first node, FP64 accumulation)"}
+
+
+def upper_output(fem, torch, asm, mesh, nnz, args, flush, stream) -> dict:
+    """The consolidation into the upper triangle (fem_alls_consolidate_upper)
+    of the same lists, timed like the full consolidation phase."""
+    asm.scatter()
+    rp, ci, v = asm.consolidate_upper()
+    cap = int(ci.numel())
+    ts = []
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fem.check(asm.lib.fem_alls_consolidate_upper(fem.C.byref(asm.cm), fem.C.byref(asm.opts), asm.ws_ptr,
+                                                     asm.ws_bytes, fem._ptr(rp), fem._ptr(ci), fem._ptr(v), cap,
+                                                     stream.cuda_stream), "fem_alls_consolidate_upper")
+        b.record(stream)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            ts.append(a.elapsed_time(b))
+    st, info = asm.read_info()
+    fem.check(st, "upper-triangle consolidation")
+    unz = int(info.nnz)
+    asm.assemble()                             # leave the full form in place
+    ms = statistics.mean(ts)
+    return {"ms": ms, "nnz_upper": unz, "nnz_full": nnz, "bytes_out": 4 * (mesh.num_dofs + 1) + 12 * unz,
+            "what": "fem_alls_consolidate_upper: count of columns >= row per node, scan, upper part of each "
+                    "sorted row (symmetric storage)"}
 
 
 def reassembly(fem, torch, asm, mesh, nnz, args, flush, stream) -> dict:

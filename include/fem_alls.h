@@ -159,6 +159,18 @@ FEM_API fem_status fem_alls_consolidate(const fem_mesh* mesh, const fem_opts* op
                                 size_t workspace_bytes, int32_t* row_ptr, int32_t* col_idx,
                                 double* values, int64_t capacity, void* stream);
 
+/* The upper triangle of the symmetric stiffness matrix in CSR (every entry
+ * with column >= row, the diagonal included): the storage a symmetric or
+ * Cholesky solver reads, about half the entries of the full form (no
+ * counterpart in the reference, whose output is the full CSR). Same arguments
+ * as fem_alls_consolidate; row_ptr [n_rows + 1], col_idx / values of the
+ * upper entries, columns sorted within each row; the info word's nnz is the
+ * upper-triangle count. The entries are those of the full form's upper part,
+ * bit for bit. Asynchronous. */
+FEM_API fem_status fem_alls_consolidate_upper(const fem_mesh* mesh, const fem_opts* opts, void* workspace,
+                                              size_t workspace_bytes, int32_t* row_ptr, int32_t* col_idx,
+                                              double* values, int64_t capacity, void* stream);
+
 /* The node-block (BSR) form of fem_alls_consolidate, for solvers that work on
  * dof_per_node^2 blocks (no counterpart in the reference, whose output is
  * scalar CSR only): one block row per node, block_row_ptr [num_nodes + 1],
