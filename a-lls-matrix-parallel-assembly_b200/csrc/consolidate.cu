@@ -406,24 +406,47 @@ __device__ void long_row_write_upper(const ListLayout& L, int n, int u, const in
 
 enum : int { kOutCsr = 0, kOutBsr = 1, kOutUpper = 2 };
 
+// Next link and slot words (kPre per lane of a G-lane group) of a node's first chunk.
+template <int G, int kPre>
+__device__ __forceinline__ void prefetch_first_chunk(const ListLayout& L, long long node, int glane, int (&w)[kPre],
+                                                     int& next) {
+    if (node < L.N) {
+        const int* meta = chunk_meta(L, (int)node);
+        next = __ldg(meta + 1);
+#pragma unroll
+        for (int q = 0; q < kPre; q++) {
+            const int s = q * G + glane;
+            w[q] = s < L.S1 ? __ldg(meta + 2 + s) : 0;
+        }
+    }
+}
+
 // kMode kOutBsr: block (BSR) output, one block row per node: block_col_idx =
 // column node, block values dpn x dpn row-major; row_ptr is then the block row
 // pointer. kOutUpper: the upper triangle in CSR (ucounts: columns >= n).
 template <int DPN, int G, int KPL, int kMode>
-__global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int* __restrict__ row_ptr,
+__global__ void __launch_bounds__(kBlockThreads, 4) k_write(ListLayout L, const int* __restrict__ row_ptr,
                                                          int* __restrict__ col_idx, double* __restrict__ values,
                                                          long long capacity, const int* __restrict__ ucounts) {
     constexpr bool kBsr = kMode == kOutBsr;
     constexpr int NPB = kBlockThreads / G;  // nodes per batch
     constexpr int NK = G * KPL;             // sort capacity per node
     constexpr int B = DPN * DPN;
+    // slot words of a node's first chunk per lane (2-D: 14 slots; Hex20: at most 94)
+    constexpr int kPre = (DPN == 2 ? 16 : 96) / G;
     __shared__ unsigned long long s_keys[NPB][NK];
+    // 2-D: the node's sorted 2x2 blocks, loaded together before the rows are written
+    __shared__ double2 s_vals[DPN == 2 ? NPB : 1][DPN == 2 ? NK : 1][2];
     if (L.info->nnz > capacity) return;  // FEM_ERR_CAPACITY already raised; write nothing
     const int tid = threadIdx.x;
     const int grp = tid / G, glane = tid % G;
     const unsigned gmask = group_mask<G>((tid & 31) / G);
     const int gshift = G == 32 ? 0 : ((tid & 31) / G) * G;
     int t_sum = 0, t_max = 0;
+    // the first chunk (next link and slot words) of the group's next node is
+    // loaded while the current node is sorted and written
+    int pre_w[kPre], pre_next = 0;
+    prefetch_first_chunk<G, kPre>(L, (long long)blockIdx.x * NPB + grp, glane, pre_w, pre_next);
     for (long long nb = (long long)blockIdx.x * NPB; nb < L.N; nb += (long long)gridDim.x * NPB) {
         const int n = (int)(nb + grp);
         const bool valid = n < L.N;
@@ -440,14 +463,28 @@ __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int
                 u = (__ldg(row_ptr + (size_t)n * DPN + 1) - (int)base) / DPN;
             }
         }
-        // 1. gather the non-empty slots of the node's chunk chain
+        // 1. gather the non-empty slots of the node's chunk chain (the first
+        // chunk from the prefetched words)
         int T = 0;
         if (valid) {
-            int c = n;
-            for (int step = 0; step < kMaxChainSteps; step++) {
+#pragma unroll
+            for (int q = 0; q < kPre; q++) {
+                if (q * G < L.S1) {
+                    const int s = q * G + glane;
+                    const int col = s < L.S1 ? (pre_w[q] & kColMask) : 0;
+                    const unsigned used = (__ballot_sync(gmask, col != 0) >> gshift) & gmask >> gshift;
+                    const int e = T + __popc(used & ((1u << glane) - 1u));
+                    if (col != 0 && e < NK)
+                        s_keys[grp][e] = ((unsigned long long)(unsigned)(col - 1) << 32) | slot_gid(L, n, s);
+                    T += __popc(used);
+                }
+            }
+            int next = pre_next;
+            for (int step = 1; next != 0 && step < kMaxChainSteps; step++) {
+                const int c = next - 1;
                 const int* meta = chunk_meta(L, c);
                 const int cap = chunk_cap(L, c);
-                const int next = __ldg(meta + 1);
+                next = __ldg(meta + 1);
                 for (int s0 = 0; s0 < cap; s0 += G) {
                     const int s = s0 + glane;
                     const int col = s < cap ? (__ldg(meta + 2 + s) & kColMask) : 0;
@@ -457,12 +494,11 @@ __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int
                         s_keys[grp][e] = ((unsigned long long)(unsigned)(col - 1) << 32) | slot_gid(L, c, s);
                     T += __popc(used);
                 }
-                if (next == 0) break;
-                c = next - 1;
             }
             const int expect = kMode == kOutUpper ? __ldg(L.counts + n) : u;
             if (glane == 0 && (T != expect || u > T)) raise_status(L.info, FEM_ERR_INTERNAL);
         }
+        prefetch_first_chunk<G, kPre>(L, nb + (long long)gridDim.x * NPB + grp, glane, pre_w, pre_next);
         t_sum += T;
         t_max = max(t_max, T);
         const bool long_row = T > NK;
@@ -479,6 +515,20 @@ __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int
 #pragma unroll
         for (int i = 0; i < KPL; i++) s_keys[grp][glane * KPL + i] = keys[i];
         __syncwarp();
+        if constexpr (DPN == 2) {
+            // all of the node's blocks in flight at once (two 16-byte loads each)
+            for (int k = glane; k < Ts; k += G) {
+                const double2* p = reinterpret_cast<const double2*>(L.vals + (size_t)(unsigned)s_keys[grp][k] * B);
+                s_vals[grp][k][0] = __ldg(p);
+                s_vals[grp][k][1] = __ldg(p + 1);
+            }
+            __syncwarp();
+        }
+        // entry v of the node's k-th sorted block
+        auto block_value = [&](int k, int v) -> double {
+            if constexpr (DPN == 2) return reinterpret_cast<const double*>(&s_vals[grp][k][0])[v];
+            return __ldg(L.vals + (size_t)(unsigned)s_keys[grp][k] * B + v);
+        };
         // 3. write the dpn rows of the node (or its block row, or its upper rows)
         if (valid && kMode == kOutUpper) {
             if (long_row) {
@@ -500,7 +550,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int
                         }
                         const unsigned long long key = s_keys[grp][k];
                         col_idx[rbase + r] = (int)(key >> 32) * DPN + b;
-                        values[rbase + r] = __ldg(L.vals + (size_t)(unsigned)key * B + a * DPN + b);
+                        values[rbase + r] = block_value(k, a * DPN + b);
                     }
                 }
             }
@@ -511,7 +561,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int
                 for (int k = glane; k < Ts; k += G) col_idx[base + k] = (int)(s_keys[grp][k] >> 32);
                 for (int idx = glane; idx < Ts * B; idx += G) {
                     const int k = idx / B, v = idx - k * B;
-                    values[base * B + idx] = __ldg(L.vals + (size_t)(unsigned)s_keys[grp][k] * B + v);
+                    values[base * B + idx] = block_value(k, v);
                 }
             }
         } else if (valid) {
@@ -525,7 +575,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_write(ListLayout L, const int
                         const int k = r / DPN, b = r - k * DPN;
                         const unsigned long long key = s_keys[grp][k];
                         col_idx[rbase + r] = (int)(key >> 32) * DPN + b;
-                        values[rbase + r] = __ldg(L.vals + (size_t)(unsigned)key * B + a * DPN + b);
+                        values[rbase + r] = block_value(k, a * DPN + b);
                     }
                 }
             }
@@ -559,6 +609,18 @@ __global__ void k_consolidate_reset(DevInfo* info) {
     info->max_row_entries = 0;
 }
 
+// Persistent grid of k_write: the CTAs that fit on the GPU at once.
+template <int DPN, int G, int KPL, int kMode>
+long long write_grid(long long batches) {
+    static int per_sm = 0;
+    if (!per_sm) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_write<DPN, G, KPL, kMode>, kBlockThreads, 0) ||
+            per_sm < 1)
+            per_sm = 1;
+    }
+    return std::max<long long>(1, std::min<long long>(batches, (long long)per_sm * sm_count()));
+}
+
 template <int DPN, int G, int KPL, bool kBsr>
 cudaError_t launch_all(const ListLayout& L, int* row_ptr, int* col_idx, double* values, long long capacity,
                        long long* tile_sums, int num_tiles, cudaStream_t s) {
@@ -572,9 +634,8 @@ cudaError_t launch_all(const ListLayout& L, int* row_ptr, int* col_idx, double* 
     if (capacity > 0) {
         constexpr int NPB = kBlockThreads / G;
         const long long batches = ((long long)L.N + NPB - 1) / NPB;
-        const long long grid = std::min<long long>(batches, (long long)sm_count() * 8);
-        k_write<DPN, G, KPL, kMode><<<(int)(grid > 0 ? grid : 1), kBlockThreads, 0, s>>>(L, row_ptr, col_idx, values,
-                                                                                       capacity, nullptr);
+        k_write<DPN, G, KPL, kMode><<<(int)write_grid<DPN, G, KPL, kMode>(batches), kBlockThreads, 0, s>>>(
+            L, row_ptr, col_idx, values, capacity, nullptr);
     }
     return cudaGetLastError();
 }
@@ -591,7 +652,8 @@ cudaError_t launch_upper(const ListLayout& L, int* ucounts, int* row_ptr, int* c
     k_scan_tiles<<<1, kScanThreads, 0, s>>>(tile_sums, num_tiles, L.info, row_ptr + (size_t)L.N * DPN, capacity, 1);
     k_row_ptr_upper<DPN><<<num_tiles, kScanThreads, 0, s>>>(ucounts, L.N, tile_sums, row_ptr);
     if (capacity > 0)
-        k_write<DPN, G, KPL, kOutUpper><<<grid, kBlockThreads, 0, s>>>(L, row_ptr, col_idx, values, capacity, ucounts);
+        k_write<DPN, G, KPL, kOutUpper><<<(int)write_grid<DPN, G, KPL, kOutUpper>(batches), kBlockThreads, 0, s>>>(
+            L, row_ptr, col_idx, values, capacity, ucounts);
     return cudaGetLastError();
 }
 
