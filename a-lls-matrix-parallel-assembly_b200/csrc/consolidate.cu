@@ -612,12 +612,12 @@ __global__ void k_consolidate_reset(DevInfo* info) {
 // Persistent grid of k_write: the CTAs that fit on the GPU at once.
 template <int DPN, int G, int KPL, int kMode>
 long long write_grid(long long batches) {
-    static int per_sm = 0;
-    if (!per_sm) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_write<DPN, G, KPL, kMode>, kBlockThreads, 0) ||
-            per_sm < 1)
-            per_sm = 1;
-    }
+    static DeviceCache cache;
+    int per_sm = 0;
+    if (per_device(cache, [](int& v) {
+            return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_write<DPN, G, KPL, kMode>, kBlockThreads, 0);
+        }, per_sm))
+        per_sm = 1;
     return std::max<long long>(1, std::min<long long>(batches, (long long)per_sm * sm_count()));
 }
 

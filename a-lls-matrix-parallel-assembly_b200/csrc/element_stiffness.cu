@@ -331,15 +331,15 @@ __global__ void __launch_bounds__(kThreads2D) k_ke_2d(MeshView m, double* __rest
 
 template <int kPrec>
 cudaError_t launch_hex20_ke(const MeshView& m, double* ke_out, int* status, cudaStream_t s) {
-    static int blocks_per_sm = 0;
+    static DeviceCache cache;
     const size_t smem = sizeof(KeSmem);
-    if (!blocks_per_sm) {
-        cudaError_t err = cudaFuncSetAttribute(k_hex20_ke<kPrec>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (err) return err;
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_hex20_ke<kPrec>, kThreads, smem);
-        if (err) return err;
-        if (blocks_per_sm < 1) blocks_per_sm = 1;
-    }
+    int blocks_per_sm = 0;
+    const cudaError_t err = per_device(cache, [&](int& v) {
+        cudaError_t e = cudaFuncSetAttribute(k_hex20_ke<kPrec>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_hex20_ke<kPrec>, kThreads, smem);
+        return e;
+    }, blocks_per_sm);
+    if (err) return err;
     const long long grid = std::min<long long>((long long)blocks_per_sm * sm_count(), m.E_count);
     k_hex20_ke<kPrec><<<(int)grid, kThreads, smem, s>>>(m, ke_out, status);
     return cudaGetLastError();

@@ -13,14 +13,15 @@ using namespace fem;
 
 namespace fem {
 int sm_count() {
-    static int n = 0;
-    if (!n) {
+    static DeviceCache cache;
+    int n = 0;
+    per_device(cache, [](int& v) {
         int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
-    return n;
+        cudaError_t err = cudaGetDevice(&dev);
+        if (!err) err = cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        return err;
+    }, n);
+    return n > 0 ? n : 1;
 }
 }  // namespace fem
 

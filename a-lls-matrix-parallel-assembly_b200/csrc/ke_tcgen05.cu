@@ -423,26 +423,29 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
 }  // namespace
 
 cudaError_t launch_hex20_ke_tcgen05(const MeshView& m, double* ke_out, int* status, cudaStream_t s) {
-    static int blocks_per_sm = 0;
+    static DeviceCache cache;
     const size_t smem = sizeof(KeTcSmem);
-    if (!blocks_per_sm) {
+    int blocks_per_sm = 0;
+    const cudaError_t err = per_device(cache, [&](int& v) {
         // Resident CTAs per SM from the kernel's registers, its shared memory
         // and the 512 tensor-memory columns of an SM (kTmemCols per CTA). The
         // runtime's occupancy query answers 1 for this kernel, which would
         // leave three quarters of the SM idle.
-        cudaError_t err = cudaFuncSetAttribute(k_hex20_ke_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (err) return err;
+        cudaError_t e = cudaFuncSetAttribute(k_hex20_ke_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncAttributes fa;
-        if ((err = cudaFuncGetAttributes(&fa, k_hex20_ke_tc))) return err;
+        if (!e) e = cudaFuncGetAttributes(&fa, k_hex20_ke_tc);
         int dev = 0, regs_sm = 0, smem_sm = 0;
-        if ((err = cudaGetDevice(&dev))) return err;
-        if ((err = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev))) return err;
-        if ((err = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev))) return err;
+        if (!e) e = cudaGetDevice(&dev);
+        if (!e) e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+        if (!e) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        if (e) return e;
         const int regs_cta = ((fa.numRegs + 7) / 8) * 8 * kThreads;
         const int by_regs = regs_cta > 0 ? regs_sm / regs_cta : 1;
         const int by_smem = smem_sm / (int)(smem + 1024);  // 1 KB per CTA is reserved by the runtime
-        blocks_per_sm = std::max(1, std::min({by_regs, by_smem, (int)(512 / kTmemCols)}));
-    }
+        v = std::min({by_regs, by_smem, (int)(512 / kTmemCols)});
+        return cudaSuccess;
+    }, blocks_per_sm);
+    if (err) return err;
     const long long npairs = ((long long)m.E_count + 1) / 2;
     const long long grid = std::min<long long>((long long)blocks_per_sm * sm_count(), npairs);
     const int bulk_out = (reinterpret_cast<uintptr_t>(ke_out) & 15u) == 0;

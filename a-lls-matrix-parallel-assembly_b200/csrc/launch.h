@@ -3,11 +3,36 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <vector>
 
 #include "fem_internal.cuh"
 
 namespace fem {
+
+// A launch-shape value (resident CTAs per SM, SM count) cached per device: it
+// is computed on the first launch on each device (compute(int& v) sets v > 0),
+// which also sets the kernel's per-device attributes. Devices past the table
+// compute it every time.
+constexpr int kMaxCachedDevices = 64;
+struct DeviceCache {
+    std::atomic<int> v[kMaxCachedDevices] = {};
+};
+template <typename F>
+cudaError_t per_device(DeviceCache& cache, F&& compute, int& out) {
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err) return err;
+    const bool cached = dev >= 0 && dev < kMaxCachedDevices;
+    int v = cached ? cache.v[dev].load(std::memory_order_acquire) : 0;
+    if (v <= 0) {
+        if ((err = compute(v))) return err;
+        if (v < 1) v = 1;
+        if (cached) cache.v[dev].store(v, std::memory_order_release);
+    }
+    out = v;
+    return cudaSuccess;
+}
 
 struct MeshView {
     const double* x;

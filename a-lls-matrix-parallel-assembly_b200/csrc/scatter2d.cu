@@ -225,13 +225,12 @@ template <int NPE, typename T>
 cudaError_t launch_scatter_2d_t(const MeshView& m, const ListLayout& L, const int* perm, const int* range,
                                 int ctas_per_sm, cudaStream_t s) {
     // A persistent grid: every warp runs the pipeline over many elements.
-    static int per_sm = 0;
-    if (!per_sm) {
-        const cudaError_t err =
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scatter_2d<NPE, T>, kThreads2D, 0);
-        if (err) return err;
-        per_sm = std::max(per_sm, 1);
-    }
+    static DeviceCache cache;
+    int per_sm = 0;
+    cudaError_t err = per_device(cache, [](int& v) {
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_scatter_2d<NPE, T>, kThreads2D, 0);
+    }, per_sm);
+    if (err) return err;
     const int use = ctas_per_sm > 0 ? std::min(ctas_per_sm, per_sm) : per_sm;
     constexpr int epw = 32 / (NPE * NPE);
     const long long warps = ((long long)m.E_count + epw - 1) / epw;

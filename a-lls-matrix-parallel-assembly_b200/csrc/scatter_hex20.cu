@@ -562,16 +562,16 @@ __global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListL
 template <bool kTc, int kOut>
 cudaError_t launch_scatter_hex20_t(const MeshView& m, const ListLayout& L, const int* perm, const MapTarget& t,
                                    const int* range, cudaStream_t s, int ctas_per_sm = 0) {
-    static int blocks_per_sm = 0;
+    static DeviceCache cache;
     const size_t smem = sizeof(Hex20Smem);
-    if (!blocks_per_sm) {
-        cudaError_t err =
+    int blocks_per_sm = 0;
+    const cudaError_t err = per_device(cache, [&](int& v) {
+        cudaError_t e =
             cudaFuncSetAttribute(k_scatter_hex20<kTc, kOut>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (err) return err;
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_scatter_hex20<kTc, kOut>, kThreads, smem);
-        if (err) return err;
-        if (blocks_per_sm < 1) blocks_per_sm = 1;
-    }
+        if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_scatter_hex20<kTc, kOut>, kThreads, smem);
+        return e;
+    }, blocks_per_sm);
+    if (err) return err;
     const int use = ctas_per_sm > 0 ? std::min(ctas_per_sm, blocks_per_sm) : blocks_per_sm;
     long long grid = (long long)use * sm_count();
     if (grid > m.E_count) grid = m.E_count > 0 ? m.E_count : 1;
