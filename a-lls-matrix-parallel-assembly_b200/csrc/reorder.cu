@@ -10,6 +10,9 @@
 //   k_bucket_scan     one CTA: exclusive scan of the histogram; the element
 //                     range of each element type (Q4 first, then T3)
 //   k_bucket_scatter  perm[offset[key]++] = e
+// When the key table fits in shared memory (up to 40 K keys), one CTA per SM
+// counts and places its elements with shared-memory atomics instead
+// (k_key_count_sm, k_key_scatter_sm), one global atomic per non-zero key.
 // The input arrays are not modified; only the order in which the scatter
 // visits elements changes (and with it the order of the FP64 atomic adds).
 //
@@ -186,6 +189,98 @@ __global__ void k_morton_scatter(MeshView m, const unsigned long long* bbox, int
         perm[atomicAdd(offsets + morton_key(m, e, bbox, bits), 1)] = e;
 }
 
+// Keys of the two orders as functors for the shared-memory histogram kernels.
+struct BucketKey {
+    MeshView m;
+    int NB;
+    __device__ __forceinline__ int operator()(int e) const { return element_key(m, e, NB); }
+};
+struct MortonKey {
+    MeshView m;
+    const unsigned long long* bbox;
+    int bits;
+    __device__ __forceinline__ int operator()(int e) const { return morton_key(m, e, bbox, bits); }
+};
+
+// Shared-memory histograms (when the key table fits): a CTA counts its
+// elements' keys with shared-memory atomics and flushes each non-zero counter
+// with one global atomic, instead of one global atomic per element.
+constexpr int kSmThreads = 1024;
+constexpr int kMaxSmemKeys = 160 * 1024 / 4;
+
+template <typename Key>
+__global__ void __launch_bounds__(kSmThreads) k_key_count_sm(Key key, int E, int nkeys, int* __restrict__ hist) {
+    extern __shared__ int s_cnt[];
+    for (int k = threadIdx.x; k < nkeys; k += blockDim.x) s_cnt[k] = 0;
+    __syncthreads();
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x)
+        atomicAdd(&s_cnt[key(e)], 1);
+    __syncthreads();
+    for (int k = threadIdx.x; k < nkeys; k += blockDim.x)
+        if (s_cnt[k]) atomicAdd(hist + k, s_cnt[k]);
+}
+
+// offsets: the exclusive scan of the histogram. A CTA counts its elements'
+// keys again, reserves one range per key (one global atomic per non-zero key)
+// and places its elements inside the ranges with shared-memory atomics.
+template <typename Key>
+__global__ void __launch_bounds__(kSmThreads) k_key_scatter_sm(Key key, int E, int nkeys, int* __restrict__ offsets,
+                                                               int* __restrict__ perm) {
+    extern __shared__ int s_pos[];
+    for (int k = threadIdx.x; k < nkeys; k += blockDim.x) s_pos[k] = 0;
+    __syncthreads();
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x)
+        atomicAdd(&s_pos[key(e)], 1);
+    __syncthreads();
+    for (int k = threadIdx.x; k < nkeys; k += blockDim.x) {
+        const int c = s_pos[k];
+        if (c) s_pos[k] = atomicAdd(offsets + k, c);
+    }
+    __syncthreads();
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x)
+        perm[atomicAdd(&s_pos[key(e)], 1)] = e;
+}
+
+// The shared-memory kernels' attribute (dynamic shared memory above 48 KB) is
+// set once per device.
+template <typename Key>
+cudaError_t smem_kernels_ready() {
+    static DeviceCache cache;
+    int ok = 0;
+    return per_device(cache, [](int& v) {
+        cudaError_t e = cudaFuncSetAttribute(k_key_count_sm<Key>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             kMaxSmemKeys * (int)sizeof(int));
+        if (!e)
+            e = cudaFuncSetAttribute(k_key_scatter_sm<Key>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     kMaxSmemKeys * (int)sizeof(int));
+        v = 1;
+        return e;
+    }, ok);
+}
+
+// Counting sort of the elements by key: histogram, scan (ranges), scatter.
+template <typename Key, typename CountK, typename ScatterK>
+cudaError_t counting_sort(const Key& key, int E, int nkeys, int NB, int mixed, int* hist, int* ranges, int* perm,
+                          int sms, CountK count_global, ScatterK scatter_global, cudaStream_t s) {
+    if (nkeys <= kMaxSmemKeys) {
+        cudaError_t err = smem_kernels_ready<Key>();
+        if (err) return err;
+        const long long want = ((long long)E + kSmThreads - 1) / kSmThreads;
+        const int grid = (int)std::min<long long>(want > 0 ? want : 1, (long long)sms);
+        const size_t smem = (size_t)nkeys * sizeof(int);
+        k_key_count_sm<Key><<<grid, kSmThreads, smem, s>>>(key, E, nkeys, hist);
+        k_bucket_scan<<<1, 1024, 0, s>>>(hist, nkeys, NB, mixed, ranges);
+        k_key_scatter_sm<Key><<<grid, kSmThreads, smem, s>>>(key, E, nkeys, hist, perm);
+    } else {
+        const long long want = ((long long)E + kThreads - 1) / kThreads;
+        const int grid = (int)std::min<long long>(want > 0 ? want : 1, (long long)sms * 8);
+        count_global(grid);
+        k_bucket_scan<<<1, 1024, 0, s>>>(hist, nkeys, NB, mixed, ranges);
+        scatter_global(grid);
+    }
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 int reorder_buckets(int num_nodes) { return (num_nodes >> kBucketShift) + 1; }
@@ -205,12 +300,10 @@ cudaError_t launch_reorder_3d(const MeshView& m, int* hist, int* ranges, int* pe
     k_bbox_init<<<1, 32, 0, s>>>(bbox);
     const long long wn = ((long long)m.N + kThreads - 1) / kThreads;
     k_bbox<<<(int)std::min<long long>(wn > 0 ? wn : 1, (long long)sms * 4), kThreads, 0, s>>>(m, bbox);
-    const long long want = ((long long)m.E_count + kThreads - 1) / kThreads;
-    const int grid = (int)std::min<long long>(want > 0 ? want : 1, (long long)sms * 8);
-    k_morton_count<<<grid, kThreads, 0, s>>>(m, bbox, bits, hist);
-    k_bucket_scan<<<1, 1024, 0, s>>>(hist, nkeys, nkeys, 0, ranges);
-    k_morton_scatter<<<grid, kThreads, 0, s>>>(m, bbox, bits, hist, perm);
-    return cudaGetLastError();
+    return counting_sort(
+        MortonKey{m, bbox, bits}, m.E_count, nkeys, nkeys, 0, hist, ranges, perm, sms,
+        [&](int grid) { k_morton_count<<<grid, kThreads, 0, s>>>(m, bbox, bits, hist); },
+        [&](int grid) { k_morton_scatter<<<grid, kThreads, 0, s>>>(m, bbox, bits, hist, perm); }, s);
 }
 
 cudaError_t launch_reorder(const MeshView& m, int* hist, int* ranges, int* perm, int sms, cudaStream_t s) {
@@ -218,12 +311,10 @@ cudaError_t launch_reorder(const MeshView& m, int* hist, int* ranges, int* perm,
     const int nkeys = (m.types ? 2 : 1) * NB;
     cudaError_t err = cudaMemsetAsync(hist, 0, (size_t)nkeys * sizeof(int), s);
     if (err) return err;
-    const long long want = ((long long)m.E_count + kThreads - 1) / kThreads;
-    const int grid = (int)std::min<long long>(want > 0 ? want : 1, (long long)sms * 8);
-    k_bucket_count<<<grid, kThreads, 0, s>>>(m, NB, hist);
-    k_bucket_scan<<<1, 1024, 0, s>>>(hist, nkeys, NB, m.types ? 1 : 0, ranges);
-    k_bucket_scatter<<<grid, kThreads, 0, s>>>(m, NB, hist, perm);
-    return cudaGetLastError();
+    return counting_sort(
+        BucketKey{m, NB}, m.E_count, nkeys, NB, m.types ? 1 : 0, hist, ranges, perm, sms,
+        [&](int grid) { k_bucket_count<<<grid, kThreads, 0, s>>>(m, NB, hist); },
+        [&](int grid) { k_bucket_scatter<<<grid, kThreads, 0, s>>>(m, NB, hist, perm); }, s);
 }
 
 }  // namespace fem
