@@ -421,13 +421,18 @@ __device__ __forceinline__ void prefetch_first_chunk(const ListLayout& L, long l
     }
 }
 
+// Resident CTAs per SM the register budget of k_write is set for (build-time tuning knob).
+#ifndef FEM_WRITE_MIN_CTAS
+#define FEM_WRITE_MIN_CTAS 4
+#endif
+
 // kMode kOutBsr: block (BSR) output, one block row per node: block_col_idx =
 // column node, block values dpn x dpn row-major; row_ptr is then the block row
 // pointer. kOutUpper: the upper triangle in CSR (ucounts: columns >= n).
 template <int DPN, int G, int KPL, int kMode>
-__global__ void __launch_bounds__(kBlockThreads, 4) k_write(ListLayout L, const int* __restrict__ row_ptr,
-                                                         int* __restrict__ col_idx, double* __restrict__ values,
-                                                         long long capacity, const int* __restrict__ ucounts) {
+__global__ void __launch_bounds__(kBlockThreads, FEM_WRITE_MIN_CTAS)
+    k_write(ListLayout L, const int* __restrict__ row_ptr, int* __restrict__ col_idx, double* __restrict__ values,
+            long long capacity, const int* __restrict__ ucounts) {
     constexpr bool kBsr = kMode == kOutBsr;
     constexpr int NPB = kBlockThreads / G;  // nodes per batch
     constexpr int NK = G * KPL;             // sort capacity per node

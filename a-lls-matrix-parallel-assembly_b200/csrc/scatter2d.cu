@@ -114,8 +114,16 @@ __device__ __forceinline__ int element_of(const int* perm, int begin, int count,
     return valid ? __ldg(perm + begin + i) : 0;
 }
 
+// Resident CTAs per SM the register budget is set for (build-time tuning knobs).
+#ifndef FEM_T3_MIN_CTAS
+#define FEM_T3_MIN_CTAS 4
+#endif
+#ifndef FEM_Q4_MIN_CTAS
+#define FEM_Q4_MIN_CTAS 2
+#endif
+
 template <int NPE, typename T>
-__global__ void __launch_bounds__(kThreads2D, NPE == 3 ? 4 : 2)
+__global__ void __launch_bounds__(kThreads2D, NPE == 3 ? FEM_T3_MIN_CTAS : FEM_Q4_MIN_CTAS)
     k_scatter_2d(MeshView m, ListLayout L, const int* __restrict__ perm, const int* __restrict__ range) {
     constexpr int G = NPE * NPE;   // lanes per element
     constexpr int EPW = 32 / G;    // elements per warp

@@ -356,13 +356,19 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
                  : "d"(a), "d"(b));
 }
 
+// Resident CTAs per SM the register budget is set for (build-time tuning knob).
+#ifndef FEM_HEX20_MIN_CTAS
+#define FEM_HEX20_MIN_CTAS 3
+#endif
+
 // kTc: the node-pair contraction on the FP16 tensor cores (hex20.cuh).
 // kOut: kOutLists = the A-LLS list scatter; kOutMap = value-only re-assembly
 // into a CSR pattern through a scatter map (atomic adds); kOutColour = the
 // colouring baseline (plain adds, elements perm[range[0], range[1]) of one colour).
 template <bool kTc, int kOut>
-__global__ void __launch_bounds__(kThreads, 3) k_scatter_hex20(MeshView m, ListLayout L, const int* __restrict__ perm,
-                                                               MapTarget target, const int* __restrict__ range) {
+__global__ void __launch_bounds__(kThreads, FEM_HEX20_MIN_CTAS)
+    k_scatter_hex20(MeshView m, ListLayout L, const int* __restrict__ perm, MapTarget target,
+                    const int* __restrict__ range) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Hex20Smem& sm = *reinterpret_cast<Hex20Smem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
