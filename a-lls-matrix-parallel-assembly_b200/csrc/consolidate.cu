@@ -421,16 +421,20 @@ __device__ __forceinline__ void prefetch_first_chunk(const ListLayout& L, long l
     }
 }
 
-// Resident CTAs per SM the register budget of k_write is set for (build-time tuning knob).
-#ifndef FEM_WRITE_MIN_CTAS
-#define FEM_WRITE_MIN_CTAS 4
+// Resident CTAs per SM the register budget of k_write is set for (build-time
+// tuning knobs; measured on B200: 5 for the 2-D kinds, 4 for Hex20).
+#ifndef FEM_WRITE_MIN_CTAS_2D
+#define FEM_WRITE_MIN_CTAS_2D 5
+#endif
+#ifndef FEM_WRITE_MIN_CTAS_3D
+#define FEM_WRITE_MIN_CTAS_3D 4
 #endif
 
 // kMode kOutBsr: block (BSR) output, one block row per node: block_col_idx =
 // column node, block values dpn x dpn row-major; row_ptr is then the block row
 // pointer. kOutUpper: the upper triangle in CSR (ucounts: columns >= n).
 template <int DPN, int G, int KPL, int kMode>
-__global__ void __launch_bounds__(kBlockThreads, FEM_WRITE_MIN_CTAS)
+__global__ void __launch_bounds__(kBlockThreads, DPN == 2 ? FEM_WRITE_MIN_CTAS_2D : FEM_WRITE_MIN_CTAS_3D)
     k_write(ListLayout L, const int* __restrict__ row_ptr, int* __restrict__ col_idx, double* __restrict__ values,
             long long capacity, const int* __restrict__ ucounts) {
     constexpr bool kBsr = kMode == kOutBsr;
