@@ -96,3 +96,62 @@ def test_host_entry_point_checks_arguments(fem):
     out = fem.FemCsr()
     assert fem.load().fem_assemble_host(ctx.ctx, C.byref(bad), None, C.byref(out), None) == fem.FEM_ERR_BAD_ARG
     ctx.close()
+
+
+def _host_workspace(fem, m, o=None):
+    """A host buffer standing in for the workspace: the calls below must return
+    before the first device access, so it is never dereferenced."""
+    n = fem.workspace_size(m, o)
+    buf = np.zeros(n + 256, np.uint8)
+    ptr = (buf.ctypes.data + 255) // 256 * 256
+    return buf, C.c_void_p(ptr), n
+
+
+def test_precision_and_grid_options_are_checked(fem):
+    import meshgen as mg
+    lib = fem.load()
+    for name, bad_prec in (("t3_small", fem.FEM_PREC_TC_F16X3), ("t3_small", fem.FEM_PREC_FP64_SIMT),
+                           ("hex20_small", fem.FEM_PREC_FP32), ("q4_small", 9)):
+        m = mg.by_name(name)
+        cm = fem.fem_mesh_struct(m, fem.host_arrays(m))
+        keep, ws, n = _host_workspace(fem, m)
+        o = fem.opts(precision=bad_prec)
+        assert lib.fem_alls_scatter(C.byref(cm), C.byref(o), ws, n, None) == fem.FEM_ERR_BAD_ARG, (name, bad_prec)
+        st = C.c_int32(0)
+        if bad_prec != fem.FEM_PREC_FP64_SIMT or m.kind != mg.HEX20:
+            assert lib.fem_element_stiffness(C.byref(cm), C.byref(o), C.c_void_p(256), C.byref(st), None) \
+                == fem.FEM_ERR_BAD_ARG, (name, bad_prec)
+    m = mg.by_name("t3_small")
+    cm = fem.fem_mesh_struct(m, fem.host_arrays(m))
+    keep, ws, n = _host_workspace(fem, m)
+    o = fem.opts(ctas_per_sm=-1)
+    assert lib.fem_alls_scatter(C.byref(cm), C.byref(o), ws, n, None) == fem.FEM_ERR_BAD_ARG
+
+
+def test_upper_output_and_autotuner_arguments(fem):
+    import meshgen as mg
+    lib = fem.load()
+    m = mg.by_name("t3_small")
+    cm = fem.fem_mesh_struct(m, fem.host_arrays(m))
+    keep, ws, n = _host_workspace(fem, m)
+    # no row pointer / no col_idx with a capacity
+    assert lib.fem_alls_consolidate_upper(C.byref(cm), None, ws, n, None, None, None, 0, None) == fem.FEM_ERR_BAD_ARG
+    assert lib.fem_alls_consolidate_upper(C.byref(cm), None, ws, n, C.c_void_p(256), None, None, 5, None) \
+        == fem.FEM_ERR_BAD_ARG
+    # the autotuner's workspace covers every candidate, so at least the default one
+    for name in ("t3_small", "hex20_small"):
+        mm = mg.by_name(name)
+        cmm = fem.fem_mesh_struct(mm, fem.host_arrays(mm))
+        t = C.c_size_t(0)
+        assert lib.fem_autotune_workspace_size(C.byref(cmm), None, C.byref(t)) == fem.FEM_OK
+        assert t.value >= fem.workspace_size(mm) and t.value % 256 == 0
+    out = fem.FemCsr(m.num_dofs, 0, 0, 0, None, None, None)
+    best = fem.FemOpts()
+    assert lib.fem_autotune(C.byref(cm), None, ws, n, C.byref(out), 0, C.byref(best), None, None) \
+        == fem.FEM_ERR_BAD_ARG          # repeats < 1
+    assert lib.fem_autotune(C.byref(cm), None, ws, n, None, 2, C.byref(best), None, None) == fem.FEM_ERR_BAD_ARG
+    k = C.c_int32(0)
+    assert lib.fem_autotune_batched(C.byref(cm), 1, None, ws, n, C.byref(out), C.c_void_p(256), 0, C.byref(k),
+                                    None, None) == fem.FEM_ERR_BAD_ARG
+    assert lib.fem_autotune_batched(C.byref(cm), 0, None, ws, n, C.byref(out), C.c_void_p(256), 1, C.byref(k),
+                                    None, None) == fem.FEM_ERR_BAD_ARG
