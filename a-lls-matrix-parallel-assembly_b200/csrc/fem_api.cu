@@ -393,6 +393,10 @@ fem_status fem_apply_dirichlet(int32_t n_rows, const int32_t* row_ptr, const int
 
 namespace {
 
+// The slot streams and their fork / join events are shared by every batched
+// call on a device: calls from several host threads enqueue one at a time.
+std::mutex g_batch_mutex;
+
 int batch_slots(int n, int concurrency) {
     int k = concurrency > 0 ? concurrency : 4;
     k = std::min(k, kMaxBatchConcurrency);
@@ -447,6 +451,7 @@ fem_status fem_assemble_batched(const fem_mesh* meshes, int32_t n, const fem_opt
         if (!outs[i].row_ptr || outs[i].capacity < 0 || (outs[i].capacity > 0 && (!outs[i].col_idx || !outs[i].values)))
             return FEM_ERR_BAD_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lock(g_batch_mutex);
     cudaError_t err = stamps ? launch_stamp(stamps, s) : cudaSuccess;
     cudaStream_t ss[kMaxBatchConcurrency];
     if (!err) err = batch_fork(slots, s, ss);
@@ -564,7 +569,7 @@ fem_status fem_autotune(const fem_mesh* mesh, const fem_opts* opts, void* worksp
     fem_status st = not_capturing(s);
     if (st) return st;
     if ((st = check_mesh(mesh))) return st;
-    bool found = false;
+    bool found = false, overflowed = false;
     float best_t = 0.0f;
     for (const fem_opts& o : tune_candidates(mesh, opts)) {
         size_t need = 0;
@@ -573,7 +578,10 @@ fem_status fem_autotune(const fem_mesh* mesh, const fem_opts* opts, void* worksp
         // one untimed run: its status decides whether the candidate counts
         fem_csr c = *out;
         st = fem_assemble(mesh, &o, workspace, workspace_bytes, &c, stream);
-        if (st == FEM_ERR_POOL_OVERFLOW) continue;
+        if (st == FEM_ERR_POOL_OVERFLOW) {
+            overflowed = true;
+            continue;
+        }
         if (st && st != FEM_ERR_DETJ) return st;
         float ms = 0.0f;
         st = time_calls(s, repeats, [&] { return fem_assemble_async(mesh, &o, workspace, workspace_bytes, &c, stream); },
@@ -585,7 +593,7 @@ fem_status fem_autotune(const fem_mesh* mesh, const fem_opts* opts, void* worksp
             *best = o;
         }
     }
-    if (!found) return FEM_ERR_WORKSPACE;
+    if (!found) return overflowed ? FEM_ERR_POOL_OVERFLOW : FEM_ERR_WORKSPACE;
     if (best_ms) *best_ms = best_t;
     // leave the chosen options' assembly in out
     return fem_assemble(mesh, best, workspace, workspace_bytes, out, stream);

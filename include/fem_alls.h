@@ -264,7 +264,9 @@ FEM_API fem_status fem_batched_workspace_size(const fem_mesh* meshes, int32_t n,
  * row_ptr and FEM_ERR_CAPACITY in its info). infos: DEVICE array [n] that
  * receives each mesh's fem_info (nnz, status bits, ...). stamps: optional
  * DEVICE array [n + 1] of GPU global-timer nanoseconds: stamps[0] at the start,
- * stamps[1 + i] when mesh i is done. outs[i].n_rows is set. Asynchronous. */
+ * stamps[1 + i] when mesh i is done. outs[i].n_rows is set. Asynchronous.
+ * The library's slot streams are shared by all batched calls on a device:
+ * calls made from several host threads are enqueued one after another. */
 FEM_API fem_status fem_assemble_batched(const fem_mesh* meshes, int32_t n, const fem_opts* opts,
                                         int32_t concurrency, void* workspace, size_t workspace_bytes,
                                         fem_csr* outs, fem_info* infos, unsigned long long* stamps, void* stream);
@@ -286,7 +288,8 @@ FEM_API fem_status fem_autotune_workspace_size(const fem_mesh* mesh, const fem_o
  * kept. out: as for fem_assemble, with capacity >= nnz; on return it holds the
  * assembly with the chosen options (status as fem_assemble's). *best: the
  * fastest options; *best_ms (may be NULL): their mean time per assembly.
- * Candidates that overflow the pool or do not fit the workspace are skipped. */
+ * Candidates that overflow the pool or do not fit the workspace are skipped
+ * (FEM_ERR_POOL_OVERFLOW or FEM_ERR_WORKSPACE when none is left). */
 FEM_API fem_status fem_autotune(const fem_mesh* mesh, const fem_opts* opts, void* workspace, size_t workspace_bytes,
                                 fem_csr* out, int32_t repeats, fem_opts* best, float* best_ms, void* stream);
 
