@@ -283,7 +283,7 @@ def run_batched(args, rank: int, world: int, local_rank: int):
                        "what": "the 256 meshes' launches one after another on one stream (concurrency 1)"},
         "speedup_vs_sequential": seq["ms"] / ms,
         "clocks": clk.summary(),
-        "gpu_launches": None,
+        "gpu_launches": args.steps * batch_launches(meshes),
         "api": "fem_assemble_batched, captured in one CUDA graph",
     }
     print(json.dumps(line), flush=True)
@@ -664,10 +664,19 @@ def colour_baseline(fem, torch, asm, mesh, nnz, args, flush, stream) -> dict:
                        ", one launch per colour and element type"}
 
 
-# k_info_init; 2-D: k_bucket_count, k_bucket_scan, k_bucket_scatter; Hex20: k_bbox_init,
-# k_bbox, k_morton_count, k_bucket_scan, k_morton_scatter; scatter kernel(s);
-# k_consolidate_reset, k_scan_reduce, k_scan_tiles, k_row_ptr, k_write
+# k_info_init; element order (2-D: key count, k_bucket_scan, key scatter; Hex20 also
+# k_bbox_init, k_bbox); scatter kernel(s) (mixed: Q4 and T3); k_consolidate_reset,
+# k_scan_reduce, k_scan_tiles, k_row_ptr, k_write
 KERNELS_PER_STEP = {"q4": 10, "t3": 10, "mixed": 11, "hex20": 12}
+
+
+def batch_launches(meshes) -> int:
+    """Library kernels of one fem_assemble_batched call: each mesh's assembly
+    (as KERNELS_PER_STEP) and its completion kernel (k_finish), plus the start
+    stamp (k_stamp)."""
+    per_kind = {0: KERNELS_PER_STEP["q4"], 1: KERNELS_PER_STEP["t3"], 2: KERNELS_PER_STEP["hex20"],
+                3: KERNELS_PER_STEP["mixed"]}
+    return 1 + sum(per_kind[m.kind] + 1 for m in meshes)
 
 
 SCATTER_KERNEL = {"q4": "k_scatter_2d<4>", "t3": "k_scatter_2d<3>", "mixed": "k_scatter_2d<4> + k_scatter_2d<3>",
