@@ -155,3 +155,27 @@ def test_upper_output_and_autotuner_arguments(fem):
                                     None, None) == fem.FEM_ERR_BAD_ARG
     assert lib.fem_autotune_batched(C.byref(cm), 0, None, ws, n, C.byref(out), C.c_void_p(256), 1, C.byref(k),
                                     None, None) == fem.FEM_ERR_BAD_ARG
+
+
+def test_batched_workspace_sizing_host_only(fem):
+    # Slots are dealt the meshes largest first, one slot per mesh until every
+    # slot has one, so a slot's size is that of its first (largest) mesh: the
+    # workspace grows with the slot count and is capped by the mesh count.
+    import meshgen as mg
+    lib = fem.load()
+    meshes = mg.batch_meshes(6, seed=3, emin=20, emax=400)
+    arrs = [fem.host_arrays(m) for m in meshes]
+    cm = (fem.FemMesh * len(meshes))(*[fem.fem_mesh_struct(m, a) for m, a in zip(meshes, arrs)])
+    single = max(fem.workspace_size(m) for m in meshes)
+    sizes = []
+    for k in (1, 2, 4, 6, 8, 16):
+        b = C.c_size_t(0)
+        assert lib.fem_batched_workspace_size(cm, len(meshes), None, k, C.byref(b)) == fem.FEM_OK
+        sizes.append(b.value)
+    assert sizes[0] >= single and sizes[0] % 256 == 0
+    assert all(a <= b for a, b in zip(sizes, sizes[1:]))
+    assert sizes[3] == sizes[4] == sizes[5]          # at most one slot per mesh
+    total = sum(-(-fem.workspace_size(m) // 256) * 256 for m in meshes)
+    assert sizes[3] == total
+    b = C.c_size_t(0)
+    assert lib.fem_batched_workspace_size(cm, 0, None, 4, C.byref(b)) == fem.FEM_ERR_BAD_ARG
