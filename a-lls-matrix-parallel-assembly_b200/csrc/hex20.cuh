@@ -1,5 +1,5 @@
-// Hex20 element definitions shared by the element-stiffness kernel
-// (hex20_ke.cu) and the A-LLS scatter (scatter_hex20.cu).
+// Hex20 element definitions shared by the element-stiffness kernels
+// (element_stiffness.cu, ke_tcgen05.cu) and the A-LLS scatter (scatter_hex20.cu).
 //
 // Element stiffness, in double. With the physical shape-function gradients
 // G_g (a 60-vector per Gauss point g, dof r = 3 node + dir) and

@@ -28,8 +28,10 @@
  *  - the CSR pattern is built on the device (the reference builds it on the host
  *    with std::set); it is identical to the reference's pattern;
  *  - errors are returned as fem_status codes instead of exit(1);
- *  - everything is stream-ordered and re-entrant: no __device__ globals (the
- *    reference reaches its pool through __device__ pointers, Q4A:384-391);
+ *  - everything is stream-ordered and re-entrant: no __device__ globals on the
+ *    assembly path (the reference reaches its pool through __device__ pointers,
+ *    Q4A:384-391); the one exception is fem_assemble_static, whose workspace is
+ *    a static device array by design;
  *  - memory the library needs beyond inputs and outputs is a caller-provided
  *    workspace (size from fem_alls_workspace_size).
  *

@@ -384,6 +384,60 @@ int64_t oracle_assemble(int kind, int32_t num_nodes, int32_t num_elems, int32_t 
     return clamped;
 }
 
+int64_t oracle_assemble_rows(int kind, int32_t num_nodes, int32_t num_elems, int32_t stride,
+                             const int32_t* conn, const uint8_t* types, const double* x,
+                             const double* y, const double* z, const double* E, const double* nu,
+                             double E0, double nu0, double thickness, const int32_t* row_ptr,
+                             const int32_t* col_idx, const uint8_t* row_node_mask, double* values) {
+    /* oracle_assemble restricted to the dof rows of the nodes marked in
+     * row_node_mask: the same serial element loop and the same per-entry
+     * addition order (Q4A:329-380), skipping elements that touch no marked node
+     * and rows of unmarked nodes. Only the marked rows of values are written. */
+    const int dpn = kind_dpn(kind);
+    for (int32_t n = 0; n < num_nodes; n++) {
+        if (!row_node_mask[n]) continue;
+        for (int d = 0; d < dpn; d++) {
+            int32_t r = n * dpn + d;
+            for (int32_t k = row_ptr[r]; k < row_ptr[r + 1]; k++) values[k] = 0.0;
+        }
+    }
+    int64_t clamped = 0;
+    double* ke = (double*)malloc(3600 * sizeof(double));
+    for (int32_t e = 0; e < num_elems; e++) {
+        const int32_t* c = conn + (int64_t)e * stride;
+        int npe = elem_nodes(kind, types, e);
+        int any = 0;
+        for (int a = 0; a < npe; a++) any |= row_node_mask[c[a]];
+        if (!any) continue;
+        double Ee = E ? E[e] : E0, nue = nu ? nu[e] : nu0;
+        double xe[20], ye[20], ze[20];
+        for (int a = 0; a < npe; a++) {
+            xe[a] = x[c[a]];
+            ye[a] = y[c[a]];
+            ze[a] = z ? z[c[a]] : 0.0;
+        }
+        if (npe == 4) clamped += oracle_ke_q4(xe, ye, Ee, nue, thickness, ke);
+        else if (npe == 3) clamped += oracle_ke_t3(xe, ye, Ee, nue, thickness, ke);
+        else clamped += oracle_ke_hex20(xe, ye, ze, Ee, nue, ke);
+        int nd = npe * dpn;
+        int32_t dofs[60];
+        for (int a = 0; a < npe; a++)
+            for (int d = 0; d < dpn; d++) dofs[a * dpn + d] = c[a] * dpn + d;
+        for (int i = 0; i < nd; i++) {
+            if (!row_node_mask[c[i / dpn]]) continue;
+            int32_t r = dofs[i];
+            int32_t lo = row_ptr[r], hi = row_ptr[r + 1] - 1;
+            for (int j = 0; j < nd; j++) {
+                int64_t pos = find_col(col_idx, lo, hi, dofs[j]);
+                if (pos < 0) { free(ke); return -1; }
+                values[pos] += ke[i * nd + j];
+            }
+        }
+    }
+    free(ke);
+    return clamped;
+}
+
 void oracle_precision(int64_t nnz, const double* ref, const double* test, double out[6]) {
     /* Q4A:896-960 (+ the |diff| > 1e-10 count of Q4A:1128-1168). */
     double fro_ref = 0.0, max_abs = 0.0, max_rel = 0.0, mean_abs = 0.0, mean_rel = 0.0, fro = 0.0;

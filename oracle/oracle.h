@@ -65,6 +65,16 @@ int64_t oracle_assemble(int kind, int32_t num_nodes, int32_t num_elems, int32_t 
                         double E0, double nu0, double thickness, const int32_t* row_ptr,
                         const int32_t* col_idx, double* values);
 
+/* oracle_assemble restricted to the dof rows of the nodes with a nonzero
+ * row_node_mask[node] (num_nodes bytes): same element loop and addition order;
+ * only those rows of values are written. For checking large meshes on a
+ * sample of rows. */
+int64_t oracle_assemble_rows(int kind, int32_t num_nodes, int32_t num_elems, int32_t stride,
+                             const int32_t* conn, const uint8_t* types, const double* x,
+                             const double* y, const double* z, const double* E, const double* nu,
+                             double E0, double nu0, double thickness, const int32_t* row_ptr,
+                             const int32_t* col_idx, const uint8_t* row_node_mask, double* values);
+
 /* Error statistics of `test` against `ref` (restates analyzePrecision,
  * ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:896-960): out[0] max abs, out[1] max
  * rel, out[2] mean abs, out[3] mean rel, out[4] Frobenius-relative error (entries

@@ -54,6 +54,9 @@ def lib():
         L.oracle_assemble.argtypes = [C.c_int, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp,
                                       f64, f64, f64, vp, vp, vp]
         L.oracle_assemble.restype = i64
+        L.oracle_assemble_rows.argtypes = [C.c_int, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp,
+                                           f64, f64, f64, vp, vp, vp, vp]
+        L.oracle_assemble_rows.restype = i64
         L.oracle_precision.argtypes = [i64, vp, vp, vp]
         _lib = L
     return _lib
@@ -120,6 +123,29 @@ def assemble(mesh, row_ptr=None, col_idx=None, E0=None, nu0=None, thickness=None
     if r < 0:
         raise ValueError("oracle_assemble: entry missing from pattern")
     return row_ptr, col_idx, vals
+
+
+def assemble_rows(mesh, row_ptr, col_idx, row_nodes):
+    """Serial FP64 assembly of the dof rows of `row_nodes` only, into the given
+    pattern; returns a values array whose other rows are zero."""
+    conn = np.ascontiguousarray(mesh.conn, np.int32)
+    types = None if mesh.types is None else np.ascontiguousarray(mesh.types, np.uint8)
+    z = None if mesh.z is None else np.ascontiguousarray(mesh.z, np.float64)
+    E = None if mesh.E is None else np.ascontiguousarray(mesh.E, np.float64)
+    nu = None if mesh.nu is None else np.ascontiguousarray(mesh.nu, np.float64)
+    mask = np.zeros(mesh.num_nodes, np.uint8)
+    mask[np.asarray(row_nodes, np.int64)] = 1
+    row_ptr = np.ascontiguousarray(row_ptr, np.int32)
+    col_idx = np.ascontiguousarray(col_idx, np.int32)
+    vals = np.zeros(col_idx.shape[0], np.float64)
+    r = lib().oracle_assemble_rows(mesh.kind, mesh.num_nodes, mesh.num_elems, mesh.stride,
+                                   _ptr(conn), _ptr(types), _ptr(np.ascontiguousarray(mesh.x)),
+                                   _ptr(np.ascontiguousarray(mesh.y)), _ptr(z), _ptr(E), _ptr(nu),
+                                   mesh.E0, mesh.nu0, mesh.thickness, _ptr(row_ptr), _ptr(col_idx),
+                                   _ptr(mask), _ptr(vals))
+    if r < 0:
+        raise ValueError("oracle_assemble_rows: entry missing from pattern")
+    return vals
 
 
 def precision(ref: np.ndarray, test: np.ndarray) -> dict:

@@ -3,9 +3,12 @@
  * Built by oracle/Makefile from the reference source.
  *
  * Exposes: the reference lattice mesh generator (H20:324-362), its host CSR
- * pattern builder (H20:364-392) and, on a GPU, its FP32 device element
- * stiffness (H20:95-195) evaluated per element by a harness kernel.
+ * pattern builder (H20:364-392), its host colouring (H20:394-418) and, on a
+ * GPU, its FP32 device element stiffness (H20:95-195) evaluated per element by
+ * a harness kernel, and its two GPU assembly methods timed by its own
+ * compareAssemblyMethods (H20:421-543).
  */
+#include <chrono>
 #include "ref_common.h"
 
 #define main alls_reference_h20_main
@@ -76,5 +79,89 @@ REF_API int ref_h20_gpu_element_ke(int num_elems, const int32_t* conn, const dou
     if (!err) err = cudaMemcpy(ke_out, d_out, (size_t)num_elems * 3600 * sizeof(float), cudaMemcpyDeviceToHost);
     cudaFree(d_els);
     cudaFree(d_out);
+    return (int)err;
+}
+
+/* One mesh through the reference's own benchmark sequence (main, H20:560-625):
+ * host pattern (buildCSRStructureHex20), host colouring (colorElementsHex20),
+ * elements grouped by colour, device buffers, then compareAssemblyMethods
+ * (H20:421-543), which times the fixed-array A-LLS kernel + its conversion
+ * kernel and the coloured kernel, 3 warm-up and 10 measured iterations each,
+ * with CUDA events and the resets outside the window. The reference's
+ * material is a __constant__ (E, nu here, as FP32). GPU only.
+ * out[0] A-LLS ms (mean), out[1] coloured ms (mean), out[2] host pattern ms,
+ * out[3] host colouring ms, out[4] colours, out[5] nnz, out[6] A-LLS atomic
+ * counter, out[7] A-LLS row-array bytes. values_alls / values_colored
+ * (optional, nnz floats each): the CSR values of each method's last
+ * iteration, in the CSR order of the host pattern (rows sorted). Returns 0 or
+ * the CUDA error code (the reference's own checks exit the process). */
+REF_API int ref_h20_gpu_compare(int num_nodes, int num_elems, const int32_t* conn, const double* x,
+                                const double* y, const double* z, double E, double nu, double* out,
+                                float* values_alls, float* values_colored, int64_t capacity) {
+    std::vector<Element> elements = make_elements(num_elems, conn, x, y, z);
+    const int total_dofs = num_nodes * DOF_PER_NODE;
+    std::vector<int> csr_row_ptr, csr_col_ind;
+    auto t0 = std::chrono::high_resolution_clock::now();
+    buildCSRStructureHex20(num_nodes, elements, csr_row_ptr, csr_col_ind);
+    auto t1 = std::chrono::high_resolution_clock::now();
+    const int nnz = csr_row_ptr[total_dofs];
+    std::vector<std::vector<int>> color_groups;
+    auto t2 = std::chrono::high_resolution_clock::now();
+    const int num_colors = colorElementsHex20(elements, color_groups);
+    auto t3 = std::chrono::high_resolution_clock::now();
+    std::vector<int> sorted_indices, h_color_offsets(num_colors), h_color_sizes(num_colors);
+    int offset = 0;
+    for (int c = 0; c < num_colors; c++) {
+        h_color_offsets[c] = offset;
+        h_color_sizes[c] = (int)color_groups[c].size();
+        sorted_indices.insert(sorted_indices.end(), color_groups[c].begin(), color_groups[c].end());
+        offset += h_color_sizes[c];
+    }
+    std::vector<Element> sorted_elements(elements.size());
+    for (size_t i = 0; i < elements.size(); i++) sorted_elements[i] = elements[sorted_indices[i]];
+
+    float Ef = (float)E, nuf = (float)nu;
+    cudaError_t err = cudaMemcpyToSymbol(d_YOUNG_MODULUS, &Ef, sizeof(float));
+    if (!err) err = cudaMemcpyToSymbol(d_POISSON_RATIO, &nuf, sizeof(float));
+    Element* d_elements = nullptr;
+    int *d_csr_row_ptr = nullptr, *d_csr_col_ind = nullptr, *d_color_offsets = nullptr, *d_color_sizes = nullptr;
+    float *d_csr_values_alls = nullptr, *d_csr_values_colored = nullptr;
+    if (!err) err = cudaMalloc(&d_elements, sorted_elements.size() * sizeof(Element));
+    if (!err) err = cudaMalloc(&d_csr_row_ptr, (total_dofs + 1) * sizeof(int));
+    if (!err) err = cudaMalloc(&d_csr_col_ind, (size_t)nnz * sizeof(int));
+    if (!err) err = cudaMalloc(&d_csr_values_alls, (size_t)nnz * sizeof(float));
+    if (!err) err = cudaMalloc(&d_csr_values_colored, (size_t)nnz * sizeof(float));
+    if (!err) err = cudaMalloc(&d_color_offsets, num_colors * sizeof(int));
+    if (!err) err = cudaMalloc(&d_color_sizes, num_colors * sizeof(int));
+    if (!err) err = cudaMemcpy(d_elements, sorted_elements.data(), sorted_elements.size() * sizeof(Element),
+                               cudaMemcpyHostToDevice);
+    if (!err) err = cudaMemcpy(d_csr_row_ptr, csr_row_ptr.data(), (total_dofs + 1) * sizeof(int), cudaMemcpyHostToDevice);
+    if (!err) err = cudaMemcpy(d_csr_col_ind, csr_col_ind.data(), (size_t)nnz * sizeof(int), cudaMemcpyHostToDevice);
+    if (!err) err = cudaMemcpy(d_color_offsets, h_color_offsets.data(), num_colors * sizeof(int), cudaMemcpyHostToDevice);
+    if (!err) err = cudaMemcpy(d_color_sizes, h_color_sizes.data(), num_colors * sizeof(int), cudaMemcpyHostToDevice);
+    if (!err) {
+        PerformanceMetrics res = compareAssemblyMethods(num_elems, total_dofs, nnz, d_elements, d_csr_row_ptr,
+                                                        d_csr_col_ind, d_csr_values_alls, d_csr_values_colored,
+                                                        d_color_offsets, d_color_sizes, num_colors, h_color_sizes);
+        out[0] = res.alls_time_ms;
+        out[1] = res.colored_time_ms;
+        out[6] = res.atomic_ops_alls;
+        out[7] = (double)res.alls_mem_usage;
+    }
+    out[2] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    out[3] = std::chrono::duration<double, std::milli>(t3 - t2).count();
+    out[4] = num_colors;
+    out[5] = nnz;
+    if (!err && values_alls && nnz <= capacity)
+        err = cudaMemcpy(values_alls, d_csr_values_alls, (size_t)nnz * sizeof(float), cudaMemcpyDeviceToHost);
+    if (!err && values_colored && nnz <= capacity)
+        err = cudaMemcpy(values_colored, d_csr_values_colored, (size_t)nnz * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(d_elements);
+    cudaFree(d_csr_row_ptr);
+    cudaFree(d_csr_col_ind);
+    cudaFree(d_csr_values_alls);
+    cudaFree(d_csr_values_colored);
+    cudaFree(d_color_offsets);
+    cudaFree(d_color_sizes);
     return (int)err;
 }

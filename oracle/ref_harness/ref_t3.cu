@@ -121,6 +121,11 @@ REF_API int ref_t3_gpu_alls_time(int num_nodes, int num_elems, int stride, const
     float total = 0.0f;
     for (int i = 0; i < warmup + iters && !err; i++) {
         err = cudaMemset(d_heads, 0, total_dofs * sizeof(ALLSNode*));
+        /* the pool too: the reference links a node (atomicExch on the head)
+         * before it stores the node's next pointer, with no fence, so a reader
+         * on another SM can see a node whose next is still the previous
+         * iteration's; cleared, such a read sees nullptr and ends the walk */
+        if (!err) err = cudaMemset(d_pool, 0, (contributions + 1) * sizeof(ALLSNode));
         if (!err) err = cudaMemset(d_idx, 0, sizeof(int));
         if (!err) err = cudaMemset(d_counter, 0, sizeof(int));
         if (!err) err = cudaEventRecord(start);
