@@ -348,10 +348,10 @@ cudaError_t launch_hex20_ke(const MeshView& m, double* ke_out, int* status, cuda
 }  // namespace
 
 cudaError_t launch_element_stiffness(const MeshView& m, int kind, int precision, double* ke_out, int* status,
-                                     cudaStream_t s) {
+                                     long long wait_ns, cudaStream_t s) {
     if (m.E_count <= 0) return cudaSuccess;
     if (kind == FEM_HEX20) {
-        if (precision == FEM_PREC_TC_F16X3) return launch_hex20_ke_tcgen05(m, ke_out, status, s);
+        if (precision == FEM_PREC_TC_F16X3) return launch_hex20_ke_tcgen05(m, ke_out, status, wait_ns, s);
         if (precision == FEM_PREC_FP64_SIMT) return launch_hex20_ke<FEM_PREC_FP64_SIMT>(m, ke_out, status, s);
         return launch_hex20_ke<FEM_PREC_FP64>(m, ke_out, status, s);
     } else {

@@ -106,6 +106,8 @@ fem_status make_layout(const fem_mesh* m, const fem_opts* o, HostLayout& h) {
         off += align_up((size_t)h.E * sizeof(int)) + align_up(4 * sizeof(int)) + align_up(nbuckets * sizeof(int)) +
                align_up(6 * sizeof(unsigned long long));
     }
+    h.off_map = off;  // Hex20: slot map of one wave of the two-pass scatter
+    if (h.kind == FEM_HEX20) off += align_up((size_t)std::min(h.E, kHex20Wave) * 400 * sizeof(int));
     h.total = off;
     return FEM_OK;
 }
@@ -234,7 +236,16 @@ fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* wo
             b + h.off_elist + align_up((size_t)h.E * sizeof(int)) + align_up(4 * sizeof(int)) +
             align_up(nbuckets * sizeof(int)));
         err = launch_reorder_3d(m, hist, ranges, perm, bbox, sm_count(), s);
-        if (!err) err = launch_scatter_hex20(m, L, precision, perm, ctas, s);
+        // two-pass scatter in waves of the spatial order: a wave's claims
+        // (entries, zeroed value blocks, slot map) complete before its value
+        // pass, and the blocks it touches are still in L2 when the values arrive
+        int* map = reinterpret_cast<int*>(b + h.off_map);
+        const long long wait_ns = wait_ns_of(opts ? opts->wait_limit_us : 0);
+        for (int i0 = 0; i0 < h.E && !err; i0 += kHex20Wave) {
+            const int i1 = std::min(h.E, i0 + kHex20Wave);
+            err = launch_claim_hex20(m, L, perm, i0, i1, map, s);
+            if (!err) err = launch_values_hex20(m, L, precision, perm, i0, i1, map, ctas, wait_ns, s);
+        }
     } else {
         err = launch_reorder(m, hist, ranges, perm, sm_count(), s);
         if (!err && h.kind != FEM_T3) err = launch_scatter_2d(m, L, 4, precision, perm, ranges + 0, ctas, s);
@@ -350,7 +361,9 @@ fem_status fem_element_stiffness(const fem_mesh* mesh, const fem_opts* opts, dou
         return FEM_ERR_BAD_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t err = cudaMemsetAsync(status, 0, sizeof(int32_t), s);
-    if (!err) err = launch_element_stiffness(mesh_view(mesh), mesh->kind, precision, ke_out, status, s);
+    if (!err)
+        err = launch_element_stiffness(mesh_view(mesh), mesh->kind, precision, ke_out, status,
+                                       wait_ns_of(opts ? opts->wait_limit_us : 0), s);
     return err ? cuda_fail(err) : FEM_OK;
 }
 

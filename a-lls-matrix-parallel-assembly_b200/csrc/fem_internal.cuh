@@ -165,7 +165,7 @@ struct HostLayout {
     int kind, dpn, B, N, E;
     int S1, S2, H1, H2, cap2;
     int num_tiles;  // scan tiles of kScanTile nodes
-    size_t off_info, off_meta1, off_meta2, off_vals, off_counts, off_ucounts, off_tiles, off_elist, total;
+    size_t off_info, off_meta1, off_meta2, off_vals, off_counts, off_ucounts, off_tiles, off_elist, off_map, total;
     size_t meta1_bytes;
 };
 

@@ -45,7 +45,7 @@ constexpr uint32_t kTmemCols = 128;
 constexpr int kRows = 128;              // operand rows: two elements x 64
 constexpr uint32_t kLBO = 128;          // bytes between the two 8-element K chunks of one MMA
 constexpr uint32_t kSBO = 512;          // bytes between 8-row groups (4 K chunks of 128 B)
-constexpr long long kSpinCycles = 1ll << 32;
+constexpr long long kDefaultWaitNs = 200ll * 1000 * 1000;  // the second, recovering wait of a timed-out CTA
 
 // Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator (bits
 // 4-5 = 1), FP16 A and B (bits 7-12 = 0), both K-major (bits 15, 16 = 0),
@@ -106,11 +106,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for the completion of the mbarrier phase of this parity.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
-    const long long t0 = clock64();
+__device__ __forceinline__ long long global_ns() {
+    long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for the completion of the mbarrier phase of this parity, for at most
+// limit_ns nanoseconds of the GPU's global timer; limit_ns <= 0: one poll.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, long long limit_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (limit_ns <= 0) return false;
+    const long long t0 = global_ns();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > kSpinCycles) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     return true;
 }
 
@@ -130,12 +139,29 @@ __device__ __forceinline__ unsigned pack_half2(__half lo, __half hi) {
     return (unsigned)__half_as_ushort(lo) | ((unsigned)__half_as_ushort(hi) << 16);
 }
 
+// Value pass of the two-pass Hex20 list scatter (kSlots): the wave of elements
+// perm[i0, i1) and the slot map of their 400 node pairs (claim_hex20.cu).
+struct SlotTarget {
+    const int* perm;
+    const int* map;
+    double* vals;
+    int i0, i1;
+    long long wait_ns;  // bound on the wait for the products (both modes)
+};
+
+// kSlots = false: the packed Ke of every element to ke_out (fem_element_stiffness).
+// kSlots = true: each Ke block added with FP64 atomics to its list entry (row
+// I, column J) and, transposed, to (row J, column I), at the slot map's ids.
+template <bool kSlots>
 __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double* __restrict__ ke_out,
-                                                             int* __restrict__ status, int bulk_out) {
+                                                             int* __restrict__ status, int bulk_out, SlotTarget tgt) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     KeTcSmem& sm = *reinterpret_cast<KeTcSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const long long npairs = ((long long)m.E_count + 1) / 2;
+    // elements: positions q of the wave (kSlots) or the mesh's elements q
+    const long long count = kSlots ? (long long)(tgt.i1 - tgt.i0) : (long long)m.E_count;
+    const long long npairs = (count + 1) / 2;
+    auto elem = [&](long long q) -> long long { return kSlots ? (long long)__ldg(tgt.perm + tgt.i0 + q) : q; };
     const uint32_t bar = smem_u32(&sm.mbar);
 
     if (tid == 0) {
@@ -172,9 +198,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
     double pre_x = 0.0, pre_y = 0.0, pre_z = 0.0;
     auto prefetch = [&](long long p) {
         if (tid >= 40) return;
-        const long long e = 2 * p + tid / 20;
+        const long long q = 2 * p + tid / 20;
         pre_state = 2;
-        if (p < npairs && e < m.E_count) {
+        if (p < npairs && q < count) {
+            const long long e = elem(q);
             pre_n = __ldg(m.conn + (size_t)e * 20 + tid % 20);
             pre_state = (pre_n >= 0 && pre_n < m.N) ? 0 : 1;
             if (pre_state == 0) {
@@ -206,9 +233,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
             if (pre_state) atomicMax(&sm.state[e], pre_state);
             if (pre_state == 1) atomicOr(status, 1 << FEM_ERR_BAD_MESH);
         } else if (tid < 42) {
-            const long long e = 2 * p + (tid - 40);
-            const double E = e < m.E_count ? (m.E ? __ldg(m.E + e) : m.E0) : 0.0;
-            const double nu = e < m.E_count ? (m.nu ? __ldg(m.nu + e) : m.nu0) : 0.0;
+            const long long q = 2 * p + (tid - 40);
+            const long long e = q < count ? elem(q) : 0;
+            const double E = q < count ? (m.E ? __ldg(m.E + e) : m.E0) : 0.0;
+            const double nu = q < count ? (m.nu ? __ldg(m.nu + e) : m.nu0) : 0.0;
             sm.lam[tid - 40] = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
             sm.mu[tid - 40] = E / (2.0 * (1.0 + nu));
         }
@@ -337,7 +365,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
             for (int k = 0; k < 2; k++) mma_f16(tmem, smem_desc(a_hi + 256u * k), smem_desc(b_hi + 256u * k), 1u);
             mma_commit(bar);
         }
-        const bool done = mbar_wait_bounded(bar, parity);
+        const bool done = mbar_wait_bounded(bar, parity, tgt.wait_ns);
         parity ^= 1u;
         if (__syncthreads_or(!done)) {
             if (tid == 0) atomicOr(status, 1 << FEM_ERR_TIMEOUT);
@@ -361,6 +389,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
             const double inv_s2 = ldexp(1.0, 2 * ex);
             const float lam = (float)sm.lam[e], mu = (float)sm.mu[e];
             double* out = sm.ke[e] + 9 * (I * 20 - I * (I - 1) / 2 - I) + 3 * a;  // + 9 J: block (I, J)
+            const long long q = 2 * p + e;  // the element's position in the wave (kSlots)
+            const int* mrow = tgt.map + (size_t)(kSlots && q < count ? q : 0) * 400;
+            const bool add = kSlots && real && q < count;
 #pragma unroll
             for (int J = 0; J < 20; J++) {
                 const int c = 32 * (J / 10) + 3 * (J % 10);
@@ -382,7 +413,25 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
                 const float k0 = fmaf(lam, o0, fmaf(mu, T0, a == 0 ? mtr : 0.0f));
                 const float k1 = fmaf(lam, o1, fmaf(mu, T1, a == 1 ? mtr : 0.0f));
                 const float k2 = fmaf(lam, o2, fmaf(mu, T2, a == 2 ? mtr : 0.0f));
-                if (real && J >= I) {
+                if (kSlots) {
+                    if (add && J >= I) {
+                        const double v0 = (double)k0 * inv_s2, v1 = (double)k1 * inv_s2, v2 = (double)k2 * inv_s2;
+                        const int g_ij = __ldg(mrow + I * 20 + J);
+                        if (g_ij >= 0) {
+                            double* d = tgt.vals + (size_t)(unsigned)g_ij * 9 + 3 * a;
+                            atomicAdd(d, v0);
+                            atomicAdd(d + 1, v1);
+                            atomicAdd(d + 2, v2);
+                        }
+                        const int g_ji = J != I ? __ldg(mrow + J * 20 + I) : -1;
+                        if (g_ji >= 0) {
+                            double* d = tgt.vals + (size_t)(unsigned)g_ji * 9 + a;
+                            atomicAdd(d, v0);
+                            atomicAdd(d + 3, v1);
+                            atomicAdd(d + 6, v2);
+                        }
+                    }
+                } else if (real && J >= I) {
                     out[9 * J] = (double)k0 * inv_s2;
                     out[9 * J + 1] = (double)k1 * inv_s2;
                     out[9 * J + 2] = (double)k2 * inv_s2;
@@ -397,6 +446,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
             sm.bound_bits[tid] = 0ull;
             sm.negmask[tid] = 0u;
         }
+        if (kSlots) continue;
         const int nvalid = 2 * p + 1 < m.E_count ? 2 : 1;
         double* dst = ke_out + (size_t)(2 * p) * kPackedHex20;
         if (bulk_out) {
@@ -410,8 +460,14 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
             for (int k = tid; k < nvalid * kPackedHex20; k += kThreads) dst[k] = (&sm.ke[0][0])[k];
         }
     }
-    if (timed_out) mbar_wait_bounded(bar, parity ^ 1u);  // the products in flight, with a limit
-    if (tid == 0 && bulk_out) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    // A CTA whose wait ran out still has its six products in flight: it waits
+    // for them again, with the default bound, before the tensor memory they
+    // write is released. If that wait runs out too, the products are presumed
+    // lost; the memory is released all the same and FEM_ERR_INTERNAL tells the
+    // caller to treat the device as suspect.
+    if (timed_out && !mbar_wait_bounded(bar, parity ^ 1u, kDefaultWaitNs) && tid == 0)
+        atomicOr(status, 1 << FEM_ERR_INTERNAL);
+    if (tid == 0 && bulk_out && !kSlots) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
@@ -420,9 +476,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
     }
 }
 
-}  // namespace
-
-cudaError_t launch_hex20_ke_tcgen05(const MeshView& m, double* ke_out, int* status, cudaStream_t s) {
+template <bool kSlots>
+cudaError_t launch_tc(const MeshView& m, double* ke_out, int* status, const SlotTarget& tgt, cudaStream_t s) {
     static DeviceCache cache;
     const size_t smem = sizeof(KeTcSmem);
     int blocks_per_sm = 0;
@@ -431,9 +486,10 @@ cudaError_t launch_hex20_ke_tcgen05(const MeshView& m, double* ke_out, int* stat
         // and the 512 tensor-memory columns of an SM (kTmemCols per CTA). The
         // runtime's occupancy query answers 1 for this kernel, which would
         // leave three quarters of the SM idle.
-        cudaError_t e = cudaFuncSetAttribute(k_hex20_ke_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e =
+            cudaFuncSetAttribute(k_hex20_ke_tc<kSlots>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncAttributes fa;
-        if (!e) e = cudaFuncGetAttributes(&fa, k_hex20_ke_tc);
+        if (!e) e = cudaFuncGetAttributes(&fa, k_hex20_ke_tc<kSlots>);
         int dev = 0, regs_sm = 0, smem_sm = 0;
         if (!e) e = cudaGetDevice(&dev);
         if (!e) e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
@@ -446,11 +502,27 @@ cudaError_t launch_hex20_ke_tcgen05(const MeshView& m, double* ke_out, int* stat
         return cudaSuccess;
     }, blocks_per_sm);
     if (err) return err;
-    const long long npairs = ((long long)m.E_count + 1) / 2;
-    const long long grid = std::min<long long>((long long)blocks_per_sm * sm_count(), npairs);
-    const int bulk_out = (reinterpret_cast<uintptr_t>(ke_out) & 15u) == 0;
-    k_hex20_ke_tc<<<(int)grid, kThreads, smem, s>>>(m, ke_out, status, bulk_out);
+    const long long count = kSlots ? (long long)(tgt.i1 - tgt.i0) : (long long)m.E_count;
+    const long long npairs = (count + 1) / 2;
+    const long long grid = std::max<long long>(1, std::min<long long>((long long)blocks_per_sm * sm_count(), npairs));
+    const int bulk_out = !kSlots && (reinterpret_cast<uintptr_t>(ke_out) & 15u) == 0;
+    k_hex20_ke_tc<kSlots><<<(int)grid, kThreads, smem, s>>>(m, ke_out, status, bulk_out, tgt);
     return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_hex20_ke_tcgen05(const MeshView& m, double* ke_out, int* status, long long wait_ns,
+                                    cudaStream_t s) {
+    SlotTarget t{};
+    t.wait_ns = wait_ns;
+    return launch_tc<false>(m, ke_out, status, t, s);
+}
+
+cudaError_t launch_values_hex20_tc(const MeshView& m, const ListLayout& L, const int* perm, int i0, int i1,
+                                   const int* map, long long wait_ns, cudaStream_t s) {
+    if (i1 <= i0) return cudaSuccess;
+    return launch_tc<true>(m, nullptr, &L.info->status_bits, SlotTarget{perm, map, L.vals, i0, i1, wait_ns}, s);
 }
 
 }  // namespace fem

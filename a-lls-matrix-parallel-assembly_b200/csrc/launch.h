@@ -66,10 +66,16 @@ constexpr int kPacked2D_Q4 = 10 * 4;   // 10 upper 2x2 node blocks (also the mix
 constexpr int kPacked2D_T3 = 6 * 4;
 // Element stiffness of every element, natural order; status gets 1 << FEM_ERR_* bits.
 cudaError_t launch_element_stiffness(const MeshView& m, int kind, int precision, double* ke_out, int* status,
-                                     cudaStream_t s);
+                                     long long wait_ns, cudaStream_t s);
 // Hex20 element stiffness with the contraction on the tcgen05 tensor cores
 // (FEM_PREC_TC_F16X3), two elements per CTA step.
-cudaError_t launch_hex20_ke_tcgen05(const MeshView& m, double* ke_out, int* status, cudaStream_t s);
+// wait_ns: bound on a CTA's wait for its products (<= 0: one poll), see fem_opts.wait_limit_us.
+cudaError_t launch_hex20_ke_tcgen05(const MeshView& m, double* ke_out, int* status, long long wait_ns,
+                                    cudaStream_t s);
+// fem_opts.wait_limit_us in nanoseconds: 0 -> 200 ms, > 0 -> that bound, < 0 -> 0 (one poll).
+inline long long wait_ns_of(int wait_limit_us) {
+    return wait_limit_us == 0 ? 200ll * 1000 * 1000 : (wait_limit_us > 0 ? 1000ll * wait_limit_us : 0);
+}
 // Target of a value-only re-assembly: CSR positions of every element block.
 struct MapTarget {
     const int* map;      // [E * npe^2] position of block (a, b) of element e at e * npe^2 + a * npe + b
@@ -91,6 +97,23 @@ cudaError_t launch_reassemble_hex20(const MeshView& m, int precision, const int*
 // plain adds at binary-searched CSR positions (t.map unused); status bits in info.
 cudaError_t launch_colour_hex20(const MeshView& m, const int* perm, const int* range, const MapTarget& t,
                                 DevInfo* info, cudaStream_t s);
+
+// Two-pass Hex20 list scatter over the elements perm[i0, i1) (one wave):
+// pass 1 claims the list entries, zeroes the claimed value blocks and writes
+// the slot map [(i1 - i0) * 400] (claim_hex20.cu); pass 2 adds the Ke blocks
+// at the mapped slots (values_hex20.cu in FP64, ke_tcgen05.cu in the
+// tensor-core form). wait_ns: see wait_ns_of.
+cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int* perm, int i0, int i1, int* map,
+                               cudaStream_t s);
+cudaError_t launch_values_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm, int i0,
+                                int i1, const int* map, int ctas_per_sm, long long wait_ns, cudaStream_t s);
+cudaError_t launch_values_hex20_fp64(const MeshView& m, const ListLayout& L, const int* perm, int i0, int i1,
+                                     const int* map, int ctas_per_sm, cudaStream_t s);
+cudaError_t launch_values_hex20_tc(const MeshView& m, const ListLayout& L, const int* perm, int i0, int i1,
+                                   const int* map, long long wait_ns, cudaStream_t s);
+// Elements per wave of the two-pass scatter: the value blocks a wave's claims
+// zero (about 17 KB per element) stay in L2 until its value pass adds to them.
+constexpr int kHex20Wave = 4096;
 
 // perm: element visit order (spatial, from launch_reorder_3d); precision FEM_PREC_*.
 cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm, int ctas_per_sm,

@@ -52,7 +52,8 @@ class FemMesh(C.Structure):
 
 class FemOpts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("first_slots", C.c_int32), ("chunk_slots", C.c_int32),
-                ("ctas_per_sm", C.c_int32), ("pool_factor", C.c_double)]
+                ("ctas_per_sm", C.c_int32), ("pool_factor", C.c_double), ("wait_limit_us", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class FemCsr(C.Structure):
@@ -135,8 +136,8 @@ FEM_PREC_FP64, FEM_PREC_TC_F16X3, FEM_PREC_FP64_SIMT, FEM_PREC_FP32 = 0, 1, 2, 3
 
 
 def opts(first_slots: int = 0, chunk_slots: int = 0, pool_factor: float = 0.0, precision: int = 0,
-         ctas_per_sm: int = 0) -> FemOpts:
-    return FemOpts(precision, first_slots, chunk_slots, ctas_per_sm, pool_factor)
+         ctas_per_sm: int = 0, wait_limit_us: int = 0) -> FemOpts:
+    return FemOpts(precision, first_slots, chunk_slots, ctas_per_sm, pool_factor, wait_limit_us, 0)
 
 
 def _ptr(t) -> Optional[int]:

@@ -48,7 +48,7 @@
 extern "C" {
 #endif
 
-#define FEM_ALLS_ABI_VERSION 1
+#define FEM_ALLS_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define FEM_API __attribute__((visibility("default")))
@@ -115,6 +115,14 @@ typedef struct fem_opts {
     int32_t ctas_per_sm;   /* resident CTAs per SM of the scatter kernel's persistent grid
                               (capped at what fits); 0 = all that fit */
     double pool_factor;    /* overflow chunks per node in the pool; 0 = default */
+    int32_t wait_limit_us; /* bound on a kernel's wait for its own tensor-core products
+                              (FEM_PREC_TC_F16X3): 0 = the default, 200 ms; > 0 = that many
+                              microseconds; < 0 = give up at the first poll that finds them
+                              unfinished. A wait that runs out raises FEM_ERR_TIMEOUT; the
+                              kernel then waits for the products with the default bound,
+                              releases its tensor memory and returns (FEM_ERR_INTERNAL too if
+                              that second wait also runs out). */
+    int32_t reserved;      /* 0 */
 } fem_opts;
 
 typedef struct fem_csr {

@@ -35,7 +35,7 @@ def test_library_exports_every_declared_symbol(fem):
 
 def test_abi_version_and_status_strings(fem):
     lib = fem.load()
-    assert lib.fem_abi_version() == 1
+    assert lib.fem_abi_version() == 2
     assert lib.fem_status_string(0) == b"ok"
     assert b"pool" in lib.fem_status_string(3)
 

@@ -1,9 +1,13 @@
 """Node-block (BSR) output of the consolidation (fem_alls_consolidate_bsr),
 through the C ABI: expanded to scalar CSR it must equal the CSR output of the
 same lists exactly (same entries, same values bit for bit), for 2x2 and 3x3
-blocks, including the long-row path (a high-degree node)."""
+blocks, including the long-row path (a high-degree node); and, expanded, it
+must match the oracle directly: the pattern of the reference's host builder
+bit for bit, the values within 1e-12 of the row/column scale."""
 import numpy as np
 import pytest
+
+from conftest import diag_scale
 
 pytestmark = pytest.mark.gpu
 
@@ -32,7 +36,7 @@ def _fan():
 
 
 @pytest.mark.parametrize("name", ["q4_small", "t3_small", "mixed_small", "hex20_small", "fan"])
-def test_bsr_equals_csr(fem, cuda_device, name):
+def test_bsr_equals_csr(fem, oracle_mod, cuda_device, name):
     import meshgen as mg
     m = _fan() if name == "fan" else mg.by_name(name)
     asm = fem.Assembler(m)
@@ -49,3 +53,9 @@ def test_bsr_equals_csr(fem, cuda_device, name):
     np.testing.assert_array_equal(erp, rp)
     np.testing.assert_array_equal(eci, ci)
     np.testing.assert_array_equal(ev, v)
+    # pinned to the oracle itself, not only to the library's own CSR
+    orp, oci, ov = oracle_mod.assemble(m)
+    np.testing.assert_array_equal(erp, orp)
+    np.testing.assert_array_equal(eci, oci)
+    scale = np.maximum(np.abs(ov), diag_scale(orp, oci, ov))
+    assert np.all(np.abs(ev - ov) <= 1e-12 * scale)

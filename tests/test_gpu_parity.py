@@ -197,8 +197,9 @@ def test_host_entry_point(fem, oracle_mod, cuda_device):
 # Full assembly with the tensor-core Ke form (FEM_PREC_TC_F16X3): the pattern
 # is the same bit for bit; values (FP64 global accumulation of the per-element
 # FP16-split contraction) agree with the FP64 oracle within TC_RTOL on the
-# row/column scale max(|K_ij|, sqrt(|K_ii K_jj|)).
-TC_RTOL = 2e-6
+# row/column scale max(|K_ij|, sqrt(|K_ii K_jj|)), bounded at the north star's
+# 1e-6 (measured: about 4e-7).
+TC_RTOL = 1e-6
 
 
 @pytest.mark.parametrize("name", ["hex20_small"])
