@@ -1,30 +1,39 @@
 """Benchmark of the FEM global-stiffness assembly (A-LLS path) on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload t3|q4|mixed|hex20]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload hex20|t3|q4|mixed|batched]
                     [--impl ours|reference]
 
 A step is one full device assembly of a seeded synthetic mesh: list reset,
-fused element stiffness + A-LLS scatter, and list -> CSR consolidation (pattern
-and FP64 values), inputs resident in HBM. The default workload is the T3
-unstructured configuration (1000x1000 grid, random diagonals, shuffled
-elements, lognormal E). ``value`` is elements/s over the whole job; nnz/s,
-the roofline, the end-to-end figure through the host-buffer C ABI entry point
-(host<->device copies inside the timed region) and a CPU baseline are added to
-the same JSON line. With --gpus N > 1 (one process per GPU under torchrun) every
-rank assembles its own replica (the path has no exchange step): weak scaling.
+element order, element stiffness + A-LLS list scatter, and list -> CSR
+consolidation (pattern and FP64 values), inputs resident in HBM. The default
+workload is the Hex20 64^3 configuration (1,085,825 nodes, 262,144 elements,
+557,286,921 CSR nonzeros). ``value`` is elements/s over the whole job; nnz/s,
+the rooflines, the accuracy of every CSR value against the serial FP64 oracle,
+the end-to-end figure through the host-buffer C ABI entry point (host<->device
+copies inside the timed region), the tensor-core Ke form, the colouring
+baseline, the value-only re-assembly, the T3 1000^2 and 256-mesh batched
+configurations and a CPU baseline are added to the same JSON line. With
+--gpus N > 1 (one process per GPU under torchrun) every rank assembles its own
+replica (the path has no exchange step): weak scaling, headline fields only.
 
-``--impl reference`` times the reference's own CPU path for the same workload:
-its host CSR pattern builder (buildCSRStructure, compiled from the reference
+``--impl reference`` runs the reference's own code for the same workload on
+the full configuration: its host CSR pattern builder (buildCSRStructureHex20,
+ALLS_Hex20_3D_Assembly_Performance.cu:364-392, compiled from the reference
 sources into oracle/_ref) plus the serial FP64 value scatter of
-assembleGlobalStiffnessHost (ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:329-380;
+assembleGlobalStiffnessHost (ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:329-380,
 the reference's own function for Q4, the oracle's restatement of it for the
-other element kinds), on a bounded sample, in parallel on the host cores.
+other element kinds, which the reference has no host assembly for), one core,
+pattern and values timed separately; and, in a `reference_gpu` field, the
+reference's GPU kernels on the same mesh and GPU, timed by the reference's own
+compareAssemblyMethods (H20:421-543).
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
+import platform
 import statistics
 import subprocess
 import sys
@@ -44,10 +53,13 @@ WORKLOADS = {
     "batched": ("batched_256", "256 independent meshes, kind uniform over {Q4, T3, mixed, Hex20}, elements "
                 "log-uniform over 1k-200k, each kind's jitter and material distributions"),
 }
-# A smaller instance of each workload's generator, for the CPU legs.
-CPU_SAMPLES = {"q4": ("q4", {}), "t3": ("t3", {"nx": 400, "ny": 400}),
-               "mixed": ("mixed", {"nx": 450, "ny": 450}), "hex20": ("hex20", {"nx": 20})}
+DEFAULT_WORKLOAD = "hex20"
 L2_BYTES = 126 * 2 ** 20
+L2_NOTE = ("a buffer of 2x L2 (252 MB) is zeroed between timed steps, outside the step events; the Hex20 64^3 "
+           "step also moves 24.6 GB of algorithmic traffic, far above L2")
+METRIC = "elements/s (device FP64 A-LLS assembly: element stiffness, list scatter, CSR pattern + values)"
+SCATTER_KERNEL = {"q4": "k_scatter_2d<4>", "t3": "k_scatter_2d<3>", "mixed": "k_scatter_2d<4> + k_scatter_2d<3>",
+                  "hex20": "k_claim_hex20 + k_values_hex20 (two-pass list scatter, in waves)"}
 
 
 def make_mesh(workload: str, size: int = 0, **kw):
@@ -63,6 +75,15 @@ def make_mesh(workload: str, size: int = 0, **kw):
     if workload == "hex20":
         return mg.hex20_grid(**kw) if kw else mg.hex20_grid(64)
     raise ValueError(workload)
+
+
+def workload_config(workload: str, mesh, nnz: int, world: int, sized: bool = False) -> dict:
+    """The configuration both arms report (identical keys and values); `sized`:
+    a smaller instance of the generator (--size), named by its mesh."""
+    name, desc = WORKLOADS[workload]
+    return {"workload": mesh.name if sized else name, "description": desc, "elements": mesh.num_elems,
+            "nodes": mesh.num_nodes, "dofs": mesh.num_dofs, "nnz": int(nnz), "l2": L2_NOTE,
+            "parallelism": f"replicas{world}"}
 
 
 def algorithmic_bytes(mesh, nnz: int) -> dict:
@@ -87,12 +108,35 @@ def job_ms(local_ms: float, world: int, device) -> float:
     return float(t.item())
 
 
-def measured_peak():
+def measured_peaks() -> dict:
+    """Denominators of the rooflines: MEASURED_PEAKS.json when present, else the
+    profiling recipe's fallback figures."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d.get("bf16_tflops", 1590.0)),
+                "kind": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "kind": "fallback"}
+
+
+def host_info() -> dict:
+    model = platform.processor() or ""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count()}
+
+
+def library_identity(path: str) -> dict:
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        for chunk in iter(lambda: f.read(1 << 20), b""):
+            h.update(chunk)
+    return {"path": os.path.relpath(path, ROOT), "sha256": h.hexdigest()}
 
 
 class ClockSampler:
@@ -142,60 +186,122 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# CPU legs (oracle / reference code)
+# The serial FP64 oracle (CPU baseline and accuracy reference)
 # ---------------------------------------------------------------------------
 
-def _cpu_sample_worker(args):
-    workload, use_reference = args
-    name, kw = CPU_SAMPLES[workload]
-    mesh = make_mesh(name, **kw)
+def oracle_full(mesh) -> dict:
+    """The serial FP64 host assembly of the whole mesh by the oracle (pattern,
+    then values), each phase timed; one core."""
     import oracle as O
     t0 = time.perf_counter()
-    if use_reference and O.ref_available("t3"):
-        rp, ci = O.ref_pattern(mesh)
-        if mesh.kind == 0:
-            vals = O.ref_q4a_host_assemble(mesh, rp, ci)  # noqa: F841 (reference material)
-        else:
-            O.assemble(mesh, rp, ci)
-        kind = "reference" if mesh.kind == 0 else "reference pattern + ported value scatter"
-    else:
-        O.assemble(mesh)
-        kind = "port"
-    dt = time.perf_counter() - t0
-    return mesh.num_elems, dt, kind, mesh.name
+    rp, ci = O.pattern(mesh)
+    t1 = time.perf_counter()
+    _, _, v = O.assemble(mesh, rp, ci)
+    t2 = time.perf_counter()
+    return {"row_ptr": rp, "col_idx": ci, "values": v, "pattern_s": t1 - t0, "values_s": t2 - t1}
 
 
-def cpu_baseline(workload: str, use_reference: bool, workers: int) -> dict:
-    """Serial assembly on a bounded sample; `workers` independent copies in parallel."""
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    t0 = time.perf_counter()
-    if workers <= 1:
-        res = [_cpu_sample_worker((workload, use_reference))]
-    else:
-        with ctx.Pool(workers) as pool:
-            res = pool.map(_cpu_sample_worker, [(workload, use_reference)] * workers)
-    wall = time.perf_counter() - t0
-    elems = sum(r[0] for r in res)
-    per = [r[0] / r[1] for r in res]
-    kind = res[0][2]
-    return {"value": float(sum(per)), "unit": "elements/s", "cores": workers,
-            "kind": "reference" if kind == "reference" else "port",
-            "sample": f"{len(res)} x {res[0][3]} ({res[0][0]} elements each), {kind}; serial pattern build + FP64 "
-                      f"values per copy, copies in parallel processes; wall {wall:.1f}s",
-            "elements": elems}
+def cpu_baseline_line(mesh, orc: dict) -> dict:
+    total = orc["pattern_s"] + orc["values_s"]
+    return {"value": mesh.num_elems / total, "unit": "elements/s", "cores": 1, "kind": "port",
+            "sample": f"the full configuration ({mesh.num_elems} elements): the oracle's serial restatement of "
+                      f"the reference's host pattern build and assembleGlobalStiffnessHost, one thread; pattern "
+                      f"{orc['pattern_s']:.2f} s, values {orc['values_s']:.2f} s",
+            "pattern_s": orc["pattern_s"], "values_s": orc["values_s"], **host_info()}
+
+
+def _diag_positions(rp: np.ndarray, ci: np.ndarray) -> np.ndarray:
+    """Position of the diagonal entry of every row (vectorised binary search)."""
+    n = rp.shape[0] - 1
+    dofs = np.arange(n, dtype=np.int64)
+    lo, hi = rp[:-1].astype(np.int64), rp[1:].astype(np.int64) - 1
+    for _ in range(40):
+        act = lo <= hi
+        if not act.any():
+            break
+        mid = (lo + hi) // 2
+        less = ci[np.clip(mid, 0, max(ci.shape[0] - 1, 0))] < dofs
+        lo = np.where(act & less, mid + 1, lo)
+        hi = np.where(act & ~less, mid - 1, hi)
+    return lo
+
+
+def accuracy(rp: np.ndarray, ci: np.ndarray, ref: np.ndarray, test: np.ndarray, chunk: int = 1 << 26) -> dict:
+    """Error of every CSR value `test` against the FP64 oracle `ref` (same
+    pattern), as the reference's analyzePrecision states it
+    (ALLS_Quad2D_Assembly_Accuracy_Analysis.cu:896-960: max / mean absolute and
+    relative error over the nonzero reference entries, Frobenius-relative error,
+    count of |diff| > 1e-10), plus the error on the row/column scale
+    max(|K_ij|, sqrt(|K_ii K_jj|)) and the per-entry relative error of the
+    entries that do not cancel between elements (|K_ij| >= 1e-8 sqrt(|K_ii K_jj|))."""
+    dpos = _diag_positions(rp, ci)
+    diag = np.abs(ref[np.clip(dpos, 0, max(ref.shape[0] - 1, 0))]) if ref.shape[0] else np.zeros(0)
+    nnz = ref.shape[0]
+    out = {"max_abs": 0.0, "max_rel": 0.0, "sum_abs": 0.0, "sum_rel": 0.0, "fro_d": 0.0, "fro_ref": 0.0,
+           "count_gt_1e-10": 0, "max_scaled": 0.0, "max_rel_significant": 0.0, "significant": 0}
+    for s in range(0, nnz, chunk):
+        e = min(nnz, s + chunk)
+        idx = np.arange(s, e, dtype=np.int64)
+        rows = np.searchsorted(rp, idx, side="right") - 1
+        r, t = ref[s:e], test[s:e]
+        d = np.abs(t - r)
+        nz = r != 0
+        rel = d[nz] / np.abs(r[nz])
+        out["max_abs"] = max(out["max_abs"], float(d[nz].max()) if nz.any() else 0.0)
+        out["max_rel"] = max(out["max_rel"], float(rel.max()) if rel.size else 0.0)
+        out["sum_abs"] += float(d[nz].sum())
+        out["sum_rel"] += float(rel.sum())
+        out["fro_d"] += float(np.sum((t[nz] - r[nz]) ** 2))
+        out["fro_ref"] += float(np.sum(r * r))
+        out["count_gt_1e-10"] += int(np.count_nonzero(d > 1e-10))
+        sc = np.sqrt(diag[rows] * diag[ci[s:e]])
+        out["max_scaled"] = max(out["max_scaled"], float(np.max(d / np.maximum(np.abs(r), np.where(sc > 0, sc, 1.0)))))
+        sig = np.abs(r) >= 1e-8 * sc
+        if sig.any():
+            out["max_rel_significant"] = max(out["max_rel_significant"], float(np.max(d[sig] / np.abs(r[sig]))))
+        out["significant"] += int(np.count_nonzero(sig))
+    return {"max_rel": out["max_rel"], "mean_rel": out["sum_rel"] / max(nnz, 1), "max_abs": out["max_abs"],
+            "mean_abs": out["sum_abs"] / max(nnz, 1),
+            "frobenius_rel": (out["fro_d"] ** 0.5) / (out["fro_ref"] ** 0.5) if out["fro_ref"] > 0 else 0.0,
+            "count_gt_1e-10": out["count_gt_1e-10"], "max_scaled": out["max_scaled"],
+            "max_rel_significant": out["max_rel_significant"], "significant_entries": out["significant"],
+            "entries": int(nnz),
+            "what": "every CSR value against the serial FP64 oracle: analyzePrecision's statistics (max_rel over "
+                    "nonzero entries, mean_rel, frobenius_rel, count_gt_1e-10), max_scaled = max |d| / "
+                    "max(|K_ij|, sqrt(|K_ii K_jj|)), max_rel_significant = max |d| / |K_ij| over entries with "
+                    "|K_ij| >= 1e-8 sqrt(|K_ii K_jj|)"}
 
 
 # ---------------------------------------------------------------------------
-# GPU leg
+# GPU legs
 # ---------------------------------------------------------------------------
 
-def run_batched(args, rank: int, world: int, local_rank: int):
+def timed_steps(torch, stream, flush, fn, steps: int, warmup: int = 0):
+    """Mean device milliseconds of fn over `steps` calls (CUDA events on the
+    launching stream, L2 flushed before each, outside the events)."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(steps):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    return statistics.mean(ts)
+
+
+def run_batched(args, rank: int, world: int, local_rank: int, compact: bool = False):
     """The batched configuration: 256 meshes assembled by fem_assemble_batched
     (one call per step, graph-captured), concurrency picked by the library's
     autotuner (fem_autotune_batched: 1/2/4/8/16 slots timed on this batch);
     concurrency 1 is the sequential baseline (the same per-mesh launches one
-    after another on one stream). value = elements/s of the whole batch."""
+    after another on one stream). value = elements/s of the whole batch.
+    compact: return the fields as a dict (the default line's batched field)."""
     import torch
     import fem_alls as fem
     import meshgen as mg
@@ -260,18 +366,12 @@ def run_batched(args, rank: int, world: int, local_rank: int):
         raise RuntimeError(f"batched assembly: status bits {st[bad[0]]} on mesh {bad[0]}")
     lat = b.latencies_ms()
     ms = job_ms(sum(ts), world, dev) / args.steps
+    del g
     if rank != 0:
-        return
+        return None
     seq = per_k[1]
-    line = {
-        "metric": "elements/s (device FP64 A-LLS assembly: element stiffness, list scatter, CSR pattern + values)",
-        "value": world * elems / (ms / 1e3), "unit": "elements/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded mesh generator)",
-        "config": {"workload": name, "description": desc, "meshes": len(meshes), "elements": elems,
-                   "nnz": int(sum(nnz)), "kinds": {k: sum(1 for m in meshes if m.kind == k) for k in range(4)},
-                   "l2": "2x L2 buffer zeroed between steps, outside the per-step events",
-                   "parallelism": f"replicas{world}", "mesh_generation_s": gen_s},
+    fields = {
+        "value": world * elems / (ms / 1e3), "unit": "elements/s", "ms_per_step": ms,
         "meshes_per_s": world * len(meshes) / (ms / 1e3),
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "what": "per-mesh completion after the batch start (GPU global timer), graph replay"},
@@ -282,67 +382,45 @@ def run_batched(args, rank: int, world: int, local_rank: int):
                        "p50_ms": seq["p50_ms"], "p99_ms": seq["p99_ms"],
                        "what": "the 256 meshes' launches one after another on one stream (concurrency 1)"},
         "speedup_vs_sequential": seq["ms"] / ms,
-        "clocks": clk.summary(),
-        "gpu_launches": args.steps * batch_launches(meshes),
+        "meshes": len(meshes), "elements": elems, "nnz": int(sum(nnz)),
+        "kinds": {k: sum(1 for m in meshes if m.kind == k) for k in range(4)}, "mesh_generation_s": gen_s,
+        "clocks": clk.summary(), "gpu_launches": args.steps * batch_launches(meshes),
         "api": "fem_assemble_batched, captured in one CUDA graph",
     }
+    if compact:
+        return fields
+    line = {"metric": METRIC, "value": fields["value"], "unit": "elements/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded mesh generator)",
+            "config": {"workload": name, "description": desc, "meshes": len(meshes), "elements": elems,
+                       "nnz": int(sum(nnz)), "l2": L2_NOTE, "parallelism": f"replicas{world}"}}
+    line.update({k: v for k, v in fields.items() if k not in line})
     print(json.dumps(line), flush=True)
+    return None
 
 
-def run_ours(args, rank: int, world: int, local_rank: int):
-    import torch
-    import fem_alls as fem
-    import build
-    build.build()
-    if args.workload == "batched":
-        run_batched(args, rank, world, local_rank)
-        return
-    if args.ke_only:
-        torch.cuda.set_device(local_rank)
-        dev = torch.device("cuda", local_rank)
-        mesh = make_mesh("hex20", args.size)
-        flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device=dev)
-        line = {"workload": mesh.name, "elements": mesh.num_elems,
-                "ke_form": ke_form(fem, torch, mesh, fem.device_arrays(mesh, dev), args, flush,
-                                   torch.cuda.current_stream())}
-        if rank == 0:
-            print(json.dumps(line), flush=True)
-        return
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    name, desc = WORKLOADS[args.workload]
-    mesh = make_mesh(args.workload, args.size)
-    if args.size:
-        name = mesh.name
-    asm = fem.Assembler(mesh, device=dev)
+def assembly_leg(torch, fem, mesh, dev, stream, flush, steps: int, warmup: int, o=None, clocks: bool = False,
+                 world: int = 1, local_rank: int = 0):
+    """Timed full assemblies (scatter phase and consolidation split by events);
+    returns (assembler, info, dict of times)."""
+    asm = fem.Assembler(mesh, o, device=dev)
     _, _, _, info = asm.assemble()          # sizes the outputs
-    nnz = int(info.nnz)
-    flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device=dev)
-    stream = torch.cuda.current_stream()
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         asm.assemble_async()
     torch.cuda.synchronize()
     st, info = asm.read_info()
     fem.check(st, "warmup assembly")
-
-    # per-kernel breakdown (untimed pass)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-    ev[0].record(stream)
-    asm.scatter()
-    ev[1].record(stream)
-    asm.consolidate()
-    ev[2].record(stream)
-    torch.cuda.synchronize()
-    t_scatter, t_cons = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
-
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    mids = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    mids = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local_rank) as clk:
-        for i in range(args.steps):
+    clk = ClockSampler(local_rank) if clocks else None
+    if clk:
+        clk.__enter__()
+    try:
+        for i in range(steps):
             flush.zero_()                      # evict L2 between steps (outside the step events)
             starts[i].record(stream)
             asm.scatter()                      # = fem_assemble_async, split to time the scatter phase
@@ -350,215 +428,156 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             asm.consolidate()
             stops[i].record(stream)
         torch.cuda.synchronize()
+    finally:
+        if clk:
+            clk.__exit__()
     if world > 1:
         torch.distributed.barrier()
     times = [s.elapsed_time(e) for s, e in zip(starts, stops)]
-    scatter_ms = statistics.mean(s.elapsed_time(e) for s, e in zip(starts, mids))
-    consolidate_ms = statistics.mean(s.elapsed_time(e) for s, e in zip(mids, stops))
     st, info = asm.read_info()
     fem.check(st, "timed assembly")
-    ms = job_ms(sum(times), world, dev) / args.steps
-    clocks = clk.summary()
+    t = {"total_ms_sum": sum(times), "ms": statistics.mean(times),
+         "scatter_ms": statistics.mean(s.elapsed_time(e) for s, e in zip(starts, mids)),
+         "consolidate_ms": statistics.mean(s.elapsed_time(e) for s, e in zip(mids, stops)),
+         "clocks": clk.summary() if clk else None}
+    return asm, info, t
 
-    # end to end through the host-buffer entry point
-    e2e = None
-    if not args.no_e2e:
-        pinned = {k: torch.from_numpy(v).pin_memory() for k, v in fem.host_arrays(mesh).items()}
-        harr = {k: v.numpy() for k, v in pinned.items()}
-        rp = torch.empty(mesh.num_dofs + 1, dtype=torch.int32).pin_memory().numpy()
-        ci = torch.empty(nnz, dtype=torch.int32).pin_memory().numpy()
-        vv = torch.empty(nnz, dtype=torch.float64).pin_memory().numpy()
-        ctx = fem.HostContext()
-        s = stream.cuda_stream
-        for _ in range(max(1, args.warmup)):
-            fem.check(ctx.assemble(mesh, harr, rp, ci, vv, stream=s)[0], "fem_assemble_host")
-        torch.cuda.synchronize()
-        e_times = []
-        for _ in range(args.steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            fem.check(ctx.assemble(mesh, harr, rp, ci, vv, stream=s)[0], "fem_assemble_host")
-            b.record(stream)
-            b.synchronize()
-            e_times.append(a.elapsed_time(b))
-        ctx.close()
-        e_ms = job_ms(sum(e_times), world, dev) / args.steps
-        h2d = sum(v.nbytes for v in harr.values())
-        d2h = rp.nbytes + ci.nbytes + vv.nbytes
-        e2e = {"value": world * mesh.num_elems / (e_ms / 1e3), "unit": "elements/s", "ms_per_step": e_ms,
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "api": "fem_assemble_host (pinned host buffers, copies inside the call)"}
 
-    colour = None
-    if not args.no_colour:
-        colour = colour_baseline(fem, torch, asm, mesh, nnz, args, flush, stream)
-    reasm = None if args.no_reassembly else reassembly(fem, torch, asm, mesh, nnz, args, flush, stream)
-    upper = None if args.no_reassembly else upper_output(fem, torch, asm, mesh, nnz, args, flush, stream)
-    kef = ke_form(fem, torch, mesh, asm.dev, args, flush, stream) if mesh.kind == 2 and not args.no_ke else None
-    f32 = fp32_form(fem, torch, asm, mesh, nnz, args, flush, stream) if mesh.kind != 2 and not args.no_ke else None
-    tuned = None
-    if not args.no_autotune:
-        t0 = time.perf_counter()
-        best, best_ms = asm.autotune(repeats=3)
-        tuned = {"api": "fem_autotune (scatter grid CTAs/SM; Hex20 also first/overflow chunk slots)",
-                 "best": {"ctas_per_sm": best.ctas_per_sm, "first_slots": best.first_slots,
-                          "chunk_slots": best.chunk_slots, "pool_factor": best.pool_factor},
-                 "best_ms": best_ms, "default_ms": ms, "tuning_s": time.perf_counter() - t0,
-                 "note": "timed back to back without the L2 flush; the headline uses the default options"}
-
-    if rank != 0:
-        return
-    peak, peak_kind = measured_peak()
+def rooflines(mesh, nnz: int, t: dict, peak: dict, workload: str) -> dict:
     ab = algorithmic_bytes(mesh, nnz)
-    achieved = ab["total"] / (ms / 1e3) / 1e9
-    # The dominant kernel is the scatter: it reads the inputs and writes every
-    # list entry once (16 B per CSR nonzero); consolidation reads the entries
-    # back and writes the CSR.
+    hbm = peak["hbm_gbs"]
+    # scatter phase: reads the inputs, writes every list entry once (16 B per
+    # CSR nonzero); consolidation reads the entries back and writes the CSR
     scatter_bytes = ab["in"] + ab["list"] // 2
     consolidate_bytes = ab["list"] // 2 + ab["out"]
-    scatter_gbs = scatter_bytes / (scatter_ms / 1e3) / 1e9
-    consolidate_gbs = consolidate_bytes / (consolidate_ms / 1e3) / 1e9
-    traffic = read_profile_traffic(args.workload)
-    line = {
-        "metric": "elements/s (device FP64 A-LLS assembly: element stiffness, list scatter, CSR pattern + values)",
-        "value": world * mesh.num_elems / (ms / 1e3),
-        "unit": "elements/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded mesh generator)",
-        "config": {"workload": name, "description": desc, "elements": mesh.num_elems, "nodes": mesh.num_nodes,
-                   "dofs": mesh.num_dofs, "nnz": nnz, "contributions": mesh.contributions(),
-                   "l2": "2x L2 buffer zeroed between steps, outside the per-step events",
-                   "parallelism": f"replicas{world}"},
-        "nnz_per_s": world * nnz / (ms / 1e3),
-        "roofline": {"bound": "hbm", "achieved": scatter_gbs, "peak": peak, "unit": "GB/s",
-                     "frac": scatter_gbs / peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": SCATTER_KERNEL[args.workload] + " (scatter phase: list reset, element order, scatter)",
+    sg = scatter_bytes / (t["scatter_ms"] / 1e3) / 1e9
+    cg = consolidate_bytes / (t["consolidate_ms"] / 1e3) / 1e9
+    step = ab["total"] / (t["ms"] / 1e3) / 1e9
+    return {
+        "roofline": {"bound": "hbm", "achieved": sg, "peak": hbm, "unit": "GB/s", "frac": sg / hbm,
+                     "traffic": read_profile_traffic(workload), "peak_kind": peak["kind"],
+                     "kernel": SCATTER_KERNEL.get(workload, "") + " (scatter phase: list reset, element order, scatter)",
                      "algorithmic_bytes_per_launch": scatter_bytes,
                      "algorithmic_bytes_per_element": scatter_bytes / max(mesh.num_elems, 1),
-                     "ms_per_launch": scatter_ms},
-        "consolidate_roofline": {"bound": "hbm", "achieved": consolidate_gbs, "peak": peak, "unit": "GB/s",
-                                 "frac": consolidate_gbs / peak, "kernel": "k_write (consolidation phase: count, "
-                                 "scan, sorted write)", "algorithmic_bytes_per_launch": consolidate_bytes,
-                                 "ms_per_launch": consolidate_ms},
-        "step_roofline": {"achieved": achieved, "frac": achieved / peak, "algorithmic_bytes": ab,
-                          "frac_nominal_8tbs": achieved / 8000.0,
-                          "compulsory_frac": (ab["in"] + ab["out"]) / (ms / 1e3) / 1e9 / peak},
-        "kernels_ms": {"scatter": scatter_ms, "consolidate": consolidate_ms,
-                       "scatter_untimed_pass": t_scatter, "consolidate_untimed_pass": t_cons},
-        "list": {"entries": int(info.list_entries), "unique": nnz // mesh.dpn ** 2,
-                 "max_row_entries": int(info.max_row_entries), "overflow_chunks": int(info.overflow_chunks)},
-        "clocks": clocks,
-        "gpu_launches": KERNELS_PER_STEP[args.workload] * args.steps,
+                     "ms_per_launch": t["scatter_ms"]},
+        "consolidate_roofline": {"bound": "hbm", "achieved": cg, "peak": hbm, "unit": "GB/s", "frac": cg / hbm,
+                                 "kernel": "k_write (consolidation phase: count, scan, sorted write)",
+                                 "algorithmic_bytes_per_launch": consolidate_bytes, "ms_per_launch": t["consolidate_ms"]},
+        "step_roofline": {"achieved": step, "frac": step / hbm, "algorithmic_bytes": ab,
+                          "frac_nominal_8tbs": step / 8000.0,
+                          "compulsory_frac": (ab["in"] + ab["out"]) / (t["ms"] / 1e3) / 1e9 / hbm},
     }
-    if e2e:
-        line["e2e"] = e2e
-    if colour:
-        line["colour_baseline"] = colour
-    if reasm:
-        line["reassembly"] = reasm
-    if upper:
-        line["upper_output"] = upper
-    if kef:
-        line["ke_form"] = kef
-    if f32:
-        line["fp32_form"] = f32
-    if tuned:
-        line["autotune"] = tuned
-    if not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(args.workload, use_reference=False, workers=1)
-    print(json.dumps(line), flush=True)
 
 
-def ke_form(fem, torch, mesh, dev_arrays, args, flush, stream) -> dict:
+def e2e_leg(torch, fem, mesh, nnz, stream, flush, steps: int, warmup: int, world: int, dev):
+    pinned = {k: torch.from_numpy(v).pin_memory() for k, v in fem.host_arrays(mesh).items()}
+    harr = {k: v.numpy() for k, v in pinned.items()}
+    rp = torch.empty(mesh.num_dofs + 1, dtype=torch.int32).pin_memory().numpy()
+    ci = torch.empty(nnz, dtype=torch.int32).pin_memory().numpy()
+    vv = torch.empty(nnz, dtype=torch.float64).pin_memory().numpy()
+    ctx = fem.HostContext()
+    s = stream.cuda_stream
+    for _ in range(max(1, warmup)):
+        fem.check(ctx.assemble(mesh, harr, rp, ci, vv, stream=s)[0], "fem_assemble_host")
+    torch.cuda.synchronize()
+    e_times = []
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fem.check(ctx.assemble(mesh, harr, rp, ci, vv, stream=s)[0], "fem_assemble_host")
+        b.record(stream)
+        b.synchronize()
+        e_times.append(a.elapsed_time(b))
+    ctx.close()
+    e_ms = job_ms(sum(e_times), world, dev) / steps
+    h2d = sum(v.nbytes for v in harr.values())
+    d2h = rp.nbytes + ci.nbytes + vv.nbytes
+    return {"value": world * mesh.num_elems / (e_ms / 1e3), "unit": "elements/s", "ms_per_step": e_ms,
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "api": "fem_assemble_host (pinned host buffers, copies inside the call)"}
+
+
+def ke_form(fem, torch, mesh, dev_arrays, args, flush, stream, peak: dict) -> dict:
     """The Hex20 element stiffness on its own (fem_element_stiffness) in its
     three forms (FP64 tensor cores, FP16-split tensor cores, plain FP64 on the
-    CUDA cores), timed alike;
-    the tensor-core values are compared with the FP64 ones per element, on the
-    scale of the element's largest diagonal entry."""
+    CUDA cores), timed alike; the tensor-core values are compared with the FP64
+    ones per element, on the scale of the element's largest diagonal entry."""
     out = {}
     kes = {}
     for prec, name in ((0, "fp64"), (1, "tc_f16x3"), (2, "fp64_simt")):
         o = fem.opts(precision=prec)
         ke, st = fem.element_stiffness(mesh, o, dev_arrays=dev_arrays)
         fem.check(0 if st == 0 else 1, f"element stiffness {name}")
-        for _ in range(args.warmup):
-            fem.element_stiffness(mesh, o, dev_arrays=dev_arrays, out=ke)
-        ts = []
-        for _ in range(args.steps):
-            flush.zero_()
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            fem.element_stiffness(mesh, o, dev_arrays=dev_arrays, out=ke)
-            b.record(stream)
-            torch.cuda.synchronize()
-            ts.append(a.elapsed_time(b))
-        out[name + "_ms"] = statistics.mean(ts)
+        out[name + "_ms"] = timed_steps(torch, stream, flush,
+                                        lambda: fem.element_stiffness(mesh, o, dev_arrays=dev_arrays, out=ke),
+                                        args.steps, args.warmup)
         kes[name] = ke
     # diagonal entries of the packed upper blocks: block (I, I) entries 0, 4, 8
     diag_idx = [9 * (i * 20 - i * (i - 1) // 2) + v for i in range(20) for v in (0, 4, 8)]
     d = kes["fp64"][:, diag_idx].abs().max(dim=1).values
     err = ((kes["tc_f16x3"] - kes["fp64"]).abs().max(dim=1).values / d).max()
-    flops = 2 * 60 * 60 * 27 * mesh.num_elems  # the node-pair contraction
+    flops = 2 * 60 * 60 * 27 * mesh.num_elems  # the node-pair contraction (dense, one pass)
+    # three FP16 products per split contraction, 64 x 64 x 32 padded tiles of the tensor pipe
+    tc_flops = 3 * 2 * 64 * 64 * 32 * mesh.num_elems
     out.update({"speedup_tc_vs_fp64": out["fp64_ms"] / out["tc_f16x3_ms"],
                 "speedup_tc_vs_fp64_simt": out["fp64_simt_ms"] / out["tc_f16x3_ms"],
                 "forms": "fp64: contraction on the FP64 tensor cores (the library's default); tc_f16x3: FP16 split "
-                         "operands on the FP16 tensor cores; fp64_simt: plain FP64 dot products on the CUDA cores",
+                         "operands on the FP16 tensor cores (tcgen05); fp64_simt: plain FP64 dot products on the "
+                         "CUDA cores",
                 "max_err_tc_vs_fp64": float(err),
                 "err_scale": "per element, max |difference| / the element's largest diagonal entry",
-                "contraction_gflop": flops / 1e9, "bytes_written": int(kes["fp64"].numel() * 8),
+                "contraction_gflop": flops / 1e9,
+                "tensor_pipe": {"issued_tflop_per_s": tc_flops / (out["tc_f16x3_ms"] / 1e3) / 1e12,
+                                "peak_tflops": peak["bf16_tflops"], "peak_kind": peak["kind"],
+                                "utilisation": tc_flops / (out["tc_f16x3_ms"] / 1e3) / 1e12 / peak["bf16_tflops"],
+                                "what": "3 split products x 2 x 64 x 64 x 32 (padded) flops per element / Ke time / "
+                                        "dense 16-bit tensor peak"},
+                "bytes_written": int(kes["fp64"].numel() * 8),
+                "write_floor_ms": kes["fp64"].numel() * 8 / (peak["hbm_gbs"] * 1e6),
                 "what": "fem_element_stiffness: packed symmetric Ke (210 3x3 blocks, 15.1 KB) of every element"})
     return out
 
 
-def row_col_scale(torch, rp, ci, v, n):
-    """max(|K_ij|, sqrt(|K_ii K_jj|)) of every entry of a CSR matrix."""
-    rows = torch.repeat_interleave(torch.arange(n, device=rp.device), (rp[1:] - rp[:-1]).long())
-    diag = torch.zeros(n, dtype=torch.float64, device=rp.device)
-    on = rows == ci.long()
-    diag[rows[on]] = v[on].abs()
-    scale = torch.maximum(v.abs(), torch.sqrt(diag[rows] * diag[ci.long()]))
-    return torch.where(scale > 0, scale, torch.ones_like(scale))
-
-
-def fp32_form(fem, torch, asm, mesh, nnz, args, flush, stream) -> dict:
+def fp32_form(fem, torch, asm, mesh, nnz, args, flush, stream, ref_values) -> dict:
     """The whole A-LLS assembly with the FP32 Ke blocks of the 2-D kinds
     (FEM_PREC_FP32), timed like the FP64 step; its values are compared with
-    the FP64 assembly's on the row/column scale."""
-    v64 = asm.values[:nnz].clone()
+    the FP64 oracle."""
     o64 = asm.opts
     asm.opts = fem.opts(precision=fem.FEM_PREC_FP32)
     try:
-        for _ in range(args.warmup):
-            asm.assemble_async()
-        ts = []
-        for _ in range(args.steps):
-            flush.zero_()
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            asm.scatter()
-            asm.consolidate()
-            b.record(stream)
-            torch.cuda.synchronize()
-            ts.append(a.elapsed_time(b))
+        ms = timed_steps(torch, stream, flush, lambda: (asm.scatter(), asm.consolidate()), args.steps, args.warmup)
         st, _ = asm.read_info()
         fem.check(st, "FP32-form assembly")
-        scale = row_col_scale(torch, asm.row_ptr, asm.col_idx[:nnz], v64, mesh.num_dofs)
-        err = float(((asm.values[:nnz] - v64).abs() / scale).max()) if nnz else 0.0
+        rp = asm.row_ptr.cpu().numpy()
+        acc = accuracy(rp, asm.col_idx[:nnz].cpu().numpy(), ref_values, asm.values[:nnz].cpu().numpy())
     finally:
         asm.opts = o64
         asm.assemble()                         # leave the FP64 values in place
-    ms = statistics.mean(ts)
-    return {"value": mesh.num_elems / (ms / 1e3), "unit": "elements/s", "ms_per_step": ms,
-            "max_scaled_err_vs_fp64": err,
-            "err_scale": "max |difference| / max(|K_ij|, sqrt(|K_ii K_jj|)) over the CSR entries",
+    return {"value": mesh.num_elems / (ms / 1e3), "unit": "elements/s", "ms_per_step": ms, "accuracy": acc,
             "what": "fem_alls_scatter + fem_alls_consolidate with FEM_PREC_FP32 (Ke blocks in FP32 from "
                     "coordinates relative to the element's first node, FP64 accumulation)"}
+
+
+def tc_assembly(fem, torch, mesh, dev, args, flush, stream, fp64_ms, ref_values) -> dict:
+    """The whole Hex20 A-LLS assembly with the tensor-core Ke form
+    (FEM_PREC_TC_F16X3), timed like the FP64 step, every value compared with
+    the FP64 oracle."""
+    o = fem.opts(precision=fem.FEM_PREC_TC_F16X3)
+    asm, info, t = assembly_leg(torch, fem, mesh, dev, stream, flush, args.steps, args.warmup, o)
+    nnz = int(info.nnz)
+    acc = accuracy(asm.row_ptr.cpu().numpy(), asm.col_idx[:nnz].cpu().numpy(), ref_values,
+                   asm.values[:nnz].cpu().numpy()) if ref_values is not None else None
+    del asm
+    torch.cuda.empty_cache()
+    return {"value": mesh.num_elems / (t["ms"] / 1e3), "unit": "elements/s", "ms_per_step": t["ms"],
+            "scatter_ms": t["scatter_ms"], "consolidate_ms": t["consolidate_ms"],
+            "speedup_vs_fp64_assembly": fp64_ms / t["ms"], "accuracy": acc,
+            "what": "fem_alls_scatter + fem_alls_consolidate with FEM_PREC_TC_F16X3 (the Ke contraction on the "
+                    "FP16 tensor cores from split operands, FP32 accumulation; Jacobians and the global "
+                    "accumulation in FP64)"}
 
 
 def upper_output(fem, torch, asm, mesh, nnz, args, flush, stream) -> dict:
@@ -567,24 +586,14 @@ def upper_output(fem, torch, asm, mesh, nnz, args, flush, stream) -> dict:
     asm.scatter()
     rp, ci, v = asm.consolidate_upper()
     cap = int(ci.numel())
-    ts = []
-    for i in range(args.warmup + args.steps):
-        flush.zero_()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        fem.check(asm.lib.fem_alls_consolidate_upper(fem.C.byref(asm.cm), fem.C.byref(asm.opts), asm.ws_ptr,
-                                                     asm.ws_bytes, fem._ptr(rp), fem._ptr(ci), fem._ptr(v), cap,
-                                                     stream.cuda_stream), "fem_alls_consolidate_upper")
-        b.record(stream)
-        torch.cuda.synchronize()
-        if i >= args.warmup:
-            ts.append(a.elapsed_time(b))
+    ms = timed_steps(torch, stream, flush, lambda: fem.check(asm.lib.fem_alls_consolidate_upper(
+        fem.C.byref(asm.cm), fem.C.byref(asm.opts), asm.ws_ptr, asm.ws_bytes, fem._ptr(rp), fem._ptr(ci),
+        fem._ptr(v), cap, stream.cuda_stream), "fem_alls_consolidate_upper"), args.steps, args.warmup)
     st, info = asm.read_info()
     fem.check(st, "upper-triangle consolidation")
     unz = int(info.nnz)
+    del rp, ci, v
     asm.assemble()                             # leave the full form in place
-    ms = statistics.mean(ts)
     return {"ms": ms, "nnz_upper": unz, "nnz_full": nnz, "bytes_out": 4 * (mesh.num_dofs + 1) + 12 * unz,
             "what": "fem_alls_consolidate_upper: count of columns >= row per node, scan, upper part of each "
                     "sorted row (symmetric storage)"}
@@ -604,24 +613,17 @@ def reassembly(fem, torch, asm, mesh, nnz, args, flush, stream) -> dict:
     torch.cuda.synchronize()
     build_ms = a.elapsed_time(b)
     vals = torch.empty(nnz, dtype=torch.float64, device=asm.row_ptr.device)
-    for _ in range(args.warmup):
-        re.reassemble(vals)
-    ts = []
-    for _ in range(args.steps):
-        flush.zero_()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        re.reassemble(vals)
-        b.record(stream)
-        torch.cuda.synchronize()
-        ts.append(a.elapsed_time(b))
+    ms = timed_steps(torch, stream, flush, lambda: re.reassemble(vals), args.steps, args.warmup)
     fem.check(re.read_info(), "re-assembly")
-    ms = statistics.mean(ts)
     v_alls = asm.values[:nnz]
-    diff = float(((vals - v_alls).abs() / v_alls.abs().clamp_min(1e-300)).max()) if nnz else 0.0
+    diff = 0.0
+    for s in range(0, nnz, 1 << 26):
+        e = min(nnz, s + (1 << 26))
+        diff = max(diff, float(((vals[s:e] - v_alls[s:e]).abs() / v_alls[s:e].abs().clamp_min(1e-300)).max()))
+    del vals, re
+    torch.cuda.empty_cache()
     return {"value": mesh.num_elems / (ms / 1e3), "unit": "elements/s", "ms_per_step": ms, "map_build_ms": build_ms,
-            "map_bytes": re.map_bytes, "max_rel_diff_vs_alls_nonzero": diff,
+            "max_rel_diff_vs_alls_nonzero": diff,
             "what": "fem_reassemble_values: values zeroed, element blocks added at scatter-map positions (FP64 "
                     "atomics); no lists, no pattern build"}
 
@@ -637,54 +639,157 @@ def colour_baseline(fem, torch, asm, mesh, nnz, args, flush, stream) -> dict:
     prep_ms = (time.perf_counter() - t0) * 1e3
     rp, ci = asm.row_ptr, asm.col_idx
     vals = torch.empty(nnz, dtype=torch.float64, device=rp.device)
-    for _ in range(args.warmup):
-        col.assemble(rp, ci, vals, nnz)
-    ts = []
-    for _ in range(args.steps):
-        flush.zero_()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        col.assemble(rp, ci, vals, nnz)
-        b.record(stream)
-        torch.cuda.synchronize()
-        ts.append(a.elapsed_time(b))
+    ms = timed_steps(torch, stream, flush, lambda: col.assemble(rp, ci, vals, nnz), args.steps, args.warmup)
     st, _ = col.read_info()
     fem.check(st, "colour assembly")
-    ms = statistics.mean(ts)
-    # agreement with the A-LLS values of the same pattern, on the row/column scale
+    # agreement with the A-LLS values of the same pattern, relative to the largest entry
     v_alls = asm.values[:nnz]
-    scale = row_col_scale(torch, rp, ci[:nnz], v_alls, mesh.num_dofs)
-    diff = float(((vals - v_alls).abs() / scale).max())
+    vmax = float(v_alls.abs().max())
+    diff = 0.0
+    for s in range(0, nnz, 1 << 26):
+        e = min(nnz, s + (1 << 26))
+        diff = max(diff, float((vals[s:e] - v_alls[s:e]).abs().max()) / vmax)
+    del vals, col
+    torch.cuda.empty_cache()
     return {"num_colours": nc, "prepare_ms": prep_ms, "assemble_ms": ms,
             "value": mesh.num_elems / (ms / 1e3), "unit": "elements/s (values into the A-LLS pattern; colouring "
             "and pattern excluded, as the reference times its coloured kernel)",
-            "max_scaled_diff_vs_alls": diff,
+            "max_diff_vs_alls_of_max_entry": diff,
             "kernels": ("k_scatter_hex20 (colour form)" if mesh.kind == 2 else "k_colour_assemble_2d") +
                        ", one launch per colour and element type"}
 
 
-# k_info_init; element order (2-D: key count, k_bucket_scan, key scatter; Hex20 also
-# k_bbox_init, k_bbox); scatter kernel(s) (mixed: Q4 and T3); k_consolidate_reset,
-# k_scan_reduce, k_scan_tiles, k_row_ptr, k_write
-KERNELS_PER_STEP = {"q4": 10, "t3": 10, "mixed": 11, "hex20": 12}
+def autotune_leg(asm, ms) -> dict:
+    t0 = time.perf_counter()
+    best, best_ms = asm.autotune(repeats=3)
+    return {"api": "fem_autotune (scatter grid CTAs/SM; Hex20 also first/overflow chunk slots)",
+            "best": {"ctas_per_sm": best.ctas_per_sm, "first_slots": best.first_slots,
+                     "chunk_slots": best.chunk_slots, "pool_factor": best.pool_factor},
+            "best_ms": best_ms, "default_ms": ms, "tuning_s": time.perf_counter() - t0,
+            "note": "timed back to back without the L2 flush; the headline uses the default options"}
+
+
+def secondary_workload(torch, fem, workload: str, dev, stream, flush, args, peak) -> dict:
+    """A compact record of another configuration (same step, same timing)."""
+    mesh = make_mesh(workload)
+    asm, info, t = assembly_leg(torch, fem, mesh, dev, stream, flush, args.steps, args.warmup)
+    nnz = int(info.nnz)
+    r = rooflines(mesh, nnz, t, peak, workload)
+    del asm
+    torch.cuda.empty_cache()
+    return {"workload": WORKLOADS[workload][0], "value": mesh.num_elems / (t["ms"] / 1e3), "unit": "elements/s",
+            "ms_per_step": t["ms"], "nnz": nnz, "nnz_per_s": nnz / (t["ms"] / 1e3),
+            "scatter_ms": t["scatter_ms"], "consolidate_ms": t["consolidate_ms"],
+            "roofline_frac": r["roofline"]["frac"], "consolidate_frac": r["consolidate_roofline"]["frac"],
+            "step_frac": r["step_roofline"]["frac"]}
+
+
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import torch
+    import fem_alls as fem
+    import build
+    if os.environ.get("FEM_ALLS_LIB"):
+        raise SystemExit("bench.py times the library built from this tree only: unset FEM_ALLS_LIB")
+    lib_path = build.build()
+    if args.workload == "batched":
+        run_batched(args, rank, world, local_rank)
+        return
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    peak = measured_peaks()
+    if args.ke_only:
+        mesh = make_mesh("hex20", args.size)
+        flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device=dev)
+        line = {"workload": mesh.name, "elements": mesh.num_elems,
+                "ke_form": ke_form(fem, torch, mesh, fem.device_arrays(mesh, dev), args, flush,
+                                   torch.cuda.current_stream(), peak)}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
+    mesh = make_mesh(args.workload, args.size)
+    flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    asm, info, t = assembly_leg(torch, fem, mesh, dev, stream, flush, args.steps, args.warmup, clocks=True,
+                                world=world, local_rank=local_rank)
+    nnz = int(info.nnz)
+    ms = job_ms(t["total_ms_sum"], world, dev) / args.steps
+    t["ms"] = ms
+    extras = world == 1 and not args.headline_only
+    e2e = None if args.no_e2e else e2e_leg(torch, fem, mesh, nnz, stream, flush, args.steps, args.warmup, world, dev)
+    line_extra = {}
+    orc = None
+    if extras:
+        if not args.no_colour:
+            line_extra["colour_baseline"] = colour_baseline(fem, torch, asm, mesh, nnz, args, flush, stream)
+        if not args.no_reassembly:
+            line_extra["reassembly"] = reassembly(fem, torch, asm, mesh, nnz, args, flush, stream)
+            line_extra["upper_output"] = upper_output(fem, torch, asm, mesh, nnz, args, flush, stream)
+        if not args.no_cpu:
+            orc = oracle_full(mesh)            # the CPU baseline and the accuracy reference at once
+            rp_h = asm.row_ptr.cpu().numpy()
+            ci_h = asm.col_idx[:nnz].cpu().numpy()
+            if not (np.array_equal(rp_h, orc["row_ptr"]) and np.array_equal(ci_h, orc["col_idx"])):
+                raise RuntimeError("CSR pattern differs from the oracle's")
+            del ci_h
+            line_extra["accuracy"] = accuracy(orc["row_ptr"], orc["col_idx"], orc["values"],
+                                              asm.values[:nnz].cpu().numpy())
+            line_extra["accuracy"]["pattern"] = "bit-exact (row_ptr and col_idx equal to the oracle's)"
+        if mesh.kind == 2 and not args.no_ke:
+            line_extra["ke_form"] = ke_form(fem, torch, mesh, asm.dev, args, flush, stream, peak)
+            line_extra["tc_assembly"] = tc_assembly(fem, torch, mesh, dev, args, flush, stream, ms,
+                                                    orc["values"] if orc else None)
+        if mesh.kind != 2 and not args.no_ke and orc:
+            line_extra["fp32_form"] = fp32_form(fem, torch, asm, mesh, nnz, args, flush, stream, orc["values"])
+        if not args.no_autotune:
+            line_extra["autotune"] = autotune_leg(asm, ms)
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": world * mesh.num_elems / (ms / 1e3), "unit": "elements/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded mesh generator)",
+        "config": workload_config(args.workload, mesh, nnz, world, bool(args.size)),
+        "nnz_per_s": world * nnz / (ms / 1e3),
+    }
+    line.update(rooflines(mesh, nnz, t, peak, args.workload))
+    line["kernels_ms"] = {"scatter": t["scatter_ms"], "consolidate": t["consolidate_ms"]}
+    line["list"] = {"entries": int(info.list_entries), "unique": nnz // mesh.dpn ** 2,
+                    "max_row_entries": int(info.max_row_entries), "overflow_chunks": int(info.overflow_chunks)}
+    line["clocks"] = t["clocks"]
+    line["gpu_launches"] = kernels_per_step(args.workload, mesh) * args.steps
+    line["library"] = library_identity(lib_path)
+    if e2e:
+        line["e2e"] = e2e
+    line.update(line_extra)
+    if orc:
+        line["cpu_baseline"] = cpu_baseline_line(mesh, orc)
+    del asm
+    torch.cuda.empty_cache()
+    if extras and args.workload == DEFAULT_WORKLOAD and not args.no_secondary and not args.size:
+        line["t3_1000x1000"] = secondary_workload(torch, fem, "t3", dev, stream, flush, args, peak)
+        line["batched_256"] = run_batched(args, rank, world, local_rank, compact=True)
+    print(json.dumps(line), flush=True)
+
+
+def kernels_per_step(workload: str, mesh) -> int:
+    """Library kernels launched by one assembly step."""
+    if workload == "hex20":
+        waves = (mesh.num_elems + 4095) // 4096
+        # k_info_init, k_bbox_init, k_bbox, Morton count / scan / scatter, two per wave,
+        # k_consolidate_reset, k_scan_reduce, k_scan_tiles, k_row_ptr, k_write
+        return 6 + 2 * waves + 5
+    return {"q4": 10, "t3": 10, "mixed": 11}[workload]
 
 
 def batch_launches(meshes) -> int:
     """Library kernels of one fem_assemble_batched call: each mesh's assembly
-    (as KERNELS_PER_STEP) and its completion kernel (k_finish), plus the start
-    stamp (k_stamp)."""
-    per_kind = {0: KERNELS_PER_STEP["q4"], 1: KERNELS_PER_STEP["t3"], 2: KERNELS_PER_STEP["hex20"],
-                3: KERNELS_PER_STEP["mixed"]}
-    return 1 + sum(per_kind[m.kind] + 1 for m in meshes)
-
-
-SCATTER_KERNEL = {"q4": "k_scatter_2d<4>", "t3": "k_scatter_2d<3>", "mixed": "k_scatter_2d<4> + k_scatter_2d<3>",
-                  "hex20": "k_scatter_hex20"}
+    and its completion kernel (k_finish), plus the start stamp (k_stamp)."""
+    return 1 + sum(kernels_per_step({0: "q4", 1: "t3", 2: "hex20", 3: "mixed"}[m.kind], m) + 1 for m in meshes)
 
 
 def read_profile_traffic(workload: str):
-    """DRAM bytes (read + write) of one scatter-kernel launch on this workload,
+    """DRAM bytes (read + write) of one scatter-phase launch on this workload,
     from the committed ncu summary, if there is one."""
     p = os.path.join(ROOT, "profiles", f"traffic_{workload}.json")
     if os.path.exists(p):
@@ -695,24 +800,119 @@ def read_profile_traffic(workload: str):
     return None
 
 
+# ---------------------------------------------------------------------------
+# The reference arm
+# ---------------------------------------------------------------------------
+
+def reference_gpu(workload: str, mesh, rp, ci, ref_values) -> dict:
+    """The reference's own GPU kernels on the same mesh, on this GPU, through
+    the harness built from its sources (oracle/_ref), timed as its driver times
+    them; their values compared with the FP64 oracle on the row/column scale."""
+    import ctypes as C
+    import oracle as O
+    vp = C.c_void_p
+    if workload == "hex20":
+        L = O.ref_lib("h20")
+        f = L.ref_h20_gpu_compare
+        f.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, C.c_double, C.c_double, vp, vp, vp, C.c_int64]
+        f.restype = C.c_int
+        out = np.zeros(8)
+        nnz = ci.shape[0]
+        va = np.zeros(nnz, np.float32)
+        vc = np.zeros(nnz, np.float32)
+        conn = np.ascontiguousarray(mesh.conn, np.int32)
+        xs = [np.ascontiguousarray(a) for a in (mesh.x, mesh.y, mesh.z)]
+        rc = f(mesh.num_nodes, mesh.num_elems, conn.ctypes.data, xs[0].ctypes.data, xs[1].ctypes.data,
+               xs[2].ctypes.data, float(mesh.E0), float(mesh.nu0), out.ctypes.data, va.ctypes.data, vc.ctypes.data,
+               nnz)
+        if rc:
+            return {"unavailable": f"reference harness CUDA error {rc}"}
+        acc_a = accuracy(rp, ci, ref_values, va.astype(np.float64))
+        acc_c = accuracy(rp, ci, ref_values, vc.astype(np.float64))
+        return {"alls_ms": out[0], "coloured_ms": out[1], "host_pattern_ms": out[2], "host_colouring_ms": out[3],
+                "colours": int(out[4]), "nnz": int(out[5]), "alls_row_array_bytes": int(out[7]),
+                "alls_value": mesh.num_elems / (out[0] / 1e3), "coloured_value": mesh.num_elems / (out[1] / 1e3),
+                "alls_total_ms_with_host_pattern": out[0] + out[2],
+                "coloured_total_ms_with_host_pattern_and_colouring": out[1] + out[2] + out[3],
+                "alls_max_scaled_err_vs_fp64": acc_a["max_scaled"],
+                "coloured_max_scaled_err_vs_fp64": acc_c["max_scaled"],
+                "what": "assembleGlobalStiffnessKernelALLSFixedArray + convertALLStoCSRKernelFixedArray and "
+                        "assembleGlobalStiffnessKernelColoredNoAtomic (ALLS_Hex20_3D_Assembly_Performance.cu:"
+                        "208-321), timed by the reference's compareAssemblyMethods (3 warm-up, 10 measured, CUDA "
+                        "events, values only: the CSR pattern is built on the host beforehand and timed apart); "
+                        "FP32 values, as the reference computes them"}
+    if workload == "t3":
+        L = O.ref_lib("t3")
+        f = L.ref_t3_gpu_alls_time
+        f.argtypes = [C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, C.c_double, C.c_double, C.c_double, vp, vp,
+                      C.c_int64, C.c_int, C.c_int, vp, C.POINTER(C.c_float)]
+        f.restype = C.c_int
+        vals = np.zeros(ci.shape[0])
+        ms = C.c_float(0.0)
+        conn = np.ascontiguousarray(mesh.conn, np.int32)
+        x, y = np.ascontiguousarray(mesh.x), np.ascontiguousarray(mesh.y)
+        # the reference's material is global: uniform-material copy of the mesh
+        rc = f(mesh.num_nodes, mesh.num_elems, 3, conn.ctypes.data, None, x.ctypes.data, y.ctypes.data, 1.0, 0.3,
+               1.0, rp.ctypes.data, ci.ctypes.data, ci.shape[0], 3, 10, vals.ctypes.data, C.byref(ms))
+        if rc:
+            return {"unavailable": f"reference harness CUDA error {rc}"}
+        return {"alls_ms": ms.value, "alls_value": mesh.num_elems / (ms.value / 1e3),
+                "what": "assembleGlobalStiffnessKernelALLS + convertALLStoCSRKernel "
+                        "(ALLS_T3_Unstructed_Elements_Assemble_Performance.cu:227-315), timed as its driver times "
+                        "them (T3:586-640), values only, uniform material E=1, nu=0.3"}
+    return {"unavailable": f"no reference GPU timing harness for {workload}"}
+
+
 def run_reference(args, rank: int, world: int):
     if rank != 0:
         return
-    import multiprocessing as mp
-    workers = max(1, min(mp.cpu_count(), 16))
-    name, desc = WORKLOADS[args.workload]
-    vals = []
-    for _ in range(max(1, args.steps)):
-        cb = cpu_baseline(args.workload, use_reference=True, workers=workers)
-        vals.append(cb["value"])
-    v = statistics.median(vals)
-    cb["value"] = v
-    line = {"impl": "reference", "metric": "elements/s (device FP64 A-LLS assembly: element stiffness, list scatter, "
-            "CSR pattern + values)", "value": v, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded mesh generator)", "config": {"workload": name, "description": desc},
-            "cpu_baseline": cb, "e2e": {"value": v, "unit": "elements/s", "h2d_bytes_per_step": 0,
-                                        "d2h_bytes_per_step": 0}}
+    import oracle as O
+    workload = args.workload
+    if workload == "batched":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference assembles one mesh per program run; "
+                          "it has no batched path"}), flush=True)
+        return
+    mesh = make_mesh(workload, args.size)
+    use_ref = O.ref_available("h20" if workload == "hex20" else "t3")
+    t0 = time.perf_counter()
+    if use_ref:
+        rp, ci = O.ref_pattern(mesh)           # the reference's own host pattern builder
+        kind = "reference"
+    else:
+        rp, ci = O.pattern(mesh)
+        kind = "port"
+    t1 = time.perf_counter()
+    if mesh.kind == 0 and use_ref:
+        vals = O.ref_q4a_host_assemble(mesh, rp, ci)
+    else:
+        _, _, vals = O.assemble(mesh, rp, ci)   # the serial value scatter of assembleGlobalStiffnessHost
+    t2 = time.perf_counter()
+    total = t2 - t0
+    v = mesh.num_elems / total
+    nnz = int(ci.shape[0])
+    cb = {"value": v, "unit": "elements/s", "cores": 1, "kind": kind,
+          "sample": f"the full configuration ({mesh.num_elems} elements), one pass: the reference's host pattern "
+                    f"builder ({'compiled from its source' if use_ref else 'oracle port'}, {t1 - t0:.2f} s) and the "
+                    f"serial FP64 value scatter of assembleGlobalStiffnessHost ({t2 - t1:.2f} s); the reference's "
+                    f"host path is single-threaded",
+          "pattern_s": t1 - t0, "values_s": t2 - t1, **host_info()}
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "elements/s", "n_gpus": world,
+            "steps": 1, "warmup": 0, "requested_steps": args.steps, "ms_per_step": total * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded mesh generator)",
+            "config": workload_config(workload, mesh, nnz, world, bool(args.size)),
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_reference_gpu:
+        try:
+            import torch
+            gpu = torch.cuda.is_available()
+        except Exception:
+            gpu = False
+        if gpu and use_ref:
+            line["reference_gpu"] = reference_gpu(workload, mesh, rp, ci, vals)
+        else:
+            line["reference_gpu"] = {"unavailable": "no GPU or no reference harness build in this run"}
     print(json.dumps(line), flush=True)
 
 
@@ -721,16 +921,19 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="t3", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=0,
                     help="grid cells per side instead of the configuration's (profiling a smaller case)")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the oracle leg (CPU baseline and accuracy)")
     ap.add_argument("--no-colour", action="store_true", help="skip the element-colouring baseline leg")
-    ap.add_argument("--no-reassembly", action="store_true", help="skip the value-only re-assembly leg")
+    ap.add_argument("--no-reassembly", action="store_true", help="skip the value-only re-assembly and upper legs")
     ap.add_argument("--no-autotune", action="store_true", help="skip the autotuner leg")
-    ap.add_argument("--no-ke", action="store_true", help="skip the precision-form leg (Hex20: element-stiffness forms; 2-D: the FP32-form assembly)")
+    ap.add_argument("--no-ke", action="store_true", help="skip the precision-form legs")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the T3 and batched fields of the default line")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="reference arm: skip its GPU kernels")
+    ap.add_argument("--headline-only", action="store_true", help="only the timed assembly and e2e")
     ap.add_argument("--ke-only", action="store_true",
                     help="Hex20: time only the element-stiffness kernels (FP64 and tensor-core forms)")
     args = ap.parse_args()
