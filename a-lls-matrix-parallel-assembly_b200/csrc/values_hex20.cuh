@@ -1,0 +1,212 @@
+// Device code of the Hex20 FP64 value pass (values_hex20.cu), shared with the
+// batched persistent kernel (batched.cu). See values_hex20.cu for the method.
+#pragma once
+
+#include "hex20.cuh"
+
+namespace fem {
+namespace {
+
+constexpr int kValueWarps = 6;  // warps that hold M tiles (one tile position each)
+constexpr int KS = 28;  // Gauss points padded to 7 k-steps of 4; row stride of the tables (doubles)
+
+// The six 8x8 tile positions (ti <= tj) of the upper triangle of the 24 x 24 node grid.
+__device__ __forceinline__ int tile_ti(int w) { return w < 3 ? 0 : (w < 5 ? 1 : 2); }
+__device__ __forceinline__ int tile_tj(int w) { return w == 0 ? 0 : (w == 1 || w == 3 ? 1 : 2); }
+
+struct ValuesSmem {
+    double dN[3][20][KS];  // dN_n / dxi_i at Gauss point g: [i][n][g]
+    double G[3][24][KS];   // physical gradients: [a][n][g]; rows 20..23 and g = 27 stay zero
+    double X[20][3];
+    double J[27][9];       // Jacobians, then their inverses
+    double w[KS];          // gauss weight * detJ (w[27] = 0)
+    int nodes[20];
+    double lam, mu;
+    int bad;
+};
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+// Shape-function derivative table and the zero padding of G and w; every
+// thread of the CTA calls it once, before values_cta.
+__device__ __forceinline__ void values_init(ValuesSmem& sm) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int idx = tid; idx < 27 * 20; idx += nt) {
+        const int g = idx / 20, n = idx - 20 * g;
+        double dx, dy, dz;
+        hex20::dshape_node(n, hex20::gauss3(g / 9), hex20::gauss3((g / 3) % 3), hex20::gauss3(g % 3), dx, dy, dz);
+        sm.dN[0][n][g] = dx;
+        sm.dN[1][n][g] = dy;
+        sm.dN[2][n][g] = dz;
+    }
+    for (int idx = tid; idx < 3 * 24 * KS; idx += nt) (&sm.G[0][0][0])[idx] = 0.0;
+    for (int idx = tid; idx < 3 * 20; idx += nt) sm.dN[idx / 20][idx % 20][27] = 0.0;
+    if (tid < KS) sm.w[tid] = 0.0;
+    __syncthreads();
+}
+
+// The value pass of the elements at positions i = i_first, i_first +
+// i_stride, ... below i1 of the visit order perm (perm NULL: element i) by
+// one CTA of at least kValueWarps warps (warps beyond them help with the
+// per-element tables only); the slot ids of position i are map row
+// i - map_origin. Every thread of the CTA calls it.
+__device__ __forceinline__ void values_cta(const MeshView& m, const ListLayout& L, const int* __restrict__ perm,
+                                           long long i_first, long long i_stride, int i1, int map_origin,
+                                           const int* __restrict__ map, ValuesSmem& sm) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
+    const bool tile_warp = warp < kValueWarps;
+    const int ti = tile_ti(warp), tj = tile_tj(warp);
+    const int fr = lane >> 2, fc = lane & 3;
+    auto elem = [&](long long i) -> int { return perm ? __ldg(perm + i) : (int)i; };
+    // node id and coordinates of the next element
+    int pre_n = 0;
+    double pre_x = 0.0, pre_y = 0.0, pre_z = 0.0;
+    if (tid < 20 && i_first < i1) {
+        pre_n = __ldg(m.conn + (size_t)elem(i_first) * 20 + tid);
+        if (pre_n >= 0 && pre_n < m.N) {
+            pre_x = __ldg(m.x + pre_n);
+            pre_y = __ldg(m.y + pre_n);
+            pre_z = __ldg(m.z + pre_n);
+        }
+    }
+    __syncthreads();
+
+    for (long long i = i_first; i < i1; i += i_stride) {
+        const int e = elem(i);
+        if (tid == 0) sm.bad = 0;
+        __syncthreads();  // the previous element's G, w, lam/mu and flag are no longer read
+        if (tid < 20) {
+            sm.nodes[tid] = pre_n;
+            if (pre_n < 0 || pre_n >= m.N) {
+                sm.bad = 1;
+            } else {
+                sm.X[tid][0] = pre_x;
+                sm.X[tid][1] = pre_y;
+                sm.X[tid][2] = pre_z;
+            }
+        }
+        if (tid == 32) {
+            const double E = m.E ? __ldg(m.E + e) : m.E0;
+            const double nu = m.nu ? __ldg(m.nu + e) : m.nu0;
+            sm.lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+            sm.mu = E / (2.0 * (1.0 + nu));
+        }
+        __syncthreads();
+        const long long i_next = i + i_stride;
+        if (tid < 20 && i_next < i1) pre_n = __ldg(m.conn + (size_t)elem(i_next) * 20 + tid);
+        if (sm.bad) {  // reported by the claim pass; nothing to add
+            if (tid < 20 && i_next < i1 && pre_n >= 0 && pre_n < m.N) {
+                pre_x = __ldg(m.x + pre_n);
+                pre_y = __ldg(m.y + pre_n);
+                pre_z = __ldg(m.z + pre_n);
+            }
+            __syncthreads();  // uniform: every thread has read the flag before it is reset
+            continue;
+        }
+        // Jacobians J[g][3i + j] = sum_n dN[i][n][g] X[n][j]
+        for (int idx = tid; idx < 243; idx += nt) {
+            const int g = idx % 27, r = idx / 27, ii = r / 3, jj = r % 3;
+            double acc = 0.0;
+#pragma unroll
+            for (int n = 0; n < 20; n++) acc = fma(sm.dN[ii][n][g], sm.X[n][jj], acc);
+            sm.J[g][r] = acc;
+        }
+        __syncthreads();
+        if (tid < 27) {
+            double* J = sm.J[tid];
+            const double c0 = J[4] * J[8] - J[5] * J[7], c1 = J[5] * J[6] - J[3] * J[8], c2 = J[3] * J[7] - J[4] * J[6];
+            const double det = J[0] * c0 + J[1] * c1 + J[2] * c2;
+            if (!(det > 0.0)) raise_status(L.info, FEM_ERR_DETJ);
+            const double r = 1.0 / det;
+            double iJ[9];
+            iJ[0] = c0 * r;
+            iJ[1] = (J[2] * J[7] - J[1] * J[8]) * r;
+            iJ[2] = (J[1] * J[5] - J[2] * J[4]) * r;
+            iJ[3] = c1 * r;
+            iJ[4] = (J[0] * J[8] - J[2] * J[6]) * r;
+            iJ[5] = (J[2] * J[3] - J[0] * J[5]) * r;
+            iJ[6] = c2 * r;
+            iJ[7] = (J[1] * J[6] - J[0] * J[7]) * r;
+            iJ[8] = (J[0] * J[4] - J[1] * J[3]) * r;
+#pragma unroll
+            for (int k = 0; k < 9; k++) J[k] = iJ[k];
+            sm.w[tid] = hex20::weight3(tid / 9) * hex20::weight3((tid / 3) % 3) * hex20::weight3(tid % 3) * det;
+        }
+        __syncthreads();
+        // physical gradients G[a][n][g] = sum_i iJ[g][3a + i] dN[i][n][g]
+        for (int idx = tid; idx < 20 * 27; idx += nt) {
+            const int n = idx / 27, g = idx - 27 * n;
+            const double* iJ = sm.J[g];
+            const double d0 = sm.dN[0][n][g], d1 = sm.dN[1][n][g], d2 = sm.dN[2][n][g];
+#pragma unroll
+            for (int a = 0; a < 3; a++) sm.G[a][n][g] = fma(iJ[3 * a], d0, fma(iJ[3 * a + 1], d1, iJ[3 * a + 2] * d2));
+        }
+        __syncthreads();
+        // the coordinates of the next element arrive during the contraction
+        if (tid < 20 && i_next < i1 && pre_n >= 0 && pre_n < m.N) {
+            pre_x = __ldg(m.x + pre_n);
+            pre_y = __ldg(m.y + pre_n);
+            pre_z = __ldg(m.z + pre_n);
+        }
+        if (!tile_warp) continue;  // the remaining warps wait at the next element's first barrier
+        // M^{ab} tiles (ti, tj): A[r][k] = w_k G[a][8 ti + r][k], B[k][c] = G[b][8 tj + c][k]
+        double acc[3][3][2];
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < 7; ks++) {
+            const int k = 4 * ks + fc;
+            const double wk = sm.w[k];
+            double A[3], B[3];
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                A[a] = wk * sm.G[a][8 * ti + fr][k];
+                B[a] = sm.G[a][8 * tj + fr][k];
+            }
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+                for (int b = 0; b < 3; b++) dmma(acc[a][b][0], acc[a][b][1], A[a], B[b]);
+        }
+        // Ke blocks of this lane's node pairs, added to both triangles
+        const double lam = sm.lam, mu = sm.mu;
+        const int* mrow = map + (size_t)(i - map_origin) * 400;
+        const int I = 8 * ti + fr;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int Jn = 8 * tj + 2 * fc + h;
+            if (I >= 20 || Jn >= 20 || (ti == tj && Jn < I)) continue;
+            const int g_ij = __ldg(mrow + I * 20 + Jn);
+            const int g_ji = I != Jn ? __ldg(mrow + Jn * 20 + I) : -1;
+            const double mtr = mu * (acc[0][0][h] + acc[1][1][h] + acc[2][2][h]);
+            double k[3][3];
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+                for (int b = 0; b < 3; b++) k[a][b] = fma(lam, acc[a][b][h], fma(mu, acc[b][a][h], a == b ? mtr : 0.0));
+            if (g_ij >= 0) {
+                double* p = L.vals + (size_t)(unsigned)g_ij * 9;
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+#pragma unroll
+                    for (int b = 0; b < 3; b++) atomicAdd(p + 3 * a + b, k[a][b]);
+            }
+            if (g_ji >= 0) {
+                double* p = L.vals + (size_t)(unsigned)g_ji * 9;
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+#pragma unroll
+                    for (int b = 0; b < 3; b++) atomicAdd(p + 3 * b + a, k[a][b]);
+            }
+        }
+    }
+}
+
+}  // namespace
+}  // namespace fem
