@@ -113,10 +113,11 @@ __device__ __forceinline__ long long global_ns() {
 }
 
 // Wait for the completion of the mbarrier phase of this parity, for at most
-// limit_ns nanoseconds of the GPU's global timer; limit_ns <= 0: one poll.
+// limit_ns nanoseconds of the GPU's global timer; limit_ns < 0: no wait at
+// all (the wait counts as run out).
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, long long limit_ns) {
+    if (limit_ns < 0) return false;
     if (mbar_try_wait(bar, parity)) return true;
-    if (limit_ns <= 0) return false;
     const long long t0 = global_ns();
     while (!mbar_try_wait(bar, parity))
         if (global_ns() - t0 > limit_ns) return false;

@@ -69,12 +69,12 @@ cudaError_t launch_element_stiffness(const MeshView& m, int kind, int precision,
                                      long long wait_ns, cudaStream_t s);
 // Hex20 element stiffness with the contraction on the tcgen05 tensor cores
 // (FEM_PREC_TC_F16X3), two elements per CTA step.
-// wait_ns: bound on a CTA's wait for its products (<= 0: one poll), see fem_opts.wait_limit_us.
+// wait_ns: bound on a CTA's wait for its products (< 0: no wait), see fem_opts.wait_limit_us.
 cudaError_t launch_hex20_ke_tcgen05(const MeshView& m, double* ke_out, int* status, long long wait_ns,
                                     cudaStream_t s);
-// fem_opts.wait_limit_us in nanoseconds: 0 -> 200 ms, > 0 -> that bound, < 0 -> 0 (one poll).
+// fem_opts.wait_limit_us in nanoseconds: 0 -> 200 ms, > 0 -> that bound, < 0 -> -1 (no wait).
 inline long long wait_ns_of(int wait_limit_us) {
-    return wait_limit_us == 0 ? 200ll * 1000 * 1000 : (wait_limit_us > 0 ? 1000ll * wait_limit_us : 0);
+    return wait_limit_us == 0 ? 200ll * 1000 * 1000 : (wait_limit_us > 0 ? 1000ll * wait_limit_us : -1);
 }
 // Target of a value-only re-assembly: CSR positions of every element block.
 struct MapTarget {

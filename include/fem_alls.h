@@ -117,8 +117,8 @@ typedef struct fem_opts {
     double pool_factor;    /* overflow chunks per node in the pool; 0 = default */
     int32_t wait_limit_us; /* bound on a kernel's wait for its own tensor-core products
                               (FEM_PREC_TC_F16X3): 0 = the default, 200 ms; > 0 = that many
-                              microseconds; < 0 = give up at the first poll that finds them
-                              unfinished. A wait that runs out raises FEM_ERR_TIMEOUT; the
+                              microseconds; < 0 = no wait at all, the wait counts as run out
+                              (exercises the recovery). A wait that runs out raises FEM_ERR_TIMEOUT; the
                               kernel then waits for the products with the default bound,
                               releases its tensor memory and returns (FEM_ERR_INTERNAL too if
                               that second wait also runs out). */

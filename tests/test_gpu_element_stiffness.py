@@ -177,8 +177,8 @@ def test_tensor_core_inverted_element(fem, oracle_mod, cuda_device):
 
 def test_tensor_core_wait_timeout_is_reported(fem, oracle_mod, cuda_device):
     # The bounded wait of the tensor-core kernels for their own products: with
-    # fem_opts.wait_limit_us < 0 every CTA gives up at its first poll, which
-    # comes before six 128x128x16 products can finish. The kernel must raise
+    # fem_opts.wait_limit_us < 0 the first wait of every CTA counts as run out
+    # while its six 128x128x16 products are in flight. The kernel must raise
     # FEM_ERR_TIMEOUT, wait for the products in flight with the default bound
     # (no FEM_ERR_INTERNAL), release its tensor memory and return; the context
     # stays usable and the next call with the default bound is exact.
