@@ -204,7 +204,8 @@ __device__ __forceinline__ void claim_warp(const MeshView& m, const ListLayout& 
                 gid = (int)slot_gid(L, rn, slot[k]);
             }
             if (st[k] == kClaimed && gid >= 0) {
-                zero_block(L.vals + (size_t)(unsigned)gid * 9);
+                // values are kept for upper blocks only (row node <= column node)
+                if (rn <= ws.node[J]) zero_block(L.vals + (size_t)(unsigned)gid * 9);
                 atomicAdd(&ws.claims[I], 1);
             }
             out[p] = gid;

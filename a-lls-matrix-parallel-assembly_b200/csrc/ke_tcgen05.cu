@@ -33,6 +33,8 @@
 #include <algorithm>
 #include <cstdint>
 
+#include <cuda_fp16.h>
+
 #include "hex20.cuh"
 
 namespace fem {
@@ -68,6 +70,7 @@ struct KeTcSmem {
     unsigned negmask[2];    // Gauss points with w_g < 0
     unsigned tmem_base;
     int state[2];           // 0 element present, 1 bad node id, 2 no element (odd tail)
+    int nodes[2][20];       // node ids of the pair (the value pass orients each block by them)
 };
 // more than 44.6 KB: at most four CTAs (4 x 128 tensor-memory columns) per SM
 static_assert(sizeof(KeTcSmem) > 46 * 1024 && sizeof(KeTcSmem) < 56 * 1024, "four CTAs per SM");
@@ -140,29 +143,39 @@ __device__ __forceinline__ unsigned pack_half2(__half lo, __half hi) {
     return (unsigned)__half_as_ushort(lo) | ((unsigned)__half_as_ushort(hi) << 16);
 }
 
-// Value pass of the two-pass Hex20 list scatter (kSlots): the wave of elements
-// perm[i0, i1) and the slot map of their 400 node pairs (claim_hex20.cu).
-struct SlotTarget {
-    const int* perm;
-    const int* map;
-    double* vals;
-    int i0, i1;
-    long long wait_ns;  // bound on the wait for the products (both modes)
+// Outputs of the kernel.
+enum TcOut : int {
+    kTcPacked = 0,  // the packed Ke of every element to ke_out (fem_element_stiffness)
+    kTcSlots = 1,   // value pass of the two-pass Hex20 list scatter: each upper Ke block added
+                    // with FP64 atomics to its list slot (slot map of claim_hex20.cu)
+    kTcCsrMap = 2   // value-only re-assembly: Ke_IJ and its transpose added with FP64 atomics at
+                    // their CSR positions (scatter map, row e)
 };
 
-// kSlots = false: the packed Ke of every element to ke_out (fem_element_stiffness).
-// kSlots = true: each Ke block added with FP64 atomics to its list entry (row
-// I, column J) and, transposed, to (row J, column I), at the slot map's ids.
-template <bool kSlots>
+// Elements and targets of the kTcSlots / kTcCsrMap modes.
+struct SlotTarget {
+    const int* perm;     // visit order: positions [i0, i1) (kTcSlots), all elements (kTcCsrMap)
+    const int* map;      // slot map (row i - i0) or scatter map (row e)
+    double* vals;        // list values (kTcSlots)
+    const int* row_ptr;  // the CSR (kTcCsrMap)
+    double* csr;
+    int i0, i1;
+    long long wait_ns;   // bound on the wait for the products (every mode)
+};
+
+template <int kMode>
 __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double* __restrict__ ke_out,
                                                              int* __restrict__ status, int bulk_out, SlotTarget tgt) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     KeTcSmem& sm = *reinterpret_cast<KeTcSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    // elements: positions q of the wave (kSlots) or the mesh's elements q
+    constexpr bool kSlots = kMode == kTcSlots, kMap = kMode == kTcCsrMap;
+    // elements: positions q of the wave (kTcSlots), of perm (kTcCsrMap) or the mesh's elements q
     const long long count = kSlots ? (long long)(tgt.i1 - tgt.i0) : (long long)m.E_count;
     const long long npairs = (count + 1) / 2;
-    auto elem = [&](long long q) -> long long { return kSlots ? (long long)__ldg(tgt.perm + tgt.i0 + q) : q; };
+    auto elem = [&](long long q) -> long long {
+        return kSlots ? (long long)__ldg(tgt.perm + tgt.i0 + q) : (kMap ? (long long)__ldg(tgt.perm + q) : q);
+    };
     const uint32_t bar = smem_u32(&sm.mbar);
 
     if (tid == 0) {
@@ -228,6 +241,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
         // 1. the pair's nodes and materials
         if (tid < 40) {
             const int e = tid / 20, k = tid % 20;
+            sm.nodes[e][k] = pre_state == 0 ? pre_n : 0;
             sm.X[e][k][0] = pre_state == 0 ? pre_x : 0.0;
             sm.X[e][k][1] = pre_state == 0 ? pre_y : 0.0;
             sm.X[e][k][2] = pre_state == 0 ? pre_z : 0.0;
@@ -390,9 +404,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
             const double inv_s2 = ldexp(1.0, 2 * ex);
             const float lam = (float)sm.lam[e], mu = (float)sm.mu[e];
             double* out = sm.ke[e] + 9 * (I * 20 - I * (I - 1) / 2 - I) + 3 * a;  // + 9 J: block (I, J)
-            const long long q = 2 * p + e;  // the element's position in the wave (kSlots)
-            const int* mrow = tgt.map + (size_t)(kSlots && q < count ? q : 0) * 400;
-            const bool add = kSlots && real && q < count;
+            const long long q = 2 * p + e;  // the element's position in the wave / in perm
+            const long long eid = (kMap && q < count) ? elem(q) : 0;
+            const int* mrow = tgt.map + (size_t)(kSlots && q < count ? q : (kMap ? eid : 0)) * 400;
+            // elements with a bad node id have no map entries (-1): nothing is added
+            const bool add = (kSlots || kMap) && real && q < count;
 #pragma unroll
             for (int J = 0; J < 20; J++) {
                 const int c = 32 * (J / 10) + 3 * (J % 10);
@@ -415,21 +431,42 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
                 const float k1 = fmaf(lam, o1, fmaf(mu, T1, a == 1 ? mtr : 0.0f));
                 const float k2 = fmaf(lam, o2, fmaf(mu, T2, a == 2 ? mtr : 0.0f));
                 if (kSlots) {
+                    // the lists hold upper blocks only (row node <= column node):
+                    // row a of Ke_IJ goes to (row I, column J) as it is, or
+                    // transposed, as column a of (row J, column I)
                     if (add && J >= I) {
                         const double v0 = (double)k0 * inv_s2, v1 = (double)k1 * inv_s2, v2 = (double)k2 * inv_s2;
-                        const int g_ij = __ldg(mrow + I * 20 + J);
-                        if (g_ij >= 0) {
-                            double* d = tgt.vals + (size_t)(unsigned)g_ij * 9 + 3 * a;
+                        const bool upper = sm.nodes[e][I] <= sm.nodes[e][J];
+                        const int g = __ldg(mrow + (upper ? I * 20 + J : J * 20 + I));
+                        if (g >= 0) {
+                            double* d = tgt.vals + (size_t)(unsigned)g * 9 + (upper ? 3 * a : a);
+                            const int st = upper ? 1 : 3;
+                            atomicAdd(d, v0);
+                            atomicAdd(d + st, v1);
+                            atomicAdd(d + 2 * st, v2);
+                        }
+                    }
+                } else if (kMap) {
+                    // the CSR holds both triangles: row a of Ke_IJ at block (I, J),
+                    // and, transposed, column a of block (J, I)
+                    if (add && J >= I) {
+                        const double v0 = (double)k0 * inv_s2, v1 = (double)k1 * inv_s2, v2 = (double)k2 * inv_s2;
+                        const int rI = 3 * sm.nodes[e][I], rJ = 3 * sm.nodes[e][J];
+                        const int pij = __ldg(mrow + I * 20 + J);
+                        if (pij >= 0) {
+                            const int len = __ldg(tgt.row_ptr + rI + 1) - __ldg(tgt.row_ptr + rI);
+                            double* d = tgt.csr + pij + (size_t)a * len;
                             atomicAdd(d, v0);
                             atomicAdd(d + 1, v1);
                             atomicAdd(d + 2, v2);
                         }
-                        const int g_ji = J != I ? __ldg(mrow + J * 20 + I) : -1;
-                        if (g_ji >= 0) {
-                            double* d = tgt.vals + (size_t)(unsigned)g_ji * 9 + a;
+                        const int pji = J != I ? __ldg(mrow + J * 20 + I) : -1;
+                        if (pji >= 0) {
+                            const int len = __ldg(tgt.row_ptr + rJ + 1) - __ldg(tgt.row_ptr + rJ);
+                            double* d = tgt.csr + pji + a;
                             atomicAdd(d, v0);
-                            atomicAdd(d + 3, v1);
-                            atomicAdd(d + 6, v2);
+                            atomicAdd(d + len, v1);
+                            atomicAdd(d + 2 * (size_t)len, v2);
                         }
                     }
                 } else if (real && J >= I) {
@@ -447,7 +484,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
             sm.bound_bits[tid] = 0ull;
             sm.negmask[tid] = 0u;
         }
-        if (kSlots) continue;
+        if (kSlots || kMap) continue;
         const int nvalid = 2 * p + 1 < m.E_count ? 2 : 1;
         double* dst = ke_out + (size_t)(2 * p) * kPackedHex20;
         if (bulk_out) {
@@ -468,7 +505,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
     // caller to treat the device as suspect.
     if (timed_out && !mbar_wait_bounded(bar, parity ^ 1u, kDefaultWaitNs) && tid == 0)
         atomicOr(status, 1 << FEM_ERR_INTERNAL);
-    if (tid == 0 && bulk_out && !kSlots) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    if (tid == 0 && bulk_out && !kSlots && !kMap) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
@@ -477,7 +514,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
     }
 }
 
-template <bool kSlots>
+template <int kMode>
 cudaError_t launch_tc(const MeshView& m, double* ke_out, int* status, const SlotTarget& tgt, cudaStream_t s) {
     static DeviceCache cache;
     const size_t smem = sizeof(KeTcSmem);
@@ -488,9 +525,9 @@ cudaError_t launch_tc(const MeshView& m, double* ke_out, int* status, const Slot
         // runtime's occupancy query answers 1 for this kernel, which would
         // leave three quarters of the SM idle.
         cudaError_t e =
-            cudaFuncSetAttribute(k_hex20_ke_tc<kSlots>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaFuncSetAttribute(k_hex20_ke_tc<kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncAttributes fa;
-        if (!e) e = cudaFuncGetAttributes(&fa, k_hex20_ke_tc<kSlots>);
+        if (!e) e = cudaFuncGetAttributes(&fa, k_hex20_ke_tc<kMode>);
         int dev = 0, regs_sm = 0, smem_sm = 0;
         if (!e) e = cudaGetDevice(&dev);
         if (!e) e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
@@ -503,11 +540,11 @@ cudaError_t launch_tc(const MeshView& m, double* ke_out, int* status, const Slot
         return cudaSuccess;
     }, blocks_per_sm);
     if (err) return err;
-    const long long count = kSlots ? (long long)(tgt.i1 - tgt.i0) : (long long)m.E_count;
+    const long long count = kMode == kTcSlots ? (long long)(tgt.i1 - tgt.i0) : (long long)m.E_count;
     const long long npairs = (count + 1) / 2;
     const long long grid = std::max<long long>(1, std::min<long long>((long long)blocks_per_sm * sm_count(), npairs));
-    const int bulk_out = !kSlots && (reinterpret_cast<uintptr_t>(ke_out) & 15u) == 0;
-    k_hex20_ke_tc<kSlots><<<(int)grid, kThreads, smem, s>>>(m, ke_out, status, bulk_out, tgt);
+    const int bulk_out = kMode == kTcPacked && (reinterpret_cast<uintptr_t>(ke_out) & 15u) == 0;
+    k_hex20_ke_tc<kMode><<<(int)grid, kThreads, smem, s>>>(m, ke_out, status, bulk_out, tgt);
     return cudaGetLastError();
 }
 
@@ -517,13 +554,22 @@ cudaError_t launch_hex20_ke_tcgen05(const MeshView& m, double* ke_out, int* stat
                                     cudaStream_t s) {
     SlotTarget t{};
     t.wait_ns = wait_ns;
-    return launch_tc<false>(m, ke_out, status, t, s);
+    return launch_tc<kTcPacked>(m, ke_out, status, t, s);
 }
 
 cudaError_t launch_values_hex20_tc(const MeshView& m, const ListLayout& L, const int* perm, int i0, int i1,
                                    const int* map, long long wait_ns, cudaStream_t s) {
     if (i1 <= i0) return cudaSuccess;
-    return launch_tc<true>(m, nullptr, &L.info->status_bits, SlotTarget{perm, map, L.vals, i0, i1, wait_ns}, s);
+    return launch_tc<kTcSlots>(m, nullptr, &L.info->status_bits,
+                               SlotTarget{perm, map, L.vals, nullptr, nullptr, i0, i1, wait_ns}, s);
+}
+
+cudaError_t launch_reassemble_hex20_tc(const MeshView& m, const int* perm, const MapTarget& mt, DevInfo* info,
+                                       cudaStream_t s) {
+    return launch_tc<kTcCsrMap>(m, nullptr, &info->status_bits,
+                                SlotTarget{perm, mt.map, nullptr, mt.row_ptr, mt.values, 0, m.E_count,
+                                           wait_ns_of(0)},
+                                s);
 }
 
 }  // namespace fem

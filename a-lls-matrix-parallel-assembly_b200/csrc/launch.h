@@ -91,6 +91,9 @@ cudaError_t launch_build_map(const MeshView& m, int kind, const int* row_ptr, co
 // {q4 begin, q4 end, t3 begin, t3 end}; Hex20 over perm (status bits in info).
 cudaError_t launch_reassemble_2d(const MeshView& m, int precision, const int* map, int G, const int* perm,
                                  const int* ranges, const int* row_ptr, double* values, int* status, cudaStream_t s);
+// The tensor-core form of the Hex20 value-only re-assembly (ke_tcgen05.cu).
+cudaError_t launch_reassemble_hex20_tc(const MeshView& m, const int* perm, const MapTarget& t, DevInfo* info,
+                                       cudaStream_t s);
 cudaError_t launch_reassemble_hex20(const MeshView& m, int precision, const int* perm, const MapTarget& t,
                                     DevInfo* info, cudaStream_t s);
 // Colouring baseline for Hex20: elements perm[range[0], range[1]) (one colour),
@@ -115,9 +118,6 @@ cudaError_t launch_values_hex20_tc(const MeshView& m, const ListLayout& L, const
 // zero (about 17 KB per element) stay in L2 until its value pass adds to them.
 constexpr int kHex20Wave = 4096;
 
-// perm: element visit order (spatial, from launch_reorder_3d); precision FEM_PREC_*.
-cudaError_t launch_scatter_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm, int ctas_per_sm,
-                                 cudaStream_t s);
 // Spatial (3-D Morton bucket) element order; hist needs 1 << (3 * morton_bits(E)) ints, bbox 6 words.
 int morton_bits(int num_elems);
 cudaError_t launch_reorder_3d(const MeshView& m, int* hist, int* ranges, int* perm, unsigned long long* bbox, int sms,

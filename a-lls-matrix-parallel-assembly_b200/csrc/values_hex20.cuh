@@ -10,6 +10,24 @@ namespace {
 constexpr int kValueWarps = 6;  // warps that hold M tiles (one tile position each)
 constexpr int KS = 28;  // Gauss points padded to 7 k-steps of 4; row stride of the tables (doubles)
 
+// Where the value pass puts an element's Ke blocks.
+enum ValueOut : int {
+    kToSlots = 0,   // FP64 atomics into the list slots of the slot map (upper blocks only)
+    kToCsrMap = 1,  // FP64 atomics into a CSR at the positions of a scatter map (both triangles)
+    kToCsrColour = 2  // plain adds into a CSR at binary-searched positions (one colour: no two
+                      // elements share a node)
+};
+
+struct ValuesTarget {
+    const int* map;       // kToSlots: slot ids, row i - map_origin; kToCsrMap: CSR positions, row e
+    int map_origin;
+    double* vals;         // kToSlots: list values
+    const int* row_ptr;   // kToCsr*: the CSR
+    const int* col_idx;
+    double* csr;
+    DevInfo* info;        // status bits
+};
+
 // The six 8x8 tile positions (ti <= tj) of the upper triangle of the 24 x 24 node grid.
 __device__ __forceinline__ int tile_ti(int w) { return w < 3 ? 0 : (w < 5 ? 1 : 2); }
 __device__ __forceinline__ int tile_tj(int w) { return w == 0 ? 0 : (w == 1 || w == 3 ? 1 : 2); }
@@ -23,6 +41,9 @@ struct ValuesSmem {
     int nodes[20];
     double lam, mu;
     int bad;
+    // per tile warp: its node-pair blocks, compacted, before they are added
+    double stage[kValueWarps][64][9];
+    int stage_gid[kValueWarps][64];
 };
 
 __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
@@ -54,9 +75,9 @@ __device__ __forceinline__ void values_init(ValuesSmem& sm) {
 // one CTA of at least kValueWarps warps (warps beyond them help with the
 // per-element tables only); the slot ids of position i are map row
 // i - map_origin. Every thread of the CTA calls it.
-__device__ __forceinline__ void values_cta(const MeshView& m, const ListLayout& L, const int* __restrict__ perm,
-                                           long long i_first, long long i_stride, int i1, int map_origin,
-                                           const int* __restrict__ map, ValuesSmem& sm) {
+template <int kOut>
+__device__ __forceinline__ void values_cta(const MeshView& m, const int* __restrict__ perm, long long i_first,
+                                           long long i_stride, int i1, const ValuesTarget& t, ValuesSmem& sm) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
     const bool tile_warp = warp < kValueWarps;
     const int ti = tile_ti(warp), tj = tile_tj(warp);
@@ -98,7 +119,8 @@ __device__ __forceinline__ void values_cta(const MeshView& m, const ListLayout& 
         __syncthreads();
         const long long i_next = i + i_stride;
         if (tid < 20 && i_next < i1) pre_n = __ldg(m.conn + (size_t)elem(i_next) * 20 + tid);
-        if (sm.bad) {  // reported by the claim pass; nothing to add
+        if (sm.bad) {  // nothing to add
+            if (tid == 0 && kOut != kToSlots) raise_status(t.info, FEM_ERR_BAD_MESH);  // else the claim pass did
             if (tid < 20 && i_next < i1 && pre_n >= 0 && pre_n < m.N) {
                 pre_x = __ldg(m.x + pre_n);
                 pre_y = __ldg(m.y + pre_n);
@@ -120,7 +142,7 @@ __device__ __forceinline__ void values_cta(const MeshView& m, const ListLayout& 
             double* J = sm.J[tid];
             const double c0 = J[4] * J[8] - J[5] * J[7], c1 = J[5] * J[6] - J[3] * J[8], c2 = J[3] * J[7] - J[4] * J[6];
             const double det = J[0] * c0 + J[1] * c1 + J[2] * c2;
-            if (!(det > 0.0)) raise_status(L.info, FEM_ERR_DETJ);
+            if (!(det > 0.0)) raise_status(t.info, FEM_ERR_DETJ);
             const double r = 1.0 / det;
             double iJ[9];
             iJ[0] = c0 * r;
@@ -174,35 +196,92 @@ __device__ __forceinline__ void values_cta(const MeshView& m, const ListLayout& 
 #pragma unroll
                 for (int b = 0; b < 3; b++) dmma(acc[a][b][0], acc[a][b][1], A[a], B[b]);
         }
-        // Ke blocks of this lane's node pairs, added to both triangles
         const double lam = sm.lam, mu = sm.mu;
-        const int* mrow = map + (size_t)(i - map_origin) * 400;
         const int I = 8 * ti + fr;
+        const int nI = I < 20 ? sm.nodes[I] : 0;
+        if constexpr (kOut == kToSlots) {
+            // Ke block of each of this lane's node pairs {I, J}, staged for the
+            // list entry of the pair's lower node id: (row I, column J) as it
+            // is when node_I <= node_J, else transposed into (row J, column I).
+            // The lists hold the values of their upper blocks only (row node <=
+            // column node); the consolidation reads the lower blocks transposed.
+            const int* mrow = t.map + (size_t)(i - t.map_origin) * 400;
+            int base = 0;
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int Jn = 8 * tj + 2 * fc + h;
-            if (I >= 20 || Jn >= 20 || (ti == tj && Jn < I)) continue;
-            const int g_ij = __ldg(mrow + I * 20 + Jn);
-            const int g_ji = I != Jn ? __ldg(mrow + Jn * 20 + I) : -1;
-            const double mtr = mu * (acc[0][0][h] + acc[1][1][h] + acc[2][2][h]);
-            double k[3][3];
+            for (int h = 0; h < 2; h++) {
+                const int Jn = 8 * tj + 2 * fc + h;
+                const bool pair = I < 20 && Jn < 20 && (ti != tj || Jn >= I);
+                const bool lower_first = pair && nI <= sm.nodes[Jn < 20 ? Jn : 0];
+                const int g = pair ? __ldg(mrow + (lower_first ? I * 20 + Jn : Jn * 20 + I)) : -1;
+                const unsigned have = __ballot_sync(0xFFFFFFFFu, g >= 0);
+                if (g >= 0) {
+                    const int slot = base + __popc(have & ((1u << lane) - 1u));
+                    const double mtr = mu * (acc[0][0][h] + acc[1][1][h] + acc[2][2][h]);
 #pragma unroll
-            for (int a = 0; a < 3; a++)
+                    for (int a = 0; a < 3; a++)
 #pragma unroll
-                for (int b = 0; b < 3; b++) k[a][b] = fma(lam, acc[a][b][h], fma(mu, acc[b][a][h], a == b ? mtr : 0.0));
-            if (g_ij >= 0) {
-                double* p = L.vals + (size_t)(unsigned)g_ij * 9;
-#pragma unroll
-                for (int a = 0; a < 3; a++)
-#pragma unroll
-                    for (int b = 0; b < 3; b++) atomicAdd(p + 3 * a + b, k[a][b]);
+                        for (int b = 0; b < 3; b++) {
+                            const double k = fma(lam, acc[a][b][h], fma(mu, acc[b][a][h], a == b ? mtr : 0.0));
+                            sm.stage[warp][slot][lower_first ? 3 * a + b : 3 * b + a] = k;
+                        }
+                    sm.stage_gid[warp][slot] = g;
+                }
+                base += __popc(have);
             }
-            if (g_ji >= 0) {
-                double* p = L.vals + (size_t)(unsigned)g_ji * 9;
+            __syncwarp();
+            // nine consecutive lanes per block, three blocks per instruction: each
+            // block's 72 bytes are one atomic pass over its three sectors
+            if (lane < 27) {
+                const int q = lane / 9, v = lane - 9 * q;
+                for (int blk = q; blk < base; blk += 3)
+                    atomicAdd(t.vals + (size_t)(unsigned)sm.stage_gid[warp][blk] * 9 + v, sm.stage[warp][blk][v]);
+            }
+            __syncwarp();
+        } else {
+            // CSR targets hold both triangles: Ke_IJ at block (I, J) and its
+            // transpose at (J, I)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int Jn = 8 * tj + 2 * fc + h;
+                if (I >= 20 || Jn >= 20 || (ti == tj && Jn < I)) continue;
+                const double mtr = mu * (acc[0][0][h] + acc[1][1][h] + acc[2][2][h]);
+                double k[3][3];
 #pragma unroll
                 for (int a = 0; a < 3; a++)
 #pragma unroll
-                    for (int b = 0; b < 3; b++) atomicAdd(p + 3 * b + a, k[a][b]);
+                    for (int b = 0; b < 3; b++) k[a][b] = fma(lam, acc[a][b][h], fma(mu, acc[b][a][h], a == b ? mtr : 0.0));
+                for (int o = 0; o < (I == Jn ? 1 : 2); o++) {
+                    const int R = o ? Jn : I, Cn = o ? I : Jn;  // block (R, Cn) of the element
+                    const int r0 = 3 * sm.nodes[R], c0 = 3 * sm.nodes[Cn];
+                    const int lo = __ldg(t.row_ptr + r0), len = __ldg(t.row_ptr + r0 + 1) - lo;
+                    int p = -1;
+                    if constexpr (kOut == kToCsrMap) {
+                        p = __ldg(t.map + (size_t)e * 400 + R * 20 + Cn);
+                    } else {
+                        int a0 = lo, a1 = lo + len - 1;
+                        while (a0 <= a1) {
+                            const int mid = (a0 + a1) >> 1;
+                            const int c = __ldg(t.col_idx + mid);
+                            if (c == c0) {
+                                p = mid;
+                                break;
+                            }
+                            if (c < c0) a0 = mid + 1;
+                            else a1 = mid - 1;
+                        }
+                        if (p < 0) raise_status(t.info, FEM_ERR_INTERNAL);  // the pattern lacks the block
+                    }
+                    if (p < 0) continue;
+#pragma unroll
+                    for (int a = 0; a < 3; a++)
+#pragma unroll
+                        for (int b = 0; b < 3; b++) {
+                            const double v = o ? k[b][a] : k[a][b];
+                            double* d = t.csr + p + (size_t)a * len + b;
+                            if constexpr (kOut == kToCsrMap) atomicAdd(d, v);
+                            else *d += v;
+                        }
+                }
             }
         }
     }

@@ -655,7 +655,7 @@ def colour_baseline(fem, torch, asm, mesh, nnz, args, flush, stream) -> dict:
             "value": mesh.num_elems / (ms / 1e3), "unit": "elements/s (values into the A-LLS pattern; colouring "
             "and pattern excluded, as the reference times its coloured kernel)",
             "max_diff_vs_alls_of_max_entry": diff,
-            "kernels": ("k_scatter_hex20 (colour form)" if mesh.kind == 2 else "k_colour_assemble_2d") +
+            "kernels": ("k_values_hex20<kToCsrColour>" if mesh.kind == 2 else "k_colour_assemble_2d") +
                        ", one launch per colour and element type"}
 
 
