@@ -82,9 +82,9 @@ __device__ __forceinline__ void claim_warp(const MeshView& m, const ListLayout& 
     int (*view)[kClaimMaxWords] = ws.view;
     for (long long ii = i_first; ii < i1; ii += i_stride) {
         const int i = (int)ii;
-        const int e = perm ? __ldg(perm + i) : i;
+        const int e = perm ? FEM_LDG(perm + i) : i;
         int n = 0;
-        if (lane < 20) n = __ldg(m.conn + (size_t)e * 20 + lane);
+        if (lane < 20) n = FEM_LDG(m.conn + (size_t)e * 20 + lane);
         const bool bad = __any_sync(0xFFFFFFFFu, lane < 20 && (n < 0 || n >= m.N));
         int* out = map + (size_t)(i - map_origin) * kPairs;
         if (bad) {

@@ -60,7 +60,7 @@ __device__ __forceinline__ void scan_reduce_tile(const int* __restrict__ counts,
 #pragma unroll
     for (int i = 0; i < kScanItems; i++) {
         const long long n = base + (long long)i * kScanThreads + threadIdx.x;
-        if (n < N) sum += __ldg(counts + n);
+        if (n < N) sum += FEM_LDG(counts + n);
     }
     long long total;
     block_exclusive_scan(sum, s_warp, total);
@@ -75,7 +75,7 @@ __device__ __forceinline__ void scan_tiles_body(long long* __restrict__ tile_sum
     long long carry = 0;
     for (int base = 0; base < num_tiles; base += kScanThreads) {
         const int t = base + threadIdx.x;
-        const long long v = t < num_tiles ? tile_sums[t] : 0;
+        const long long v = t < num_tiles ? __ldcg(tile_sums + t) : 0;
         long long total;
         const long long ex = block_exclusive_scan(v, s_warp, total);
         if (t < num_tiles) tile_sums[t] = carry + ex;
@@ -103,11 +103,11 @@ __device__ __forceinline__ void row_ptr_tile(const int* __restrict__ counts, int
 #pragma unroll
     for (int i = 0; i < kScanItems; i++) {
         const long long n = base + i;
-        c[i] = n < N ? __ldg(counts + n) : 0;
+        c[i] = n < N ? FEM_LDG(counts + n) : 0;
         sum += c[i];
     }
     long long total;
-    long long off = tile_offsets[tile] + (long long)B * block_exclusive_scan(sum, s_warp, total);
+    long long off = __ldcg(tile_offsets + tile) + (long long)B * block_exclusive_scan(sum, s_warp, total);
 #pragma unroll
     for (int i = 0; i < kScanItems; i++) {
         const long long n = base + i;
@@ -155,9 +155,9 @@ __global__ void __launch_bounds__(kBlockThreads) k_count_upper(ListLayout L, int
             for (int step = 0; step < kMaxChainSteps; step++) {
                 const int* meta = chunk_meta(L, c);
                 const int cap = chunk_cap(L, c);
-                const int next = __ldg(meta + 1);
+                const int next = FEM_LDG(meta + 1);
                 for (int s = glane; s < cap; s += G) {
-                    const int col = (__ldg(meta + 2 + s) & kColMask) - 1;
+                    const int col = (FEM_LDG(meta + 2 + s) & kColMask) - 1;
                     cnt += col >= n;
                 }
                 if (next == 0) break;
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_reduce_upper(const int* _
 #pragma unroll
     for (int i = 0; i < kScanItems; i++) {
         const long long n = base + (long long)i * kScanThreads + threadIdx.x;
-        if (n < N) sum += upper_node_entries<DPN>(__ldg(ucounts + n));
+        if (n < N) sum += upper_node_entries<DPN>(FEM_LDG(ucounts + n));
     }
     long long total;
     block_exclusive_scan(sum, s_warp, total);
@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(kScanThreads) k_row_ptr_upper(const int* __res
 #pragma unroll
     for (int i = 0; i < kScanItems; i++) {
         const long long n = base + i;
-        c[i] = n < N ? __ldg(ucounts + n) : 0;
+        c[i] = n < N ? FEM_LDG(ucounts + n) : 0;
         sum += upper_node_entries<DPN>(c[i]);
     }
     long long total;
@@ -266,9 +266,9 @@ __device__ int long_row_next_col(const ListLayout& L, int n, int after, int glan
     for (int step = 0; step < kMaxChainSteps; step++) {
         const int* meta = chunk_meta(L, c);
         const int cap = chunk_cap(L, c);
-        const int next = __ldg(meta + 1);
+        const int next = FEM_LDG(meta + 1);
         for (int s = glane; s < cap; s += G) {
-            const int col = (__ldg(meta + 2 + s) & kColMask) - 1;
+            const int col = (FEM_LDG(meta + 2 + s) & kColMask) - 1;
             if (col > after && col < best) best = col;
         }
         if (next == 0) break;
@@ -294,12 +294,12 @@ __device__ void long_row_write(const ListLayout& L, int n, int u, long long base
         for (int step = 0; step < kMaxChainSteps; step++) {
             const int* meta = chunk_meta(L, c);
             const int cap = chunk_cap(L, c);
-            const int next = __ldg(meta + 1);
+            const int next = FEM_LDG(meta + 1);
             for (int s = glane; s < cap; s += G) {
-                if ((__ldg(meta + 2 + s) & kColMask) - 1 == col) {
+                if ((FEM_LDG(meta + 2 + s) & kColMask) - 1 == col) {
                     const double* p = L.vals + (size_t)slot_gid(L, c, s) * B;
 #pragma unroll
-                    for (int v = 0; v < B; v++) sum[v] += __ldg(p + v);
+                    for (int v = 0; v < B; v++) sum[v] += FEM_LDG(p + v);
                 }
             }
             if (next == 0) break;
@@ -316,7 +316,7 @@ __device__ void long_row_write(const ListLayout& L, int n, int u, long long base
                 if (g == kNoSlot && glane == 0) raise_status(L.info, FEM_ERR_INTERNAL);
 #pragma unroll
                 for (int v = 0; v < B; v++)
-                    sum[v] = g == kNoSlot ? 0.0 : __ldg(L.vals + (size_t)g * B + (v % DPN) * DPN + v / DPN);
+                    sum[v] = g == kNoSlot ? 0.0 : FEM_LDG(L.vals + (size_t)g * B + (v % DPN) * DPN + v / DPN);
             }
         }
         if (glane == 0) {
@@ -348,12 +348,12 @@ __device__ void long_row_write_bsr(const ListLayout& L, int n, int u, long long 
         for (int step = 0; step < kMaxChainSteps; step++) {
             const int* meta = chunk_meta(L, c);
             const int cap = chunk_cap(L, c);
-            const int next = __ldg(meta + 1);
+            const int next = FEM_LDG(meta + 1);
             for (int s = glane; s < cap; s += G) {
-                if ((__ldg(meta + 2 + s) & kColMask) - 1 == col) {
+                if ((FEM_LDG(meta + 2 + s) & kColMask) - 1 == col) {
                     const double* p = L.vals + (size_t)slot_gid(L, c, s) * B;
 #pragma unroll
-                    for (int v = 0; v < B; v++) sum[v] += __ldg(p + v);
+                    for (int v = 0; v < B; v++) sum[v] += FEM_LDG(p + v);
                 }
             }
             if (next == 0) break;
@@ -370,7 +370,7 @@ __device__ void long_row_write_bsr(const ListLayout& L, int n, int u, long long 
                 if (g == kNoSlot && glane == 0) raise_status(L.info, FEM_ERR_INTERNAL);
 #pragma unroll
                 for (int v = 0; v < B; v++)
-                    sum[v] = g == kNoSlot ? 0.0 : __ldg(L.vals + (size_t)g * B + (v % DPN) * DPN + v / DPN);
+                    sum[v] = g == kNoSlot ? 0.0 : FEM_LDG(L.vals + (size_t)g * B + (v % DPN) * DPN + v / DPN);
             }
         }
         if (glane == 0) {
@@ -398,12 +398,12 @@ __device__ void long_row_write_upper(const ListLayout& L, int n, int u, const in
         for (int step = 0; step < kMaxChainSteps; step++) {
             const int* meta = chunk_meta(L, c);
             const int cap = chunk_cap(L, c);
-            const int next = __ldg(meta + 1);
+            const int next = FEM_LDG(meta + 1);
             for (int s = glane; s < cap; s += G) {
-                if ((__ldg(meta + 2 + s) & kColMask) - 1 == col) {
+                if ((FEM_LDG(meta + 2 + s) & kColMask) - 1 == col) {
                     const double* p = L.vals + (size_t)slot_gid(L, c, s) * B;
 #pragma unroll
-                    for (int v = 0; v < B; v++) sum[v] += __ldg(p + v);
+                    for (int v = 0; v < B; v++) sum[v] += FEM_LDG(p + v);
                 }
             }
             if (next == 0) break;
@@ -417,7 +417,7 @@ __device__ void long_row_write_upper(const ListLayout& L, int n, int u, const in
         if (glane == 0) {
 #pragma unroll
             for (int a = 0; a < DPN; a++) {
-                const long long rbase = __ldg(row_ptr + (size_t)n * DPN + a);
+                const long long rbase = FEM_LDG(row_ptr + (size_t)n * DPN + a);
 #pragma unroll
                 for (int b = 0; b < DPN; b++) {
                     if (k == 0 && b < a) continue;  // below the diagonal
@@ -438,11 +438,11 @@ __device__ __forceinline__ void prefetch_first_chunk(const ListLayout& L, long l
                                                      int& next) {
     if (node < L.N) {
         const int* meta = chunk_meta(L, (int)node);
-        next = __ldg(meta + 1);
+        next = FEM_LDG(meta + 1);
 #pragma unroll
         for (int q = 0; q < kPre; q++) {
             const int s = q * G + glane;
-            w[q] = s < L.S1 ? __ldg(meta + 2 + s) : 0;
+            w[q] = s < L.S1 ? FEM_LDG(meta + 2 + s) : 0;
         }
     }
 }
@@ -482,7 +482,7 @@ __device__ __forceinline__ void write_batches(const ListLayout& L, const int* __
     constexpr int kPre = (DPN == 2 ? 16 : 96) / G;
     auto& s_keys = sm.keys;
     auto& s_vals = sm.vals;
-    if (L.info->nnz > capacity) return;  // FEM_ERR_CAPACITY already raised; write nothing
+    if (__ldcg(&L.info->nnz) > capacity) return;  // FEM_ERR_CAPACITY already raised; write nothing
     const int tid = threadIdx.x;
     const int grp = tid / G, glane = tid % G;
     const unsigned gmask = group_mask<G>((tid & 31) / G);
@@ -499,13 +499,13 @@ __device__ __forceinline__ void write_batches(const ListLayout& L, const int* __
         long long base = 0;
         if (valid) {
             if (kMode == kOutUpper) {
-                u = __ldg(ucounts + n);  // columns >= n (the full row count is in L.counts)
+                u = FEM_LDG(ucounts + n);  // columns >= n (the full row count is in L.counts)
             } else if (kBsr) {
-                base = __ldg(row_ptr + n);
-                u = __ldg(row_ptr + n + 1) - (int)base;
+                base = FEM_LDG(row_ptr + n);
+                u = FEM_LDG(row_ptr + n + 1) - (int)base;
             } else {
-                base = __ldg(row_ptr + (size_t)n * DPN);
-                u = (__ldg(row_ptr + (size_t)n * DPN + 1) - (int)base) / DPN;
+                base = FEM_LDG(row_ptr + (size_t)n * DPN);
+                u = (FEM_LDG(row_ptr + (size_t)n * DPN + 1) - (int)base) / DPN;
             }
         }
         // 1. gather the non-empty slots of the node's chunk chain (the first
@@ -529,10 +529,10 @@ __device__ __forceinline__ void write_batches(const ListLayout& L, const int* __
                 const int c = next - 1;
                 const int* meta = chunk_meta(L, c);
                 const int cap = chunk_cap(L, c);
-                next = __ldg(meta + 1);
+                next = FEM_LDG(meta + 1);
                 for (int s0 = 0; s0 < cap; s0 += G) {
                     const int s = s0 + glane;
-                    const int col = s < cap ? (__ldg(meta + 2 + s) & kColMask) : 0;
+                    const int col = s < cap ? (FEM_LDG(meta + 2 + s) & kColMask) : 0;
                     const unsigned used = (__ballot_sync(gmask, col != 0) >> gshift) & gmask >> gshift;
                     const int e = T + __popc(used & ((1u << glane) - 1u));
                     if (col != 0 && e < NK)
@@ -540,7 +540,7 @@ __device__ __forceinline__ void write_batches(const ListLayout& L, const int* __
                     T += __popc(used);
                 }
             }
-            const int expect = kMode == kOutUpper ? __ldg(L.counts + n) : u;
+            const int expect = kMode == kOutUpper ? FEM_LDG(L.counts + n) : u;
             if (glane == 0 && (T != expect || u > T)) raise_status(L.info, FEM_ERR_INTERNAL);
         }
         if constexpr (kSymLists<DPN> && kMode != kOutUpper) {
@@ -579,8 +579,8 @@ __device__ __forceinline__ void write_batches(const ListLayout& L, const int* __
             // all of the node's blocks in flight at once (two 16-byte loads each)
             for (int k = glane; k < Ts; k += G) {
                 const double2* p = reinterpret_cast<const double2*>(L.vals + (size_t)(unsigned)s_keys[grp][k] * B);
-                s_vals[grp][k][0] = __ldg(p);
-                s_vals[grp][k][1] = __ldg(p + 1);
+                s_vals[grp][k][0] = FEM_LDG(p);
+                s_vals[grp][k][1] = FEM_LDG(p + 1);
             }
             __syncwarp();
         }
@@ -589,7 +589,7 @@ __device__ __forceinline__ void write_batches(const ListLayout& L, const int* __
             if constexpr (DPN == 2) return reinterpret_cast<const double*>(&s_vals[grp][k][0])[v];
             const unsigned g = (unsigned)s_keys[grp][k];
             const int vv = (g & kTransposed) ? (v % DPN) * DPN + v / DPN : v;
-            return __ldg(L.vals + (size_t)(g & ~kTransposed) * B + vv);
+            return FEM_LDG(L.vals + (size_t)(g & ~kTransposed) * B + vv);
         };
         // 3. write the dpn rows of the node (or its block row, or its upper rows)
         if (valid && kMode == kOutUpper) {
@@ -598,7 +598,7 @@ __device__ __forceinline__ void write_batches(const ListLayout& L, const int* __
             } else if (u > 0 && u <= Ts) {
                 const int k0 = Ts - u;  // the sorted row's first column >= n (n itself)
                 for (int a = 0; a < DPN; a++) {
-                    const long long rbase = __ldg(row_ptr + (size_t)n * DPN + a);
+                    const long long rbase = FEM_LDG(row_ptr + (size_t)n * DPN + a);
                     const int len = (u - 1) * DPN + (DPN - a);
                     for (int r = glane; r < len; r += G) {
                         int k, b;

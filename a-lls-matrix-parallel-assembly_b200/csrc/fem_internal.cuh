@@ -89,6 +89,14 @@ __device__ __forceinline__ void gid_chunk(const ListLayout& L, unsigned gid, int
     }
 }
 
+// Loads of data that no kernel of the launch writes go through the read-only
+// path. The batched persistent kernel (batched.cu), whose work items read what
+// earlier items of the same launch wrote, defines FEM_LDG as an L2 load before
+// it includes the kernels' device code.
+#ifndef FEM_LDG
+#define FEM_LDG(p) __ldg(p)
+#endif
+
 // L2-coherent loads (bypass L1: list words change under other SMs' writes).
 __device__ __forceinline__ int ld_cg(const int* p) { return __ldcg(p); }
 __device__ __forceinline__ int4 ld_cg4(const int* p) { return __ldcg(reinterpret_cast<const int4*>(p)); }

@@ -77,9 +77,14 @@ __device__ __forceinline__ int resolve_2d(const ListLayout& L, int row, int key,
 }
 
 // Element id of work item `i` of this lane (valid: inside the range).
-__device__ __forceinline__ int element_of(const int* perm, int begin, int count, long long i, bool ok, bool& valid) {
+// want_type >= 0: only the elements of that type (mixed meshes without a
+// type-grouped order) are taken; the others leave their lanes idle.
+__device__ __forceinline__ int element_of(const MeshView& m, const int* perm, int begin, int count, long long i,
+                                          bool ok, int want_type, bool& valid) {
     valid = ok && i < count;
-    return valid ? (perm ? __ldg(perm + begin + i) : begin + (int)i) : 0;
+    const int e = valid ? (perm ? FEM_LDG(perm + begin + i) : begin + (int)i) : 0;
+    if (valid && want_type >= 0) valid = FEM_LDG(m.types + e) == want_type;
+    return e;
 }
 
 // Resident CTAs per SM the register budget is set for (build-time tuning knobs).
@@ -103,7 +108,7 @@ struct Scatter2DWarpSmem {
 template <int NPE, typename T>
 __device__ __forceinline__ void scatter2d_warp(const MeshView& m, const ListLayout& L, const int* __restrict__ perm,
                                                int begin, int count, long long warp_id, long long num_warps,
-                                               Scatter2DWarpSmem& ws) {
+                                               Scatter2DWarpSmem& ws, int want_type = -1) {
     constexpr int G = NPE * NPE;   // lanes per element
     constexpr int EPW = 32 / G;    // elements per warp
     constexpr unsigned kFull = 0xFFFFFFFFu;
@@ -121,15 +126,15 @@ __device__ __forceinline__ void scatter2d_warp(const MeshView& m, const ListLayo
     // are in flight.
     long long base = warp_id * EPW;
     bool valid, valid1, valid2;
-    int e = element_of(perm, begin, count, base + eslot, lane_used, valid);
-    int e1 = element_of(perm, begin, count, base + stride + eslot, lane_used, valid1);
+    int e = element_of(m, perm, begin, count, base + eslot, lane_used, want_type, valid);
+    int e1 = element_of(m, perm, begin, count, base + stride + eslot, lane_used, want_type, valid1);
     int nodes[NPE], nodes1[NPE];
 #pragma unroll
     for (int k = 0; k < NPE; k++) {
-        nodes[k] = valid ? __ldg(m.conn + (size_t)e * m.stride + k) : 0;
-        nodes1[k] = valid1 ? __ldg(m.conn + (size_t)e1 * m.stride + k) : 0;
+        nodes[k] = valid ? FEM_LDG(m.conn + (size_t)e * m.stride + k) : 0;
+        nodes1[k] = valid1 ? FEM_LDG(m.conn + (size_t)e1 * m.stride + k) : 0;
     }
-    int e2 = element_of(perm, begin, count, base + 2 * stride + eslot, lane_used, valid2);
+    int e2 = element_of(m, perm, begin, count, base + 2 * stride + eslot, lane_used, want_type, valid2);
     double xe[NPE], ye[NPE], Ee = 0.0, nue = 0.0;
     auto load_element = [&]() {
         bool bad = false;
@@ -141,11 +146,11 @@ __device__ __forceinline__ void scatter2d_warp(const MeshView& m, const ListLayo
         }
 #pragma unroll
         for (int k = 0; k < NPE; k++) {
-            xe[k] = valid ? __ldg(m.x + nodes[k]) : 0.0;
-            ye[k] = valid ? __ldg(m.y + nodes[k]) : 0.0;
+            xe[k] = valid ? FEM_LDG(m.x + nodes[k]) : 0.0;
+            ye[k] = valid ? FEM_LDG(m.y + nodes[k]) : 0.0;
         }
-        Ee = !valid ? 0.0 : (m.E ? __ldg(m.E + e) : m.E0);
-        nue = !valid ? 0.0 : (m.nu ? __ldg(m.nu + e) : m.nu0);
+        Ee = !valid ? 0.0 : (m.E ? FEM_LDG(m.E + e) : m.E0);
+        nue = !valid ? 0.0 : (m.nu ? FEM_LDG(m.nu + e) : m.nu0);
     };
     load_element();
 
@@ -196,8 +201,8 @@ __device__ __forceinline__ void scatter2d_warp(const MeshView& m, const ListLayo
         e1 = e2;
         valid1 = valid2;
 #pragma unroll
-        for (int k = 0; k < NPE; k++) nodes1[k] = valid1 ? __ldg(m.conn + (size_t)e1 * m.stride + k) : 0;
-        e2 = element_of(perm, begin, count, base + 3 * stride + eslot, lane_used, valid2);
+        for (int k = 0; k < NPE; k++) nodes1[k] = valid1 ? FEM_LDG(m.conn + (size_t)e1 * m.stride + k) : 0;
+        e2 = element_of(m, perm, begin, count, base + 3 * stride + eslot, lane_used, want_type, valid2);
         load_element();
     }
 }

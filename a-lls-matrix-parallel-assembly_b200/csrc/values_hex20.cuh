@@ -82,16 +82,16 @@ __device__ __forceinline__ void values_cta(const MeshView& m, const int* __restr
     const bool tile_warp = warp < kValueWarps;
     const int ti = tile_ti(warp), tj = tile_tj(warp);
     const int fr = lane >> 2, fc = lane & 3;
-    auto elem = [&](long long i) -> int { return perm ? __ldg(perm + i) : (int)i; };
+    auto elem = [&](long long i) -> int { return perm ? FEM_LDG(perm + i) : (int)i; };
     // node id and coordinates of the next element
     int pre_n = 0;
     double pre_x = 0.0, pre_y = 0.0, pre_z = 0.0;
     if (tid < 20 && i_first < i1) {
-        pre_n = __ldg(m.conn + (size_t)elem(i_first) * 20 + tid);
+        pre_n = FEM_LDG(m.conn + (size_t)elem(i_first) * 20 + tid);
         if (pre_n >= 0 && pre_n < m.N) {
-            pre_x = __ldg(m.x + pre_n);
-            pre_y = __ldg(m.y + pre_n);
-            pre_z = __ldg(m.z + pre_n);
+            pre_x = FEM_LDG(m.x + pre_n);
+            pre_y = FEM_LDG(m.y + pre_n);
+            pre_z = FEM_LDG(m.z + pre_n);
         }
     }
     __syncthreads();
@@ -111,20 +111,20 @@ __device__ __forceinline__ void values_cta(const MeshView& m, const int* __restr
             }
         }
         if (tid == 32) {
-            const double E = m.E ? __ldg(m.E + e) : m.E0;
-            const double nu = m.nu ? __ldg(m.nu + e) : m.nu0;
+            const double E = m.E ? FEM_LDG(m.E + e) : m.E0;
+            const double nu = m.nu ? FEM_LDG(m.nu + e) : m.nu0;
             sm.lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
             sm.mu = E / (2.0 * (1.0 + nu));
         }
         __syncthreads();
         const long long i_next = i + i_stride;
-        if (tid < 20 && i_next < i1) pre_n = __ldg(m.conn + (size_t)elem(i_next) * 20 + tid);
+        if (tid < 20 && i_next < i1) pre_n = FEM_LDG(m.conn + (size_t)elem(i_next) * 20 + tid);
         if (sm.bad) {  // nothing to add
             if (tid == 0 && kOut != kToSlots) raise_status(t.info, FEM_ERR_BAD_MESH);  // else the claim pass did
             if (tid < 20 && i_next < i1 && pre_n >= 0 && pre_n < m.N) {
-                pre_x = __ldg(m.x + pre_n);
-                pre_y = __ldg(m.y + pre_n);
-                pre_z = __ldg(m.z + pre_n);
+                pre_x = FEM_LDG(m.x + pre_n);
+                pre_y = FEM_LDG(m.y + pre_n);
+                pre_z = FEM_LDG(m.z + pre_n);
             }
             __syncthreads();  // uniform: every thread has read the flag before it is reset
             continue;
@@ -170,9 +170,9 @@ __device__ __forceinline__ void values_cta(const MeshView& m, const int* __restr
         __syncthreads();
         // the coordinates of the next element arrive during the contraction
         if (tid < 20 && i_next < i1 && pre_n >= 0 && pre_n < m.N) {
-            pre_x = __ldg(m.x + pre_n);
-            pre_y = __ldg(m.y + pre_n);
-            pre_z = __ldg(m.z + pre_n);
+            pre_x = FEM_LDG(m.x + pre_n);
+            pre_y = FEM_LDG(m.y + pre_n);
+            pre_z = FEM_LDG(m.z + pre_n);
         }
         if (!tile_warp) continue;  // the remaining warps wait at the next element's first barrier
         // M^{ab} tiles (ti, tj): A[r][k] = w_k G[a][8 ti + r][k], B[k][c] = G[b][8 tj + c][k]
@@ -212,7 +212,7 @@ __device__ __forceinline__ void values_cta(const MeshView& m, const int* __restr
                 const int Jn = 8 * tj + 2 * fc + h;
                 const bool pair = I < 20 && Jn < 20 && (ti != tj || Jn >= I);
                 const bool lower_first = pair && nI <= sm.nodes[Jn < 20 ? Jn : 0];
-                const int g = pair ? __ldg(mrow + (lower_first ? I * 20 + Jn : Jn * 20 + I)) : -1;
+                const int g = pair ? FEM_LDG(mrow + (lower_first ? I * 20 + Jn : Jn * 20 + I)) : -1;
                 const unsigned have = __ballot_sync(0xFFFFFFFFu, g >= 0);
                 if (g >= 0) {
                     const int slot = base + __popc(have & ((1u << lane) - 1u));
@@ -253,15 +253,15 @@ __device__ __forceinline__ void values_cta(const MeshView& m, const int* __restr
                 for (int o = 0; o < (I == Jn ? 1 : 2); o++) {
                     const int R = o ? Jn : I, Cn = o ? I : Jn;  // block (R, Cn) of the element
                     const int r0 = 3 * sm.nodes[R], c0 = 3 * sm.nodes[Cn];
-                    const int lo = __ldg(t.row_ptr + r0), len = __ldg(t.row_ptr + r0 + 1) - lo;
+                    const int lo = FEM_LDG(t.row_ptr + r0), len = FEM_LDG(t.row_ptr + r0 + 1) - lo;
                     int p = -1;
                     if constexpr (kOut == kToCsrMap) {
-                        p = __ldg(t.map + (size_t)e * 400 + R * 20 + Cn);
+                        p = FEM_LDG(t.map + (size_t)e * 400 + R * 20 + Cn);
                     } else {
                         int a0 = lo, a1 = lo + len - 1;
                         while (a0 <= a1) {
                             const int mid = (a0 + a1) >> 1;
-                            const int c = __ldg(t.col_idx + mid);
+                            const int c = FEM_LDG(t.col_idx + mid);
                             if (c == c0) {
                                 p = mid;
                                 break;
