@@ -1,74 +1,242 @@
 // Batched assembly: many independent meshes of uneven sizes and element kinds
-// in one stream-ordered call (graph-capturable).
+// in one persistent launch (graph-capturable).
 //
-// The reference assembles one mesh per program run. Here the meshes are dealt
-// to `concurrency` workspace slots; each slot has its own library stream and
-// assembles its meshes one after another (scatter, consolidation, then a tiny
-// kernel that copies the mesh's info word into the caller's array and stamps
-// the completion time with the GPU's global timer). The slots' streams fork
-// from the caller's stream and join it again through events, so the whole
-// batch is ordered on the caller's stream and can be captured into a CUDA
-// graph; small meshes of different slots run side by side on the GPU instead
-// of one after another. Meshes are dealt largest first to the slot with the
-// least estimated work (elements weighted by kind); each slot then runs its
-// meshes smallest first.
+// The reference assembles one mesh per program run (each driver's main, e.g.
+// ALLS_Q4_T3_Mixed_Elements_Assembly_Performance.cu:742-854). Here the host
+// turns the batch into a schedule: for each mesh its phases (list reset,
+// 2-D scatter or Hex20 claim / value waves, consolidation scan, row pointers,
+// sorted write, completion) as segments of work items, the meshes in rounds
+// of `slots` (the workspace holds that many meshes' lists at once), each
+// round phase by phase. One persistent kernel then runs the whole schedule:
+// every CTA takes the next ticket from one counter, finds its segment, waits
+// (bounded) until the mesh's phase counters say the items it depends on are
+// finished, runs the item with the same device code as the single-mesh
+// kernels (claim_hex20.cuh, values_hex20.cuh, scatter2d.cuh, consolidate.cuh)
+// and counts it done. An item only ever depends on items with smaller
+// tickets, which CTAs already running have taken, so the kernel always makes
+// progress. A mesh's last item copies its info word into the caller's array
+// and stamps its completion with the GPU global timer.
+//
+// The mesh descriptors and the schedule travel as kernel parameters of small
+// copy kernels into the workspace, so a captured CUDA graph holds them; the
+// counters and the ticket are zeroed by a kernel of the same sequence.
+#define FEM_LDG(p) __ldcg(p)  // items read what earlier items of the launch wrote
+
 #include <algorithm>
 #include <mutex>
 #include <numeric>
 #include <vector>
 
-#include "launch.h"
+#include "claim_hex20.cuh"
+#include "consolidate.cuh"
+#include "scatter2d.cuh"
+#include "values_hex20.cuh"
 
 namespace fem {
 namespace {
 
-__global__ void k_stamp(unsigned long long* out) {
+constexpr int kBatchThreads = 256;
+constexpr int kBatchWarps = kBatchThreads / 32;
+static_assert(kBatchThreads == kScanThreads && kBatchThreads == kBlockThreads, "one CTA shape for every item");
+static_assert(kBatchWarps * kBatchClaim / kBatchWarps == kBatchClaim, "claim items: whole warps");
+
+// Shared memory of the item kinds (one at a time).
+union BatchSmem {
+    ClaimWarpSmem claim[kBatchWarps];
+    ValuesSmem values;
+    Scatter2DWarpSmem scatter[kBatchWarps];
+    WriteSmem<2, 8, 2> write2;
+    WriteSmem<3, 32, 4> write3;
+    long long scan[kScanThreads / 32 + 1];
+};
+
+constexpr int kMeshChunk = 96;   // descriptors per copy kernel (kernel parameters stay under 32 KB)
+constexpr int kSegChunk = 700;   // segments per copy kernel
+struct MeshChunk {
+    int first, count;
+    BatchMesh m[kMeshChunk];
+};
+struct SegChunk {
+    int first, count;
+    BatchSegment s[kSegChunk];
+};
+static_assert(sizeof(MeshChunk) < 32000 && sizeof(SegChunk) < 32000, "kernel parameter size");
+
+__global__ void k_copy_meshes(const MeshChunk c, BatchMesh* dst) {
+    constexpr int kWords = sizeof(BatchMesh) / 8;
+    static_assert(sizeof(BatchMesh) % 8 == 0, "descriptor copy in 8-byte words");
+    for (int i = threadIdx.x; i < c.count * kWords; i += blockDim.x) {
+        const int k = i / kWords, w = i - k * kWords;
+        reinterpret_cast<unsigned long long*>(dst + c.first + k)[w] =
+            reinterpret_cast<const unsigned long long*>(&c.m[k])[w];
+    }
+}
+
+__global__ void k_copy_segments(const SegChunk c, BatchSegment* dst) {
+    for (int i = threadIdx.x; i < c.count; i += blockDim.x) dst[c.first + i] = c.s[i];
+}
+
+__device__ __forceinline__ unsigned long long global_timer() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    *out = t;
+    return t;
 }
 
-// Copies a mesh's device info into the batch's info array; stamps its completion.
-__global__ void k_finish(const DevInfo* info, fem_info* dst, unsigned long long* stamp) {
-    static_assert(sizeof(fem_info) % 8 == 0, "fem_info copy in 8-byte words");
-    const int i = threadIdx.x;
-    if (i < (int)(sizeof(fem_info) / 8))
-        reinterpret_cast<unsigned long long*>(dst)[i] = reinterpret_cast<const unsigned long long*>(info)[i];
-    if (i == 0 && stamp) {
-        unsigned long long t;
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-        *stamp = t;
+__global__ void k_batch_start(int* counters, int n, int* ticket, unsigned long long* stamp0) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) counters[i] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *ticket = 0;
+        if (stamp0) *stamp0 = global_timer();
     }
 }
 
-// Library streams and events for the slots, per device, created on first use.
-struct SlotStreams {
-    cudaStream_t stream[kMaxBatchConcurrency] = {};
-    cudaEvent_t fork = nullptr, join[kMaxBatchConcurrency] = {};
-    bool ready = false;
-};
-constexpr int kMaxDevices = 64;
-std::mutex g_slot_mutex;
-SlotStreams g_slots[kMaxDevices];
-
-cudaError_t slot_streams(SlotStreams*& out) {
-    int dev = 0;
-    cudaError_t err = cudaGetDevice(&dev);
-    if (err) return err;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_slot_mutex);
-    SlotStreams& s = g_slots[dev];
-    if (!s.ready) {
-        err = cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming);
-        for (int k = 0; k < kMaxBatchConcurrency && !err; k++) {
-            err = cudaStreamCreateWithFlags(&s.stream[k], cudaStreamNonBlocking);
-            if (!err) err = cudaEventCreateWithFlags(&s.join[k], cudaEventDisableTiming);
+// Clears bytes [lo, hi) of the concatenation of the mesh's reset ranges.
+__device__ void reset_range(const BatchMesh& bm, long long lo, long long hi) {
+    long long base = 0;
+    for (int r = 0; r < 3; r++) {
+        const long long len = bm.zero_bytes[r];
+        const long long a = max(lo, base), b = min(hi, base + len);
+        if (a < b) {
+            unsigned char* p = bm.zero_ptr[r] + (a - base);
+            const long long nb = b - a;
+            // the ranges and the item bounds are 16-byte multiples except the
+            // counts' tail: 16-byte stores, then bytes
+            const long long n16 = nb >> 4;
+            for (long long i = threadIdx.x; i < n16; i += blockDim.x)
+                reinterpret_cast<int4*>(p)[i] = make_int4(0, 0, 0, 0);
+            for (long long i = (n16 << 4) + threadIdx.x; i < nb; i += blockDim.x) p[i] = 0;
         }
-        if (err) return err;
-        s.ready = true;
+        base += len;
     }
-    out = &s;
-    return cudaSuccess;
+}
+
+// Bounded wait of thread 0 until counters[c] >= target; false when it ran out.
+__device__ bool wait_counter(const int* counters, int c, int target, long long wait_ns) {
+    const volatile int* p = counters + c;
+    if (*p >= target) return true;
+    const unsigned long long t0 = global_timer();
+    while (*p < target) {
+        if ((long long)(global_timer() - t0) > wait_ns) return false;
+        __nanosleep(256);
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(kBatchThreads, 2)
+    k_batch(const BatchMesh* __restrict__ meshes, const BatchSegment* __restrict__ segs, int nseg, int total,
+            int* counters, int* ticket, long long wait_ns) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BatchSmem& sm = *reinterpret_cast<BatchSmem*>(smem_raw);
+    __shared__ int s_ticket, s_seg;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    for (;;) {
+        if (tid == 0) {
+            const int t = atomicAdd(ticket, 1);
+            int lo = 0, hi = nseg - 1;  // the last segment whose first ticket is <= t
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (__ldg(&segs[mid].first) <= t) lo = mid;
+                else hi = mid - 1;
+            }
+            s_ticket = t;
+            s_seg = lo;
+            if (t < total) {
+                const BatchSegment& sg = segs[lo];
+                for (int d = 0; d < 2; d++)
+                    if (sg.dep_ctr[d] >= 0 && !wait_counter(counters, sg.dep_ctr[d], sg.dep_target[d], wait_ns))
+                        raise_status(meshes[sg.mesh].L.info, FEM_ERR_TIMEOUT);
+                __threadfence();  // what the awaited items wrote is seen after the counters
+            }
+        }
+        __syncthreads();
+        const int t = s_ticket;
+        if (t >= total) break;
+        const BatchSegment sg = segs[s_seg];
+        const BatchMesh& bm = meshes[sg.mesh];
+        const int k = t - sg.first;
+        const MeshView& m = bm.m;
+        const ListLayout& L = bm.L;
+        switch (sg.phase) {
+            case kBpReset: {
+                reset_range(bm, (long long)k * kBatchResetBytes, (long long)(k + 1) * kBatchResetBytes);
+                if (k == 0) {
+                    __syncthreads();
+                    if (tid == 0) L.info->pool_chunks = L.cap2;
+                }
+                break;
+            }
+            case kBpScatter2D: {
+                const int b = k * kBatchScatter2D, cnt = min(kBatchScatter2D, m.E_count - b);
+                if (bm.kind == FEM_Q4) {
+                    scatter2d_warp<4, double>(m, L, nullptr, b, cnt, warp, kBatchWarps, sm.scatter[warp]);
+                } else if (bm.kind == FEM_T3) {
+                    scatter2d_warp<3, double>(m, L, nullptr, b, cnt, warp, kBatchWarps, sm.scatter[warp]);
+                } else {
+                    scatter2d_warp<4, double>(m, L, nullptr, b, cnt, warp, kBatchWarps, sm.scatter[warp], FEM_Q4);
+                    scatter2d_warp<3, double>(m, L, nullptr, b, cnt, warp, kBatchWarps, sm.scatter[warp], FEM_T3);
+                }
+                break;
+            }
+            case kBpClaim: {
+                const int w0 = sg.arg * kHex20Wave, w1 = min(m.E_count, w0 + kHex20Wave);
+                const int b = w0 + k * kBatchClaim, e1 = min(w1, b + kBatchClaim);
+                claim_warp(m, L, nullptr, b + warp, kBatchWarps, e1, w0, bm.map[sg.arg & 1], sm.claim[warp]);
+                break;
+            }
+            case kBpValues: {
+                const int w0 = sg.arg * kHex20Wave, w1 = min(m.E_count, w0 + kHex20Wave);
+                const int b = w0 + k * kBatchValues, e1 = min(w1, b + kBatchValues);
+                ValuesTarget vt{};
+                vt.map = bm.map[sg.arg & 1];
+                vt.map_origin = w0;
+                vt.vals = L.vals;
+                vt.info = L.info;
+                values_init(sm.values);
+                values_cta<kToSlots>(m, nullptr, b, 1, e1, vt, sm.values);
+                break;
+            }
+            case kBpScanReduce:
+                if (bm.dpn == 3) scan_reduce_tile<9>(L.counts, L.N, bm.tiles, k, sm.scan);
+                else scan_reduce_tile<4>(L.counts, L.N, bm.tiles, k, sm.scan);
+                break;
+            case kBpScanTop:
+                scan_tiles_body(bm.tiles, bm.num_tiles, L.info, bm.row_ptr + (size_t)L.N * bm.dpn, bm.capacity, 1,
+                                sm.scan);
+                break;
+            case kBpRowPtr:
+                if (bm.dpn == 3) row_ptr_tile<3, false>(L.counts, L.N, bm.tiles, bm.row_ptr, k, sm.scan);
+                else row_ptr_tile<2, false>(L.counts, L.N, bm.tiles, bm.row_ptr, k, sm.scan);
+                break;
+            case kBpWrite:
+                if (bm.dpn == 3) {
+                    constexpr int NPB = kBlockThreads / 32;
+                    const long long b = (long long)k * NPB * kBatchWriteBatches;
+                    write_batches<3, 32, 4, kOutCsr>(L, bm.row_ptr, bm.col_idx, bm.values, bm.capacity, nullptr, b,
+                                                     NPB, min((long long)L.N, b + NPB * kBatchWriteBatches),
+                                                     sm.write3);
+                } else {
+                    constexpr int NPB = kBlockThreads / 8;
+                    const long long b = (long long)k * NPB * kBatchWriteBatches;
+                    write_batches<2, 8, 2, kOutCsr>(L, bm.row_ptr, bm.col_idx, bm.values, bm.capacity, nullptr, b,
+                                                    NPB, min((long long)L.N, b + NPB * kBatchWriteBatches),
+                                                    sm.write2);
+                }
+                break;
+            case kBpFinish:
+                if (tid < (int)(sizeof(fem_info) / 8))
+                    reinterpret_cast<unsigned long long*>(bm.info_out)[tid] =
+                        __ldcg(reinterpret_cast<const unsigned long long*>(L.info) + tid);
+                if (tid == 0 && bm.stamp) *bm.stamp = global_timer();
+                break;
+            default:
+                break;
+        }
+        __syncthreads();  // the item is finished (and the shared memory free) before it is counted
+        if (tid == 0) {
+            __threadfence();
+            atomicAdd(counters + sg.done_ctr, 1);
+        }
+    }
 }
 
 }  // namespace
@@ -92,35 +260,46 @@ std::vector<int> batch_schedule(const fem_mesh* meshes, int n, int slots) {
     return slot_of;
 }
 
-cudaError_t batch_fork(int slots, cudaStream_t s, cudaStream_t* out_streams) {
-    SlotStreams* ss = nullptr;
-    cudaError_t err = slot_streams(ss);
+cudaError_t launch_batch(const BatchMesh* meshes, int n, const BatchSegment* segs, int nseg, int total_items,
+                         BatchMesh* d_meshes, BatchSegment* d_segs, int* d_counters, int* d_ticket,
+                         unsigned long long* stamp0, long long wait_ns, int ctas_per_sm, cudaStream_t s) {
+    static MeshChunk mc;  // staging of the kernel parameters (copied at each launch)
+    static SegChunk sc;
+    static std::mutex mtx;
+    std::lock_guard<std::mutex> lock(mtx);
+    cudaError_t err = cudaSuccess;
+    for (int f = 0; f < n && !err; f += kMeshChunk) {
+        mc.first = f;
+        mc.count = std::min(kMeshChunk, n - f);
+        std::copy(meshes + f, meshes + f + mc.count, mc.m);
+        k_copy_meshes<<<1, 256, 0, s>>>(mc, d_meshes);
+        err = cudaGetLastError();
+    }
+    for (int f = 0; f < nseg && !err; f += kSegChunk) {
+        sc.first = f;
+        sc.count = std::min(kSegChunk, nseg - f);
+        std::copy(segs + f, segs + f + sc.count, sc.s);
+        k_copy_segments<<<1, 256, 0, s>>>(sc, d_segs);
+        err = cudaGetLastError();
+    }
     if (err) return err;
-    err = cudaEventRecord(ss->fork, s);
-    for (int k = 0; k < slots && !err; k++) {
-        out_streams[k] = ss->stream[k];
-        err = cudaStreamWaitEvent(ss->stream[k], ss->fork, 0);
-    }
-    return err;
-}
-
-cudaError_t batch_join(int slots, cudaStream_t s) {
-    SlotStreams* ss = nullptr;
-    cudaError_t err = slot_streams(ss);
-    for (int k = 0; k < slots && !err; k++) {
-        err = cudaEventRecord(ss->join[k], ss->stream[k]);
-        if (!err) err = cudaStreamWaitEvent(s, ss->join[k], 0);
-    }
-    return err;
-}
-
-cudaError_t launch_stamp(unsigned long long* out, cudaStream_t s) {
-    k_stamp<<<1, 1, 0, s>>>(out);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_finish(const DevInfo* info, fem_info* dst, unsigned long long* stamp, cudaStream_t s) {
-    k_finish<<<1, 32, 0, s>>>(info, dst, stamp);
+    k_batch_start<<<std::max(1, std::min(64, (n * kBatchCounters + 255) / 256)), 256, 0, s>>>(
+        d_counters, n * kBatchCounters, d_ticket, stamp0);
+    if ((err = cudaGetLastError())) return err;
+    static DeviceCache cache;
+    const size_t smem = sizeof(BatchSmem);
+    int per_sm = 0;
+    err = per_device(cache, [&](int& v) {
+        cudaError_t e = cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_batch, kBatchThreads, smem);
+        return e;
+    }, per_sm);
+    if (err) return err;
+    // every CTA of the grid is resident at once: a CTA that waits never holds
+    // back one that has not started
+    const int use = ctas_per_sm > 0 ? std::min(ctas_per_sm, per_sm) : per_sm;
+    const long long grid = std::max<long long>(1, std::min<long long>(total_items, (long long)use * sm_count()));
+    k_batch<<<(int)grid, kBatchThreads, smem, s>>>(d_meshes, d_segs, nseg, total_items, d_counters, d_ticket, wait_ns);
     return cudaGetLastError();
 }
 

@@ -11,7 +11,7 @@ constexpr int kClaimMaxWords = 96;   // first-chunk meta rows of at most 96 word
 constexpr int kPairs = 400;
 constexpr int kPerLane = (kPairs + 31) / 32;  // 13
 
-enum : unsigned char { kFound = 0, kTry = 1, kClaimed = 2, kChain = 3 };
+enum : unsigned char { kCFound = 0, kCTry = 1, kCClaimed = 2, kCChain = 3 };
 
 // Shared memory of one claiming warp.
 struct ClaimWarpSmem {
@@ -111,25 +111,25 @@ __device__ __forceinline__ void claim_warp(const MeshView& m, const ListLayout& 
 #pragma unroll
         for (int k = 0; k < kPerLane; k++) {
             const int p = lane + 32 * k;
-            st[k] = kFound;
+            st[k] = kCFound;
             slot[k] = -1;
             if (p < kPairs) {
                 const int I = p / 20, J = p - 20 * I;
                 const int key = ws.node[J] + 1;
                 const int* v = view[I] + 2;
                 const int p0 = probe_start(key, S1);
-                st[k] = kChain;
+                st[k] = kCChain;
                 for (int t = 0; t < S1; t++) {
                     int s = p0 + t;
                     if (s >= S1) s -= S1;
                     const int x = v[s];
                     if (x == key) {
-                        st[k] = kFound;
+                        st[k] = kCFound;
                         slot[k] = s;
                         break;
                     }
                     if (x == 0) {
-                        st[k] = kTry;
+                        st[k] = kCTry;
                         slot[k] = s;
                         break;
                     }
@@ -141,29 +141,29 @@ __device__ __forceinline__ void claim_warp(const MeshView& m, const ListLayout& 
 #pragma unroll
         for (int k = 0; k < kPerLane; k++) {
             old[k] = 0;
-            if (st[k] == kTry) {
+            if (st[k] == kCTry) {
                 const int p = lane + 32 * k, I = p / 20, J = p - 20 * I;
                 old[k] = atomicCAS(L.meta1 + (size_t)ws.node[I] * H1 + 2 + slot[k], 0, ws.node[J] + 1);
             }
         }
 #pragma unroll
         for (int k = 0; k < kPerLane; k++) {
-            if (st[k] != kTry) continue;
+            if (st[k] != kCTry) continue;
             const int p = lane + 32 * k, I = p / 20, J = p - 20 * I;
             const int key = ws.node[J] + 1;
             const int p0 = probe_start(key, S1);
             int* meta = L.meta1 + (size_t)ws.node[I] * H1 + 2;
             int s = slot[k], x = old[k];
-            st[k] = kChain;
+            st[k] = kCChain;
             // walk on from the contested slot: slots non-empty in the copy stay
             // non-empty, so only its empty ones are candidates
             for (int t = 0; t < S1; t++) {
                 if (x == 0) {
-                    st[k] = kClaimed;
+                    st[k] = kCClaimed;
                     break;
                 }
                 if (x == key) {
-                    st[k] = kFound;
+                    st[k] = kCFound;
                     break;
                 }
                 int u = -1;
@@ -196,14 +196,14 @@ __device__ __forceinline__ void claim_warp(const MeshView& m, const ListLayout& 
             const int I = p / 20, J = p - 20 * I;
             const int rn = ws.node[I];
             int gid;
-            if (st[k] == kChain) {
+            if (st[k] == kCChain) {
                 bool claimed = false;
                 gid = resolve_chain(L, rn, ws.node[J] + 1, spare, claimed);
-                if (claimed) st[k] = kClaimed;
+                if (claimed) st[k] = kCClaimed;
             } else {
                 gid = (int)slot_gid(L, rn, slot[k]);
             }
-            if (st[k] == kClaimed && gid >= 0) {
+            if (st[k] == kCClaimed && gid >= 0) {
                 // values are kept for upper blocks only (row node <= column node)
                 if (rn <= ws.node[J]) zero_block(L.vals + (size_t)(unsigned)gid * 9);
                 atomicAdd(&ws.claims[I], 1);

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <numeric>
 
 #include "launch.h"
 
@@ -406,35 +407,86 @@ fem_status fem_apply_dirichlet(int32_t n_rows, const int32_t* row_ptr, const int
 
 namespace {
 
-// The slot streams and their fork / join events are shared by every batched
-// call on a device: calls from several host threads enqueue one at a time.
-std::mutex g_batch_mutex;
-
 int batch_slots(int n, int concurrency) {
     int k = concurrency > 0 ? concurrency : 4;
     k = std::min(k, kMaxBatchConcurrency);
     return std::max(1, std::min(k, n));
 }
 
-// Workspace offset of each slot (bytes), sized for the largest mesh of the slot.
-fem_status batch_layout(const fem_mesh* meshes, int n, const fem_opts* opts, int slots, std::vector<int>& slot_of,
-                        std::vector<size_t>& slot_off, size_t& total) {
-    slot_of = batch_schedule(meshes, n, slots);
+// Workspace of a batch: the control block (mesh descriptors, schedule,
+// per-mesh counters, ticket) and `slots` list workspaces, each sized for the
+// largest mesh dealt to it (Hex20: plus a second wave's slot map).
+struct BatchLayout {
+    std::vector<int> slot_of;
+    std::vector<size_t> slot_off;
+    size_t off_meshes, off_counters, off_ticket, off_segs, total;
+};
+
+size_t batch_mesh_bytes(const fem_mesh& m, const fem_opts* opts, fem_status& st) {
+    HostLayout h;
+    st = make_layout(&m, opts, h);
+    if (st) return 0;
+    return h.total + (h.kind == FEM_HEX20 ? align_up((size_t)std::min(h.E, kHex20Wave) * 400 * sizeof(int)) : 0);
+}
+
+// Work items of one mesh in the batch schedule (an upper bound of the
+// segments too), used to size the schedule.
+int batch_segments_bound(const fem_mesh& m) {
+    const int waves = m.kind == FEM_HEX20 ? (m.num_elems + kHex20Wave - 1) / kHex20Wave : 0;
+    return 8 + 2 * waves;
+}
+
+fem_status batch_layout(const fem_mesh* meshes, int n, const fem_opts* opts, int slots, BatchLayout& bl) {
+    bl.slot_of = batch_schedule(meshes, n, slots);
     std::vector<size_t> need(slots, 0);
+    long long segs = 0;
     for (int i = 0; i < n; i++) {
-        size_t b = 0;
-        fem_status st = fem_alls_workspace_size(&meshes[i], opts, &b);
+        fem_status st;
+        const size_t b = batch_mesh_bytes(meshes[i], opts, st);
         if (st) return st;
-        need[slot_of[i]] = std::max(need[slot_of[i]], b);
+        need[bl.slot_of[i]] = std::max(need[bl.slot_of[i]], b);
+        segs += batch_segments_bound(meshes[i]);
     }
-    slot_off.assign(slots, 0);
-    total = 0;
+    size_t off = 0;
+    bl.off_meshes = off;
+    off += align_up((size_t)n * sizeof(BatchMesh));
+    bl.off_counters = off;
+    off += align_up((size_t)n * kBatchCounters * sizeof(int));
+    bl.off_ticket = off;
+    off += align_up(sizeof(int));
+    bl.off_segs = off;
+    off += align_up((size_t)segs * sizeof(BatchSegment));
+    bl.slot_off.assign(slots, 0);
     for (int k = 0; k < slots; k++) {
-        slot_off[k] = total;
-        total += align_up(need[k]);
+        bl.slot_off[k] = off;
+        off += align_up(need[k]);
     }
+    bl.total = off;
     return FEM_OK;
 }
+
+// Appends a segment of `count` items of one phase of mesh j.
+struct ScheduleBuilder {
+    std::vector<BatchSegment> segs;
+    int total = 0;
+    void add(int j, int phase, int count, int arg, int done, int dep0 = -1, int target0 = 0, int dep1 = -1,
+             int target1 = 0) {
+        if (count <= 0) return;
+        BatchSegment g{};
+        g.mesh = j;
+        g.phase = phase;
+        g.first = total;
+        g.count = count;
+        g.arg = arg;
+        g.dep_ctr[0] = dep0;
+        g.dep_target[0] = target0;
+        g.dep_ctr[1] = dep1;
+        g.dep_target[1] = target1;
+        g.done_ctr = done;
+        segs.push_back(g);
+        total += count;
+    }
+};
 
 }  // namespace
 
@@ -443,53 +495,154 @@ extern "C" {
 fem_status fem_batched_workspace_size(const fem_mesh* meshes, int32_t n, const fem_opts* opts, int32_t concurrency,
                                       size_t* bytes) {
     if (!meshes || n <= 0 || !bytes) return FEM_ERR_BAD_ARG;
-    std::vector<int> slot_of;
-    std::vector<size_t> slot_off;
-    return batch_layout(meshes, n, opts, batch_slots(n, concurrency), slot_of, slot_off, *bytes);
+    BatchLayout bl;
+    fem_status st = batch_layout(meshes, n, opts, batch_slots(n, concurrency), bl);
+    if (!st) *bytes = bl.total;
+    return st;
 }
 
 fem_status fem_assemble_batched(const fem_mesh* meshes, int32_t n, const fem_opts* opts, int32_t concurrency,
                                 void* workspace, size_t workspace_bytes, fem_csr* outs, fem_info* infos,
                                 unsigned long long* stamps, void* stream) {
     if (!meshes || n <= 0 || !outs || !infos) return FEM_ERR_BAD_ARG;
+    if (opts && opts->precision != FEM_PREC_FP64) return FEM_ERR_BAD_ARG;  // the batch assembles in FP64
     const int slots = batch_slots(n, concurrency);
-    std::vector<int> slot_of;
-    std::vector<size_t> slot_off;
-    size_t total = 0;
-    fem_status st = batch_layout(meshes, n, opts, slots, slot_of, slot_off, total);
+    BatchLayout bl;
+    fem_status st = batch_layout(meshes, n, opts, slots, bl);
     if (st) return st;
-    if (!workspace || workspace_bytes < total || reinterpret_cast<uintptr_t>(workspace) % kAlign)
+    if (!workspace || workspace_bytes < bl.total || reinterpret_cast<uintptr_t>(workspace) % kAlign)
         return FEM_ERR_WORKSPACE;
     for (int i = 0; i < n; i++)
         if (!outs[i].row_ptr || outs[i].capacity < 0 || (outs[i].capacity > 0 && (!outs[i].col_idx || !outs[i].values)))
             return FEM_ERR_BAD_ARG;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    std::lock_guard<std::mutex> lock(g_batch_mutex);
-    cudaError_t err = stamps ? launch_stamp(stamps, s) : cudaSuccess;
-    cudaStream_t ss[kMaxBatchConcurrency];
-    if (!err) err = batch_fork(slots, s, ss);
-    if (err) return cuda_fail(err);
-    // each slot: its meshes smallest first (the slots were filled largest first
-    // for balance; within a slot the shortest jobs go first, which lowers the
-    // meshes' completion times without changing the slot's total)
-    std::vector<int> order(n);
-    for (int i = 0; i < n; i++) order[i] = i;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int a, int b) { return batch_cost(meshes[a]) < batch_cost(meshes[b]); });
     unsigned char* base = static_cast<unsigned char*>(workspace);
-    for (int i : order) {
-        const int k = slot_of[i];
-        void* ws = base + slot_off[k];
-        const size_t wsb = (k + 1 < slots ? slot_off[k + 1] : total) - slot_off[k];
-        if ((st = fem_alls_scatter(&meshes[i], opts, ws, wsb, ss[k]))) return st;
-        if ((st = fem_alls_consolidate(&meshes[i], opts, ws, wsb, outs[i].row_ptr, outs[i].col_idx, outs[i].values,
-                                       outs[i].capacity, ss[k])))
-            return st;
-        err = launch_finish(static_cast<const DevInfo*>(ws), infos + i, stamps ? stamps + 1 + i : nullptr, ss[k]);
-        if (err) return cuda_fail(err);
+    // descriptors
+    std::vector<BatchMesh> bms(n);
+    std::vector<HostLayout> hl(n);
+    for (int i = 0; i < n; i++) {
+        if ((st = make_layout(&meshes[i], opts, hl[i]))) return st;
+        const HostLayout& h = hl[i];
+        unsigned char* ws = base + bl.slot_off[bl.slot_of[i]];
+        BatchMesh& bm = bms[i];
+        bm = BatchMesh{};
+        bm.m = mesh_view(&meshes[i]);
+        bm.L = device_layout(h, ws);
+        bm.tiles = reinterpret_cast<long long*>(ws + h.off_tiles);
+        bm.map[0] = reinterpret_cast<int*>(ws + h.off_map);
+        bm.map[1] = reinterpret_cast<int*>(ws + h.total);
+        bm.row_ptr = outs[i].row_ptr;
+        bm.col_idx = outs[i].col_idx;
+        bm.values = outs[i].values;
+        bm.capacity = outs[i].capacity;
+        bm.info_out = infos + i;
+        bm.stamp = stamps ? stamps + 1 + i : nullptr;
+        bm.zero_ptr[0] = ws;  // info word and first chunks
+        bm.zero_bytes[0] = (long long)(h.off_meta1 + h.meta1_bytes);
+        bm.zero_ptr[1] = ws + h.off_vals;  // 2-D: the first chunks' values (every contribution is an atomic add)
+        bm.zero_bytes[1] = h.dpn == 2 ? (long long)h.N * h.S1 * h.B * (long long)sizeof(double) : 0;
+        bm.zero_ptr[2] = ws + h.off_counts;
+        bm.zero_bytes[2] = (long long)h.N * (long long)sizeof(int);
+        bm.kind = h.kind;
+        bm.dpn = h.dpn;
+        bm.num_tiles = h.num_tiles;
         outs[i].n_rows = meshes[i].num_nodes * kind_dpn(meshes[i].kind);
     }
-    err = batch_join(slots, s);
+    // rounds: the r-th mesh of every slot (slots keep their meshes smallest
+    // first, which brings the meshes' completions forward)
+    std::vector<std::vector<int>> per_slot(slots);
+    {
+        std::vector<int> order(n);
+        for (int i = 0; i < n; i++) order[i] = i;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return batch_cost(meshes[a]) < batch_cost(meshes[b]); });
+        for (int i : order) per_slot[bl.slot_of[i]].push_back(i);
+    }
+    size_t rounds = 0;
+    for (auto& v : per_slot) rounds = std::max(rounds, v.size());
+    ScheduleBuilder sb;
+    std::vector<int> prev_in_slot(n, -1);
+    for (auto& v : per_slot)
+        for (size_t r = 1; r < v.size(); r++) prev_in_slot[v[r]] = v[r - 1];
+    auto ctr = [](int j, int c) { return j * kBatchCounters + c; };
+    for (size_t r = 0; r < rounds; r++) {
+        std::vector<int> round;
+        for (auto& v : per_slot)
+            if (r < v.size()) round.push_back(v[r]);
+        // largest first within a round, so that the long meshes start early
+        std::stable_sort(round.begin(), round.end(),
+                         [&](int a, int b) { return batch_cost(meshes[a]) > batch_cost(meshes[b]); });
+        std::vector<int> resets(n, 0), scatter_items(n, 0), write_items(n, 0);
+        for (int j : round) {
+            const BatchMesh& bm = bms[j];
+            const long long zb = bm.zero_bytes[0] + bm.zero_bytes[1] + bm.zero_bytes[2];
+            resets[j] = (int)((zb + kBatchResetBytes - 1) / kBatchResetBytes);
+            const int p = prev_in_slot[j];
+            sb.add(j, kBpReset, resets[j], 0, ctr(j, kBcReset), p >= 0 ? ctr(p, kBcFinish) : -1, 1);
+        }
+        for (int j : round) {
+            const int E = meshes[j].num_elems;
+            if (E <= 0) continue;
+            if (bms[j].kind == FEM_HEX20) {
+                const int nw = (E + kHex20Wave - 1) / kHex20Wave;
+                std::vector<int> claims(nw), values(nw);
+                for (int w = 0; w < nw; w++) {
+                    const int ew = std::min(kHex20Wave, E - w * kHex20Wave);
+                    claims[w] = (ew + kBatchClaim - 1) / kBatchClaim;
+                    values[w] = (ew + kBatchValues - 1) / kBatchValues;
+                }
+                std::vector<int> claims_upto(nw), values_upto(nw);
+                std::partial_sum(claims.begin(), claims.end(), claims_upto.begin());
+                std::partial_sum(values.begin(), values.end(), values_upto.begin());
+                // C0, C1, V0, C2, V1, ...: a wave's values follow the claims of
+                // the next wave; a wave's claims reuse the slot map of the wave
+                // two before, once its values are in
+                auto claim = [&](int w) {
+                    sb.add(j, kBpClaim, claims[w], w, ctr(j, kBcScatter), ctr(j, kBcReset), resets[j],
+                           w >= 2 ? ctr(j, kBcValues) : -1, w >= 2 ? values_upto[w - 2] : 0);
+                };
+                auto value = [&](int w) {
+                    sb.add(j, kBpValues, values[w], w, ctr(j, kBcValues), ctr(j, kBcScatter),
+                           claims_upto[std::min(w + 1, nw - 1)]);
+                };
+                claim(0);
+                for (int w = 0; w < nw; w++) {
+                    if (w + 1 < nw) claim(w + 1);
+                    value(w);
+                }
+                scatter_items[j] = values_upto[nw - 1];
+            } else {
+                scatter_items[j] = (E + kBatchScatter2D - 1) / kBatchScatter2D;
+                sb.add(j, kBpScatter2D, scatter_items[j], 0, ctr(j, kBcScatter), ctr(j, kBcReset), resets[j]);
+            }
+        }
+        for (int j : round) {
+            const int sc = bms[j].kind == FEM_HEX20 ? kBcValues : kBcScatter;
+            if (meshes[j].num_elems > 0)
+                sb.add(j, kBpScanReduce, bms[j].num_tiles, 0, ctr(j, kBcScanReduce), ctr(j, sc), scatter_items[j]);
+            else
+                sb.add(j, kBpScanReduce, bms[j].num_tiles, 0, ctr(j, kBcScanReduce), ctr(j, kBcReset), resets[j]);
+        }
+        for (int j : round)
+            sb.add(j, kBpScanTop, 1, 0, ctr(j, kBcScanTop), ctr(j, kBcScanReduce), bms[j].num_tiles);
+        for (int j : round) sb.add(j, kBpRowPtr, bms[j].num_tiles, 0, ctr(j, kBcRowPtr), ctr(j, kBcScanTop), 1);
+        for (int j : round) {
+            const int npb = bms[j].dpn == 3 ? kBlockThreads / 32 : kBlockThreads / 8;
+            const long long per = (long long)npb * kBatchWriteBatches;
+            write_items[j] = outs[j].capacity > 0 ? (int)((meshes[j].num_nodes + per - 1) / per) : 0;
+            sb.add(j, kBpWrite, write_items[j], 0, ctr(j, kBcWrite), ctr(j, kBcRowPtr), bms[j].num_tiles);
+        }
+        for (int j : round)
+            sb.add(j, kBpFinish, 1, 0, ctr(j, kBcFinish), ctr(j, kBcWrite), write_items[j],
+                   ctr(j, kBcRowPtr), bms[j].num_tiles);
+    }
+    long long seg_bound = 0;
+    for (int i = 0; i < n; i++) seg_bound += batch_segments_bound(meshes[i]);
+    if ((long long)sb.segs.size() > seg_bound) return FEM_ERR_INTERNAL;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const cudaError_t err = launch_batch(
+        bms.data(), n, sb.segs.data(), (int)sb.segs.size(), sb.total, reinterpret_cast<BatchMesh*>(base + bl.off_meshes),
+        reinterpret_cast<BatchSegment*>(base + bl.off_segs), reinterpret_cast<int*>(base + bl.off_counters),
+        reinterpret_cast<int*>(base + bl.off_ticket), stamps, 2000ll * 1000 * 1000, opts ? opts->ctas_per_sm : 0, s);
     return err ? cuda_fail(err) : FEM_OK;
 }
 

@@ -143,16 +143,61 @@ cudaError_t launch_dirichlet(int n_rows, const int* row_ptr, const int* col_idx,
                              const unsigned char* fixed, const double* u, cudaStream_t s);
 
 // ---- batched assembly (batched.cu) ----
-constexpr int kMaxBatchConcurrency = 16;
+// One persistent kernel assembles every mesh of a batch: its CTAs take work
+// items from one ticket counter in a fixed order (the schedule) and wait,
+// bounded, on per-mesh phase counters for the items an item depends on.
+constexpr int kMaxBatchConcurrency = 256;  // meshes whose lists are live at once (workspace slots)
 // Estimated work of a mesh (elements weighted by kind) and the slot of each
 // mesh (largest first onto the least loaded slot).
 double batch_cost(const fem_mesh& m);
 std::vector<int> batch_schedule(const fem_mesh* meshes, int n, int slots);
-// The slots' library streams wait for the caller's stream / the caller's stream waits for them.
-cudaError_t batch_fork(int slots, cudaStream_t s, cudaStream_t* out_streams);
-cudaError_t batch_join(int slots, cudaStream_t s);
-cudaError_t launch_stamp(unsigned long long* out, cudaStream_t s);
-cudaError_t launch_finish(const DevInfo* info, fem_info* dst, unsigned long long* stamp, cudaStream_t s);
+
+// Everything the batched kernel needs to know about one mesh (device copy).
+struct BatchMesh {
+    MeshView m;
+    ListLayout L;
+    long long* tiles;          // scan partials
+    int* map[2];               // Hex20: slot maps of even / odd waves
+    int* row_ptr;              // the caller's CSR
+    int* col_idx;
+    double* values;
+    long long capacity;
+    fem_info* info_out;        // the caller's info array entry
+    unsigned long long* stamp; // completion stamp (may be NULL)
+    unsigned char* zero_ptr[3];  // what the reset clears: info + first chunks, 2-D first-chunk values, counts
+    long long zero_bytes[3];
+    int kind, dpn, num_tiles, pad;
+};
+
+// Phases of a mesh (work item kinds); a segment is a run of consecutive
+// tickets of one phase of one mesh.
+enum BatchPhase : int {
+    kBpReset = 0, kBpScatter2D, kBpClaim, kBpValues, kBpScanReduce, kBpScanTop, kBpRowPtr, kBpWrite, kBpFinish
+};
+// Per-mesh completion counters (index within the mesh's group of kBatchCounters).
+enum BatchCounter : int {
+    kBcReset = 0, kBcScatter, kBcValues, kBcScanReduce, kBcScanTop, kBcRowPtr, kBcWrite, kBcFinish
+};
+constexpr int kBatchCounters = 8;
+struct BatchSegment {
+    int mesh, phase, first, count;
+    int arg;                 // Hex20 claim / value items: the wave
+    int dep_ctr[2];          // counter indices (-1: none) and the values they must reach first
+    int dep_target[2];
+    int done_ctr;            // the counter each finished item increments
+};
+// Work item sizes.
+constexpr int kBatchResetBytes = 1 << 20;  // bytes cleared per reset item
+constexpr int kBatchScatter2D = 2048;      // 2-D elements per scatter item
+constexpr int kBatchClaim = 64;            // Hex20 elements per claim item (8 warps, one element each)
+constexpr int kBatchValues = 16;           // Hex20 elements per value item (one CTA, one element at a time)
+constexpr int kBatchWriteBatches = 16;     // node batches per write item
+
+// Copies the tables into the workspace and zeroes the counters and the
+// ticket (with the start stamp), then launches the persistent kernel.
+cudaError_t launch_batch(const BatchMesh* meshes, int n, const BatchSegment* segs, int nseg, int total_items,
+                         BatchMesh* d_meshes, BatchSegment* d_segs, int* d_counters, int* d_ticket,
+                         unsigned long long* stamp0, long long wait_ns, int ctas_per_sm, cudaStream_t s);
 
 // ---- element-colouring baseline (colour.cu) ----
 constexpr int kMaxColours = 64;         // colours per mesh (a 64-bit mask of neighbour colours)

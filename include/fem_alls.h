@@ -259,11 +259,16 @@ FEM_API fem_status fem_apply_dirichlet(int32_t n_rows, const int32_t* row_ptr, c
  * Many independent meshes (any element kinds, uneven sizes) in one
  * stream-ordered call; the reference assembles one mesh per program run
  * (its drivers' main, e.g. ALLS_Q4_T3_Mixed_Elements_Assembly_Performance.cu:742-854).
+ * One persistent kernel assembles the whole batch from a schedule of work
+ * items (list resets, 2-D scatter tiles, Hex20 claim and value tiles in
+ * waves, scan tiles, row pointers, sorted-write tiles, completion), which
+ * its CTAs take in order and run once the items they depend on are done.
  * The meshes are dealt (largest first, to the least loaded) to `concurrency`
- * workspace slots (0 = 4, at most 16); each slot assembles its meshes one after
- * another, smallest first, on a library stream that forks from and joins
- * `stream`, so slots run side by side and the whole call can be captured into a
- * CUDA graph (make one uncaptured call first: it creates the library streams). */
+ * workspace slots (0 = 4, at most 256): a slot holds one mesh's lists at a
+ * time, so the meshes are assembled in rounds of `concurrency`. The call is a
+ * few small copy kernels and the persistent kernel on `stream`; it can be
+ * captured into a CUDA graph, and calls on different streams are independent
+ * (each uses only its own workspace). FP64 (opts->precision FEM_PREC_FP64). */
 
 /* Bytes of workspace for this batch (the slots are sized for their largest mesh). */
 FEM_API fem_status fem_batched_workspace_size(const fem_mesh* meshes, int32_t n, const fem_opts* opts,

@@ -159,8 +159,10 @@ def test_upper_output_and_autotuner_arguments(fem):
 
 def test_batched_workspace_sizing_host_only(fem):
     # Slots are dealt the meshes largest first, one slot per mesh until every
-    # slot has one, so a slot's size is that of its first (largest) mesh: the
-    # workspace grows with the slot count and is capped by the mesh count.
+    # slot has one, so a slot's size is that of its first (largest) mesh (a
+    # Hex20 mesh's slot also holds a second wave's slot map): the workspace
+    # grows with the slot count and is capped by the mesh count. A control
+    # block (descriptors, schedule, counters) comes first.
     import meshgen as mg
     lib = fem.load()
     meshes = mg.batch_meshes(6, seed=3, emin=20, emax=400)
@@ -175,7 +177,9 @@ def test_batched_workspace_sizing_host_only(fem):
     assert sizes[0] >= single and sizes[0] % 256 == 0
     assert all(a <= b for a, b in zip(sizes, sizes[1:]))
     assert sizes[3] == sizes[4] == sizes[5]          # at most one slot per mesh
-    total = sum(-(-fem.workspace_size(m) // 256) * 256 for m in meshes)
-    assert sizes[3] == total
+    up = lambda v: -(-v // 256) * 256  # noqa: E731
+    total = sum(up(fem.workspace_size(m)) + (up(min(m.num_elems, 4096) * 1600) if m.kind == 2 else 0)
+                for m in meshes)
+    assert total < sizes[3] <= total + 64 * 1024
     b = C.c_size_t(0)
     assert lib.fem_batched_workspace_size(cm, 0, None, 4, C.byref(b)) == fem.FEM_ERR_BAD_ARG
