@@ -280,8 +280,8 @@ FEM_API fem_status fem_batched_workspace_size(const fem_mesh* meshes, int32_t n,
  * receives each mesh's fem_info (nnz, status bits, ...). stamps: optional
  * DEVICE array [n + 1] of GPU global-timer nanoseconds: stamps[0] at the start,
  * stamps[1 + i] when mesh i is done. outs[i].n_rows is set. Asynchronous.
- * The library's slot streams are shared by all batched calls on a device:
- * calls made from several host threads are enqueued one after another. */
+ * A wait inside the kernel that runs out (2 s) raises FEM_ERR_TIMEOUT in the
+ * info of the mesh whose item waited. */
 FEM_API fem_status fem_assemble_batched(const fem_mesh* meshes, int32_t n, const fem_opts* opts,
                                         int32_t concurrency, void* workspace, size_t workspace_bytes,
                                         fem_csr* outs, fem_info* infos, unsigned long long* stamps, void* stream);
