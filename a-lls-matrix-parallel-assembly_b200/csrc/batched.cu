@@ -4,7 +4,8 @@
 // The reference assembles one mesh per program run (each driver's main, e.g.
 // ALLS_Q4_T3_Mixed_Elements_Assembly_Performance.cu:742-854). Here the host
 // turns the batch into a schedule: for each mesh its phases (list reset,
-// 2-D scatter or Hex20 claim / value waves, consolidation scan, row pointers,
+// 2-D scatter or Hex20 claim / value waves of element groups, consolidation
+// scan, row pointers,
 // sorted write, completion) as segments of work items, the meshes in rounds
 // of `slots` (the workspace holds that many meshes' lists at once), each
 // round phase by phase. One persistent kernel then runs the whole schedule:
@@ -38,12 +39,20 @@ namespace {
 constexpr int kBatchThreads = 256;
 constexpr int kBatchWarps = kBatchThreads / 32;
 static_assert(kBatchThreads == kScanThreads && kBatchThreads == kBlockThreads, "one CTA shape for every item");
-static_assert(kBatchWarps * kBatchClaim / kBatchWarps == kBatchClaim, "claim items: whole warps");
+static_assert(kBatchClaim % kGroup == 0 && kBatchValues == kGroup, "claim and value items of whole groups");
+
+// A Hex20 value item: one group's topology and the element pass. Every pair
+// is shared in the batch (the claim items get no node degrees), so each
+// element's blocks are added atomically to slots that their claimers zeroed.
+struct BatchValuesSmem {
+    ValuesSmem values;
+    GroupTopo topo;
+};
 
 // Shared memory of the item kinds (one at a time).
 union BatchSmem {
-    ClaimWarpSmem claim[kBatchWarps];
-    ValuesSmem values;
+    ClaimSmem claim;
+    BatchValuesSmem gv;
     Scatter2DWarpSmem scatter[kBatchWarps];
     WriteSmem<2, 8, 2> write2;
     WriteSmem<3, 32, 4> write3;
@@ -180,19 +189,24 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
             case kBpClaim: {
                 const int w0 = sg.arg * kHex20Wave, w1 = min(m.E_count, w0 + kHex20Wave);
                 const int b = w0 + k * kBatchClaim, e1 = min(w1, b + kBatchClaim);
-                claim_warp(m, L, nullptr, b + warp, kBatchWarps, e1, w0, bm.map[sg.arg & 1], sm.claim[warp]);
+                for (int gb = b; gb < e1; gb += kGroup)
+                    claim_group(m, L, nullptr, nullptr, gb, min(kGroup, e1 - gb),
+                                bm.map[sg.arg & 1] + (size_t)((gb - w0) / kGroup) * kGroupMapWords, sm.claim);
                 break;
             }
             case kBpValues: {
                 const int w0 = sg.arg * kHex20Wave, w1 = min(m.E_count, w0 + kHex20Wave);
-                const int b = w0 + k * kBatchValues, e1 = min(w1, b + kBatchValues);
+                const int b = w0 + k * kBatchValues, ne = min(kGroup, w1 - b);
+                group_topology(m, nullptr, b, ne, sm.gv.topo);
+                if (sm.gv.topo.bad) break;  // the claim item raised it
                 ValuesTarget vt{};
-                vt.map = bm.map[sg.arg & 1];
-                vt.map_origin = w0;
+                vt.topo = &sm.gv.topo;
+                vt.rec = bm.map[sg.arg & 1] + (size_t)((b - w0) / kGroup) * kGroupMapWords;
+                vt.g0 = b;
                 vt.vals = L.vals;
                 vt.info = L.info;
-                values_init(sm.values);
-                values_cta<kToSlots>(m, nullptr, b, 1, e1, vt, sm.values);
+                values_init(sm.gv.values);
+                values_cta<kToSlots>(m, nullptr, b, 1, b + ne, vt, sm.gv.values);
                 break;
             }
             case kBpScanReduce:

@@ -1,32 +1,35 @@
-// Hex20 A-LLS scatter, pass 1 of 2: list entries (the pattern) and the slot
-// map.
+// Hex20 A-LLS scatter, pass 1 of 2: list entries (the pattern) and the map
+// records of the element groups.
 //
 // Replaces the insert half of assembleGlobalStiffnessKernelALLSFixedArray
 // (ALLS_Hex20_3D_Assembly_Performance.cu:226-256: a linear scan of the row's
 // columns, a slot claimed with atomicAdd on the row count, no fence), whose
 // racing inserts duplicate or drop columns.
 //
-// One warp per element, persistent over the elements perm[i0, i1) (a wave of
-// the spatial element order). For each of the element's 20 row nodes the warp
-// copies the node's first list chunk (next link + S1 hashed slots, at most
-// 384 bytes) into shared memory with cp.async, all 20 rows at once, so the
-// element costs one round trip for its list reads instead of one per row.
-// Each lane then resolves its share of the 400 (row node, column node) pairs
-// in the shared copy: a column found on its probe sequence is an existing
-// entry; otherwise the first empty slot of the sequence is claimed with
-// atomicCAS(0 -> column + 1), all of the lane's claims in flight together. A
-// CAS that meets another column moves on along the sequence (slots are never
-// freed, so a column is found or placed at the first empty slot of its
-// sequence, never twice); a full chunk continues in the row's overflow chunks
-// (taken from the pool and linked with atomicCAS), read from global memory.
+// One CTA per element group (group_hex20.cuh: kGroup consecutive positions of
+// the spatial order), persistent over the groups of a wave. The CTA numbers
+// the group's nodes and node pairs, so an ordered pair (row node, column node)
+// that several of the group's elements share is resolved once. Row nodes go
+// in batches of kClaimRows: the batch's first list chunks (next link + S1
+// hashed slots, at most 384 bytes each) are copied into shared memory with
+// cp.async, then every thread resolves ordered pairs of the batch in the copy:
+// a column found on its probe sequence is an existing entry; otherwise the
+// first slot of the sequence that is empty in the copy is claimed with
+// atomicCAS(0 -> column + 1), moving on along the sequence when the CAS meets
+// a column that another group put there (slots are never freed, so a column
+// is found or placed at the first empty slot of its sequence, never twice). A
+// full first chunk continues in the row's overflow chunks (taken from the pool
+// and linked with atomicCAS), read from global memory.
 //
-// The claimer of a slot zeroes the slot's value block and counts the entry
-// for its row; every pair's global slot id goes to the slot map (i - i0) * 400
-// + 20 * I + J, which the value pass (values_hex20.cu, or the tensor-core form
-// in ke_tcgen05.cu) reads to add the element's Ke blocks with FP64 atomics.
-// The two passes are separate launches, so every value block is zeroed before
-// any addition reaches it and no entry is ever in a half-written state: no
-// pending flags, no fences, no waits.
+// Ownership: a pair {u, v} belongs to the group alone when u or v has every
+// one of its occurrences in the mesh (deg, counted once per mesh) inside the
+// group, since then every element with both nodes is one of the group's. The
+// value pass stores such a pair's blocks once; the claimer of any other slot
+// zeroes its value block for the atomic adds of several groups. Each claimed
+// entry is counted for its row, and the slot id (with the shared flag) goes to
+// the group's map record. The two passes are separate launches, so every
+// value block is zeroed before any addition reaches it and no entry is ever
+// in a half-written state: no pending flags, no fences, no waits.
 #include <algorithm>
 
 #include "claim_hex20.cuh"
@@ -34,20 +37,40 @@
 namespace fem {
 namespace {
 
-constexpr int kWarps = 4;
-constexpr int kThreads = kWarps * 32;
+constexpr int kThreads = 128;
 
 __global__ void __launch_bounds__(kThreads) k_claim_hex20(MeshView m, ListLayout L, const int* __restrict__ perm,
-                                                          int i0, int i1, int* __restrict__ map) {
-    __shared__ ClaimWarpSmem sm[kWarps];
-    const int w = threadIdx.x >> 5;
-    claim_warp(m, L, perm, (long long)i0 + blockIdx.x * kWarps + w, (long long)gridDim.x * kWarps, i1, i0, map, sm[w]);
+                                                          const int* __restrict__ deg, int i0, int i1,
+                                                          unsigned* __restrict__ map) {
+    __shared__ ClaimSmem sm;
+    const int ngroups = (i1 - i0 + kGroup - 1) / kGroup;
+    for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        const long long g0 = (long long)i0 + (long long)g * kGroup;
+        claim_group(m, L, perm, deg, g0, min(kGroup, i1 - (int)g0), map + (size_t)g * kGroupMapWords, sm);
+    }
+}
+
+__global__ void k_node_degree(MeshView m, int* __restrict__ deg) {
+    const long long n = (long long)m.E_count * 20;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const int v = __ldg(m.conn + k);
+        if (v >= 0 && v < m.N) atomicAdd(deg + v, 1);
+    }
 }
 
 }  // namespace
 
-cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int* perm, int i0, int i1, int* map,
-                               cudaStream_t s) {
+cudaError_t launch_node_degree(const MeshView& m, int* deg, cudaStream_t s) {
+    cudaError_t err = cudaMemsetAsync(deg, 0, (size_t)m.N * sizeof(int), s);
+    if (err || m.E_count <= 0) return err;
+    const long long n = (long long)m.E_count * 20;
+    const long long grid = std::max<long long>(1, std::min<long long>((n + 255) / 256, 8ll * sm_count()));
+    k_node_degree<<<(int)grid, 256, 0, s>>>(m, deg);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int* perm, const int* deg, int i0,
+                               int i1, unsigned* map, cudaStream_t s) {
     if (i1 <= i0) return cudaSuccess;
     static DeviceCache cache;
     int per_sm = 0;
@@ -55,9 +78,9 @@ cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int
         return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_claim_hex20, kThreads, 0);
     }, per_sm);
     if (err) return err;
-    const long long need = (i1 - i0 + kWarps - 1) / kWarps;
+    const long long need = (i1 - i0 + kGroup - 1) / kGroup;
     const long long grid = std::max<long long>(1, std::min<long long>(need, (long long)per_sm * sm_count()));
-    k_claim_hex20<<<(int)grid, kThreads, 0, s>>>(m, L, perm, i0, i1, map);
+    k_claim_hex20<<<(int)grid, kThreads, 0, s>>>(m, L, perm, deg, i0, i1, map);
     return cudaGetLastError();
 }
 

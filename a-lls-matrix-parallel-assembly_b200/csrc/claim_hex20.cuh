@@ -2,22 +2,23 @@
 // batched persistent kernel (batched.cu). See claim_hex20.cu for the method.
 #pragma once
 
-#include "launch.h"
+#include "group_hex20.cuh"
 
 namespace fem {
 namespace {
 
-constexpr int kClaimMaxWords = 96;   // first-chunk meta rows of at most 96 words (S1 <= 94, checked on the host)
-constexpr int kPairs = 400;
-constexpr int kPerLane = (kPairs + 31) / 32;  // 13
+constexpr int kClaimMaxWords = 96;  // first-chunk meta rows of at most 96 words (S1 <= 94, checked on the host)
+constexpr int kClaimRows = 32;      // row nodes whose first chunks are copied at once
 
 enum : unsigned char { kCFound = 0, kCTry = 1, kCClaimed = 2, kCChain = 3 };
 
-// Shared memory of one claiming warp.
-struct ClaimWarpSmem {
-    alignas(16) int view[20][kClaimMaxWords];  // first chunks of the element's 20 row nodes
-    int node[20];
-    int claims[20];                            // entries claimed per row node
+// Shared memory of one claiming CTA.
+struct ClaimSmem {
+    GroupTopo T;
+    alignas(16) int view[kClaimRows][kClaimMaxWords];  // first chunks of a batch of row nodes
+    int claims[kClaimRows];                            // entries claimed per row node of the batch
+    int obase[kClaimRows + 1];                         // ordered pairs before each row of the batch
+    unsigned inner[kNbWords];                          // nodes whose every element is in the group
 };
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
@@ -69,150 +70,130 @@ __device__ int resolve_chain(const ListLayout& L, int n, int key, int& spare, bo
     return -1;
 }
 
-// Claims of the elements at positions i = i_first, i_first + i_stride, ...
-// below i1 of the visit order perm (perm NULL: element i), by one warp; the
-// slot ids of position i go to map row i - map_origin. Every lane of the
-// warp calls it.
-__device__ __forceinline__ void claim_warp(const MeshView& m, const ListLayout& L, const int* __restrict__ perm,
-                                           long long i_first, long long i_stride, int i1, int map_origin,
-                                           int* __restrict__ map, ClaimWarpSmem& ws) {
-    const int lane = threadIdx.x & 31;
-    const int S1 = L.S1, H1 = L.H1;
+// Finds or claims column key `key` in the first chunk of row node rn, whose
+// copy (taken at the start of the batch) is `view`: the key's probe sequence
+// in the copy; the first slot empty in the copy is claimed with atomicCAS.
+// A CAS that meets another column moves on along the sequence: slots are
+// never freed, so a column sits at the first slot of its sequence that was
+// empty when it was inserted and is never inserted twice. Returns the slot
+// (state kCFound / kCClaimed) or kCChain when the first chunk's sequence is
+// full.
+__device__ __forceinline__ unsigned char claim_first_chunk(const ListLayout& L, int rn, const int* view, int key,
+                                                           int& slot) {
+    const int S1 = L.S1;
+    const int p0 = probe_start(key, S1);
+    int* meta = L.meta1 + (size_t)rn * L.H1 + 2;
+    const int* v = view + 2;
+    for (int t = 0; t < S1; t++) {
+        int s = p0 + t;
+        if (s >= S1) s -= S1;
+        const int x = v[s];
+        if (x == key) {
+            slot = s;
+            return kCFound;
+        }
+        if (x != 0) continue;
+        const int old = atomicCAS(meta + s, 0, key);
+        if (old == 0) {
+            slot = s;
+            return kCClaimed;
+        }
+        if (old == key) {
+            slot = s;
+            return kCFound;
+        }
+    }
+    return kCChain;
+}
+
+// Claim pass of the group of positions [g0, g0 + ne) of the visit order
+// (perm NULL: element i). deg: occurrences of every node in the whole mesh;
+// NULL makes every pair shared (every claimed block is zeroed). rec: the
+// group's map record. Every thread of the CTA calls it.
+__device__ void claim_group(const MeshView& m, const ListLayout& L, const int* __restrict__ perm,
+                            const int* __restrict__ deg, long long g0, int ne, unsigned* __restrict__ rec,
+                            ClaimSmem& sm) {
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
+    GroupTopo& T = sm.T;
+    if (tid < kNbWords) sm.inner[tid] = 0u;
+    group_topology(m, perm, g0, ne, T);
+    if (T.bad) {
+        if (tid == 0) raise_status(L.info, FEM_ERR_BAD_MESH);
+        __syncthreads();
+        return;
+    }
+    const int nu = T.nu;
+    if (deg) {
+        for (int u = tid; u < nu; u += nt)
+            if (T.gcount[u] == FEM_LDG(deg + T.node[u])) atomicOr(&sm.inner[u >> 5], 1u << (u & 31));
+    }
     int spare = -1;
-    int (*view)[kClaimMaxWords] = ws.view;
-    for (long long ii = i_first; ii < i1; ii += i_stride) {
-        const int i = (int)ii;
-        const int e = perm ? FEM_LDG(perm + i) : i;
-        int n = 0;
-        if (lane < 20) n = FEM_LDG(m.conn + (size_t)e * 20 + lane);
-        const bool bad = __any_sync(0xFFFFFFFFu, lane < 20 && (n < 0 || n >= m.N));
-        int* out = map + (size_t)(i - map_origin) * kPairs;
-        if (bad) {
-            if (lane == 0) raise_status(L.info, FEM_ERR_BAD_MESH);
-            for (int p = lane; p < kPairs; p += 32) out[p] = -1;
-            continue;
+    for (int rb = 0; rb < nu; rb += kClaimRows) {
+        const int nrows = min(kClaimRows, nu - rb);
+        // the batch's first chunks, H1 / 4 16-byte pieces each
+        const int pieces = L.H1 >> 2;
+        for (int q = tid; q < nrows * pieces; q += nt) {
+            const int r = q / pieces, k = q - r * pieces;
+            cp_async16(&sm.view[r][4 * k], L.meta1 + (size_t)T.node[rb + r] * L.H1 + 4 * k);
         }
-        if (lane < 20) {
-            ws.node[lane] = n;
-            ws.claims[lane] = 0;
-        }
-        __syncwarp();
-        // the 20 first chunks, H1 / 4 16-byte pieces each
-        const int pieces = H1 >> 2;
-        for (int q = lane; q < 20 * pieces; q += 32) {
-            const int I = q / pieces, k = q - I * pieces;
-            cp_async16(&view[I][4 * k], L.meta1 + (size_t)ws.node[I] * H1 + 4 * k);
+        if (tid < 32) {
+            int c = 0;
+            if (lane < nrows) {
+#pragma unroll
+                for (int w = 0; w < kNbWords; w++) c += __popc(T.nb[rb + lane][w]);
+            }
+            int incl = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+                if (lane >= d) incl += y;
+            }
+            if (lane < nrows) {
+                sm.obase[lane] = incl - c;
+                sm.claims[lane] = 0;
+            }
+            if (lane == nrows - 1) sm.obase[nrows] = incl;
         }
         cp_async_wait_all();
-        __syncwarp();
-        // resolve this lane's pairs p = lane + 32 k: row I = p / 20, column J = p % 20
-        int slot[kPerLane];
-        unsigned char st[kPerLane];
-#pragma unroll
-        for (int k = 0; k < kPerLane; k++) {
-            const int p = lane + 32 * k;
-            st[k] = kCFound;
-            slot[k] = -1;
-            if (p < kPairs) {
-                const int I = p / 20, J = p - 20 * I;
-                const int key = ws.node[J] + 1;
-                const int* v = view[I] + 2;
-                const int p0 = probe_start(key, S1);
-                st[k] = kCChain;
-                for (int t = 0; t < S1; t++) {
-                    int s = p0 + t;
-                    if (s >= S1) s -= S1;
-                    const int x = v[s];
-                    if (x == key) {
-                        st[k] = kCFound;
-                        slot[k] = s;
-                        break;
-                    }
-                    if (x == 0) {
-                        st[k] = kCTry;
-                        slot[k] = s;
-                        break;
-                    }
-                }
+        __syncthreads();
+        const int total = sm.obase[nrows];
+        for (int f = tid; f < total; f += nt) {
+            int lo = 0, hi = nrows - 1;  // the last row whose first pair is <= f
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (sm.obase[mid] <= f) lo = mid;
+                else hi = mid - 1;
             }
-        }
-        // all claims of the lane in flight at once
-        int old[kPerLane];
-#pragma unroll
-        for (int k = 0; k < kPerLane; k++) {
-            old[k] = 0;
-            if (st[k] == kCTry) {
-                const int p = lane + 32 * k, I = p / 20, J = p - 20 * I;
-                old[k] = atomicCAS(L.meta1 + (size_t)ws.node[I] * H1 + 2 + slot[k], 0, ws.node[J] + 1);
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < kPerLane; k++) {
-            if (st[k] != kCTry) continue;
-            const int p = lane + 32 * k, I = p / 20, J = p - 20 * I;
-            const int key = ws.node[J] + 1;
-            const int p0 = probe_start(key, S1);
-            int* meta = L.meta1 + (size_t)ws.node[I] * H1 + 2;
-            int s = slot[k], x = old[k];
-            st[k] = kCChain;
-            // walk on from the contested slot: slots non-empty in the copy stay
-            // non-empty, so only its empty ones are candidates
-            for (int t = 0; t < S1; t++) {
-                if (x == 0) {
-                    st[k] = kCClaimed;
-                    break;
-                }
-                if (x == key) {
-                    st[k] = kCFound;
-                    break;
-                }
-                int u = -1;
-                for (int r = 1; r < S1; r++) {
-                    int s2 = s + r;
-                    if (s2 >= S1) s2 -= S1;
-                    if (s2 == p0) break;  // wrapped around the sequence
-                    const int y = view[I][2 + s2];
-                    if (y == key) {
-                        u = s2;
-                        x = key;
-                        break;
-                    }
-                    if (y == 0) {
-                        u = s2;
-                        x = atomicCAS(meta + s2, 0, key);
-                        break;
-                    }
-                }
-                if (u < 0) break;  // no empty slot left on the sequence: overflow chunks
-                s = u;
-            }
-            slot[k] = s;
-        }
-        // global slot ids; overflow chunks for rows whose first chunk is full
-#pragma unroll
-        for (int k = 0; k < kPerLane; k++) {
-            const int p = lane + 32 * k;
-            if (p >= kPairs) continue;
-            const int I = p / 20, J = p - 20 * I;
-            const int rn = ws.node[I];
+            const int r = lo, u = rb + r;
+            const int v = nb_member(T, u, f - sm.obase[r]);
+            const int rn = T.node[u], key = T.node[v] + 1;
+            int slot = -1;
+            unsigned char st = claim_first_chunk(L, rn, sm.view[r], key, slot);
             int gid;
-            if (st[k] == kCChain) {
+            if (st == kCChain) {
                 bool claimed = false;
-                gid = resolve_chain(L, rn, ws.node[J] + 1, spare, claimed);
-                if (claimed) st[k] = kCClaimed;
+                gid = resolve_chain(L, rn, key, spare, claimed);
+                st = claimed ? kCClaimed : kCFound;
             } else {
-                gid = (int)slot_gid(L, rn, slot[k]);
+                gid = (int)slot_gid(L, rn, slot);
             }
-            if (st[k] == kCClaimed && gid >= 0) {
-                // values are kept for upper blocks only (row node <= column node)
-                if (rn <= ws.node[J]) zero_block(L.vals + (size_t)(unsigned)gid * 9);
-                atomicAdd(&ws.claims[I], 1);
+            const bool owned = ((sm.inner[u >> 5] >> (u & 31)) | (sm.inner[v >> 5] >> (v & 31))) & 1u;
+            if (gid >= 0 && st == kCClaimed) {
+                if (!owned) zero_block(L.vals + (size_t)(unsigned)gid * 9);
+                atomicAdd(&sm.claims[r], 1);
             }
-            out[p] = gid;
+            const unsigned word = gid < 0 ? kMapNone : ((unsigned)gid | (owned ? 0u : kPairShared));
+            if (u <= v) {
+                const int p = pair_index(T, u, v);
+                rec[2 * p] = word;
+                if (u == v) rec[2 * p + 1] = kMapNone;
+            } else {
+                rec[2 * pair_index(T, v, u) + 1] = word;
+            }
         }
-        __syncwarp();
-        if (lane < 20 && ws.claims[lane]) atomicAdd(L.counts + ws.node[lane], ws.claims[lane]);
-        __syncwarp();
+        __syncthreads();
+        if (tid < nrows && sm.claims[tid]) atomicAdd(L.counts + T.node[rb + tid], sm.claims[tid]);
+        __syncthreads();  // the batch's copies and counters are free
     }
 }
 

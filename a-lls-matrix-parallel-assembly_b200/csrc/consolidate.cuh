@@ -12,36 +12,6 @@ namespace {
 
 constexpr unsigned long long kEmptyKey = ~0ull;
 
-// Hex20 lists hold the values of their upper blocks only (row node <= column
-// node; claim_hex20.cu): the consolidation reads each lower block (n, c < n)
-// transposed from c's list. The 2-D lists hold every block.
-template <int DPN>
-constexpr bool kSymLists = DPN == 3;
-constexpr unsigned kTransposed = 0x80000000u;  // slot id flag: read the block transposed
-constexpr unsigned kNoSlot = 0xFFFFFFFFu;
-
-// Slot of column key `key` (column node + 1) in the list of row node `row`:
-// the key's probe sequence in each chunk of the chain; an empty slot on the
-// sequence means the key was never inserted (kNoSlot).
-__device__ __forceinline__ unsigned find_slot(const ListLayout& L, int row, int key) {
-    int c = row;
-    for (int step = 0; step < kMaxChainSteps; step++) {
-        const int* meta = chunk_meta(L, c);
-        const int S = chunk_cap(L, c);
-        const int p0 = probe_start(key, S);
-        for (int t = 0; t < S; t++) {
-            int s = p0 + t;
-            if (s >= S) s -= S;
-            const int v = ld_cg(meta + 2 + s) & kColMask;
-            if (v == key) return slot_gid(L, c, s);
-            if (v == 0) return kNoSlot;
-        }
-        const int nx = ld_cg(meta + 1);
-        if (nx == 0) return kNoSlot;
-        c = nx - 1;
-    }
-    return kNoSlot;
-}
 constexpr int kScanItems = kScanTile / kScanThreads;  // 16 nodes per thread
 
 __device__ __forceinline__ unsigned long long shfl_xor_u64(unsigned long long v, int m) {
@@ -310,15 +280,6 @@ __device__ void long_row_write(const ListLayout& L, int n, int u, long long base
 #pragma unroll
             for (int d = G / 2; d > 0; d >>= 1) sum[v] += __shfl_xor_sync(mask, sum[v], d);
         }
-        if constexpr (kSymLists<DPN>) {
-            if (col < n) {  // a lower block: the upper block (col, n), transposed
-                const unsigned g = find_slot(L, col, n + 1);
-                if (g == kNoSlot && glane == 0) raise_status(L.info, FEM_ERR_INTERNAL);
-#pragma unroll
-                for (int v = 0; v < B; v++)
-                    sum[v] = g == kNoSlot ? 0.0 : FEM_LDG(L.vals + (size_t)g * B + (v % DPN) * DPN + v / DPN);
-            }
-        }
         if (glane == 0) {
 #pragma unroll
             for (int a = 0; a < DPN; a++)
@@ -363,15 +324,6 @@ __device__ void long_row_write_bsr(const ListLayout& L, int n, int u, long long 
         for (int v = 0; v < B; v++) {
 #pragma unroll
             for (int d = G / 2; d > 0; d >>= 1) sum[v] += __shfl_xor_sync(mask, sum[v], d);
-        }
-        if constexpr (kSymLists<DPN>) {
-            if (col < n) {  // a lower block: the upper block (col, n), transposed
-                const unsigned g = find_slot(L, col, n + 1);
-                if (g == kNoSlot && glane == 0) raise_status(L.info, FEM_ERR_INTERNAL);
-#pragma unroll
-                for (int v = 0; v < B; v++)
-                    sum[v] = g == kNoSlot ? 0.0 : FEM_LDG(L.vals + (size_t)g * B + (v % DPN) * DPN + v / DPN);
-            }
         }
         if (glane == 0) {
             col_idx[base + k] = col;
@@ -543,21 +495,6 @@ __device__ __forceinline__ void write_batches(const ListLayout& L, const int* __
             const int expect = kMode == kOutUpper ? FEM_LDG(L.counts + n) : u;
             if (glane == 0 && (T != expect || u > T)) raise_status(L.info, FEM_ERR_INTERNAL);
         }
-        if constexpr (kSymLists<DPN> && kMode != kOutUpper) {
-            // a lower block (column node c < n) has its values in c's list, as
-            // the upper block (c, n): its slot, read transposed (bit 31)
-            __syncwarp();
-            const int Tl = valid ? min(T, NK) : 0;
-            for (int e = glane; e < Tl; e += G) {
-                const unsigned long long key = s_keys[grp][e];
-                const int col = (int)(key >> 32);
-                if (col < n) {
-                    const unsigned g = find_slot(L, col, n + 1);
-                    if (g == kNoSlot) raise_status(L.info, FEM_ERR_INTERNAL);
-                    else s_keys[grp][e] = (key & 0xFFFFFFFF00000000ull) | kTransposed | g;
-                }
-            }
-        }
         if (nb + nb_stride < nb_end) prefetch_first_chunk<G, kPre>(L, nb + nb_stride + grp, glane, pre_w, pre_next);
         t_sum += T;
         t_max = max(t_max, T);
@@ -587,9 +524,7 @@ __device__ __forceinline__ void write_batches(const ListLayout& L, const int* __
         // entry v of the node's k-th sorted block
         auto block_value = [&](int k, int v) -> double {
             if constexpr (DPN == 2) return reinterpret_cast<const double*>(&s_vals[grp][k][0])[v];
-            const unsigned g = (unsigned)s_keys[grp][k];
-            const int vv = (g & kTransposed) ? (v % DPN) * DPN + v / DPN : v;
-            return FEM_LDG(L.vals + (size_t)(g & ~kTransposed) * B + vv);
+            return FEM_LDG(L.vals + (size_t)(unsigned)s_keys[grp][k] * B + v);
         };
         // 3. write the dpn rows of the node (or its block row, or its upper rows)
         if (valid && kMode == kOutUpper) {

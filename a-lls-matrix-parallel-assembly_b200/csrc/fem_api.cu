@@ -54,6 +54,12 @@ fem_status check_mesh(const fem_mesh* m, bool device_pointers_needed = true) {
     return FEM_OK;
 }
 
+// Map records of one wave of the Hex20 scatter for a mesh of E elements.
+size_t hex20_map_bytes(int E) {
+    const size_t groups = ((size_t)std::min(E, kHex20Wave) + kHex20GroupSize - 1) / kHex20GroupSize;
+    return groups * kHex20GroupMapWords * sizeof(unsigned);
+}
+
 fem_status make_layout(const fem_mesh* m, const fem_opts* o, HostLayout& h) {
     fem_status st = check_mesh(m);
     if (st) return st;
@@ -107,8 +113,15 @@ fem_status make_layout(const fem_mesh* m, const fem_opts* o, HostLayout& h) {
         off += align_up((size_t)h.E * sizeof(int)) + align_up(4 * sizeof(int)) + align_up(nbuckets * sizeof(int)) +
                align_up(6 * sizeof(unsigned long long));
     }
-    h.off_map = off;  // Hex20: slot map of one wave of the two-pass scatter
-    if (h.kind == FEM_HEX20) off += align_up((size_t)std::min(h.E, kHex20Wave) * 400 * sizeof(int));
+    // Hex20: node degrees, the map records of one wave of the two-pass scatter,
+    // and (tensor-core form) the staged Ke of one wave
+    h.off_deg = off;
+    if (h.kind == FEM_HEX20) off += align_up((size_t)h.N * sizeof(int));
+    h.off_map = off;
+    if (h.kind == FEM_HEX20) off += align_up(hex20_map_bytes(h.E));
+    h.off_stage = off;
+    if (h.kind == FEM_HEX20 && o->precision == FEM_PREC_TC_F16X3)
+        off += align_up((size_t)std::min(h.E, kHex20Wave) * kPackedHex20 * sizeof(double));
     h.total = off;
     return FEM_OK;
 }
@@ -238,14 +251,18 @@ fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* wo
             align_up(nbuckets * sizeof(int)));
         err = launch_reorder_3d(m, hist, ranges, perm, bbox, sm_count(), s);
         // two-pass scatter in waves of the spatial order: a wave's claims
-        // (entries, zeroed value blocks, slot map) complete before its value
-        // pass, and the blocks it touches are still in L2 when the values arrive
-        int* map = reinterpret_cast<int*>(b + h.off_map);
+        // (entries, zeroed value blocks, map records) complete before its
+        // value pass, and the blocks it touches are still in L2 when the
+        // values arrive
+        int* deg = reinterpret_cast<int*>(b + h.off_deg);
+        unsigned* map = reinterpret_cast<unsigned*>(b + h.off_map);
+        double* stage = reinterpret_cast<double*>(b + h.off_stage);
         const long long wait_ns = wait_ns_of(opts ? opts->wait_limit_us : 0);
+        if (!err) err = launch_node_degree(m, deg, s);
         for (int i0 = 0; i0 < h.E && !err; i0 += kHex20Wave) {
             const int i1 = std::min(h.E, i0 + kHex20Wave);
-            err = launch_claim_hex20(m, L, perm, i0, i1, map, s);
-            if (!err) err = launch_values_hex20(m, L, precision, perm, i0, i1, map, ctas, wait_ns, s);
+            err = launch_claim_hex20(m, L, perm, deg, i0, i1, map, s);
+            if (!err) err = launch_values_hex20(m, L, precision, perm, i0, i1, map, stage, wait_ns, s);
         }
     } else {
         err = launch_reorder(m, hist, ranges, perm, sm_count(), s);
@@ -426,7 +443,7 @@ size_t batch_mesh_bytes(const fem_mesh& m, const fem_opts* opts, fem_status& st)
     HostLayout h;
     st = make_layout(&m, opts, h);
     if (st) return 0;
-    return h.total + (h.kind == FEM_HEX20 ? align_up((size_t)std::min(h.E, kHex20Wave) * 400 * sizeof(int)) : 0);
+    return h.total + (h.kind == FEM_HEX20 ? align_up(hex20_map_bytes(h.E)) : 0);
 }
 
 // Work items of one mesh in the batch schedule (an upper bound of the
@@ -528,8 +545,8 @@ fem_status fem_assemble_batched(const fem_mesh* meshes, int32_t n, const fem_opt
         bm.m = mesh_view(&meshes[i]);
         bm.L = device_layout(h, ws);
         bm.tiles = reinterpret_cast<long long*>(ws + h.off_tiles);
-        bm.map[0] = reinterpret_cast<int*>(ws + h.off_map);
-        bm.map[1] = reinterpret_cast<int*>(ws + h.total);
+        bm.map[0] = reinterpret_cast<unsigned*>(ws + h.off_map);
+        bm.map[1] = reinterpret_cast<unsigned*>(ws + h.total);
         bm.row_ptr = outs[i].row_ptr;
         bm.col_idx = outs[i].col_idx;
         bm.values = outs[i].values;

@@ -11,15 +11,15 @@
 // Chunk metadata is a row of H = S + 2 int32 words:
 //     word 0 = reserved (0)
 //     word 1 = next  (chunk id + 1 of the next chunk, 0 = none)
-//     word 2+s = slot s: 0 = empty, col+1 = column node col (published),
-//                (col+1) | kPending = claimed, values being written
+//     word 2+s = slot s: 0 = empty, col+1 = column node col
 // Within a chunk a column's slot is found by open addressing (linear probing
 // from a hash of the column); a chunk with no free slot on the probe sequence
-// continues in the next chunk. A slot is claimed by atomicCAS(0 -> col|pending),
-// so every column appears at most once per row. The claimer stores the initial
-// block values, fences, and publishes the column (clears kPending); other
-// contributors atomicAdd into published slots and wait (bounded) for pending
-// ones, but only after publishing their own claims, so no wait is circular.
+// continues in the next chunk. A slot is claimed by atomicCAS(0 -> col+1), so
+// every column appears at most once per row. Block values are never written by
+// a claim: they are zero before the first addition (2-D: the value array is
+// cleared with the lists; Hex20: the claimer zeroes the block in the claim
+// pass, and values are added in a later launch), so no contributor ever waits
+// for another.
 // Slot values are stored slot-major: vals[gid * B + v], B = dpn^2, where gid is
 // the global slot id (first-chunk slots first, then overflow-chunk slots), so a
 // slot's block is contiguous (one 32-byte sector in 2-D, 72 bytes for Hex20).
@@ -125,7 +125,6 @@ __device__ __forceinline__ int alloc_chunk(const ListLayout& L) {
 // Bound on retry loops (chunk chains, claims); hitting it raises FEM_ERR_TIMEOUT.
 constexpr int kMaxChainSteps = 1 << 20;
 
-constexpr int kPending = (int)0x80000000;
 constexpr int kColMask = 0x7FFFFFFF;
 
 // Start of the probe sequence of column key `key` (col + 1) in a chunk of S slots.
@@ -156,24 +155,13 @@ __device__ __forceinline__ int next_chunk(const ListLayout& L, int c, int& spare
     return nx - 1;
 }
 
-// Bounded wait until a pending slot is published. Returns false (and raises
-// FEM_ERR_TIMEOUT) if it is not published within the bound.
-constexpr int kMaxPendingSpins = 1 << 22;
-__device__ __forceinline__ bool wait_published(const ListLayout& L, const int* word) {
-    for (int i = 0; i < kMaxPendingSpins; i++) {
-        if ((ld_cg(word) & kPending) == 0) return true;
-        __nanosleep(32);
-    }
-    raise_status(L.info, FEM_ERR_TIMEOUT);
-    return false;
-}
-
 // Host-side layout description (sizes in bytes, offsets from the workspace base).
 struct HostLayout {
     int kind, dpn, B, N, E;
     int S1, S2, H1, H2, cap2;
     int num_tiles;  // scan tiles of kScanTile nodes
-    size_t off_info, off_meta1, off_meta2, off_vals, off_counts, off_ucounts, off_tiles, off_elist, off_map, total;
+    size_t off_info, off_meta1, off_meta2, off_vals, off_counts, off_ucounts, off_tiles, off_elist, off_deg, off_map,
+        off_stage, total;
     size_t meta1_bytes;
 };
 

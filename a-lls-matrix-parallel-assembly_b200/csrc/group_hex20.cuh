@@ -1,0 +1,169 @@
+// Element groups of the Hex20 list scatter (claim_hex20.cuh, values_group.cuh,
+// and the batched kernel).
+//
+// A group is kGroup consecutive positions of the spatial element order (a
+// 2x2x2 brick of a structured mesh in Morton order). Its kGroup * 20 node
+// occurrences name nu <= 160 distinct nodes, numbered u = 0..nu-1 in order of
+// first occurrence ("group-local nodes"). Two group-local nodes are
+// neighbours when some element of the group has both; node u's neighbour set
+// nb[u] (u included) is a 160-bit set, and the group's node pairs {u <= v}
+// (v in nb[u]) are numbered by
+//     pair_index(u, v) = ubase[u] + #{v' in nb[u] : u <= v' < v},
+// so pair {u, u} is ubase[u] and the pairs of u are contiguous.
+//
+// The claim pass resolves every ordered pair (row node u, column node v) of
+// the group once, however many of the group's elements have both nodes, and
+// writes the group's map record: word 2 * pair_index(u, v) holds the slot id
+// of (row u, column v) and word 2 * pair_index(u, v) + 1 the slot id of
+// (row v, column u) (kMapNone for a diagonal pair or an unresolved slot).
+// Bit 31 (kPairShared) marks a pair that elements outside the group also
+// have: its slots are zeroed by their claimer and receive atomic adds; the
+// other pairs belong to this group alone and their blocks are stored once.
+#pragma once
+
+#include "launch.h"
+
+namespace fem {
+namespace {
+
+constexpr int kGroup = 8;                        // elements per group
+constexpr int kGroupOcc = kGroup * 20;           // node occurrences of a group
+constexpr int kNbWords = kGroupOcc / 32;         // words of a set of group-local nodes
+constexpr int kGroupPairs = kGroup * 210;        // bound on a group's node pairs {u <= v}
+constexpr int kGroupMapWords = 2 * kGroupPairs;  // map record words per group
+constexpr unsigned kPairShared = 0x80000000u;    // map word flag: other groups add to the pair
+constexpr unsigned kMapNone = 0xFFFFFFFFu;       // map word of no slot
+static_assert(kNbWords * 32 == kGroupOcc, "whole words of group-local nodes");
+static_assert(kGroup == kHex20GroupSize && kGroupMapWords == kHex20GroupMapWords, "host-side sizes");
+static_assert(kHex20Wave % kGroup == 0, "waves of whole groups");
+
+// Whether a map word names a slot (slot ids are below 2^31 - 1: the layout
+// keeps the slot count below 2^31).
+__device__ __forceinline__ bool map_has_slot(unsigned w) { return (w & ~kPairShared) != (kMapNone & ~kPairShared); }
+
+struct GroupTopo {
+    int node[kGroupOcc];                   // group-local node u -> node id (u < nu)
+    int occ[kGroupOcc];                    // occurrence 20 e + a -> node id of node a of element e
+    int gcount[kGroupOcc];                 // occurrences of group-local node u in the group
+    unsigned nb[kGroupOcc][kNbWords];      // neighbour sets
+    unsigned first[kNbWords];              // occurrences that are their node's first
+    unsigned short ubase[kGroupOcc + 1];   // pair index of {u, u}; ubase[nu] = number of pairs
+    unsigned char lidx[kGroupOcc];         // occurrence -> group-local node
+    int ne, nu, npairs, bad;
+};
+
+// Pair index of {u, v}, u <= v, v in nb[u].
+__device__ __forceinline__ int pair_index(const GroupTopo& T, int u, int v) {
+    int r = T.ubase[u];
+    const int wu = u >> 5, wv = v >> 5;
+    for (int w = wu; w <= wv; w++) {
+        unsigned bits = T.nb[u][w];
+        if (w == wu) bits &= ~0u << (u & 31);
+        if (w == wv) bits &= (1u << (v & 31)) - 1u;
+        r += __popc(bits);
+    }
+    return r;
+}
+
+// The k-th (from 0) member of node u's neighbour set.
+__device__ __forceinline__ int nb_member(const GroupTopo& T, int u, int k) {
+    for (int w = 0; w < kNbWords; w++) {
+        unsigned bits = T.nb[u][w];
+        const int c = __popc(bits);
+        if (k < c) {
+            for (int i = 0; i < k; i++) bits &= bits - 1u;
+            return 32 * w + __ffs(bits) - 1;
+        }
+        k -= c;
+    }
+    return -1;
+}
+
+// Topology of the group of positions [g0, g0 + ne) of the visit order perm
+// (NULL: element i is position i). Every thread of the CTA calls it; it ends
+// with a barrier. A node id outside [0, N) sets T.bad (and leaves the rest
+// undefined).
+__device__ void group_topology(const MeshView& m, const int* __restrict__ perm, long long g0, int ne, GroupTopo& T) {
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
+    const int nocc = ne * 20;
+    if (tid == 0) {
+        T.bad = 0;
+        T.ne = ne;
+    }
+    if (tid < kNbWords) T.first[tid] = 0;
+    for (int k = tid; k < kGroupOcc * kNbWords; k += nt) (&T.nb[0][0])[k] = 0u;
+    for (int k = tid; k < kGroupOcc; k += nt) T.gcount[k] = 0;
+    __syncthreads();
+    for (int k = tid; k < nocc; k += nt) {
+        const long long i = g0 + k / 20;
+        const int e = perm ? FEM_LDG(perm + i) : (int)i;
+        const int n = FEM_LDG(m.conn + (size_t)e * 20 + k % 20);
+        T.occ[k] = n;
+        if (n < 0 || n >= m.N) T.bad = 1;
+    }
+    __syncthreads();
+    if (T.bad) return;  // uniform
+    // first occurrence of each occurrence's node
+    for (int k = tid; k < nocc; k += nt) {
+        const int n = T.occ[k];
+        int j = 0;
+        while (T.occ[j] != n) j++;
+        T.lidx[k] = (unsigned char)j;
+        if (j == k) atomicOr(&T.first[k >> 5], 1u << (k & 31));
+    }
+    __syncthreads();
+    // group-local node = rank of the first occurrence among the first occurrences
+    for (int k = tid; k < nocc; k += nt) {
+        const int j = T.lidx[k];
+        int u = __popc(T.first[j >> 5] & ((1u << (j & 31)) - 1u));
+        for (int w = 0; w < (j >> 5); w++) u += __popc(T.first[w]);
+        T.lidx[k] = (unsigned char)u;
+        if (j == k) T.node[u] = T.occ[k];
+    }
+    __syncthreads();
+    // neighbour sets (every node pair of every element, the node itself included)
+    for (int k = tid; k < ne * 400; k += nt) {
+        const int e = k / 400, p = k - 400 * e, a = p / 20, b = p - 20 * a;
+        const int u = T.lidx[20 * e + a], v = T.lidx[20 * e + b];
+        atomicOr(&T.nb[u][v >> 5], 1u << (v & 31));
+    }
+    for (int k = tid; k < nocc; k += nt) atomicAdd(&T.gcount[T.lidx[k]], 1);
+    __syncthreads();
+    // pair numbering: ubase = exclusive prefix of the counts of {u <= v}
+    if (tid < 32) {
+        int nu = 0;
+#pragma unroll
+        for (int w = 0; w < kNbWords; w++) nu += __popc(T.first[w]);
+        int carry = 0;
+        for (int u0 = 0; u0 < nu; u0 += 32) {
+            const int u = u0 + lane;
+            int c = 0;
+            if (u < nu) {
+#pragma unroll
+                for (int w = 0; w < kNbWords; w++) {
+                    unsigned bits = T.nb[u][w];
+                    if (w < (u >> 5)) bits = 0u;
+                    else if (w == (u >> 5)) bits &= ~0u << (u & 31);
+                    c += __popc(bits);
+                }
+            }
+            int incl = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+                if (lane >= d) incl += y;
+            }
+            if (u < nu) T.ubase[u] = (unsigned short)(carry + incl - c);
+            carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
+        }
+        if (lane == 0) {
+            T.ubase[nu] = (unsigned short)carry;
+            T.nu = nu;
+            T.npairs = carry;
+        }
+    }
+    __syncthreads();
+}
+
+}  // namespace
+}  // namespace fem

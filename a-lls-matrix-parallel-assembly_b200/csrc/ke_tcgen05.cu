@@ -146,17 +146,16 @@ __device__ __forceinline__ unsigned pack_half2(__half lo, __half hi) {
 // Outputs of the kernel.
 enum TcOut : int {
     kTcPacked = 0,  // the packed Ke of every element to ke_out (fem_element_stiffness)
-    kTcSlots = 1,   // value pass of the two-pass Hex20 list scatter: each upper Ke block added
-                    // with FP64 atomics to its list slot (slot map of claim_hex20.cu)
+    kTcWave = 1,    // the packed Ke of a wave's elements perm[i0, i1) to ke_out, row q - i0 for
+                    // position q (staging of the group value pass, values_hex20.cu)
     kTcCsrMap = 2   // value-only re-assembly: Ke_IJ and its transpose added with FP64 atomics at
                     // their CSR positions (scatter map, row e)
 };
 
-// Elements and targets of the kTcSlots / kTcCsrMap modes.
+// Elements and targets of the kTcWave / kTcCsrMap modes.
 struct SlotTarget {
-    const int* perm;     // visit order: positions [i0, i1) (kTcSlots), all elements (kTcCsrMap)
-    const int* map;      // slot map (row i - i0) or scatter map (row e)
-    double* vals;        // list values (kTcSlots)
+    const int* perm;     // visit order: positions [i0, i1) (kTcWave), all elements (kTcCsrMap)
+    const int* map;      // scatter map, row e (kTcCsrMap)
     const int* row_ptr;  // the CSR (kTcCsrMap)
     double* csr;
     int i0, i1;
@@ -169,12 +168,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
     extern __shared__ __align__(128) unsigned char smem_raw[];
     KeTcSmem& sm = *reinterpret_cast<KeTcSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr bool kSlots = kMode == kTcSlots, kMap = kMode == kTcCsrMap;
-    // elements: positions q of the wave (kTcSlots), of perm (kTcCsrMap) or the mesh's elements q
-    const long long count = kSlots ? (long long)(tgt.i1 - tgt.i0) : (long long)m.E_count;
+    constexpr bool kWave = kMode == kTcWave, kMap = kMode == kTcCsrMap;
+    // elements: positions q of the wave (kTcWave), of perm (kTcCsrMap) or the mesh's elements q
+    const long long count = kWave ? (long long)(tgt.i1 - tgt.i0) : (long long)m.E_count;
     const long long npairs = (count + 1) / 2;
     auto elem = [&](long long q) -> long long {
-        return kSlots ? (long long)__ldg(tgt.perm + tgt.i0 + q) : (kMap ? (long long)__ldg(tgt.perm + q) : q);
+        return kWave ? (long long)__ldg(tgt.perm + tgt.i0 + q) : (kMap ? (long long)__ldg(tgt.perm + q) : q);
     };
     const uint32_t bar = smem_u32(&sm.mbar);
 
@@ -406,9 +405,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
             double* out = sm.ke[e] + 9 * (I * 20 - I * (I - 1) / 2 - I) + 3 * a;  // + 9 J: block (I, J)
             const long long q = 2 * p + e;  // the element's position in the wave / in perm
             const long long eid = (kMap && q < count) ? elem(q) : 0;
-            const int* mrow = tgt.map + (size_t)(kSlots && q < count ? q : (kMap ? eid : 0)) * 400;
+            const int* mrow = tgt.map + (size_t)eid * 400;
             // elements with a bad node id have no map entries (-1): nothing is added
-            const bool add = (kSlots || kMap) && real && q < count;
+            const bool add = kMap && real && q < count;
 #pragma unroll
             for (int J = 0; J < 20; J++) {
                 const int c = 32 * (J / 10) + 3 * (J % 10);
@@ -430,23 +429,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
                 const float k0 = fmaf(lam, o0, fmaf(mu, T0, a == 0 ? mtr : 0.0f));
                 const float k1 = fmaf(lam, o1, fmaf(mu, T1, a == 1 ? mtr : 0.0f));
                 const float k2 = fmaf(lam, o2, fmaf(mu, T2, a == 2 ? mtr : 0.0f));
-                if (kSlots) {
-                    // the lists hold upper blocks only (row node <= column node):
-                    // row a of Ke_IJ goes to (row I, column J) as it is, or
-                    // transposed, as column a of (row J, column I)
-                    if (add && J >= I) {
-                        const double v0 = (double)k0 * inv_s2, v1 = (double)k1 * inv_s2, v2 = (double)k2 * inv_s2;
-                        const bool upper = sm.nodes[e][I] <= sm.nodes[e][J];
-                        const int g = __ldg(mrow + (upper ? I * 20 + J : J * 20 + I));
-                        if (g >= 0) {
-                            double* d = tgt.vals + (size_t)(unsigned)g * 9 + (upper ? 3 * a : a);
-                            const int st = upper ? 1 : 3;
-                            atomicAdd(d, v0);
-                            atomicAdd(d + st, v1);
-                            atomicAdd(d + 2 * st, v2);
-                        }
-                    }
-                } else if (kMap) {
+                if (kMap) {
                     // the CSR holds both triangles: row a of Ke_IJ at block (I, J),
                     // and, transposed, column a of block (J, I)
                     if (add && J >= I) {
@@ -484,8 +467,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
             sm.bound_bits[tid] = 0ull;
             sm.negmask[tid] = 0u;
         }
-        if (kSlots || kMap) continue;
-        const int nvalid = 2 * p + 1 < m.E_count ? 2 : 1;
+        if (kMap) continue;
+        const int nvalid = 2 * p + 1 < count ? 2 : 1;
         double* dst = ke_out + (size_t)(2 * p) * kPackedHex20;
         if (bulk_out) {
             if (tid == 0) {
@@ -505,7 +488,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_hex20_ke_tc(MeshView m, double*
     // caller to treat the device as suspect.
     if (timed_out && !mbar_wait_bounded(bar, parity ^ 1u, kDefaultWaitNs) && tid == 0)
         atomicOr(status, 1 << FEM_ERR_INTERNAL);
-    if (tid == 0 && bulk_out && !kSlots && !kMap) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    if (tid == 0 && bulk_out && !kMap) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
@@ -540,10 +523,10 @@ cudaError_t launch_tc(const MeshView& m, double* ke_out, int* status, const Slot
         return cudaSuccess;
     }, blocks_per_sm);
     if (err) return err;
-    const long long count = kMode == kTcSlots ? (long long)(tgt.i1 - tgt.i0) : (long long)m.E_count;
+    const long long count = kMode == kTcWave ? (long long)(tgt.i1 - tgt.i0) : (long long)m.E_count;
     const long long npairs = (count + 1) / 2;
     const long long grid = std::max<long long>(1, std::min<long long>((long long)blocks_per_sm * sm_count(), npairs));
-    const int bulk_out = kMode == kTcPacked && (reinterpret_cast<uintptr_t>(ke_out) & 15u) == 0;
+    const int bulk_out = kMode != kTcCsrMap && (reinterpret_cast<uintptr_t>(ke_out) & 15u) == 0;
     k_hex20_ke_tc<kMode><<<(int)grid, kThreads, smem, s>>>(m, ke_out, status, bulk_out, tgt);
     return cudaGetLastError();
 }
@@ -557,17 +540,16 @@ cudaError_t launch_hex20_ke_tcgen05(const MeshView& m, double* ke_out, int* stat
     return launch_tc<kTcPacked>(m, ke_out, status, t, s);
 }
 
-cudaError_t launch_values_hex20_tc(const MeshView& m, const ListLayout& L, const int* perm, int i0, int i1,
-                                   const int* map, long long wait_ns, cudaStream_t s) {
+cudaError_t launch_stage_hex20_tc(const MeshView& m, const int* perm, int i0, int i1, double* stage, int* status,
+                                  long long wait_ns, cudaStream_t s) {
     if (i1 <= i0) return cudaSuccess;
-    return launch_tc<kTcSlots>(m, nullptr, &L.info->status_bits,
-                               SlotTarget{perm, map, L.vals, nullptr, nullptr, i0, i1, wait_ns}, s);
+    return launch_tc<kTcWave>(m, stage, status, SlotTarget{perm, nullptr, nullptr, nullptr, i0, i1, wait_ns}, s);
 }
 
 cudaError_t launch_reassemble_hex20_tc(const MeshView& m, const int* perm, const MapTarget& mt, DevInfo* info,
                                        cudaStream_t s) {
     return launch_tc<kTcCsrMap>(m, nullptr, &info->status_bits,
-                                SlotTarget{perm, mt.map, nullptr, mt.row_ptr, mt.values, 0, m.E_count,
+                                SlotTarget{perm, mt.map, mt.row_ptr, mt.values, 0, m.E_count,
                                            wait_ns_of(0)},
                                 s);
 }

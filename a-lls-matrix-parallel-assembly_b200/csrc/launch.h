@@ -101,22 +101,29 @@ cudaError_t launch_reassemble_hex20(const MeshView& m, int precision, const int*
 cudaError_t launch_colour_hex20(const MeshView& m, const int* perm, const int* range, const MapTarget& t,
                                 DevInfo* info, cudaStream_t s);
 
-// Two-pass Hex20 list scatter over the elements perm[i0, i1) (one wave):
-// pass 1 claims the list entries, zeroes the claimed value blocks and writes
-// the slot map [(i1 - i0) * 400] (claim_hex20.cu); pass 2 adds the Ke blocks
-// at the mapped slots (values_hex20.cu in FP64, ke_tcgen05.cu in the
-// tensor-core form). wait_ns: see wait_ns_of.
-cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int* perm, int i0, int i1, int* map,
-                               cudaStream_t s);
+// Two-pass Hex20 list scatter over the element groups of positions
+// perm[i0, i1) (one wave; i0 a multiple of the group size). deg: occurrences
+// of every node in the mesh (launch_node_degree). Pass 1 claims the list
+// entries, zeroes the value blocks of the entries several groups add to and
+// writes the groups' map records (claim_hex20.cu); pass 2 adds the Ke blocks
+// (values_hex20.cu; in the tensor-core form the wave's Ke are computed into
+// stage first, ke_tcgen05.cu). map: kHex20WaveMapWords words; stage:
+// kHex20Wave * kPackedHex20 doubles (tensor-core form only). wait_ns: see
+// wait_ns_of.
+cudaError_t launch_node_degree(const MeshView& m, int* deg, cudaStream_t s);
+cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int* perm, const int* deg, int i0,
+                               int i1, unsigned* map, cudaStream_t s);
 cudaError_t launch_values_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm, int i0,
-                                int i1, const int* map, int ctas_per_sm, long long wait_ns, cudaStream_t s);
-cudaError_t launch_values_hex20_fp64(const MeshView& m, const ListLayout& L, const int* perm, int i0, int i1,
-                                     const int* map, int ctas_per_sm, cudaStream_t s);
-cudaError_t launch_values_hex20_tc(const MeshView& m, const ListLayout& L, const int* perm, int i0, int i1,
-                                   const int* map, long long wait_ns, cudaStream_t s);
+                                int i1, const unsigned* map, double* stage, long long wait_ns, cudaStream_t s);
+// The packed Ke of the elements perm[i0, i1) on the tensor cores, row q - i0 for position q.
+cudaError_t launch_stage_hex20_tc(const MeshView& m, const int* perm, int i0, int i1, double* stage, int* status,
+                                  long long wait_ns, cudaStream_t s);
 // Elements per wave of the two-pass scatter: the value blocks a wave's claims
-// zero (about 17 KB per element) stay in L2 until its value pass adds to them.
+// zero stay in L2 until its value pass adds to them.
 constexpr int kHex20Wave = 4096;
+constexpr int kHex20GroupSize = 8;            // elements per group (group_hex20.cuh)
+constexpr int kHex20GroupMapWords = 3360;     // map record words per group (2 x 210 x 8)
+constexpr size_t kHex20WaveMapWords = (size_t)kHex20Wave / kHex20GroupSize * kHex20GroupMapWords;
 
 // Spatial (3-D Morton bucket) element order; hist needs 1 << (3 * morton_bits(E)) ints, bbox 6 words.
 int morton_bits(int num_elems);
@@ -157,7 +164,7 @@ struct BatchMesh {
     MeshView m;
     ListLayout L;
     long long* tiles;          // scan partials
-    int* map[2];               // Hex20: slot maps of even / odd waves
+    unsigned* map[2];          // Hex20: map records of even / odd waves
     int* row_ptr;              // the caller's CSR
     int* col_idx;
     double* values;
@@ -189,8 +196,8 @@ struct BatchSegment {
 // Work item sizes.
 constexpr int kBatchResetBytes = 1 << 20;  // bytes cleared per reset item
 constexpr int kBatchScatter2D = 2048;      // 2-D elements per scatter item
-constexpr int kBatchClaim = 64;            // Hex20 elements per claim item (8 warps, one element each)
-constexpr int kBatchValues = 16;           // Hex20 elements per value item (one CTA, one element at a time)
+constexpr int kBatchClaim = 64;            // Hex20 elements per claim item (element groups, one at a time)
+constexpr int kBatchValues = 8;            // Hex20 elements per value item (one group, one element at a time)
 constexpr int kBatchWriteBatches = 16;     // node batches per write item
 
 // Copies the tables into the workspace and zeroes the counters and the

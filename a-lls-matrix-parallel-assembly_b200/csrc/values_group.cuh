@@ -1,0 +1,240 @@
+// Device code of the Hex20 group value pass (values_hex20.cu). See
+// values_hex20.cu for the method.
+#pragma once
+
+#include "group_hex20.cuh"
+#include "values_hex20.cuh"
+
+namespace fem {
+namespace {
+
+struct GroupValuesSmem {
+    double acc[kGroupPairs * 9];  // the group's node-pair blocks, pair index-major (row node u <= column node v)
+    double dN[3][20][KS];         // dN_n / dxi_i at Gauss point g: [i][n][g]
+    double X[kGroup][20][3];      // per warp: its element's node coordinates
+    double iJw[kGroup][KS][10];   // per warp: inverse Jacobian (9) and weight * detJ at each Gauss point; row 27 zero
+    double lam[kGroup], mu[kGroup];
+    GroupTopo T;
+    unsigned char pI[210], pJ[210];  // packed upper block p -> node pair (I, J), I <= J
+};
+
+// Adds the element block Ke_IJ (row-major 3x3, element nodes I <= J of the
+// group's element w) to the group's block of its node pair, transposed when
+// the pair's lower group-local node is J's. Shared-memory FP64 atomics: the
+// group's elements are added at the same time by different warps.
+__device__ __forceinline__ void group_add_block(GroupValuesSmem& sm, int w, int I, int J, const double (&k)[9]) {
+    const GroupTopo& T = sm.T;
+    const int u = T.lidx[20 * w + I], v = T.lidx[20 * w + J];
+    if (u <= v) {
+        double* a = sm.acc + 9 * pair_index(T, u, v);
+#pragma unroll
+        for (int q = 0; q < 9; q++) atomicAdd(a + q, k[q]);
+        if (u == v && I != J) {  // an element with a repeated node: both orientations land on one block
+#pragma unroll
+            for (int q = 0; q < 9; q++) atomicAdd(a + (q % 3) * 3 + q / 3, k[q]);
+        }
+    } else {
+        double* a = sm.acc + 9 * pair_index(T, v, u);
+#pragma unroll
+        for (int q = 0; q < 9; q++) atomicAdd(a + (q % 3) * 3 + q / 3, k[q]);
+    }
+}
+
+// Tables of the group value pass; every thread of the CTA calls it once.
+__device__ __forceinline__ void values_group_init(GroupValuesSmem& sm) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int idx = tid; idx < 27 * 20; idx += nt) {
+        const int g = idx / 20, n = idx - 20 * g;
+        double dx, dy, dz;
+        hex20::dshape_node(n, hex20::gauss3(g / 9), hex20::gauss3((g / 3) % 3), hex20::gauss3(g % 3), dx, dy, dz);
+        sm.dN[0][n][g] = dx;
+        sm.dN[1][n][g] = dy;
+        sm.dN[2][n][g] = dz;
+    }
+    for (int idx = tid; idx < 3 * 20; idx += nt) sm.dN[idx / 20][idx % 20][27] = 0.0;
+    for (int idx = tid; idx < kGroup * KS * 10; idx += nt) (&sm.iJw[0][0][0])[idx] = 0.0;
+    for (int idx = tid; idx < kGroupPairs * 9; idx += nt) sm.acc[idx] = 0.0;
+    if (tid < 20) {
+        const int I = tid, p0 = I * 20 - I * (I - 1) / 2;  // packed index of block (I, I)
+        for (int J = I; J < 20; J++) {
+            sm.pI[p0 + J - I] = (unsigned char)I;
+            sm.pJ[p0 + J - I] = (unsigned char)J;
+        }
+    }
+    __syncthreads();
+}
+
+// Ke of the group's element w (node ids in T.occ, element id e), computed by
+// one warp and added to the group's blocks.
+__device__ __forceinline__ void group_element_fp64(const MeshView& m, int e, int w, DevInfo* info,
+                                                   GroupValuesSmem& sm) {
+    const int lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
+    if (lane < 20) {
+        const int n = sm.T.occ[20 * w + lane];
+        sm.X[w][lane][0] = FEM_LDG(m.x + n);
+        sm.X[w][lane][1] = FEM_LDG(m.y + n);
+        sm.X[w][lane][2] = FEM_LDG(m.z + n);
+    }
+    if (lane == 20) {
+        const double E = m.E ? FEM_LDG(m.E + e) : m.E0;
+        const double nu = m.nu ? FEM_LDG(m.nu + e) : m.nu0;
+        sm.lam[w] = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+        sm.mu[w] = E / (2.0 * (1.0 + nu));
+    }
+    __syncwarp();
+    if (lane < 27) {
+        // Jacobian at Gauss point g = lane: J[3i + j] = sum_n dN[i][n][g] X[n][j]
+        const int g = lane;
+        double J[9];
+#pragma unroll
+        for (int r = 0; r < 9; r++) J[r] = 0.0;
+#pragma unroll 4
+        for (int n = 0; n < 20; n++) {
+            const double d0 = sm.dN[0][n][g], d1 = sm.dN[1][n][g], d2 = sm.dN[2][n][g];
+            const double x0 = sm.X[w][n][0], x1 = sm.X[w][n][1], x2 = sm.X[w][n][2];
+            J[0] = fma(d0, x0, J[0]);
+            J[1] = fma(d0, x1, J[1]);
+            J[2] = fma(d0, x2, J[2]);
+            J[3] = fma(d1, x0, J[3]);
+            J[4] = fma(d1, x1, J[4]);
+            J[5] = fma(d1, x2, J[5]);
+            J[6] = fma(d2, x0, J[6]);
+            J[7] = fma(d2, x1, J[7]);
+            J[8] = fma(d2, x2, J[8]);
+        }
+        const double c0 = J[4] * J[8] - J[5] * J[7], c1 = J[5] * J[6] - J[3] * J[8], c2 = J[3] * J[7] - J[4] * J[6];
+        const double det = J[0] * c0 + J[1] * c1 + J[2] * c2;
+        if (!(det > 0.0)) raise_status(info, FEM_ERR_DETJ);
+        const double r = 1.0 / det;
+        double* o = sm.iJw[w][g];
+        o[0] = c0 * r;
+        o[1] = (J[2] * J[7] - J[1] * J[8]) * r;
+        o[2] = (J[1] * J[5] - J[2] * J[4]) * r;
+        o[3] = c1 * r;
+        o[4] = (J[0] * J[8] - J[2] * J[6]) * r;
+        o[5] = (J[2] * J[3] - J[0] * J[5]) * r;
+        o[6] = c2 * r;
+        o[7] = (J[1] * J[6] - J[0] * J[7]) * r;
+        o[8] = (J[0] * J[4] - J[1] * J[3]) * r;
+        o[9] = hex20::weight3(g / 9) * hex20::weight3((g / 3) % 3) * hex20::weight3(g % 3) * det;
+    }
+    __syncwarp();
+    // physical gradients of the lane's (node, Gauss point) entries, held in
+    // registers: G[t][s][a] = dN_n / dx_a at g, n = 8 t + fr, g = 4 s + fc
+    // (zero in the padding n >= 20, g = 27)
+    double G[3][7][3], wk[7];
+#pragma unroll
+    for (int s = 0; s < 7; s++) {
+        const int g = 4 * s + fc;
+        const double* iJ = sm.iJw[w][g];
+        wk[s] = iJ[9];
+#pragma unroll
+        for (int t = 0; t < 3; t++) {
+            const int n = 8 * t + fr;
+            const bool ok = n < 20 && g < 27;
+            const int nn = ok ? n : 0;
+            const double d0 = sm.dN[0][nn][g], d1 = sm.dN[1][nn][g], d2 = sm.dN[2][nn][g];
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+                G[t][s][a] = ok ? fma(iJ[3 * a], d0, fma(iJ[3 * a + 1], d1, iJ[3 * a + 2] * d2)) : 0.0;
+        }
+    }
+    const double lam = sm.lam[w], mu = sm.mu[w];
+    // the six 8x8 tile positions (ti <= tj) of the upper triangle of the
+    // 24 x 24 node grid; all nine M^{ab} tiles of each on the FP64 tensor cores
+#pragma unroll
+    for (int tile = 0; tile < 6; tile++) {
+        const int ti = tile < 3 ? 0 : (tile < 5 ? 1 : 2);
+        const int tj = tile == 0 ? 0 : (tile == 1 || tile == 3 ? 1 : 2);
+        double c[3][3][2];
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++) c[a][b][0] = c[a][b][1] = 0.0;
+#pragma unroll
+        for (int s = 0; s < 7; s++) {
+            double A[3];
+#pragma unroll
+            for (int a = 0; a < 3; a++) A[a] = wk[s] * G[ti][s][a];
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+                for (int b = 0; b < 3; b++) dmma(c[a][b][0], c[a][b][1], A[a], G[tj][s][b]);
+        }
+        const int I = 8 * ti + fr;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int J = 8 * tj + 2 * fc + h;
+            if (I >= 20 || J >= 20 || (ti == tj && J < I)) continue;
+            const double mtr = mu * (c[0][0][h] + c[1][1][h] + c[2][2][h]);
+            double k[9];
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+                for (int b = 0; b < 3; b++)
+                    k[3 * a + b] = fma(lam, c[a][b][h], fma(mu, c[b][a][h], a == b ? mtr : 0.0));
+            group_add_block(sm, w, I, J, k);
+        }
+    }
+}
+
+// Group value pass over the groups of positions [i0, i1) of the visit order
+// perm, group g = blockIdx.x, blockIdx.x + gridDim.x, ...; map record of
+// group g at map + g * kGroupMapWords. stage: NULL (Ke in FP64 here) or the
+// packed upper Ke blocks of the wave's elements, row q - i0 for position q
+// (the tensor-core form). kGroup warps; every thread calls it.
+__device__ void values_group(const MeshView& m, const int* __restrict__ perm, int i0, int i1,
+                             const unsigned* __restrict__ map, const double* __restrict__ stage, double* vals,
+                             DevInfo* info, GroupValuesSmem& sm) {
+    const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31;
+    const int ngroups = (i1 - i0 + kGroup - 1) / kGroup;
+    for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        const long long g0 = (long long)i0 + (long long)g * kGroup;
+        const int ne = min(kGroup, i1 - (int)g0);
+        group_topology(m, perm, g0, ne, sm.T);
+        if (sm.T.bad) {  // the claim pass raised it; the group adds nothing
+            __syncthreads();
+            continue;
+        }
+        if (warp < ne) {
+            const int e = perm ? FEM_LDG(perm + g0 + warp) : (int)(g0 + warp);
+            if (stage) {
+                const double* ke = stage + (size_t)(g0 + warp - i0) * kPackedHex20;
+                for (int p = lane; p < 210; p += 32) {
+                    double k[9];
+#pragma unroll
+                    for (int q = 0; q < 9; q++) k[q] = FEM_LDG(ke + 9 * p + q);
+                    group_add_block(sm, warp, sm.pI[p], sm.pJ[p], k);
+                }
+            } else {
+                group_element_fp64(m, e, warp, info, sm);
+            }
+        }
+        __syncthreads();
+        // every block of the group once: stored where the group is the pair's
+        // only contributor, added atomically where other groups add too;
+        // (row u, column v) as accumulated, (row v, column u) transposed
+        const unsigned* rec = map + (size_t)g * kGroupMapWords;
+        const int n9 = sm.T.npairs * 9;
+        for (int idx = tid; idx < n9; idx += nt) {
+            const int r = idx / 9, q = idx - 9 * r;
+            const double val = sm.acc[idx];
+            sm.acc[idx] = 0.0;
+            const unsigned w0 = FEM_LDG(rec + 2 * r), w1 = FEM_LDG(rec + 2 * r + 1);
+            if (map_has_slot(w0)) {
+                double* d = vals + (size_t)(w0 & ~kPairShared) * 9 + q;
+                if (w0 & kPairShared) atomicAdd(d, val);
+                else *d = val;
+            }
+            if (map_has_slot(w1)) {
+                double* d = vals + (size_t)(w1 & ~kPairShared) * 9 + (q % 3) * 3 + q / 3;
+                if (w1 & kPairShared) atomicAdd(d, val);
+                else *d = val;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+}  // namespace fem

@@ -1,6 +1,8 @@
-// Hex20 A-LLS scatter, pass 2 of 2: element stiffness in FP64 and the atomic
+// Hex20 A-LLS scatter, pass 2 of 2: element stiffness in FP64 and the
 // accumulation of its blocks into the list entries that pass 1
-// (claim_hex20.cu) claimed and mapped.
+// (claim_hex20.cu) claimed and recorded in the groups' map records; also the
+// CTA-cooperative element pass of the value-only re-assembly and of the
+// colouring baseline.
 //
 // Replaces the value half of assembleGlobalStiffnessKernelALLSFixedArray
 // (ALLS_Hex20_3D_Assembly_Performance.cu:212-256: one thread per element with
@@ -15,22 +17,34 @@
 //     Ke_IJ[a][b] = lambda M^{ab}_IJ + mu M^{ba}_IJ + mu delta_ab (M^{xx} + M^{yy} + M^{zz})_IJ,
 // which is the reference's per-Gauss-point block formula (H20:173-191) summed
 // over the Gauss points. Padded to 24 x 24 (8x8 tiles) and K = 28, the upper
-// triangle of the node grid is six tile positions; warp w owns one and
-// computes all nine M^{ab} tiles there on the FP64 tensor cores
-// (mma.sync.m8n8k4.f64: 9 x 7 per warp), so each lane holds, for its two
-// (I, J) node pairs, all nine M^{ab}_IJ and forms Ke_IJ without exchanging
-// anything with other lanes. It then adds Ke_IJ to the list entry of (row I,
-// column J) and, for I != J, its transpose to the entry of (row J, column I):
-// FP64 atomics at the slot ids of the slot map, so the 210 upper blocks give
-// all 400 blocks of Ke exactly symmetrically.
+// triangle of the node grid is six tile positions, each with nine M^{ab}
+// tiles on the FP64 tensor cores (mma.sync.m8n8k4.f64, seven k-steps), so a
+// lane holds, for its two (I, J) node pairs of a tile, all nine M^{ab}_IJ and
+// forms Ke_IJ without exchanging anything with other lanes.
 //
-// One 6-warp CTA per element at a time, persistent over the wave's elements
-// (perm[i0, i1), the spatial order); the shape-function derivatives at the 27
-// Gauss points (H20:95-128) are tabulated once per CTA; the next element's
-// node ids and coordinates are loaded while the current one is computed.
+// Group value pass (k_values_group): one CTA of kGroup warps per element
+// group, persistent over the wave's groups. Warp w computes the Ke of the
+// group's element w alone: the lanes' gradients G_a(n, g) for the fragment
+// rows n = 8 t + lane / 4 and k-columns g = 4 s + lane % 4 are the same
+// values for the A and the B operands, so they stay in registers (63 per
+// lane) and all six tile positions run from registers. The 210 upper blocks
+// are added with shared-memory FP64 atomics into the group's accumulator,
+// one block per node pair of the group (pair_index), so a pair that several
+// of the group's elements share leaves the CTA once. The flush then writes
+// each pair's block to the slot of (row u, column v) and its transpose to
+// (row v, column u): a plain store for a pair only this group has (its slots
+// were not zeroed), an FP64 atomic add for a shared pair (zeroed by its
+// claimer). The tensor-core form computes the wave's Ke in ke_tcgen05.cu
+// into a staging buffer first, and the same kernel adds the staged blocks.
+//
+// Element pass (k_values_hex20, kToCsrMap / kToCsrColour): one 6-warp CTA
+// per element at a time, warp w owning tile position w; the shape-function
+// derivatives at the 27 Gauss points (H20:95-128) are tabulated once per CTA
+// and the next element's node ids and coordinates are loaded while the
+// current one is computed.
 #include <algorithm>
 
-#include "values_hex20.cuh"
+#include "values_group.cuh"
 
 namespace fem {
 namespace {
@@ -40,9 +54,8 @@ namespace {
 #endif
 constexpr int kThreads = kValueWarps * 32;
 
-// kOut as values_cta. kToSlots: positions perm[i0, i1) of one wave, slot map
-// row i - i0. kToCsrMap: all elements in the order perm (scatter map row e).
-// kToCsrColour: the elements perm[range[0], range[1]) of one colour.
+// kOut as values_cta (kToCsrMap: all elements in the order perm, scatter map
+// row e; kToCsrColour: the elements perm[range[0], range[1]) of one colour).
 template <int kOut>
 __global__ void __launch_bounds__(kThreads, FEM_VALUES_MIN_CTAS)
     k_values_hex20(MeshView m, const int* __restrict__ perm, int i0, int i1, const int* __restrict__ range,
@@ -77,23 +90,44 @@ cudaError_t launch_values(const MeshView& m, const int* perm, int i0, int i1, co
     return cudaGetLastError();
 }
 
-}  // namespace
+constexpr int kGroupThreads = kGroup * 32;
 
-cudaError_t launch_values_hex20_fp64(const MeshView& m, const ListLayout& L, const int* perm, int i0, int i1,
-                                     const int* map, int ctas_per_sm, cudaStream_t s) {
-    if (i1 <= i0) return cudaSuccess;
-    ValuesTarget t{};
-    t.map = map;
-    t.map_origin = i0;
-    t.vals = L.vals;
-    t.info = L.info;
-    return launch_values<kToSlots>(m, perm, i0, i1, nullptr, t, ctas_per_sm, s);
+__global__ void __launch_bounds__(kGroupThreads, 1)
+    k_values_group(MeshView m, const int* __restrict__ perm, int i0, int i1, const unsigned* __restrict__ map,
+                   const double* __restrict__ stage, double* vals, DevInfo* info) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GroupValuesSmem& sm = *reinterpret_cast<GroupValuesSmem*>(smem_raw);
+    values_group_init(sm);
+    values_group(m, perm, i0, i1, map, stage, vals, info, sm);
 }
 
+cudaError_t launch_group_values(const MeshView& m, const ListLayout& L, const int* perm, int i0, int i1,
+                                const unsigned* map, const double* stage, cudaStream_t s) {
+    static DeviceCache cache;
+    const size_t smem = sizeof(GroupValuesSmem);
+    int per_sm = 0;
+    const cudaError_t err = per_device(cache, [&](int& v) {
+        cudaError_t e = cudaFuncSetAttribute(k_values_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_values_group, kGroupThreads, smem);
+        return e;
+    }, per_sm);
+    if (err) return err;
+    const long long groups = (i1 - i0 + kGroup - 1) / kGroup;
+    const long long grid = std::max<long long>(1, std::min<long long>(groups, (long long)per_sm * sm_count()));
+    k_values_group<<<(int)grid, kGroupThreads, smem, s>>>(m, perm, i0, i1, map, stage, L.vals, L.info);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
 cudaError_t launch_values_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm, int i0,
-                                int i1, const int* map, int ctas_per_sm, long long wait_ns, cudaStream_t s) {
-    return precision == FEM_PREC_TC_F16X3 ? launch_values_hex20_tc(m, L, perm, i0, i1, map, wait_ns, s)
-                                          : launch_values_hex20_fp64(m, L, perm, i0, i1, map, ctas_per_sm, s);
+                                int i1, const unsigned* map, double* stage, long long wait_ns, cudaStream_t s) {
+    if (i1 <= i0) return cudaSuccess;
+    if (precision == FEM_PREC_TC_F16X3) {
+        cudaError_t err = launch_stage_hex20_tc(m, perm, i0, i1, stage, &L.info->status_bits, wait_ns, s);
+        return err ? err : launch_group_values(m, L, perm, i0, i1, map, stage, s);
+    }
+    return launch_group_values(m, L, perm, i0, i1, map, nullptr, s);
 }
 
 cudaError_t launch_reassemble_hex20(const MeshView& m, int precision, const int* perm, const MapTarget& mt,

@@ -1,7 +1,10 @@
-// Device code of the Hex20 FP64 value pass (values_hex20.cu), shared with the
-// batched persistent kernel (batched.cu). See values_hex20.cu for the method.
+// Device code of the CTA-cooperative Hex20 FP64 element pass: the value-only
+// re-assembly and the colouring baseline (values_hex20.cu), and the value
+// items of the batched persistent kernel (batched.cu). See values_hex20.cu for
+// the method.
 #pragma once
 
+#include "group_hex20.cuh"
 #include "hex20.cuh"
 
 namespace fem {
@@ -12,16 +15,18 @@ constexpr int KS = 28;  // Gauss points padded to 7 k-steps of 4; row stride of 
 
 // Where the value pass puts an element's Ke blocks.
 enum ValueOut : int {
-    kToSlots = 0,   // FP64 atomics into the list slots of the slot map (upper blocks only)
+    kToSlots = 0,   // FP64 atomics into the list slots of a group's map record (both orientations)
     kToCsrMap = 1,  // FP64 atomics into a CSR at the positions of a scatter map (both triangles)
     kToCsrColour = 2  // plain adds into a CSR at binary-searched positions (one colour: no two
                       // elements share a node)
 };
 
 struct ValuesTarget {
-    const int* map;       // kToSlots: slot ids, row i - map_origin; kToCsrMap: CSR positions, row e
-    int map_origin;
-    double* vals;         // kToSlots: list values
+    const int* map;          // kToCsrMap: CSR positions, row e
+    const GroupTopo* topo;   // kToSlots: topology of the group of the elements
+    const unsigned* rec;     // kToSlots: the group's map record
+    long long g0;            // kToSlots: position of the group's first element
+    double* vals;            // kToSlots: list values
     const int* row_ptr;   // kToCsr*: the CSR
     const int* col_idx;
     double* csr;
@@ -198,45 +203,64 @@ __device__ __forceinline__ void values_cta(const MeshView& m, const int* __restr
         }
         const double lam = sm.lam, mu = sm.mu;
         const int I = 8 * ti + fr;
-        const int nI = I < 20 ? sm.nodes[I] : 0;
         if constexpr (kOut == kToSlots) {
-            // Ke block of each of this lane's node pairs {I, J}, staged for the
-            // list entry of the pair's lower node id: (row I, column J) as it
-            // is when node_I <= node_J, else transposed into (row J, column I).
-            // The lists hold the values of their upper blocks only (row node <=
-            // column node); the consolidation reads the lower blocks transposed.
-            const int* mrow = t.map + (size_t)(i - t.map_origin) * 400;
-            int base = 0;
+            // Ke block of each of this lane's node pairs {I, J}, staged for two
+            // atomic passes: Ke_IJ to the slot of (row node I, column node J),
+            // then its transpose to the slot of (row J, column I), the slots
+            // from the group's map record
+            const GroupTopo& T = *t.topo;
+            const int w = (int)(i - t.g0);
+            unsigned tgt[2][2];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int Jn = 8 * tj + 2 * fc + h;
-                const bool pair = I < 20 && Jn < 20 && (ti != tj || Jn >= I);
-                const bool lower_first = pair && nI <= sm.nodes[Jn < 20 ? Jn : 0];
-                const int g = pair ? FEM_LDG(mrow + (lower_first ? I * 20 + Jn : Jn * 20 + I)) : -1;
-                const unsigned have = __ballot_sync(0xFFFFFFFFu, g >= 0);
-                if (g >= 0) {
-                    const int slot = base + __popc(have & ((1u << lane) - 1u));
-                    const double mtr = mu * (acc[0][0][h] + acc[1][1][h] + acc[2][2][h]);
-#pragma unroll
-                    for (int a = 0; a < 3; a++)
-#pragma unroll
-                        for (int b = 0; b < 3; b++) {
-                            const double k = fma(lam, acc[a][b][h], fma(mu, acc[b][a][h], a == b ? mtr : 0.0));
-                            sm.stage[warp][slot][lower_first ? 3 * a + b : 3 * b + a] = k;
-                        }
-                    sm.stage_gid[warp][slot] = g;
+                tgt[h][0] = tgt[h][1] = kMapNone;
+                if (I < 20 && Jn < 20 && (ti != tj || Jn >= I)) {
+                    const int u = T.lidx[20 * w + I], v = T.lidx[20 * w + Jn];
+                    if (u <= v) {
+                        const int p = pair_index(T, u, v);
+                        tgt[h][0] = FEM_LDG(t.rec + 2 * p);
+                        // a repeated node of one element: both orientations on one block
+                        tgt[h][1] = u == v ? (I != Jn ? tgt[h][0] : kMapNone) : FEM_LDG(t.rec + 2 * p + 1);
+                    } else {
+                        const int p = pair_index(T, v, u);
+                        tgt[h][0] = FEM_LDG(t.rec + 2 * p + 1);
+                        tgt[h][1] = FEM_LDG(t.rec + 2 * p);
+                    }
                 }
-                base += __popc(have);
             }
-            __syncwarp();
-            // nine consecutive lanes per block, three blocks per instruction: each
-            // block's 72 bytes are one atomic pass over its three sectors
-            if (lane < 27) {
-                const int q = lane / 9, v = lane - 9 * q;
-                for (int blk = q; blk < base; blk += 3)
-                    atomicAdd(t.vals + (size_t)(unsigned)sm.stage_gid[warp][blk] * 9 + v, sm.stage[warp][blk][v]);
+#pragma unroll
+            for (int o = 0; o < 2; o++) {
+                int base = 0;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const unsigned g = tgt[h][o];
+                    const bool ok = map_has_slot(g);
+                    const unsigned have = __ballot_sync(0xFFFFFFFFu, ok);
+                    if (ok) {
+                        const int slot = base + __popc(have & ((1u << lane) - 1u));
+                        const double mtr = mu * (acc[0][0][h] + acc[1][1][h] + acc[2][2][h]);
+#pragma unroll
+                        for (int a = 0; a < 3; a++)
+#pragma unroll
+                            for (int b = 0; b < 3; b++) {
+                                const double k = fma(lam, acc[a][b][h], fma(mu, acc[b][a][h], a == b ? mtr : 0.0));
+                                sm.stage[warp][slot][o ? 3 * b + a : 3 * a + b] = k;
+                            }
+                        sm.stage_gid[warp][slot] = (int)(g & ~kPairShared);
+                    }
+                    base += __popc(have);
+                }
+                __syncwarp();
+                // nine consecutive lanes per block, three blocks per instruction:
+                // each block's 72 bytes are one atomic pass over its three sectors
+                if (lane < 27) {
+                    const int q = lane / 9, v = lane - 9 * q;
+                    for (int blk = q; blk < base; blk += 3)
+                        atomicAdd(t.vals + (size_t)(unsigned)sm.stage_gid[warp][blk] * 9 + v, sm.stage[warp][blk][v]);
+                }
+                __syncwarp();
             }
-            __syncwarp();
         } else {
             // CSR targets hold both triangles: Ke_IJ at block (I, J) and its
             // transpose at (J, I)

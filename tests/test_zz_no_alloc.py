@@ -78,3 +78,25 @@ def test_static_workspace_refuses_large_meshes(fem, cuda_device):
     st = lib.fem_assemble_static(C.byref(cm), None, C.byref(out),
                                  C.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert st == fem.FEM_ERR_WORKSPACE
+
+
+def test_static_second_call_allocates_nothing(fem, cuda_device):
+    # After a first call (which may load the module), a second call of the
+    # same mesh leaves the device's free memory exactly as it was: nothing is
+    # allocated or freed by the library.
+    import torch
+    import meshgen as mg
+    lib = fem.load()
+    lib.fem_assemble_static.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    stream = torch.cuda.current_stream().cuda_stream
+    m = mg.hex20_grid(4, 3, 3, seed=33)
+    dev = fem.device_arrays(m, cuda_device)
+    cm = fem.fem_mesh_struct(m, dev)
+    out, rp, ci, v = _csr(fem, torch, m, m.contributions(), cuda_device)
+    assert lib.fem_assemble_static(C.byref(cm), None, C.byref(out), C.c_void_p(stream)) == fem.FEM_OK
+    torch.cuda.synchronize()
+    free0, total0 = torch.cuda.mem_get_info()
+    assert lib.fem_assemble_static(C.byref(cm), None, C.byref(out), C.c_void_p(stream)) == fem.FEM_OK
+    torch.cuda.synchronize()
+    free1, total1 = torch.cuda.mem_get_info()
+    assert (free1, total1) == (free0, total0)
