@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                 const int w0 = sg.arg * kHex20Wave, w1 = min(m.E_count, w0 + kHex20Wave);
                 const int b = w0 + k * kBatchClaim, e1 = min(w1, b + kBatchClaim);
                 for (int gb = b; gb < e1; gb += kGroup)
-                    claim_group(m, L, nullptr, nullptr, gb, min(kGroup, e1 - gb),
+                    claim_group(m, L, nullptr, nullptr, nullptr, gb, min(kGroup, e1 - gb),
                                 bm.map[sg.arg & 1] + (size_t)((gb - w0) / kGroup) * kGroupMapWords, sm.claim);
                 break;
             }

@@ -21,15 +21,16 @@
 // full first chunk continues in the row's overflow chunks (taken from the pool
 // and linked with atomicCAS), read from global memory.
 //
-// Ownership: a pair {u, v} belongs to the group alone when u or v has every
-// one of its occurrences in the mesh (deg, counted once per mesh) inside the
-// group, since then every element with both nodes is one of the group's. The
-// value pass stores such a pair's blocks once; the claimer of any other slot
-// zeroes its value block for the atomic adds of several groups. Each claimed
-// entry is counted for its row, and the slot id (with the shared flag) goes to
-// the group's map record. The two passes are separate launches, so every
-// value block is zeroed before any addition reaches it and no entry is ever
-// in a half-written state: no pending flags, no fences, no waits.
+// Ownership: a pair {u, v} belongs to the group alone when no element outside
+// the group has both nodes: the elements of u and of v outside the group
+// (from the mesh's node -> element incidence lists, built once per mesh)
+// have none in common. The value pass stores such a pair's blocks once; the
+// claimer of any other slot zeroes its value block for the atomic adds of
+// several groups. Each claimed entry is counted for its row, and the slot id
+// (with the shared flag) goes to the group's map record. The two passes are
+// separate launches, so every value block is zeroed before any addition
+// reaches it and no entry is ever in a half-written state: no pending flags,
+// no fences, no waits.
 #include <algorithm>
 
 #include "claim_hex20.cuh"
@@ -40,37 +41,20 @@ namespace {
 constexpr int kThreads = 128;
 
 __global__ void __launch_bounds__(kThreads) k_claim_hex20(MeshView m, ListLayout L, const int* __restrict__ perm,
-                                                          const int* __restrict__ deg, int i0, int i1,
-                                                          unsigned* __restrict__ map) {
+                                                          const int* __restrict__ inc_off, const int* __restrict__ inc,
+                                                          int i0, int i1, unsigned* __restrict__ map) {
     __shared__ ClaimSmem sm;
     const int ngroups = (i1 - i0 + kGroup - 1) / kGroup;
     for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
         const long long g0 = (long long)i0 + (long long)g * kGroup;
-        claim_group(m, L, perm, deg, g0, min(kGroup, i1 - (int)g0), map + (size_t)g * kGroupMapWords, sm);
-    }
-}
-
-__global__ void k_node_degree(MeshView m, int* __restrict__ deg) {
-    const long long n = (long long)m.E_count * 20;
-    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-        const int v = __ldg(m.conn + k);
-        if (v >= 0 && v < m.N) atomicAdd(deg + v, 1);
+        claim_group(m, L, perm, inc_off, inc, g0, min(kGroup, i1 - (int)g0), map + (size_t)g * kGroupMapWords, sm);
     }
 }
 
 }  // namespace
 
-cudaError_t launch_node_degree(const MeshView& m, int* deg, cudaStream_t s) {
-    cudaError_t err = cudaMemsetAsync(deg, 0, (size_t)m.N * sizeof(int), s);
-    if (err || m.E_count <= 0) return err;
-    const long long n = (long long)m.E_count * 20;
-    const long long grid = std::max<long long>(1, std::min<long long>((n + 255) / 256, 8ll * sm_count()));
-    k_node_degree<<<(int)grid, 256, 0, s>>>(m, deg);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int* perm, const int* deg, int i0,
-                               int i1, unsigned* map, cudaStream_t s) {
+cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int* perm, const int* inc_off,
+                               const int* inc, int i0, int i1, unsigned* map, cudaStream_t s) {
     if (i1 <= i0) return cudaSuccess;
     static DeviceCache cache;
     int per_sm = 0;
@@ -80,7 +64,7 @@ cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int
     if (err) return err;
     const long long need = (i1 - i0 + kGroup - 1) / kGroup;
     const long long grid = std::max<long long>(1, std::min<long long>(need, (long long)per_sm * sm_count()));
-    k_claim_hex20<<<(int)grid, kThreads, 0, s>>>(m, L, perm, deg, i0, i1, map);
+    k_claim_hex20<<<(int)grid, kThreads, 0, s>>>(m, L, perm, inc_off, inc, i0, i1, map);
     return cudaGetLastError();
 }
 

@@ -9,6 +9,7 @@ namespace {
 
 constexpr int kClaimMaxWords = 96;  // first-chunk meta rows of at most 96 words (S1 <= 94, checked on the host)
 constexpr int kClaimRows = 32;      // row nodes whose first chunks are copied at once
+constexpr int kExtMax = 8;          // elements outside the group kept per node (more: its pairs count as shared)
 
 enum : unsigned char { kCFound = 0, kCTry = 1, kCClaimed = 2, kCChain = 3 };
 
@@ -18,8 +19,26 @@ struct ClaimSmem {
     alignas(16) int view[kClaimRows][kClaimMaxWords];  // first chunks of a batch of row nodes
     int claims[kClaimRows];                            // entries claimed per row node of the batch
     int obase[kClaimRows + 1];                         // ordered pairs before each row of the batch
-    unsigned inner[kNbWords];                          // nodes whose every element is in the group
+    int ext[kGroupOcc][kExtMax];                       // node u's elements outside the group, ascending
+    unsigned char next[kGroupOcc];                     // their number (kExtMax + 1: more than kExtMax)
+    int gelem[kGroup];                                 // the group's elements
 };
+
+// Whether every element with both group-local nodes u and v is in the group:
+// no element outside the group has both.
+__device__ __forceinline__ bool pair_owned(const ClaimSmem& sm, int u, int v) {
+    const int cu = sm.next[u], cv = sm.next[v];
+    if (cu == 0 || cv == 0) return true;
+    if (cu > kExtMax || cv > kExtMax) return false;
+    int i = 0, j = 0;
+    while (i < cu && j < cv) {
+        const int a = sm.ext[u][i], b = sm.ext[v][j];
+        if (a == b) return false;
+        if (a < b) i++;
+        else j++;
+    }
+    return true;
+}
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
@@ -107,15 +126,15 @@ __device__ __forceinline__ unsigned char claim_first_chunk(const ListLayout& L, 
 }
 
 // Claim pass of the group of positions [g0, g0 + ne) of the visit order
-// (perm NULL: element i). deg: occurrences of every node in the whole mesh;
-// NULL makes every pair shared (every claimed block is zeroed). rec: the
-// group's map record. Every thread of the CTA calls it.
+// (perm NULL: element i). inc_off / inc: the mesh's node -> element incidence
+// lists; NULL makes every pair shared (every claimed block is zeroed). rec:
+// the group's map record. Every thread of the CTA calls it.
 __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* __restrict__ perm,
-                            const int* __restrict__ deg, long long g0, int ne, unsigned* __restrict__ rec,
-                            ClaimSmem& sm) {
+                            const int* __restrict__ inc_off, const int* __restrict__ inc, long long g0, int ne,
+                            unsigned* __restrict__ rec, ClaimSmem& sm) {
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
     GroupTopo& T = sm.T;
-    if (tid < kNbWords) sm.inner[tid] = 0u;
+    if (tid < ne) sm.gelem[tid] = perm ? FEM_LDG(perm + g0 + tid) : (int)(g0 + tid);
     group_topology(m, perm, g0, ne, T);
     if (T.bad) {
         if (tid == 0) raise_status(L.info, FEM_ERR_BAD_MESH);
@@ -123,9 +142,31 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         return;
     }
     const int nu = T.nu;
-    if (deg) {
-        for (int u = tid; u < nu; u += nt)
-            if (T.gcount[u] == FEM_LDG(deg + T.node[u])) atomicOr(&sm.inner[u >> 5], 1u << (u & 31));
+    // each node's elements outside the group (sorted, at most kExtMax kept)
+    for (int u = tid; u < nu; u += nt) {
+        int c = kExtMax + 1;
+        if (inc_off) {
+            const int n = T.node[u];
+            const int o1 = FEM_LDG(inc_off + n + 1);
+            c = 0;
+            for (int k = FEM_LDG(inc_off + n); k < o1; k++) {
+                const int e = FEM_LDG(inc + k);
+                bool in = false;
+                for (int w = 0; w < ne; w++) in |= sm.gelem[w] == e;
+                if (in) continue;
+                if (c < kExtMax) {
+                    int p = c;
+                    while (p > 0 && sm.ext[u][p - 1] > e) {
+                        sm.ext[u][p] = sm.ext[u][p - 1];
+                        p--;
+                    }
+                    sm.ext[u][p] = e;
+                }
+                c++;
+            }
+            c = min(c, kExtMax + 1);
+        }
+        sm.next[u] = (unsigned char)c;
     }
     int spare = -1;
     for (int rb = 0; rb < nu; rb += kClaimRows) {
@@ -177,7 +218,7 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
             } else {
                 gid = (int)slot_gid(L, rn, slot);
             }
-            const bool owned = ((sm.inner[u >> 5] >> (u & 31)) | (sm.inner[v >> 5] >> (v & 31))) & 1u;
+            const bool owned = pair_owned(sm, u, v);
             if (gid >= 0 && st == kCClaimed) {
                 if (!owned) zero_block(L.vals + (size_t)(unsigned)gid * 9);
                 atomicAdd(&sm.claims[r], 1);

@@ -11,7 +11,7 @@
 // never reorder the elements by colour.
 //
 // Rebuilt here so that it is correct and uses the whole GPU:
-//   k_inc_count / scan / k_inc_fill   node -> element incidence lists (CSR)
+//   launch_incidence                  node -> element incidence lists (CSR)
 //   k_jp_round (repeated)             Jones-Plassmann colouring: in each round
 //                                     an uncoloured element whose priority (a
 //                                     hash of its id) beats every uncoloured
@@ -33,7 +33,6 @@
 
 #include "element2d.cuh"
 #include "launch.h"
-#include "scan.cuh"
 
 namespace fem {
 namespace {
@@ -58,89 +57,6 @@ __device__ __forceinline__ bool beats(int f, unsigned pf, int e, unsigned pe) {
     return pf > pe || (pf == pe && f > e);
 }
 
-__global__ void k_inc_count(MeshView m, int* __restrict__ cnt, ColourInfo* info) {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m.E_count; e += gridDim.x * blockDim.x) {
-        const int npe = elem_npe(m, e);
-        for (int k = 0; k < npe; k++) {
-            const int n = __ldg(m.conn + (size_t)e * m.stride + k);
-            if (n < 0 || n >= m.N) {
-                atomicOr(&info->status_bits, 1 << FEM_ERR_BAD_MESH);
-                continue;
-            }
-            atomicAdd(cnt + n, 1);
-        }
-    }
-}
-
-// Tile sums of cnt (kScanTile entries per CTA).
-__global__ void __launch_bounds__(kScanThreads) k_tile_sums(const int* __restrict__ cnt, int N,
-                                                            long long* __restrict__ tiles) {
-    __shared__ long long s_warp[kScanThreads / 32 + 1];
-    long long sum = 0;
-    for (int i = 0; i < kScanTile / kScanThreads; i++) {
-        const long long n = (long long)blockIdx.x * kScanTile + (long long)i * kScanThreads + threadIdx.x;
-        if (n < N) sum += cnt[n];
-    }
-    long long total;
-    block_exclusive_scan(sum, s_warp, total);
-    if (threadIdx.x == 0) tiles[blockIdx.x] = total;
-}
-
-// Exclusive scan of the tile sums in place (one CTA); off[N] = total.
-__global__ void __launch_bounds__(kScanThreads) k_tile_scan(long long* __restrict__ tiles, int num_tiles,
-                                                            int* __restrict__ off_end, ColourInfo* info) {
-    __shared__ long long s_warp[kScanThreads / 32 + 1];
-    long long carry = 0;
-    for (int base = 0; base < num_tiles; base += kScanThreads) {
-        const int t = base + threadIdx.x;
-        const long long v = t < num_tiles ? tiles[t] : 0;
-        long long total;
-        const long long ex = block_exclusive_scan(v, s_warp, total);
-        if (t < num_tiles) tiles[t] = carry + ex;
-        carry += total;
-    }
-    if (threadIdx.x == 0) {
-        *off_end = (int)carry;
-        if (carry > 0x7FFFFFFFll) atomicOr(&info->status_bits, 1 << FEM_ERR_RANGE);
-    }
-}
-
-// off[n] = exclusive prefix of cnt; cnt is cleared for the fill pass.
-__global__ void __launch_bounds__(kScanThreads) k_tile_apply(int* __restrict__ cnt, int N,
-                                                             const long long* __restrict__ tiles,
-                                                             int* __restrict__ off) {
-    constexpr int kItems = kScanTile / kScanThreads;
-    __shared__ long long s_warp[kScanThreads / 32 + 1];
-    const long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kItems;
-    int c[kItems];
-    long long sum = 0;
-#pragma unroll
-    for (int i = 0; i < kItems; i++) {
-        c[i] = base + i < N ? cnt[base + i] : 0;
-        sum += c[i];
-    }
-    long long total;
-    long long o = tiles[blockIdx.x] + block_exclusive_scan(sum, s_warp, total);
-#pragma unroll
-    for (int i = 0; i < kItems; i++) {
-        if (base + i < N) {
-            off[base + i] = (int)o;
-            cnt[base + i] = 0;
-        }
-        o += c[i];
-    }
-}
-
-__global__ void k_inc_fill(MeshView m, const int* __restrict__ off, int* __restrict__ cursor, int* __restrict__ inc) {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m.E_count; e += gridDim.x * blockDim.x) {
-        const int npe = elem_npe(m, e);
-        for (int k = 0; k < npe; k++) {
-            const int n = __ldg(m.conn + (size_t)e * m.stride + k);
-            if (n < 0 || n >= m.N) continue;
-            inc[off[n] + atomicAdd(cursor + n, 1)] = e;
-        }
-    }
-}
 
 // One Jones-Plassmann round. colour[e] = -1 (uncoloured) or round << 8 | c.
 __global__ void k_jp_round(MeshView m, const int* __restrict__ off, const int* __restrict__ inc,
@@ -313,18 +229,11 @@ int grid_for(long long work, int sms) {
 cudaError_t launch_colour_prepare(const MeshView& m, const ColourLayout& C, int sms, cudaStream_t s, int* num_colours,
                                   int* status_bits) {
     cudaError_t err = cudaMemsetAsync(C.info, 0, sizeof(ColourInfo), s);
-    if (!err) err = cudaMemsetAsync(C.cnt, 0, (size_t)m.N * sizeof(int), s);
     if (!err) err = cudaMemsetAsync(C.colour, 0xFF, (size_t)m.E_count * sizeof(int), s);
     if (!err) err = cudaMemsetAsync(C.hist, 0, 2 * kMaxColours * sizeof(int), s);
     if (err) return err;
-    const int num_tiles = (m.N + kScanTile - 1) / kScanTile;
+    if ((err = launch_incidence(m, C.cnt, C.off, C.inc, C.tiles, &C.info->status_bits, sms, s))) return err;
     const int ge = grid_for(m.E_count, sms);
-    k_inc_count<<<ge, kThreads, 0, s>>>(m, C.cnt, C.info);
-    k_tile_sums<<<num_tiles, kScanThreads, 0, s>>>(C.cnt, m.N, C.tiles);
-    k_tile_scan<<<1, kScanThreads, 0, s>>>(C.tiles, num_tiles, C.off + m.N, C.info);
-    k_tile_apply<<<num_tiles, kScanThreads, 0, s>>>(C.cnt, m.N, C.tiles, C.off);
-    k_inc_fill<<<ge, kThreads, 0, s>>>(m, C.off, C.cnt, C.inc);
-    if ((err = cudaGetLastError())) return err;
     // Colouring rounds until every element has a colour (each round colours
     // at least the element of highest priority among the uncoloured ones).
     int left = m.E_count;

@@ -113,10 +113,12 @@ fem_status make_layout(const fem_mesh* m, const fem_opts* o, HostLayout& h) {
         off += align_up((size_t)h.E * sizeof(int)) + align_up(4 * sizeof(int)) + align_up(nbuckets * sizeof(int)) +
                align_up(6 * sizeof(unsigned long long));
     }
-    // Hex20: node degrees, the map records of one wave of the two-pass scatter,
-    // and (tensor-core form) the staged Ke of one wave
-    h.off_deg = off;
-    if (h.kind == FEM_HEX20) off += align_up((size_t)h.N * sizeof(int));
+    // Hex20: node -> element incidence (counts, offsets, lists), the map
+    // records of one wave of the two-pass scatter, and (tensor-core form) the
+    // staged Ke of one wave
+    h.off_inc = off;
+    if (h.kind == FEM_HEX20)
+        off += 2 * align_up((size_t)(h.N + 1) * sizeof(int)) + align_up((size_t)h.E * 20 * sizeof(int));
     h.off_map = off;
     if (h.kind == FEM_HEX20) off += align_up(hex20_map_bytes(h.E));
     h.off_stage = off;
@@ -254,14 +256,17 @@ fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* wo
         // (entries, zeroed value blocks, map records) complete before its
         // value pass, and the blocks it touches are still in L2 when the
         // values arrive
-        int* deg = reinterpret_cast<int*>(b + h.off_deg);
+        int* inc_cnt = reinterpret_cast<int*>(b + h.off_inc);
+        int* inc_off = inc_cnt + align_up((size_t)(h.N + 1) * sizeof(int)) / sizeof(int);
+        int* inc = inc_off + align_up((size_t)(h.N + 1) * sizeof(int)) / sizeof(int);
         unsigned* map = reinterpret_cast<unsigned*>(b + h.off_map);
         double* stage = reinterpret_cast<double*>(b + h.off_stage);
+        long long* tiles = reinterpret_cast<long long*>(b + h.off_tiles);  // free until the consolidation
         const long long wait_ns = wait_ns_of(opts ? opts->wait_limit_us : 0);
-        if (!err) err = launch_node_degree(m, deg, s);
+        if (!err) err = launch_incidence(m, inc_cnt, inc_off, inc, tiles, &L.info->status_bits, sm_count(), s);
         for (int i0 = 0; i0 < h.E && !err; i0 += kHex20Wave) {
             const int i1 = std::min(h.E, i0 + kHex20Wave);
-            err = launch_claim_hex20(m, L, perm, deg, i0, i1, map, s);
+            err = launch_claim_hex20(m, L, perm, inc_off, inc, i0, i1, map, s);
             if (!err) err = launch_values_hex20(m, L, precision, perm, i0, i1, map, stage, wait_ns, s);
         }
     } else {

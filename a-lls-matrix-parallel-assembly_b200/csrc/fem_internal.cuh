@@ -160,7 +160,7 @@ struct HostLayout {
     int kind, dpn, B, N, E;
     int S1, S2, H1, H2, cap2;
     int num_tiles;  // scan tiles of kScanTile nodes
-    size_t off_info, off_meta1, off_meta2, off_vals, off_counts, off_ucounts, off_tiles, off_elist, off_deg, off_map,
+    size_t off_info, off_meta1, off_meta2, off_vals, off_counts, off_ucounts, off_tiles, off_elist, off_inc, off_map,
         off_stage, total;
     size_t meta1_bytes;
 };

@@ -44,7 +44,6 @@ __device__ __forceinline__ bool map_has_slot(unsigned w) { return (w & ~kPairSha
 struct GroupTopo {
     int node[kGroupOcc];                   // group-local node u -> node id (u < nu)
     int occ[kGroupOcc];                    // occurrence 20 e + a -> node id of node a of element e
-    int gcount[kGroupOcc];                 // occurrences of group-local node u in the group
     unsigned nb[kGroupOcc][kNbWords];      // neighbour sets
     unsigned first[kNbWords];              // occurrences that are their node's first
     unsigned short ubase[kGroupOcc + 1];   // pair index of {u, u}; ubase[nu] = number of pairs
@@ -92,7 +91,6 @@ __device__ void group_topology(const MeshView& m, const int* __restrict__ perm, 
     }
     if (tid < kNbWords) T.first[tid] = 0;
     for (int k = tid; k < kGroupOcc * kNbWords; k += nt) (&T.nb[0][0])[k] = 0u;
-    for (int k = tid; k < kGroupOcc; k += nt) T.gcount[k] = 0;
     __syncthreads();
     for (int k = tid; k < nocc; k += nt) {
         const long long i = g0 + k / 20;
@@ -127,7 +125,6 @@ __device__ void group_topology(const MeshView& m, const int* __restrict__ perm, 
         const int u = T.lidx[20 * e + a], v = T.lidx[20 * e + b];
         atomicOr(&T.nb[u][v >> 5], 1u << (v & 31));
     }
-    for (int k = tid; k < nocc; k += nt) atomicAdd(&T.gcount[T.lidx[k]], 1);
     __syncthreads();
     // pair numbering: ubase = exclusive prefix of the counts of {u <= v}
     if (tid < 32) {

@@ -101,18 +101,23 @@ cudaError_t launch_reassemble_hex20(const MeshView& m, int precision, const int*
 cudaError_t launch_colour_hex20(const MeshView& m, const int* perm, const int* range, const MapTarget& t,
                                 DevInfo* info, cudaStream_t s);
 
+// Node -> element incidence lists (incidence.cu): cnt [N] (counts), off
+// [N + 1], inc [sum of nodes per element], tiles [ceil(N / kScanTile)]
+// scratch; status gets 1 << FEM_ERR_* bits.
+cudaError_t launch_incidence(const MeshView& m, int* cnt, int* off, int* inc, long long* tiles, int* status, int sms,
+                             cudaStream_t s);
 // Two-pass Hex20 list scatter over the element groups of positions
-// perm[i0, i1) (one wave; i0 a multiple of the group size). deg: occurrences
-// of every node in the mesh (launch_node_degree). Pass 1 claims the list
+// perm[i0, i1) (one wave; i0 a multiple of the group size). inc_off / inc:
+// the mesh's node -> element incidence lists (launch_incidence; NULL: every
+// node pair counts as shared by several groups). Pass 1 claims the list
 // entries, zeroes the value blocks of the entries several groups add to and
 // writes the groups' map records (claim_hex20.cu); pass 2 adds the Ke blocks
 // (values_hex20.cu; in the tensor-core form the wave's Ke are computed into
 // stage first, ke_tcgen05.cu). map: kHex20WaveMapWords words; stage:
 // kHex20Wave * kPackedHex20 doubles (tensor-core form only). wait_ns: see
 // wait_ns_of.
-cudaError_t launch_node_degree(const MeshView& m, int* deg, cudaStream_t s);
-cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int* perm, const int* deg, int i0,
-                               int i1, unsigned* map, cudaStream_t s);
+cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int* perm, const int* inc_off,
+                               const int* inc, int i0, int i1, unsigned* map, cudaStream_t s);
 cudaError_t launch_values_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm, int i0,
                                 int i1, const unsigned* map, double* stage, long long wait_ns, cudaStream_t s);
 // The packed Ke of the elements perm[i0, i1) on the tensor cores, row q - i0 for position q.
