@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                 const int b = w0 + k * kBatchClaim, e1 = min(w1, b + kBatchClaim);
                 for (int gb = b; gb < e1; gb += kGroup)
                     claim_group(m, L, nullptr, nullptr, nullptr, gb, min(kGroup, e1 - gb),
-                                bm.map[sg.arg & 1] + (size_t)((gb - w0) / kGroup) * kGroupMapWords, sm.claim);
+                                bm.map[sg.arg & 1] + (size_t)((gb - w0) / kGroup) * kGroupRecWords, sm.claim);
                 break;
             }
             case kBpValues: {
@@ -201,7 +201,8 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                 if (sm.gv.topo.bad) break;  // the claim item raised it
                 ValuesTarget vt{};
                 vt.topo = &sm.gv.topo;
-                vt.rec = bm.map[sg.arg & 1] + (size_t)((b - w0) / kGroup) * kGroupMapWords;
+                vt.rec = reinterpret_cast<const unsigned*>(bm.map[sg.arg & 1] + (size_t)((b - w0) / kGroup) * kGroupRecWords +
+                                                           kRecMap);
                 vt.g0 = b;
                 vt.vals = L.vals;
                 vt.info = L.info;

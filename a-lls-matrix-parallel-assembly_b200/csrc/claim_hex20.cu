@@ -38,33 +38,31 @@
 namespace fem {
 namespace {
 
-constexpr int kThreads = 128;
-
-__global__ void __launch_bounds__(kThreads) k_claim_hex20(MeshView m, ListLayout L, const int* __restrict__ perm,
+__global__ void __launch_bounds__(kClaimThreads, 3) k_claim_hex20(MeshView m, ListLayout L, const int* __restrict__ perm,
                                                           const int* __restrict__ inc_off, const int* __restrict__ inc,
-                                                          int i0, int i1, unsigned* __restrict__ map) {
+                                                          int i0, int i1, int* __restrict__ map) {
     __shared__ ClaimSmem sm;
     const int ngroups = (i1 - i0 + kGroup - 1) / kGroup;
     for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
         const long long g0 = (long long)i0 + (long long)g * kGroup;
-        claim_group(m, L, perm, inc_off, inc, g0, min(kGroup, i1 - (int)g0), map + (size_t)g * kGroupMapWords, sm);
+        claim_group(m, L, perm, inc_off, inc, g0, min(kGroup, i1 - (int)g0), map + (size_t)g * kGroupRecWords, sm);
     }
 }
 
 }  // namespace
 
 cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int* perm, const int* inc_off,
-                               const int* inc, int i0, int i1, unsigned* map, cudaStream_t s) {
+                               const int* inc, int i0, int i1, int* map, cudaStream_t s) {
     if (i1 <= i0) return cudaSuccess;
     static DeviceCache cache;
     int per_sm = 0;
     const cudaError_t err = per_device(cache, [](int& v) {
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_claim_hex20, kThreads, 0);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_claim_hex20, kClaimThreads, 0);
     }, per_sm);
     if (err) return err;
     const long long need = (i1 - i0 + kGroup - 1) / kGroup;
     const long long grid = std::max<long long>(1, std::min<long long>(need, (long long)per_sm * sm_count()));
-    k_claim_hex20<<<(int)grid, kThreads, 0, s>>>(m, L, perm, inc_off, inc, i0, i1, map);
+    k_claim_hex20<<<(int)grid, kClaimThreads, 0, s>>>(m, L, perm, inc_off, inc, i0, i1, map);
     return cudaGetLastError();
 }
 

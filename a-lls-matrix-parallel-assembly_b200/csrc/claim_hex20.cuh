@@ -11,7 +11,7 @@ constexpr int kClaimMaxWords = 96;  // first-chunk meta rows of at most 96 words
 constexpr int kClaimRows = 32;      // row nodes whose first chunks are copied at once
 constexpr int kExtMax = 8;          // elements outside the group kept per node (more: its pairs count as shared)
 
-enum : unsigned char { kCFound = 0, kCTry = 1, kCClaimed = 2, kCChain = 3 };
+enum : unsigned char { kCFound = 0, kCTry = 1, kCClaimed = 2, kCChain = 3, kCNone = 4 };
 
 // Shared memory of one claiming CTA.
 struct ClaimSmem {
@@ -89,59 +89,83 @@ __device__ int resolve_chain(const ListLayout& L, int n, int key, int& spare, bo
     return -1;
 }
 
-// Finds or claims column key `key` in the first chunk of row node rn, whose
-// copy (taken at the start of the batch) is `view`: the key's probe sequence
-// in the copy; the first slot empty in the copy is claimed with atomicCAS.
-// A CAS that meets another column moves on along the sequence: slots are
-// never freed, so a column sits at the first slot of its sequence that was
-// empty when it was inserted and is never inserted twice. Returns the slot
-// (state kCFound / kCClaimed) or kCChain when the first chunk's sequence is
-// full.
-__device__ __forceinline__ unsigned char claim_first_chunk(const ListLayout& L, int rn, const int* view, int key,
-                                                           int& slot) {
+// Walks the probe sequence of column key `key` in the first chunk of row node
+// rn from step t0 on, against `view` (the chunk's copy taken at the start of
+// the batch): a slot holding the key is found; the first slot empty in the
+// copy is claimed with atomicCAS. A CAS that meets another column moves on
+// along the sequence: slots are never freed, so a column sits at the first
+// slot of its sequence that was empty when it was inserted and is never
+// inserted twice. Returns kCFound / kCClaimed with the slot, or kCChain when
+// the first chunk's sequence is full.
+__device__ unsigned char claim_walk(const ListLayout& L, int rn, const int* view, int key, int t0, int& slot) {
     const int S1 = L.S1;
     const int p0 = probe_start(key, S1);
     int* meta = L.meta1 + (size_t)rn * L.H1 + 2;
-    const int* v = view + 2;
-    for (int t = 0; t < S1; t++) {
+    for (int t = t0; t < S1; t++) {
         int s = p0 + t;
         if (s >= S1) s -= S1;
-        const int x = v[s];
+        const int x = view[2 + s];
         if (x == key) {
             slot = s;
             return kCFound;
         }
         if (x != 0) continue;
         const int old = atomicCAS(meta + s, 0, key);
-        if (old == 0) {
+        if (old == 0 || old == key) {
             slot = s;
-            return kCClaimed;
-        }
-        if (old == key) {
-            slot = s;
-            return kCFound;
+            return old == 0 ? kCClaimed : kCFound;
         }
     }
     return kCChain;
 }
 
+// Threads of a claiming CTA (a lane takes the columns lane, lane + 32, ... of
+// kClaimRows / kClaimWarps rows of a batch).
+constexpr int kClaimThreads = 256;
+constexpr int kClaimWarps = kClaimThreads / 32;
+constexpr int kCand = kClaimRows / kClaimWarps * kNbWords;  // candidate pairs per lane and batch
+static_assert(kClaimRows % kClaimWarps == 0, "whole rows per warp");
+
 // Claim pass of the group of positions [g0, g0 + ne) of the visit order
 // (perm NULL: element i). inc_off / inc: the mesh's node -> element incidence
 // lists; NULL makes every pair shared (every claimed block is zeroed). rec:
-// the group's map record. Every thread of the CTA calls it.
+// the group's record (group_hex20.cuh). Every thread of the kClaimThreads-
+// thread CTA calls it.
 __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* __restrict__ perm,
                             const int* __restrict__ inc_off, const int* __restrict__ inc, long long g0, int ne,
-                            unsigned* __restrict__ rec, ClaimSmem& sm) {
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
+                            int* __restrict__ rec, ClaimSmem& sm) {
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     GroupTopo& T = sm.T;
     if (tid < ne) sm.gelem[tid] = perm ? FEM_LDG(perm + g0 + tid) : (int)(g0 + tid);
     group_topology(m, perm, g0, ne, T);
     if (T.bad) {
-        if (tid == 0) raise_status(L.info, FEM_ERR_BAD_MESH);
+        if (tid == 0) {
+            raise_status(L.info, FEM_ERR_BAD_MESH);
+            rec[0] = 0;
+            rec[1] = 0;
+        }
         __syncthreads();
         return;
     }
     const int nu = T.nu;
+    // the record: header, node ids, block table
+    if (tid == 0) {
+        rec[0] = T.npairs;
+        rec[1] = ne;
+    }
+    if (tid < ne) rec[2 + tid] = sm.gelem[tid];
+    for (int k = tid; k < ne * 20; k += nt) rec[kRecOcc + k] = T.occ[k];
+    unsigned short* tab = reinterpret_cast<unsigned short*>(rec + kRecTab);
+    for (int k = tid; k < ne * 210; k += nt) {
+        const int w = k / 210, p = k - 210 * w;
+        int I = 0;
+        while (I < 19 && packed_block(I + 1, I + 1) <= p) I++;
+        const int J = I + p - packed_block(I, I);
+        const int u = T.lidx[20 * w + I], v = T.lidx[20 * w + J];
+        unsigned e = u <= v ? (unsigned)pair_index(T, u, v) : ((unsigned)pair_index(T, v, u) | kTabTransposed);
+        if (u == v && I != J) e |= kTabBoth;
+        tab[k] = (unsigned short)e;
+    }
     // each node's elements outside the group (sorted, at most kExtMax kept)
     for (int u = tid; u < nu; u += nt) {
         int c = kExtMax + 1;
@@ -168,7 +192,9 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         }
         sm.next[u] = (unsigned char)c;
     }
+    unsigned* map = reinterpret_cast<unsigned*>(rec + kRecMap);
     int spare = -1;
+    const int S1 = L.S1;
     for (int rb = 0; rb < nu; rb += kClaimRows) {
         const int nrows = min(kClaimRows, nu - rb);
         // the batch's first chunks, H1 / 4 16-byte pieces each
@@ -177,59 +203,82 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
             const int r = q / pieces, k = q - r * pieces;
             cp_async16(&sm.view[r][4 * k], L.meta1 + (size_t)T.node[rb + r] * L.H1 + 4 * k);
         }
-        if (tid < 32) {
-            int c = 0;
-            if (lane < nrows) {
-#pragma unroll
-                for (int w = 0; w < kNbWords; w++) c += __popc(T.nb[rb + lane][w]);
-            }
-            int incl = c;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const int y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
-                if (lane >= d) incl += y;
-            }
-            if (lane < nrows) {
-                sm.obase[lane] = incl - c;
-                sm.claims[lane] = 0;
-            }
-            if (lane == nrows - 1) sm.obase[nrows] = incl;
-        }
+        if (tid < nrows) sm.claims[tid] = 0;
         cp_async_wait_all();
         __syncthreads();
-        const int total = sm.obase[nrows];
-        for (int f = tid; f < total; f += nt) {
-            int lo = 0, hi = nrows - 1;  // the last row whose first pair is <= f
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (sm.obase[mid] <= f) lo = mid;
-                else hi = mid - 1;
+        // this lane's candidates: row r = warp + kClaimWarps i, column 32 w + lane
+        int slot[kCand], old[kCand];
+        unsigned char st[kCand];
+#pragma unroll
+        for (int c = 0; c < kCand; c++) {
+            const int r = warp + kClaimWarps * (c / kNbWords), w = c % kNbWords;
+            st[c] = kCNone;
+            slot[c] = 0;
+            if (r < nrows && ((T.nb[rb + r][w] >> lane) & 1u)) {
+                const int key = T.node[32 * w + lane] + 1;
+                const int p0 = probe_start(key, S1);
+                st[c] = kCChain;
+                for (int t = 0; t < S1; t++) {
+                    int s = p0 + t;
+                    if (s >= S1) s -= S1;
+                    const int x = sm.view[r][2 + s];
+                    if (x == key || x == 0) {
+                        st[c] = x == key ? kCFound : kCTry;
+                        slot[c] = x == key ? s : t;  // kCTry: the step of the sequence
+                        break;
+                    }
+                }
             }
-            const int r = lo, u = rb + r;
-            const int v = nb_member(T, u, f - sm.obase[r]);
+        }
+        // every claim of the lane in flight at once
+#pragma unroll
+        for (int c = 0; c < kCand; c++) {
+            old[c] = 0;
+            if (st[c] == kCTry) {
+                const int r = warp + kClaimWarps * (c / kNbWords), w = c % kNbWords;
+                const int key = T.node[32 * w + lane] + 1;
+                int s = probe_start(key, S1) + slot[c];
+                if (s >= S1) s -= S1;
+                old[c] = atomicCAS(L.meta1 + (size_t)T.node[rb + r] * L.H1 + 2 + s, 0, key);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < kCand; c++) {
+            if (st[c] == kCNone) continue;
+            const int r = warp + kClaimWarps * (c / kNbWords), w = c % kNbWords;
+            const int u = rb + r, v = 32 * w + lane;
             const int rn = T.node[u], key = T.node[v] + 1;
-            int slot = -1;
-            unsigned char st = claim_first_chunk(L, rn, sm.view[r], key, slot);
-            int gid;
-            if (st == kCChain) {
+            int gid = -1;
+            if (st[c] == kCTry) {
+                const int t = slot[c];
+                int s = probe_start(key, S1) + t;
+                if (s >= S1) s -= S1;
+                if (old[c] == 0 || old[c] == key) {
+                    st[c] = old[c] == 0 ? kCClaimed : kCFound;
+                    slot[c] = s;
+                } else {
+                    st[c] = claim_walk(L, rn, sm.view[r], key, t + 1, slot[c]);
+                }
+            }
+            if (st[c] == kCChain) {
                 bool claimed = false;
                 gid = resolve_chain(L, rn, key, spare, claimed);
-                st = claimed ? kCClaimed : kCFound;
+                st[c] = claimed ? kCClaimed : kCFound;
             } else {
-                gid = (int)slot_gid(L, rn, slot);
+                gid = (int)slot_gid(L, rn, slot[c]);
             }
             const bool owned = pair_owned(sm, u, v);
-            if (gid >= 0 && st == kCClaimed) {
+            if (gid >= 0 && st[c] == kCClaimed) {
                 if (!owned) zero_block(L.vals + (size_t)(unsigned)gid * 9);
                 atomicAdd(&sm.claims[r], 1);
             }
             const unsigned word = gid < 0 ? kMapNone : ((unsigned)gid | (owned ? 0u : kPairShared));
             if (u <= v) {
                 const int p = pair_index(T, u, v);
-                rec[2 * p] = word;
-                if (u == v) rec[2 * p + 1] = kMapNone;
+                map[2 * p] = word;
+                if (u == v) map[2 * p + 1] = kMapNone;
             } else {
-                rec[2 * pair_index(T, v, u) + 1] = word;
+                map[2 * pair_index(T, v, u) + 1] = word;
             }
         }
         __syncthreads();

@@ -57,7 +57,7 @@ fem_status check_mesh(const fem_mesh* m, bool device_pointers_needed = true) {
 // Map records of one wave of the Hex20 scatter for a mesh of E elements.
 size_t hex20_map_bytes(int E) {
     const size_t groups = ((size_t)std::min(E, kHex20Wave) + kHex20GroupSize - 1) / kHex20GroupSize;
-    return groups * kHex20GroupMapWords * sizeof(unsigned);
+    return groups * kHex20GroupRecWords * sizeof(unsigned);
 }
 
 fem_status make_layout(const fem_mesh* m, const fem_opts* o, HostLayout& h) {
@@ -259,7 +259,7 @@ fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* wo
         int* inc_cnt = reinterpret_cast<int*>(b + h.off_inc);
         int* inc_off = inc_cnt + align_up((size_t)(h.N + 1) * sizeof(int)) / sizeof(int);
         int* inc = inc_off + align_up((size_t)(h.N + 1) * sizeof(int)) / sizeof(int);
-        unsigned* map = reinterpret_cast<unsigned*>(b + h.off_map);
+        int* map = reinterpret_cast<int*>(b + h.off_map);
         double* stage = reinterpret_cast<double*>(b + h.off_stage);
         long long* tiles = reinterpret_cast<long long*>(b + h.off_tiles);  // free until the consolidation
         const long long wait_ns = wait_ns_of(opts ? opts->wait_limit_us : 0);
@@ -550,8 +550,8 @@ fem_status fem_assemble_batched(const fem_mesh* meshes, int32_t n, const fem_opt
         bm.m = mesh_view(&meshes[i]);
         bm.L = device_layout(h, ws);
         bm.tiles = reinterpret_cast<long long*>(ws + h.off_tiles);
-        bm.map[0] = reinterpret_cast<unsigned*>(ws + h.off_map);
-        bm.map[1] = reinterpret_cast<unsigned*>(ws + h.total);
+        bm.map[0] = reinterpret_cast<int*>(ws + h.off_map);
+        bm.map[1] = reinterpret_cast<int*>(ws + h.total);
         bm.row_ptr = outs[i].row_ptr;
         bm.col_idx = outs[i].col_idx;
         bm.values = outs[i].values;

@@ -13,12 +13,21 @@
 //
 // The claim pass resolves every ordered pair (row node u, column node v) of
 // the group once, however many of the group's elements have both nodes, and
-// writes the group's map record: word 2 * pair_index(u, v) holds the slot id
-// of (row u, column v) and word 2 * pair_index(u, v) + 1 the slot id of
-// (row v, column u) (kMapNone for a diagonal pair or an unresolved slot).
-// Bit 31 (kPairShared) marks a pair that elements outside the group also
-// have: its slots are zeroed by their claimer and receive atomic adds; the
-// other pairs belong to this group alone and their blocks are stored once.
+// writes the group's record (int32 words):
+//   [0] number of node pairs, [1] elements (0: the group has a bad node id),
+//   [2 + w] element id of the group's element w;
+//   kRecOcc + 20 w + a: node id of node a of element w;
+//   kRecTab: per element w and packed upper block p (I <= J, p = 20 I -
+//     I (I - 1) / 2 + J - I) a 16-bit entry: the pair index of the block's
+//     node pair, bit 15 set when the block lies transposed in it (u > v), bit
+//     14 set when both orientations fall on one diagonal block (an element
+//     with a repeated node);
+//   kRecMap + 2 r: slot id of (row u, column v) of pair r = {u <= v}, and
+//   kRecMap + 2 r + 1: slot id of (row v, column u) (kMapNone for a diagonal
+//     pair or an unresolved slot). Bit 31 (kPairShared) marks a pair that
+//     elements outside the group also have: its slots are zeroed by their
+//     claimer and receive atomic adds; the other pairs belong to this group
+//     alone and their blocks are stored once.
 #pragma once
 
 #include "launch.h"
@@ -33,13 +42,23 @@ constexpr int kGroupPairs = kGroup * 210;        // bound on a group's node pair
 constexpr int kGroupMapWords = 2 * kGroupPairs;  // map record words per group
 constexpr unsigned kPairShared = 0x80000000u;    // map word flag: other groups add to the pair
 constexpr unsigned kMapNone = 0xFFFFFFFFu;       // map word of no slot
+constexpr int kRecOcc = 16;                                 // record words: header, then occurrences,
+constexpr int kRecTab = kRecOcc + kGroupOcc;                // block table (two 16-bit entries a word),
+constexpr int kRecMap = kRecTab + kGroup * 210 / 2;         // slot words
+constexpr int kGroupRecWords = kRecMap + kGroupMapWords;
+constexpr unsigned kTabTransposed = 0x8000u, kTabBoth = 0x4000u, kTabPair = 0x07FFu;
 static_assert(kNbWords * 32 == kGroupOcc, "whole words of group-local nodes");
-static_assert(kGroup == kHex20GroupSize && kGroupMapWords == kHex20GroupMapWords, "host-side sizes");
+static_assert(kGroupPairs <= kTabPair + 1, "pair index in 11 bits");
+static_assert(kRecTab % 4 == 0 && kRecMap % 4 == 0 && kGroupRecWords % 4 == 0, "16-byte sections");
+static_assert(kGroup == kHex20GroupSize && kGroupRecWords == kHex20GroupRecWords, "host-side sizes");
 static_assert(kHex20Wave % kGroup == 0, "waves of whole groups");
 
 // Whether a map word names a slot (slot ids are below 2^31 - 1: the layout
 // keeps the slot count below 2^31).
 __device__ __forceinline__ bool map_has_slot(unsigned w) { return (w & ~kPairShared) != (kMapNone & ~kPairShared); }
+
+// Packed index of the upper block (I, J), I <= J, of a Hex20 element.
+__device__ __forceinline__ int packed_block(int I, int J) { return I * 20 - I * (I - 1) / 2 + J - I; }
 
 struct GroupTopo {
     int node[kGroupOcc];                   // group-local node u -> node id (u < nu)

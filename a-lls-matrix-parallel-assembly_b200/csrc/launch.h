@@ -113,13 +113,14 @@ cudaError_t launch_incidence(const MeshView& m, int* cnt, int* off, int* inc, lo
 // entries, zeroes the value blocks of the entries several groups add to and
 // writes the groups' map records (claim_hex20.cu); pass 2 adds the Ke blocks
 // (values_hex20.cu; in the tensor-core form the wave's Ke are computed into
-// stage first, ke_tcgen05.cu). map: kHex20WaveMapWords words; stage:
+// stage first, ke_tcgen05.cu). map: kHex20WaveMapWords words (the groups'
+// records, group_hex20.cuh); stage:
 // kHex20Wave * kPackedHex20 doubles (tensor-core form only). wait_ns: see
 // wait_ns_of.
 cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int* perm, const int* inc_off,
-                               const int* inc, int i0, int i1, unsigned* map, cudaStream_t s);
+                               const int* inc, int i0, int i1, int* map, cudaStream_t s);
 cudaError_t launch_values_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm, int i0,
-                                int i1, const unsigned* map, double* stage, long long wait_ns, cudaStream_t s);
+                                int i1, const int* map, double* stage, long long wait_ns, cudaStream_t s);
 // The packed Ke of the elements perm[i0, i1) on the tensor cores, row q - i0 for position q.
 cudaError_t launch_stage_hex20_tc(const MeshView& m, const int* perm, int i0, int i1, double* stage, int* status,
                                   long long wait_ns, cudaStream_t s);
@@ -127,8 +128,8 @@ cudaError_t launch_stage_hex20_tc(const MeshView& m, const int* perm, int i0, in
 // zero stay in L2 until its value pass adds to them.
 constexpr int kHex20Wave = 4096;
 constexpr int kHex20GroupSize = 8;            // elements per group (group_hex20.cuh)
-constexpr int kHex20GroupMapWords = 3360;     // map record words per group (2 x 210 x 8)
-constexpr size_t kHex20WaveMapWords = (size_t)kHex20Wave / kHex20GroupSize * kHex20GroupMapWords;
+constexpr int kHex20GroupRecWords = 4376;     // record words per group (header, nodes, block table, slots)
+constexpr size_t kHex20WaveMapWords = (size_t)kHex20Wave / kHex20GroupSize * kHex20GroupRecWords;
 
 // Spatial (3-D Morton bucket) element order; hist needs 1 << (3 * morton_bits(E)) ints, bbox 6 words.
 int morton_bits(int num_elems);
@@ -169,7 +170,7 @@ struct BatchMesh {
     MeshView m;
     ListLayout L;
     long long* tiles;          // scan partials
-    unsigned* map[2];          // Hex20: map records of even / odd waves
+    int* map[2];               // Hex20: group records of even / odd waves
     int* row_ptr;              // the caller's CSR
     int* col_idx;
     double* values;

@@ -14,27 +14,28 @@ struct GroupValuesSmem {
     double X[kGroup][20][3];      // per warp: its element's node coordinates
     double iJw[kGroup][KS][10];   // per warp: inverse Jacobian (9) and weight * detJ at each Gauss point; row 27 zero
     double lam[kGroup], mu[kGroup];
-    GroupTopo T;
-    unsigned char pI[210], pJ[210];  // packed upper block p -> node pair (I, J), I <= J
+    alignas(16) int rec[2][kGroupRecWords];  // the current and the next group's record
 };
 
-// Adds the element block Ke_IJ (row-major 3x3, element nodes I <= J of the
-// group's element w) to the group's block of its node pair, transposed when
-// the pair's lower group-local node is J's. Shared-memory FP64 atomics: the
+__device__ __forceinline__ void cp_async16_v(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
+// Adds the element block Ke_IJ (row-major 3x3, I <= J) of a group element to
+// the group's block of its node pair, as the block table entry says (pair
+// index, transposed, both orientations). Shared-memory FP64 atomics: the
 // group's elements are added at the same time by different warps.
-__device__ __forceinline__ void group_add_block(GroupValuesSmem& sm, int w, int I, int J, const double (&k)[9]) {
-    const GroupTopo& T = sm.T;
-    const int u = T.lidx[20 * w + I], v = T.lidx[20 * w + J];
-    if (u <= v) {
-        double* a = sm.acc + 9 * pair_index(T, u, v);
+__device__ __forceinline__ void group_add_block(double* __restrict__ acc, unsigned e, const double (&k)[9]) {
+    double* a = acc + 9 * (e & kTabPair);
+    if (e & kTabTransposed) {
+#pragma unroll
+        for (int q = 0; q < 9; q++) atomicAdd(a + (q % 3) * 3 + q / 3, k[q]);
+    } else {
 #pragma unroll
         for (int q = 0; q < 9; q++) atomicAdd(a + q, k[q]);
-        if (u == v && I != J) {  // an element with a repeated node: both orientations land on one block
-#pragma unroll
-            for (int q = 0; q < 9; q++) atomicAdd(a + (q % 3) * 3 + q / 3, k[q]);
-        }
-    } else {
-        double* a = sm.acc + 9 * pair_index(T, v, u);
+    }
+    if (e & kTabBoth) {  // an element with a repeated node: both orientations land on one block
 #pragma unroll
         for (int q = 0; q < 9; q++) atomicAdd(a + (q % 3) * 3 + q / 3, k[q]);
     }
@@ -54,34 +55,15 @@ __device__ __forceinline__ void values_group_init(GroupValuesSmem& sm) {
     for (int idx = tid; idx < 3 * 20; idx += nt) sm.dN[idx / 20][idx % 20][27] = 0.0;
     for (int idx = tid; idx < kGroup * KS * 10; idx += nt) (&sm.iJw[0][0][0])[idx] = 0.0;
     for (int idx = tid; idx < kGroupPairs * 9; idx += nt) sm.acc[idx] = 0.0;
-    if (tid < 20) {
-        const int I = tid, p0 = I * 20 - I * (I - 1) / 2;  // packed index of block (I, I)
-        for (int J = I; J < 20; J++) {
-            sm.pI[p0 + J - I] = (unsigned char)I;
-            sm.pJ[p0 + J - I] = (unsigned char)J;
-        }
-    }
     __syncthreads();
 }
 
-// Ke of the group's element w (node ids in T.occ, element id e), computed by
-// one warp and added to the group's blocks.
-__device__ __forceinline__ void group_element_fp64(const MeshView& m, int e, int w, DevInfo* info,
+// Ke of element w of the group (coordinates already in sm.X[w], material in
+// sm.lam / sm.mu), computed by one warp and added to the group's blocks
+// through the block table `tab` (210 entries of element w).
+__device__ __forceinline__ void group_element_fp64(int w, const unsigned short* __restrict__ tab, DevInfo* info,
                                                    GroupValuesSmem& sm) {
     const int lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
-    if (lane < 20) {
-        const int n = sm.T.occ[20 * w + lane];
-        sm.X[w][lane][0] = FEM_LDG(m.x + n);
-        sm.X[w][lane][1] = FEM_LDG(m.y + n);
-        sm.X[w][lane][2] = FEM_LDG(m.z + n);
-    }
-    if (lane == 20) {
-        const double E = m.E ? FEM_LDG(m.E + e) : m.E0;
-        const double nu = m.nu ? FEM_LDG(m.nu + e) : m.nu0;
-        sm.lam[w] = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
-        sm.mu[w] = E / (2.0 * (1.0 + nu));
-    }
-    __syncwarp();
     if (lane < 27) {
         // Jacobian at Gauss point g = lane: J[3i + j] = sum_n dN[i][n][g] X[n][j]
         const int g = lane;
@@ -173,54 +155,89 @@ __device__ __forceinline__ void group_element_fp64(const MeshView& m, int e, int
 #pragma unroll
                 for (int b = 0; b < 3; b++)
                     k[3 * a + b] = fma(lam, c[a][b][h], fma(mu, c[b][a][h], a == b ? mtr : 0.0));
-            group_add_block(sm, w, I, J, k);
+            group_add_block(sm.acc, tab[packed_block(I, J)], k);
         }
     }
 }
 
-// Group value pass over the groups of positions [i0, i1) of the visit order
-// perm, group g = blockIdx.x, blockIdx.x + gridDim.x, ...; map record of
-// group g at map + g * kGroupMapWords. stage: NULL (Ke in FP64 here) or the
-// packed upper Ke blocks of the wave's elements, row q - i0 for position q
-// (the tensor-core form). kGroup warps; every thread calls it.
-__device__ void values_group(const MeshView& m, const int* __restrict__ perm, int i0, int i1,
-                             const unsigned* __restrict__ map, const double* __restrict__ stage, double* vals,
-                             DevInfo* info, GroupValuesSmem& sm) {
+// Group value pass over the groups of positions [i0, i1) of the visit order,
+// group g = blockIdx.x, blockIdx.x + gridDim.x, ...; the record of group g at
+// recs + g * kGroupRecWords (written by the claim pass). stage: NULL (Ke in
+// FP64 here) or the packed upper Ke blocks of the wave's elements, row q - i0
+// for position q (the tensor-core form). kGroup warps; every thread calls it.
+__device__ void values_group(const MeshView& m, int i0, int i1, const int* __restrict__ recs,
+                             const double* __restrict__ stage, double* vals, DevInfo* info, GroupValuesSmem& sm) {
     const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31;
     const int ngroups = (i1 - i0 + kGroup - 1) / kGroup;
-    for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
-        const long long g0 = (long long)i0 + (long long)g * kGroup;
-        const int ne = min(kGroup, i1 - (int)g0);
-        group_topology(m, perm, g0, ne, sm.T);
-        if (sm.T.bad) {  // the claim pass raised it; the group adds nothing
-            __syncthreads();
-            continue;
+    auto fetch_record = [&](int g, int buf) {
+        const int* src = recs + (size_t)g * kGroupRecWords;
+        for (int q = tid; q < kGroupRecWords / 4; q += nt) cp_async16_v(&sm.rec[buf][4 * q], src + 4 * q);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    // coordinates and material of warp `warp`'s element of the group whose record is R
+    double px = 0.0, py = 0.0, pz = 0.0, pE = 0.0, pnu = 0.0;
+    auto fetch_element = [&](const int* R) {
+        if (warp >= R[1]) return;
+        if (lane < 20) {
+            const int n = R[kRecOcc + 20 * warp + lane];
+            px = FEM_LDG(m.x + n);
+            py = FEM_LDG(m.y + n);
+            pz = FEM_LDG(m.z + n);
+        } else if (lane == 20) {
+            const int e = R[2 + warp];
+            pE = m.E ? FEM_LDG(m.E + e) : m.E0;
+            pnu = m.nu ? FEM_LDG(m.nu + e) : m.nu0;
         }
+    };
+    int g = blockIdx.x, buf = 0;
+    if (g < ngroups) {
+        fetch_record(g, 0);
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads();
+        fetch_element(sm.rec[0]);
+    }
+    for (; g < ngroups; g += gridDim.x) {
+        const int* R = sm.rec[buf];
+        const int ne = R[1], npairs = R[0];
+        const int gn = g + gridDim.x;
+        if (gn < ngroups) fetch_record(gn, buf ^ 1);
         if (warp < ne) {
-            const int e = perm ? FEM_LDG(perm + g0 + warp) : (int)(g0 + warp);
+            const unsigned short* tab = reinterpret_cast<const unsigned short*>(R + kRecTab) + warp * 210;
             if (stage) {
+                const long long g0 = (long long)i0 + (long long)g * kGroup;
                 const double* ke = stage + (size_t)(g0 + warp - i0) * kPackedHex20;
                 for (int p = lane; p < 210; p += 32) {
                     double k[9];
 #pragma unroll
                     for (int q = 0; q < 9; q++) k[q] = FEM_LDG(ke + 9 * p + q);
-                    group_add_block(sm, warp, sm.pI[p], sm.pJ[p], k);
+                    group_add_block(sm.acc, tab[p], k);
                 }
             } else {
-                group_element_fp64(m, e, warp, info, sm);
+                if (lane < 20) {
+                    sm.X[warp][lane][0] = px;
+                    sm.X[warp][lane][1] = py;
+                    sm.X[warp][lane][2] = pz;
+                } else if (lane == 20) {
+                    sm.lam[warp] = pE * pnu / ((1.0 + pnu) * (1.0 - 2.0 * pnu));
+                    sm.mu[warp] = pE / (2.0 * (1.0 + pnu));
+                }
+                __syncwarp();
+                group_element_fp64(warp, tab, info, sm);
             }
         }
-        __syncthreads();
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads();  // the group's blocks are complete; the next record is in
+        if (gn < ngroups && !stage) fetch_element(sm.rec[buf ^ 1]);
         // every block of the group once: stored where the group is the pair's
         // only contributor, added atomically where other groups add too;
         // (row u, column v) as accumulated, (row v, column u) transposed
-        const unsigned* rec = map + (size_t)g * kGroupMapWords;
-        const int n9 = sm.T.npairs * 9;
+        const unsigned* slots = reinterpret_cast<const unsigned*>(R + kRecMap);
+        const int n9 = npairs * 9;
         for (int idx = tid; idx < n9; idx += nt) {
             const int r = idx / 9, q = idx - 9 * r;
             const double val = sm.acc[idx];
             sm.acc[idx] = 0.0;
-            const unsigned w0 = FEM_LDG(rec + 2 * r), w1 = FEM_LDG(rec + 2 * r + 1);
+            const unsigned w0 = slots[2 * r], w1 = slots[2 * r + 1];
             if (map_has_slot(w0)) {
                 double* d = vals + (size_t)(w0 & ~kPairShared) * 9 + q;
                 if (w0 & kPairShared) atomicAdd(d, val);
@@ -232,7 +249,8 @@ __device__ void values_group(const MeshView& m, const int* __restrict__ perm, in
                 else *d = val;
             }
         }
-        __syncthreads();
+        __syncthreads();  // the accumulator is zero again and the record buffer free
+        buf ^= 1;
     }
 }
 

@@ -93,16 +93,16 @@ cudaError_t launch_values(const MeshView& m, const int* perm, int i0, int i1, co
 constexpr int kGroupThreads = kGroup * 32;
 
 __global__ void __launch_bounds__(kGroupThreads, 1)
-    k_values_group(MeshView m, const int* __restrict__ perm, int i0, int i1, const unsigned* __restrict__ map,
-                   const double* __restrict__ stage, double* vals, DevInfo* info) {
+    k_values_group(MeshView m, int i0, int i1, const int* __restrict__ recs, const double* __restrict__ stage,
+                   double* vals, DevInfo* info) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GroupValuesSmem& sm = *reinterpret_cast<GroupValuesSmem*>(smem_raw);
     values_group_init(sm);
-    values_group(m, perm, i0, i1, map, stage, vals, info, sm);
+    values_group(m, i0, i1, recs, stage, vals, info, sm);
 }
 
-cudaError_t launch_group_values(const MeshView& m, const ListLayout& L, const int* perm, int i0, int i1,
-                                const unsigned* map, const double* stage, cudaStream_t s) {
+cudaError_t launch_group_values(const MeshView& m, const ListLayout& L, int i0, int i1, const int* recs,
+                                const double* stage, cudaStream_t s) {
     static DeviceCache cache;
     const size_t smem = sizeof(GroupValuesSmem);
     int per_sm = 0;
@@ -114,20 +114,20 @@ cudaError_t launch_group_values(const MeshView& m, const ListLayout& L, const in
     if (err) return err;
     const long long groups = (i1 - i0 + kGroup - 1) / kGroup;
     const long long grid = std::max<long long>(1, std::min<long long>(groups, (long long)per_sm * sm_count()));
-    k_values_group<<<(int)grid, kGroupThreads, smem, s>>>(m, perm, i0, i1, map, stage, L.vals, L.info);
+    k_values_group<<<(int)grid, kGroupThreads, smem, s>>>(m, i0, i1, recs, stage, L.vals, L.info);
     return cudaGetLastError();
 }
 
 }  // namespace
 
 cudaError_t launch_values_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm, int i0,
-                                int i1, const unsigned* map, double* stage, long long wait_ns, cudaStream_t s) {
+                                int i1, const int* map, double* stage, long long wait_ns, cudaStream_t s) {
     if (i1 <= i0) return cudaSuccess;
     if (precision == FEM_PREC_TC_F16X3) {
         cudaError_t err = launch_stage_hex20_tc(m, perm, i0, i1, stage, &L.info->status_bits, wait_ns, s);
-        return err ? err : launch_group_values(m, L, perm, i0, i1, map, stage, s);
+        return err ? err : launch_group_values(m, L, i0, i1, map, stage, s);
     }
-    return launch_group_values(m, L, perm, i0, i1, map, nullptr, s);
+    return launch_group_values(m, L, i0, i1, map, nullptr, s);
 }
 
 cudaError_t launch_reassemble_hex20(const MeshView& m, int precision, const int* perm, const MapTarget& mt,

@@ -24,7 +24,7 @@ enum ValueOut : int {
 struct ValuesTarget {
     const int* map;          // kToCsrMap: CSR positions, row e
     const GroupTopo* topo;   // kToSlots: topology of the group of the elements
-    const unsigned* rec;     // kToSlots: the group's map record
+    const unsigned* rec;     // kToSlots: the slot words of the group's record
     long long g0;            // kToSlots: position of the group's first element
     double* vals;            // kToSlots: list values
     const int* row_ptr;   // kToCsr*: the CSR
