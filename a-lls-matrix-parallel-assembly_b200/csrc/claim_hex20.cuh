@@ -19,15 +19,18 @@ struct ClaimSmem {
     alignas(16) int view[kClaimRows][kClaimMaxWords];  // first chunks of a batch of row nodes
     int claims[kClaimRows];                            // entries claimed per row node of the batch
     int obase[kClaimRows + 1];                         // ordered pairs before each row of the batch
+    unsigned char cols[kClaimRows * kGroupOcc];        // the batch's ordered pairs: column node of each
     int ext[kGroupOcc][kExtMax];                       // node u's elements outside the group, ascending
-    unsigned char next[kGroupOcc];                     // their number (kExtMax + 1: more than kExtMax)
+    int inc_lo[kGroupOcc], inc_n[kGroupOcc];           // node u's incidence list (offset, length)
+    int inc_base[kGroupOcc + 1];                       // flattened incidence entries before node u
+    int next[kGroupOcc];                               // elements outside the group kept for u (capped)
     int gelem[kGroup];                                 // the group's elements
 };
 
 // Whether every element with both group-local nodes u and v is in the group:
 // no element outside the group has both.
 __device__ __forceinline__ bool pair_owned(const ClaimSmem& sm, int u, int v) {
-    const int cu = sm.next[u], cv = sm.next[v];
+    const int cu = min(sm.next[u], kExtMax + 1), cv = min(sm.next[v], kExtMax + 1);
     if (cu == 0 || cv == 0) return true;
     if (cu > kExtMax || cv > kExtMax) return false;
     int i = 0, j = 0;
@@ -90,27 +93,30 @@ __device__ int resolve_chain(const ListLayout& L, int n, int key, int& spare, bo
 }
 
 // Walks the probe sequence of column key `key` in the first chunk of row node
-// rn from step t0 on, against `view` (the chunk's copy taken at the start of
-// the batch): a slot holding the key is found; the first slot empty in the
-// copy is claimed with atomicCAS. A CAS that meets another column moves on
-// along the sequence: slots are never freed, so a column sits at the first
-// slot of its sequence that was empty when it was inserted and is never
-// inserted twice. Returns kCFound / kCClaimed with the slot, or kCChain when
-// the first chunk's sequence is full.
-__device__ unsigned char claim_walk(const ListLayout& L, int rn, const int* view, int key, int t0, int& slot) {
+// rn from step t0 on, against `view`, the chunk's copy in shared memory: a
+// slot holding the key is found; the first slot empty in the copy is claimed
+// with atomicCAS. The copy only ever holds what the slot truly holds: each
+// CAS's outcome is written back to it (the key, or the column another claimer
+// put there), so the other threads of the CTA see it. A CAS that meets another
+// column moves on along the sequence: slots are never freed, so a column sits
+// at the first slot of its sequence that was empty when it was inserted and is
+// never inserted twice. Returns kCFound / kCClaimed with the slot, or kCChain
+// when the first chunk's sequence is full.
+__device__ unsigned char claim_walk(const ListLayout& L, int rn, volatile int* view, int key, int t0, int& slot) {
     const int S1 = L.S1;
     const int p0 = probe_start(key, S1);
     int* meta = L.meta1 + (size_t)rn * L.H1 + 2;
     for (int t = t0; t < S1; t++) {
         int s = p0 + t;
         if (s >= S1) s -= S1;
-        const int x = view[2 + s];
+        const int x = view[s];
         if (x == key) {
             slot = s;
             return kCFound;
         }
         if (x != 0) continue;
         const int old = atomicCAS(meta + s, 0, key);
+        view[s] = old == 0 ? key : old;
         if (old == 0 || old == key) {
             slot = s;
             return old == 0 ? kCClaimed : kCFound;
@@ -119,22 +125,17 @@ __device__ unsigned char claim_walk(const ListLayout& L, int rn, const int* view
     return kCChain;
 }
 
-// Threads of a claiming CTA (a lane takes the columns lane, lane + 32, ... of
-// kClaimRows / kClaimWarps rows of a batch).
 constexpr int kClaimThreads = 256;
-constexpr int kClaimWarps = kClaimThreads / 32;
-constexpr int kCand = kClaimRows / kClaimWarps * kNbWords;  // candidate pairs per lane and batch
-static_assert(kClaimRows % kClaimWarps == 0, "whole rows per warp");
+constexpr int kClaimInFlight = 4;  // ordered pairs a thread resolves at once
 
 // Claim pass of the group of positions [g0, g0 + ne) of the visit order
 // (perm NULL: element i). inc_off / inc: the mesh's node -> element incidence
 // lists; NULL makes every pair shared (every claimed block is zeroed). rec:
-// the group's record (group_hex20.cuh). Every thread of the kClaimThreads-
-// thread CTA calls it.
+// the group's record (group_hex20.cuh). Every thread of the CTA calls it.
 __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* __restrict__ perm,
                             const int* __restrict__ inc_off, const int* __restrict__ inc, long long g0, int ne,
                             int* __restrict__ rec, ClaimSmem& sm) {
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
     GroupTopo& T = sm.T;
     if (tid < ne) sm.gelem[tid] = perm ? FEM_LDG(perm + g0 + tid) : (int)(g0 + tid);
     group_topology(m, perm, g0, ne, T);
@@ -166,31 +167,63 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         if (u == v && I != J) e |= kTabBoth;
         tab[k] = (unsigned short)e;
     }
-    // each node's elements outside the group (sorted, at most kExtMax kept)
+    // each node's elements outside the group (at most kExtMax kept, sorted):
+    // the incidence entries of all the group's nodes are read in parallel
     for (int u = tid; u < nu; u += nt) {
-        int c = kExtMax + 1;
+        sm.next[u] = inc_off ? 0 : kExtMax + 1;
         if (inc_off) {
             const int n = T.node[u];
-            const int o1 = FEM_LDG(inc_off + n + 1);
-            c = 0;
-            for (int k = FEM_LDG(inc_off + n); k < o1; k++) {
-                const int e = FEM_LDG(inc + k);
-                bool in = false;
-                for (int w = 0; w < ne; w++) in |= sm.gelem[w] == e;
-                if (in) continue;
-                if (c < kExtMax) {
-                    int p = c;
-                    while (p > 0 && sm.ext[u][p - 1] > e) {
-                        sm.ext[u][p] = sm.ext[u][p - 1];
-                        p--;
-                    }
-                    sm.ext[u][p] = e;
-                }
-                c++;
-            }
-            c = min(c, kExtMax + 1);
+            const int lo = FEM_LDG(inc_off + n);
+            sm.inc_lo[u] = lo;
+            sm.inc_n[u] = FEM_LDG(inc_off + n + 1) - lo;
+        } else {
+            sm.inc_n[u] = 0;
         }
-        sm.next[u] = (unsigned char)c;
+    }
+    __syncthreads();
+    if (tid < 32) {
+        int carry = 0;
+        for (int u0 = 0; u0 < nu; u0 += 32) {
+            const int c = u0 + lane < nu ? sm.inc_n[u0 + lane] : 0;
+            int incl = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+                if (lane >= d) incl += y;
+            }
+            if (u0 + lane < nu) sm.inc_base[u0 + lane] = carry + incl - c;
+            carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
+        }
+        if (lane == 0) sm.inc_base[nu] = carry;
+    }
+    __syncthreads();
+    for (int q = tid; q < sm.inc_base[nu]; q += nt) {
+        int lo = 0, hi = nu - 1;  // the last node whose first entry is <= q
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (sm.inc_base[mid] <= q) lo = mid;
+            else hi = mid - 1;
+        }
+        const int e = FEM_LDG(inc + sm.inc_lo[lo] + q - sm.inc_base[lo]);
+        bool in = false;
+        for (int w = 0; w < ne; w++) in |= sm.gelem[w] == e;
+        if (!in) {
+            const int k = atomicAdd(&sm.next[lo], 1);
+            if (k < kExtMax) sm.ext[lo][k] = e;
+        }
+    }
+    __syncthreads();
+    for (int u = tid; u < nu; u += nt) {
+        const int c = min(sm.next[u], kExtMax);
+        for (int i = 1; i < c; i++) {
+            const int e = sm.ext[u][i];
+            int p = i;
+            while (p > 0 && sm.ext[u][p - 1] > e) {
+                sm.ext[u][p] = sm.ext[u][p - 1];
+                p--;
+            }
+            sm.ext[u][p] = e;
+        }
     }
     unsigned* map = reinterpret_cast<unsigned*>(rec + kRecMap);
     int spare = -1;
@@ -203,82 +236,123 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
             const int r = q / pieces, k = q - r * pieces;
             cp_async16(&sm.view[r][4 * k], L.meta1 + (size_t)T.node[rb + r] * L.H1 + 4 * k);
         }
-        if (tid < nrows) sm.claims[tid] = 0;
+        if (tid < 32) {
+            int c = 0;
+            if (lane < nrows) {
+#pragma unroll
+                for (int w = 0; w < kNbWords; w++) c += __popc(T.nb[rb + lane][w]);
+            }
+            int incl = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+                if (lane >= d) incl += y;
+            }
+            if (lane < nrows) {
+                sm.obase[lane] = incl - c;
+                sm.claims[lane] = 0;
+            }
+            if (lane == nrows - 1) sm.obase[nrows] = incl;
+        }
+        __syncthreads();
+        // the batch's ordered pairs as a flat list of column nodes, row by row
+        for (int r = warp; r < nrows; r += nwarps) {
+            int base = sm.obase[r];
+#pragma unroll
+            for (int w = 0; w < kNbWords; w++) {
+                const unsigned bits = T.nb[rb + r][w];
+                if ((bits >> lane) & 1u) sm.cols[base + __popc(bits & ((1u << lane) - 1u))] = (unsigned char)(32 * w + lane);
+                base += __popc(bits);
+            }
+        }
         cp_async_wait_all();
         __syncthreads();
-        // this lane's candidates: row r = warp + kClaimWarps i, column 32 w + lane
-        int slot[kCand], old[kCand];
-        unsigned char st[kCand];
+        const int total = sm.obase[nrows];
+        for (int f0 = tid; f0 < total; f0 += nt * kClaimInFlight) {
+            int row[kClaimInFlight], col[kClaimInFlight], slot[kClaimInFlight], old[kClaimInFlight];
+            unsigned char st[kClaimInFlight];
+            // probe the copies
 #pragma unroll
-        for (int c = 0; c < kCand; c++) {
-            const int r = warp + kClaimWarps * (c / kNbWords), w = c % kNbWords;
-            st[c] = kCNone;
-            slot[c] = 0;
-            if (r < nrows && ((T.nb[rb + r][w] >> lane) & 1u)) {
-                const int key = T.node[32 * w + lane] + 1;
-                const int p0 = probe_start(key, S1);
-                st[c] = kCChain;
-                for (int t = 0; t < S1; t++) {
-                    int s = p0 + t;
-                    if (s >= S1) s -= S1;
-                    const int x = sm.view[r][2 + s];
-                    if (x == key || x == 0) {
-                        st[c] = x == key ? kCFound : kCTry;
-                        slot[c] = x == key ? s : t;  // kCTry: the step of the sequence
-                        break;
+            for (int j = 0; j < kClaimInFlight; j++) {
+                const int f = f0 + j * nt;
+                st[j] = kCNone;
+                row[j] = 0;
+                col[j] = 0;
+                slot[j] = 0;
+                if (f < total) {
+                    int lo = 0, hi = nrows - 1;  // the last row whose first pair is <= f
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (sm.obase[mid] <= f) lo = mid;
+                        else hi = mid - 1;
+                    }
+                    row[j] = lo;
+                    col[j] = sm.cols[f];
+                    const int key = T.node[col[j]] + 1;
+                    const volatile int* v = sm.view[lo] + 2;
+                    const int p0 = probe_start(key, S1);
+                    st[j] = kCChain;
+                    for (int t = 0; t < S1; t++) {
+                        int s = p0 + t;
+                        if (s >= S1) s -= S1;
+                        const int x = v[s];
+                        if (x == key || x == 0) {
+                            st[j] = x == key ? kCFound : kCTry;
+                            slot[j] = x == key ? s : t;  // kCTry: the step of the sequence
+                            break;
+                        }
                     }
                 }
             }
-        }
-        // every claim of the lane in flight at once
+            // the claims in flight at once
 #pragma unroll
-        for (int c = 0; c < kCand; c++) {
-            old[c] = 0;
-            if (st[c] == kCTry) {
-                const int r = warp + kClaimWarps * (c / kNbWords), w = c % kNbWords;
-                const int key = T.node[32 * w + lane] + 1;
-                int s = probe_start(key, S1) + slot[c];
-                if (s >= S1) s -= S1;
-                old[c] = atomicCAS(L.meta1 + (size_t)T.node[rb + r] * L.H1 + 2 + s, 0, key);
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < kCand; c++) {
-            if (st[c] == kCNone) continue;
-            const int r = warp + kClaimWarps * (c / kNbWords), w = c % kNbWords;
-            const int u = rb + r, v = 32 * w + lane;
-            const int rn = T.node[u], key = T.node[v] + 1;
-            int gid = -1;
-            if (st[c] == kCTry) {
-                const int t = slot[c];
-                int s = probe_start(key, S1) + t;
-                if (s >= S1) s -= S1;
-                if (old[c] == 0 || old[c] == key) {
-                    st[c] = old[c] == 0 ? kCClaimed : kCFound;
-                    slot[c] = s;
-                } else {
-                    st[c] = claim_walk(L, rn, sm.view[r], key, t + 1, slot[c]);
+            for (int j = 0; j < kClaimInFlight; j++) {
+                old[j] = 0;
+                if (st[j] == kCTry) {
+                    const int key = T.node[col[j]] + 1;
+                    int s = probe_start(key, S1) + slot[j];
+                    if (s >= S1) s -= S1;
+                    old[j] = atomicCAS(L.meta1 + (size_t)T.node[rb + row[j]] * L.H1 + 2 + s, 0, key);
+                    sm.view[row[j]][2 + s] = old[j] == 0 ? key : old[j];
                 }
             }
-            if (st[c] == kCChain) {
-                bool claimed = false;
-                gid = resolve_chain(L, rn, key, spare, claimed);
-                st[c] = claimed ? kCClaimed : kCFound;
-            } else {
-                gid = (int)slot_gid(L, rn, slot[c]);
-            }
-            const bool owned = pair_owned(sm, u, v);
-            if (gid >= 0 && st[c] == kCClaimed) {
-                if (!owned) zero_block(L.vals + (size_t)(unsigned)gid * 9);
-                atomicAdd(&sm.claims[r], 1);
-            }
-            const unsigned word = gid < 0 ? kMapNone : ((unsigned)gid | (owned ? 0u : kPairShared));
-            if (u <= v) {
-                const int p = pair_index(T, u, v);
-                map[2 * p] = word;
-                if (u == v) map[2 * p + 1] = kMapNone;
-            } else {
-                map[2 * pair_index(T, v, u) + 1] = word;
+#pragma unroll
+            for (int j = 0; j < kClaimInFlight; j++) {
+                if (st[j] == kCNone) continue;
+                const int r = row[j], u = rb + r, v = col[j];
+                const int rn = T.node[u], key = T.node[v] + 1;
+                int gid = -1;
+                if (st[j] == kCTry) {
+                    const int t = slot[j];
+                    int s = probe_start(key, S1) + t;
+                    if (s >= S1) s -= S1;
+                    if (old[j] == 0 || old[j] == key) {
+                        st[j] = old[j] == 0 ? kCClaimed : kCFound;
+                        slot[j] = s;
+                    } else {
+                        st[j] = claim_walk(L, rn, sm.view[r] + 2, key, t + 1, slot[j]);
+                    }
+                }
+                if (st[j] == kCChain) {
+                    bool claimed = false;
+                    gid = resolve_chain(L, rn, key, spare, claimed);
+                    st[j] = claimed ? kCClaimed : kCFound;
+                } else {
+                    gid = (int)slot_gid(L, rn, slot[j]);
+                }
+                const bool owned = pair_owned(sm, u, v);
+                if (gid >= 0 && st[j] == kCClaimed) {
+                    if (!owned) zero_block(L.vals + (size_t)(unsigned)gid * 9);
+                    atomicAdd(&sm.claims[r], 1);
+                }
+                const unsigned word = gid < 0 ? kMapNone : ((unsigned)gid | (owned ? 0u : kPairShared));
+                if (u <= v) {
+                    const int p = pair_index(T, u, v);
+                    map[2 * p] = word;
+                    if (u == v) map[2 * p + 1] = kMapNone;
+                } else {
+                    map[2 * pair_index(T, v, u) + 1] = word;
+                }
             }
         }
         __syncthreads();

@@ -59,7 +59,7 @@ L2_NOTE = ("a buffer of 2x L2 (252 MB) is zeroed between timed steps, outside th
            "step also moves 24.6 GB of algorithmic traffic, far above L2")
 METRIC = "elements/s (device FP64 A-LLS assembly: element stiffness, list scatter, CSR pattern + values)"
 SCATTER_KERNEL = {"q4": "k_scatter_2d<4>", "t3": "k_scatter_2d<3>", "mixed": "k_scatter_2d<4> + k_scatter_2d<3>",
-                  "hex20": "k_claim_hex20 + k_values_hex20 (two-pass list scatter, in waves)"}
+                  "hex20": "k_claim_hex20 + k_values_group (two-pass list scatter by element groups, in waves)"}
 
 
 def make_mesh(workload: str, size: int = 0, **kw):
