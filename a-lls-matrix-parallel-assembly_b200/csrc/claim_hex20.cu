@@ -41,7 +41,8 @@ namespace {
 __global__ void __launch_bounds__(kClaimThreads, 3) k_claim_hex20(MeshView m, ListLayout L, const int* __restrict__ perm,
                                                           const int* __restrict__ inc_off, const int* __restrict__ inc,
                                                           int i0, int i1, int* __restrict__ map) {
-    __shared__ ClaimSmem sm;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ClaimSmem& sm = *reinterpret_cast<ClaimSmem*>(smem_raw);
     const int ngroups = (i1 - i0 + kGroup - 1) / kGroup;
     for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
         const long long g0 = (long long)i0 + (long long)g * kGroup;
@@ -55,14 +56,17 @@ cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int
                                const int* inc, int i0, int i1, int* map, cudaStream_t s) {
     if (i1 <= i0) return cudaSuccess;
     static DeviceCache cache;
+    const size_t smem = sizeof(ClaimSmem);
     int per_sm = 0;
-    const cudaError_t err = per_device(cache, [](int& v) {
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_claim_hex20, kClaimThreads, 0);
+    const cudaError_t err = per_device(cache, [&](int& v) {
+        cudaError_t e = cudaFuncSetAttribute(k_claim_hex20, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_claim_hex20, kClaimThreads, smem);
+        return e;
     }, per_sm);
     if (err) return err;
     const long long need = (i1 - i0 + kGroup - 1) / kGroup;
     const long long grid = std::max<long long>(1, std::min<long long>(need, (long long)per_sm * sm_count()));
-    k_claim_hex20<<<(int)grid, kClaimThreads, 0, s>>>(m, L, perm, inc_off, inc, i0, i1, map);
+    k_claim_hex20<<<(int)grid, kClaimThreads, smem, s>>>(m, L, perm, inc_off, inc, i0, i1, map);
     return cudaGetLastError();
 }
 

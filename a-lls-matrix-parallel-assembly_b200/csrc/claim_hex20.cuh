@@ -8,7 +8,8 @@ namespace fem {
 namespace {
 
 constexpr int kClaimMaxWords = 96;  // first-chunk meta rows of at most 96 words (S1 <= 94, checked on the host)
-constexpr int kClaimRows = 32;      // row nodes whose first chunks are copied at once
+constexpr int kViewStride = 100;    // words between the copied rows (16-byte rows, banks spread)
+constexpr int kClaimRows = 96;      // row nodes whose first chunks are copied at once (a 2x2x2 brick has 81)
 constexpr int kExtMax = 8;          // elements outside the group kept per node (more: its pairs count as shared)
 
 enum : unsigned char { kCFound = 0, kCTry = 1, kCClaimed = 2, kCChain = 3, kCNone = 4 };
@@ -16,10 +17,12 @@ enum : unsigned char { kCFound = 0, kCTry = 1, kCClaimed = 2, kCChain = 3, kCNon
 // Shared memory of one claiming CTA.
 struct ClaimSmem {
     GroupTopo T;
-    alignas(16) int view[kClaimRows][kClaimMaxWords];  // first chunks of a batch of row nodes
+    alignas(16) int view[kClaimRows][kViewStride];     // first chunks of a batch of row nodes
     int claims[kClaimRows];                            // entries claimed per row node of the batch
     int obase[kClaimRows + 1];                         // ordered pairs before each row of the batch
-    unsigned char cols[kClaimRows * kGroupOcc];        // the batch's ordered pairs: column node of each
+    unsigned char cols[kGroup * 400];                  // the batch's ordered pairs: column node of each
+    int mult[kGroupPairs];                             // blocks of the group's elements on each node pair
+    unsigned short tab[kGroup * 210];                  // the block table before it is written
     int ext[kGroupOcc][kExtMax];                       // node u's elements outside the group, ascending
     int inc_lo[kGroupOcc], inc_n[kGroupOcc];           // node u's incidence list (offset, length)
     int inc_base[kGroupOcc + 1];                       // flattened incidence entries before node u
@@ -126,7 +129,7 @@ __device__ unsigned char claim_walk(const ListLayout& L, int rn, volatile int* v
 }
 
 constexpr int kClaimThreads = 256;
-constexpr int kClaimInFlight = 4;  // ordered pairs a thread resolves at once
+constexpr int kClaimInFlight = 10;  // ordered pairs a thread resolves at once (a brick's 2,485: one round)
 
 // Claim pass of the group of positions [g0, g0 + ne) of the visit order
 // (perm NULL: element i). inc_off / inc: the mesh's node -> element incidence
@@ -156,7 +159,8 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
     }
     if (tid < ne) rec[2 + tid] = sm.gelem[tid];
     for (int k = tid; k < ne * 20; k += nt) rec[kRecOcc + k] = T.occ[k];
-    unsigned short* tab = reinterpret_cast<unsigned short*>(rec + kRecTab);
+    for (int k = tid; k < T.npairs; k += nt) sm.mult[k] = 0;
+    __syncthreads();
     for (int k = tid; k < ne * 210; k += nt) {
         const int w = k / 210, p = k - 210 * w;
         int I = 0;
@@ -165,7 +169,14 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         const int u = T.lidx[20 * w + I], v = T.lidx[20 * w + J];
         unsigned e = u <= v ? (unsigned)pair_index(T, u, v) : ((unsigned)pair_index(T, v, u) | kTabTransposed);
         if (u == v && I != J) e |= kTabBoth;
-        tab[k] = (unsigned short)e;
+        sm.tab[k] = (unsigned short)e;
+        atomicAdd(&sm.mult[e & kTabPair], (e & kTabBoth) ? 2 : 1);
+    }
+    __syncthreads();
+    unsigned short* tab = reinterpret_cast<unsigned short*>(rec + kRecTab);
+    for (int k = tid; k < ne * 210; k += nt) {
+        const unsigned e = sm.tab[k];
+        tab[k] = (unsigned short)(sm.mult[e & kTabPair] == 1 ? e | kTabSole : e);
     }
     // each node's elements outside the group (at most kExtMax kept, sorted):
     // the incidence entries of all the group's nodes are read in parallel
@@ -237,22 +248,27 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
             cp_async16(&sm.view[r][4 * k], L.meta1 + (size_t)T.node[rb + r] * L.H1 + 4 * k);
         }
         if (tid < 32) {
-            int c = 0;
-            if (lane < nrows) {
+            int carry = 0;
+            for (int r0 = 0; r0 < nrows; r0 += 32) {
+                const int r = r0 + lane;
+                int c = 0;
+                if (r < nrows) {
 #pragma unroll
-                for (int w = 0; w < kNbWords; w++) c += __popc(T.nb[rb + lane][w]);
-            }
-            int incl = c;
+                    for (int w = 0; w < kNbWords; w++) c += __popc(T.nb[rb + r][w]);
+                }
+                int incl = c;
 #pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const int y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
-                if (lane >= d) incl += y;
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+                    if (lane >= d) incl += y;
+                }
+                if (r < nrows) {
+                    sm.obase[r] = carry + incl - c;
+                    sm.claims[r] = 0;
+                }
+                carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
             }
-            if (lane < nrows) {
-                sm.obase[lane] = incl - c;
-                sm.claims[lane] = 0;
-            }
-            if (lane == nrows - 1) sm.obase[nrows] = incl;
+            if (lane == 0) sm.obase[nrows] = carry;
         }
         __syncthreads();
         // the batch's ordered pairs as a flat list of column nodes, row by row
@@ -269,7 +285,7 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         __syncthreads();
         const int total = sm.obase[nrows];
         for (int f0 = tid; f0 < total; f0 += nt * kClaimInFlight) {
-            int row[kClaimInFlight], col[kClaimInFlight], slot[kClaimInFlight], old[kClaimInFlight];
+            int row[kClaimInFlight], col[kClaimInFlight], slot[kClaimInFlight], old[kClaimInFlight], gids[kClaimInFlight];
             unsigned char st[kClaimInFlight];
             // probe the copies
 #pragma unroll
@@ -340,6 +356,13 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
                 } else {
                     gid = (int)slot_gid(L, rn, slot[j]);
                 }
+                gids[j] = gid;
+            }
+            // the stores after every atomic of the round
+#pragma unroll
+            for (int j = 0; j < kClaimInFlight; j++) {
+                if (st[j] == kCNone) continue;
+                const int r = row[j], u = rb + r, v = col[j], gid = gids[j];
                 const bool owned = pair_owned(sm, u, v);
                 if (gid >= 0 && st[j] == kCClaimed) {
                     if (!owned) zero_block(L.vals + (size_t)(unsigned)gid * 9);
@@ -356,7 +379,8 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
             }
         }
         __syncthreads();
-        if (tid < nrows && sm.claims[tid]) atomicAdd(L.counts + T.node[rb + tid], sm.claims[tid]);
+        for (int r = tid; r < nrows; r += nt)
+            if (sm.claims[r]) atomicAdd(L.counts + T.node[rb + r], sm.claims[r]);
         __syncthreads();  // the batch's copies and counters are free
     }
 }

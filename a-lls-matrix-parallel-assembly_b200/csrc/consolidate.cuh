@@ -564,34 +564,6 @@ __device__ __forceinline__ void write_batches(const ListLayout& L, const int* __
         } else if (valid) {
             if (long_row) {
                 long_row_write<DPN, G>(L, n, u, base, glane, gmask, col_idx, values);
-            } else if constexpr (DPN == 3) {
-                // the node's dpn rows as one index space, eight values of a
-                // lane in flight before they are stored (the blocks are read
-                // from the list values, not staged)
-                constexpr int kBatch = 8;
-                const int row_len = DPN * Ts, total = DPN * row_len;
-                for (int i0 = glane; i0 < total; i0 += G * kBatch) {
-                    double v[kBatch];
-#pragma unroll
-                    for (int j = 0; j < kBatch; j++) {
-                        const int i = i0 + j * G;
-                        v[j] = 0.0;
-                        if (i < total) {
-                            const int a = i / row_len, r = i - a * row_len, k = r / DPN;
-                            v[j] = block_value(k, a * DPN + r - k * DPN);
-                        }
-                    }
-#pragma unroll
-                    for (int j = 0; j < kBatch; j++) {
-                        const int i = i0 + j * G;
-                        if (i < total) {
-                            const int a = i / row_len, r = i - a * row_len, k = r / DPN;
-                            const long long pos = base + (long long)a * DPN * u + r;
-                            col_idx[pos] = (int)(s_keys[grp][k] >> 32) * DPN + (r - k * DPN);
-                            values[pos] = v[j];
-                        }
-                    }
-                }
             } else {
                 const int row_len = DPN * Ts;
                 for (int a = 0; a < DPN; a++) {

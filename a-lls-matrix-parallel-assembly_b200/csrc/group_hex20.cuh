@@ -21,7 +21,8 @@
 //     I (I - 1) / 2 + J - I) a 16-bit entry: the pair index of the block's
 //     node pair, bit 15 set when the block lies transposed in it (u > v), bit
 //     14 set when both orientations fall on one diagonal block (an element
-//     with a repeated node);
+//     with a repeated node), bit 13 set when no other block of the group
+//     falls on the pair;
 //   kRecMap + 2 r: slot id of (row u, column v) of pair r = {u <= v}, and
 //   kRecMap + 2 r + 1: slot id of (row v, column u) (kMapNone for a diagonal
 //     pair or an unresolved slot). Bit 31 (kPairShared) marks a pair that
@@ -46,7 +47,7 @@ constexpr int kRecOcc = 16;                                 // record words: hea
 constexpr int kRecTab = kRecOcc + kGroupOcc;                // block table (two 16-bit entries a word),
 constexpr int kRecMap = kRecTab + kGroup * 210 / 2;         // slot words
 constexpr int kGroupRecWords = kRecMap + kGroupMapWords;
-constexpr unsigned kTabTransposed = 0x8000u, kTabBoth = 0x4000u, kTabPair = 0x07FFu;
+constexpr unsigned kTabTransposed = 0x8000u, kTabBoth = 0x4000u, kTabSole = 0x2000u, kTabPair = 0x07FFu;
 static_assert(kNbWords * 32 == kGroupOcc, "whole words of group-local nodes");
 static_assert(kGroupPairs <= kTabPair + 1, "pair index in 11 bits");
 static_assert(kRecTab % 4 == 0 && kRecMap % 4 == 0 && kGroupRecWords % 4 == 0, "16-byte sections");

@@ -24,11 +24,15 @@ __device__ __forceinline__ void cp_async16_v(void* dst, const void* src) {
 
 // Adds the element block Ke_IJ (row-major 3x3, I <= J) of a group element to
 // the group's block of its node pair, as the block table entry says (pair
-// index, transposed, both orientations). Shared-memory FP64 atomics: the
-// group's elements are added at the same time by different warps.
+// index, transposed, both orientations, sole block of the pair). Shared-memory
+// FP64 atomics, since the group's elements are added at the same time by
+// different warps; a pair's sole block is stored (the accumulator holds zero).
 __device__ __forceinline__ void group_add_block(double* __restrict__ acc, unsigned e, const double (&k)[9]) {
     double* a = acc + 9 * (e & kTabPair);
-    if (e & kTabTransposed) {
+    if (e & kTabSole) {
+#pragma unroll
+        for (int q = 0; q < 9; q++) a[(e & kTabTransposed) ? (q % 3) * 3 + q / 3 : q] = k[q];
+    } else if (e & kTabTransposed) {
 #pragma unroll
         for (int q = 0; q < 9; q++) atomicAdd(a + (q % 3) * 3 + q / 3, k[q]);
     } else {
