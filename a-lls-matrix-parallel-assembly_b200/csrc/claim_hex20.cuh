@@ -10,40 +10,47 @@ namespace {
 constexpr int kClaimMaxWords = 96;  // first-chunk meta rows of at most 96 words (S1 <= 94, checked on the host)
 constexpr int kViewStride = 100;    // words between the copied rows (16-byte rows, banks spread)
 constexpr int kClaimRows = 96;      // row nodes whose first chunks are copied at once (a 2x2x2 brick has 81)
-constexpr int kExtMax = 8;          // elements outside the group kept per node (more: its pairs count as shared)
+constexpr int kOutBits = 64;        // elements outside the group that get a bit of the ownership masks
+constexpr int kOutTable = 256;      // hash table of the outside elements
 
 enum : unsigned char { kCFound = 0, kCTry = 1, kCClaimed = 2, kCChain = 3, kCNone = 4 };
 
-// Shared memory of one claiming CTA.
+// Shared memory of one claiming CTA. The block-table scratch and the
+// incidence bounds are used before the row batches, the chunk copies and the
+// pair list during them.
 struct ClaimSmem {
     GroupTopo T;
-    alignas(16) int view[kClaimRows][kViewStride];     // first chunks of a batch of row nodes
-    int claims[kClaimRows];                            // entries claimed per row node of the batch
-    int obase[kClaimRows + 1];                         // ordered pairs before each row of the batch
-    unsigned char cols[kGroup * 400];                  // the batch's ordered pairs: column node of each
-    int mult[kGroupPairs];                             // blocks of the group's elements on each node pair
-    unsigned short tab[kGroup * 210];                  // the block table before it is written
-    int ext[kGroupOcc][kExtMax];                       // node u's elements outside the group, ascending
-    int inc_lo[kGroupOcc], inc_n[kGroupOcc];           // node u's incidence list (offset, length)
-    int inc_base[kGroupOcc + 1];                       // flattened incidence entries before node u
-    int next[kGroupOcc];                               // elements outside the group kept for u (capped)
-    int gelem[kGroup];                                 // the group's elements
+    union {
+        struct {
+            int mult[kGroupPairs];                 // blocks of the group's elements on each node pair
+            unsigned short tab[kGroup * 210];      // the block table before it is written
+            int inc_lo[kGroupOcc], inc_n[kGroupOcc], inc_base[kGroupOcc + 1];  // incidence of each node
+        } pre;
+        struct {
+            alignas(16) int view[kClaimRows][kViewStride];  // first chunks of a batch of row nodes
+            unsigned pairs[kGroup * 400];          // the batch's ordered pairs: row | column << 8 | record word << 16
+        } batch;
+    };
+    unsigned long long extm[kGroupOcc];   // node u's elements outside the group (mask bits)
+    unsigned unk[kNbWords];               // nodes with an outside element that has no mask bit
+    int okey[kOutTable];                  // outside elements (hash table, -1 empty)
+    unsigned char obit[kOutTable];        // their mask bits (kOutBits: none)
+    unsigned ouse[kOutTable / 32];        // occupancy of the table
+    int claims[kClaimRows];               // entries claimed per row node of the batch
+    int obase[kClaimRows + 1];            // ordered pairs before each row of the batch
+    unsigned short pdec[210];             // packed block p -> I | J << 8
+    int gelem[kGroup];                    // the group's elements
 };
 
 // Whether every element with both group-local nodes u and v is in the group:
-// no element outside the group has both.
+// no element outside the group has both (the masks of their outside
+// elements do not meet; a node with an unnumbered outside element only
+// decides when the other node has no outside element at all).
 __device__ __forceinline__ bool pair_owned(const ClaimSmem& sm, int u, int v) {
-    const int cu = min(sm.next[u], kExtMax + 1), cv = min(sm.next[v], kExtMax + 1);
-    if (cu == 0 || cv == 0) return true;
-    if (cu > kExtMax || cv > kExtMax) return false;
-    int i = 0, j = 0;
-    while (i < cu && j < cv) {
-        const int a = sm.ext[u][i], b = sm.ext[v][j];
-        if (a == b) return false;
-        if (a < b) i++;
-        else j++;
-    }
-    return true;
+    const bool ku = (sm.unk[u >> 5] >> (u & 31)) & 1u, kv = (sm.unk[v >> 5] >> (v & 31)) & 1u;
+    const unsigned long long mu = sm.extm[u], mv = sm.extm[v];
+    if ((!ku && mu == 0) || (!kv && mv == 0)) return true;
+    return !ku && !kv && (mu & mv) == 0;
 }
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
@@ -105,7 +112,8 @@ __device__ int resolve_chain(const ListLayout& L, int n, int key, int& spare, bo
 // at the first slot of its sequence that was empty when it was inserted and is
 // never inserted twice. Returns kCFound / kCClaimed with the slot, or kCChain
 // when the first chunk's sequence is full.
-__device__ unsigned char claim_walk(const ListLayout& L, int rn, volatile int* view, int key, int t0, int& slot) {
+__device__ __forceinline__ unsigned char claim_walk(const ListLayout& L, int rn, volatile int* view, int key, int t0,
+                                                    int& slot) {
     const int S1 = L.S1;
     const int p0 = probe_start(key, S1);
     int* meta = L.meta1 + (size_t)rn * L.H1 + 2;
@@ -129,7 +137,26 @@ __device__ unsigned char claim_walk(const ListLayout& L, int rn, volatile int* v
 }
 
 constexpr int kClaimThreads = 256;
-constexpr int kClaimInFlight = 10;  // ordered pairs a thread resolves at once (a brick's 2,485: one round)
+
+// Exclusive prefix sum of f(i) for i < n into out[0..n] by the first warp.
+template <typename F>
+__device__ __forceinline__ void warp_scan_into(int n, int* out, F f) {
+    const int lane = threadIdx.x & 31;
+    int carry = 0;
+    for (int i0 = 0; i0 < n; i0 += 32) {
+        const int i = i0 + lane;
+        const int c = i < n ? f(i) : 0;
+        int incl = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+            if (lane >= d) incl += y;
+        }
+        if (i < n) out[i] = carry + incl - c;
+        carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
+    }
+    if (lane == 0) out[n] = carry;
+}
 
 // Claim pass of the group of positions [g0, g0 + ne) of the visit order
 // (perm NULL: element i). inc_off / inc: the mesh's node -> element incidence
@@ -141,6 +168,13 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
     GroupTopo& T = sm.T;
     if (tid < ne) sm.gelem[tid] = perm ? FEM_LDG(perm + g0 + tid) : (int)(g0 + tid);
+    if (tid < 20) {
+        const int p0 = packed_block(tid, tid);
+        for (int J = tid; J < 20; J++) sm.pdec[p0 + J - tid] = (unsigned short)(tid | (J << 8));
+    }
+    for (int k = tid; k < kOutTable; k += nt) sm.okey[k] = -1;
+    for (int k = tid; k < kGroupOcc; k += nt) sm.extm[k] = 0ull;
+    if (tid < kNbWords) sm.unk[tid] = 0u;
     group_topology(m, perm, g0, ne, T);
     if (T.bad) {
         if (tid == 0) {
@@ -152,237 +186,169 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         return;
     }
     const int nu = T.nu;
-    // the record: header, node ids, block table
+    // the record: header, node ids, block table (with the sole-block flag)
     if (tid == 0) {
         rec[0] = T.npairs;
         rec[1] = ne;
     }
     if (tid < ne) rec[2 + tid] = sm.gelem[tid];
     for (int k = tid; k < ne * 20; k += nt) rec[kRecOcc + k] = T.occ[k];
-    for (int k = tid; k < T.npairs; k += nt) sm.mult[k] = 0;
+    for (int k = tid; k < T.npairs; k += nt) sm.pre.mult[k] = 0;
+    for (int u = tid; u < nu; u += nt) {
+        if (inc_off) {
+            const int n = T.node[u];
+            const int lo = FEM_LDG(inc_off + n);
+            sm.pre.inc_lo[u] = lo;
+            sm.pre.inc_n[u] = FEM_LDG(inc_off + n + 1) - lo;
+        } else {
+            sm.pre.inc_n[u] = 0;
+            atomicOr(&sm.unk[u >> 5], 1u << (u & 31));  // no incidence: every pair counts as shared
+        }
+    }
     __syncthreads();
+    if (tid < 32) warp_scan_into(nu, sm.pre.inc_base, [&](int u) { return sm.pre.inc_n[u]; });
     for (int k = tid; k < ne * 210; k += nt) {
-        const int w = k / 210, p = k - 210 * w;
-        int I = 0;
-        while (I < 19 && packed_block(I + 1, I + 1) <= p) I++;
-        const int J = I + p - packed_block(I, I);
+        const int w = k / 210, d = sm.pdec[k - 210 * w], I = d & 0xFF, J = d >> 8;
         const int u = T.lidx[20 * w + I], v = T.lidx[20 * w + J];
         unsigned e = u <= v ? (unsigned)pair_index(T, u, v) : ((unsigned)pair_index(T, v, u) | kTabTransposed);
         if (u == v && I != J) e |= kTabBoth;
-        sm.tab[k] = (unsigned short)e;
-        atomicAdd(&sm.mult[e & kTabPair], (e & kTabBoth) ? 2 : 1);
+        sm.pre.tab[k] = (unsigned short)e;
+        atomicAdd(&sm.pre.mult[e & kTabPair], (e & kTabBoth) ? 2 : 1);
     }
     __syncthreads();
     unsigned short* tab = reinterpret_cast<unsigned short*>(rec + kRecTab);
     for (int k = tid; k < ne * 210; k += nt) {
-        const unsigned e = sm.tab[k];
-        tab[k] = (unsigned short)(sm.mult[e & kTabPair] == 1 ? e | kTabSole : e);
+        const unsigned e = sm.pre.tab[k];
+        tab[k] = (unsigned short)(sm.pre.mult[e & kTabPair] == 1 ? e | kTabSole : e);
     }
-    // each node's elements outside the group (at most kExtMax kept, sorted):
-    // the incidence entries of all the group's nodes are read in parallel
-    for (int u = tid; u < nu; u += nt) {
-        sm.next[u] = inc_off ? 0 : kExtMax + 1;
-        if (inc_off) {
-            const int n = T.node[u];
-            const int lo = FEM_LDG(inc_off + n);
-            sm.inc_lo[u] = lo;
-            sm.inc_n[u] = FEM_LDG(inc_off + n + 1) - lo;
-        } else {
-            sm.inc_n[u] = 0;
-        }
-    }
-    __syncthreads();
-    if (tid < 32) {
-        int carry = 0;
-        for (int u0 = 0; u0 < nu; u0 += 32) {
-            const int c = u0 + lane < nu ? sm.inc_n[u0 + lane] : 0;
-            int incl = c;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const int y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
-                if (lane >= d) incl += y;
-            }
-            if (u0 + lane < nu) sm.inc_base[u0 + lane] = carry + incl - c;
-            carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
-        }
-        if (lane == 0) sm.inc_base[nu] = carry;
-    }
-    __syncthreads();
-    for (int q = tid; q < sm.inc_base[nu]; q += nt) {
+    // ownership masks: the elements outside the group that have a node of
+    // the group, numbered through a hash table (the first kOutBits get a bit)
+    const int ninc = sm.pre.inc_base[nu];
+    auto inc_entry = [&](int q, int& u) {
         int lo = 0, hi = nu - 1;  // the last node whose first entry is <= q
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (sm.inc_base[mid] <= q) lo = mid;
+            if (sm.pre.inc_base[mid] <= q) lo = mid;
             else hi = mid - 1;
         }
-        const int e = FEM_LDG(inc + sm.inc_lo[lo] + q - sm.inc_base[lo]);
-        bool in = false;
-        for (int w = 0; w < ne; w++) in |= sm.gelem[w] == e;
-        if (!in) {
-            const int k = atomicAdd(&sm.next[lo], 1);
-            if (k < kExtMax) sm.ext[lo][k] = e;
+        u = lo;
+        const int e = FEM_LDG(inc + sm.pre.inc_lo[lo] + q - sm.pre.inc_base[lo]);
+        for (int w = 0; w < ne; w++)
+            if (sm.gelem[w] == e) return -1;
+        return e;
+    };
+    auto out_slot = [&](int e) { return (int)(((unsigned)e * 2654435761u) >> 24); };
+    for (int q = tid; q < ninc; q += nt) {
+        int u;
+        const int e = inc_entry(q, u);
+        if (e < 0) continue;
+        int h = out_slot(e);
+        for (int i = 0; i < kOutTable; i++) {
+            const int old = atomicCAS(&sm.okey[h], -1, e);
+            if (old == -1 || old == e) break;
+            h = (h + 1) & (kOutTable - 1);
         }
     }
     __syncthreads();
-    for (int u = tid; u < nu; u += nt) {
-        const int c = min(sm.next[u], kExtMax);
-        for (int i = 1; i < c; i++) {
-            const int e = sm.ext[u][i];
-            int p = i;
-            while (p > 0 && sm.ext[u][p - 1] > e) {
-                sm.ext[u][p] = sm.ext[u][p - 1];
-                p--;
+    for (int s0 = warp * 32; s0 < kOutTable; s0 += nwarps * 32) {
+        const unsigned b = __ballot_sync(0xFFFFFFFFu, sm.okey[s0 + lane] != -1);
+        if (lane == 0) sm.ouse[s0 >> 5] = b;
+    }
+    __syncthreads();
+    for (int s = tid; s < kOutTable; s += nt) {
+        int r = __popc(sm.ouse[s >> 5] & ((1u << (s & 31)) - 1u));
+        for (int w = 0; w < (s >> 5); w++) r += __popc(sm.ouse[w]);
+        sm.obit[s] = (unsigned char)min(r, kOutBits);
+    }
+    __syncthreads();
+    for (int q = tid; q < ninc; q += nt) {
+        int u;
+        const int e = inc_entry(q, u);
+        if (e < 0) continue;
+        int h = out_slot(e), b = kOutBits;
+        for (int i = 0; i < kOutTable; i++) {
+            if (sm.okey[h] == e) {
+                b = sm.obit[h];
+                break;
             }
-            sm.ext[u][p] = e;
+            h = (h + 1) & (kOutTable - 1);
         }
+        if (b < kOutBits) atomicOr(&sm.extm[u], 1ull << b);
+        else atomicOr(&sm.unk[u >> 5], 1u << (u & 31));
     }
     unsigned* map = reinterpret_cast<unsigned*>(rec + kRecMap);
     int spare = -1;
     const int S1 = L.S1;
     for (int rb = 0; rb < nu; rb += kClaimRows) {
         const int nrows = min(kClaimRows, nu - rb);
+        __syncthreads();  // the block-table scratch (first batch) or the previous batch is free
         // the batch's first chunks, H1 / 4 16-byte pieces each
         const int pieces = L.H1 >> 2;
         for (int q = tid; q < nrows * pieces; q += nt) {
             const int r = q / pieces, k = q - r * pieces;
-            cp_async16(&sm.view[r][4 * k], L.meta1 + (size_t)T.node[rb + r] * L.H1 + 4 * k);
+            cp_async16(&sm.batch.view[r][4 * k], L.meta1 + (size_t)T.node[rb + r] * L.H1 + 4 * k);
         }
-        if (tid < 32) {
-            int carry = 0;
-            for (int r0 = 0; r0 < nrows; r0 += 32) {
-                const int r = r0 + lane;
+        for (int r = tid; r < nrows; r += nt) sm.claims[r] = 0;
+        if (tid < 32)
+            warp_scan_into(nrows, sm.obase, [&](int r) {
                 int c = 0;
-                if (r < nrows) {
 #pragma unroll
-                    for (int w = 0; w < kNbWords; w++) c += __popc(T.nb[rb + r][w]);
-                }
-                int incl = c;
-#pragma unroll
-                for (int d = 1; d < 32; d <<= 1) {
-                    const int y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
-                    if (lane >= d) incl += y;
-                }
-                if (r < nrows) {
-                    sm.obase[r] = carry + incl - c;
-                    sm.claims[r] = 0;
-                }
-                carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
-            }
-            if (lane == 0) sm.obase[nrows] = carry;
-        }
+                for (int w = 0; w < kNbWords; w++) c += __popc(T.nb[rb + r][w]);
+                return c;
+            });
         __syncthreads();
-        // the batch's ordered pairs as a flat list of column nodes, row by row
+        // the batch's ordered pairs, row by row: column, and the record word of
+        // the pair's slot (2 pair_index(u, v) for u <= v, 2 pair_index(v, u) + 1 else)
         for (int r = warp; r < nrows; r += nwarps) {
-            int base = sm.obase[r];
+            const int u = rb + r, base = sm.obase[r];
+            int below = 0;  // neighbours of u before u
 #pragma unroll
             for (int w = 0; w < kNbWords; w++) {
-                const unsigned bits = T.nb[rb + r][w];
-                if ((bits >> lane) & 1u) sm.cols[base + __popc(bits & ((1u << lane) - 1u))] = (unsigned char)(32 * w + lane);
-                base += __popc(bits);
+                const unsigned bits = T.nb[u][w];
+                below += w < (u >> 5) ? __popc(bits) : (w == (u >> 5) ? __popc(bits & ((1u << (u & 31)) - 1u)) : 0);
+            }
+            int cum = 0;
+#pragma unroll
+            for (int w = 0; w < kNbWords; w++) {
+                const unsigned bits = T.nb[u][w];
+                if ((bits >> lane) & 1u) {
+                    const int k = cum + __popc(bits & ((1u << lane) - 1u)), v = 32 * w + lane;
+                    const int word = u <= v ? 2 * (T.ubase[u] + k - below) : 2 * pair_index(T, v, u) + 1;
+                    sm.batch.pairs[base + k] = (unsigned)r | ((unsigned)v << 8) | ((unsigned)word << 16);
+                }
+                cum += __popc(bits);
             }
         }
         cp_async_wait_all();
         __syncthreads();
         const int total = sm.obase[nrows];
-        for (int f0 = tid; f0 < total; f0 += nt * kClaimInFlight) {
-            int row[kClaimInFlight], col[kClaimInFlight], slot[kClaimInFlight], old[kClaimInFlight], gids[kClaimInFlight];
-            unsigned char st[kClaimInFlight];
-            // probe the copies
-#pragma unroll
-            for (int j = 0; j < kClaimInFlight; j++) {
-                const int f = f0 + j * nt;
-                st[j] = kCNone;
-                row[j] = 0;
-                col[j] = 0;
-                slot[j] = 0;
-                if (f < total) {
-                    int lo = 0, hi = nrows - 1;  // the last row whose first pair is <= f
-                    while (lo < hi) {
-                        const int mid = (lo + hi + 1) >> 1;
-                        if (sm.obase[mid] <= f) lo = mid;
-                        else hi = mid - 1;
-                    }
-                    row[j] = lo;
-                    col[j] = sm.cols[f];
-                    const int key = T.node[col[j]] + 1;
-                    const volatile int* v = sm.view[lo] + 2;
-                    const int p0 = probe_start(key, S1);
-                    st[j] = kCChain;
-                    for (int t = 0; t < S1; t++) {
-                        int s = p0 + t;
-                        if (s >= S1) s -= S1;
-                        const int x = v[s];
-                        if (x == key || x == 0) {
-                            st[j] = x == key ? kCFound : kCTry;
-                            slot[j] = x == key ? s : t;  // kCTry: the step of the sequence
-                            break;
-                        }
-                    }
-                }
+        for (int f = tid; f < total; f += nt) {
+            const unsigned pr = sm.batch.pairs[f];
+            const int r = pr & 0xFF, v = (pr >> 8) & 0xFF, word_idx = pr >> 16, u = rb + r;
+            const int rn = T.node[u], key = T.node[v] + 1;
+            int slot = -1;
+            unsigned char st = claim_walk(L, rn, sm.batch.view[r] + 2, key, 0, slot);
+            int gid;
+            if (st == kCChain) {
+                bool claimed = false;
+                gid = resolve_chain(L, rn, key, spare, claimed);
+                st = claimed ? kCClaimed : kCFound;
+            } else {
+                gid = (int)slot_gid(L, rn, slot);
             }
-            // the claims in flight at once
-#pragma unroll
-            for (int j = 0; j < kClaimInFlight; j++) {
-                old[j] = 0;
-                if (st[j] == kCTry) {
-                    const int key = T.node[col[j]] + 1;
-                    int s = probe_start(key, S1) + slot[j];
-                    if (s >= S1) s -= S1;
-                    old[j] = atomicCAS(L.meta1 + (size_t)T.node[rb + row[j]] * L.H1 + 2 + s, 0, key);
-                    sm.view[row[j]][2 + s] = old[j] == 0 ? key : old[j];
-                }
+            const bool owned = pair_owned(sm, u, v);
+            if (gid >= 0 && st == kCClaimed) {
+                if (!owned) zero_block(L.vals + (size_t)(unsigned)gid * 9);
+                atomicAdd(&sm.claims[r], 1);
             }
-#pragma unroll
-            for (int j = 0; j < kClaimInFlight; j++) {
-                if (st[j] == kCNone) continue;
-                const int r = row[j], u = rb + r, v = col[j];
-                const int rn = T.node[u], key = T.node[v] + 1;
-                int gid = -1;
-                if (st[j] == kCTry) {
-                    const int t = slot[j];
-                    int s = probe_start(key, S1) + t;
-                    if (s >= S1) s -= S1;
-                    if (old[j] == 0 || old[j] == key) {
-                        st[j] = old[j] == 0 ? kCClaimed : kCFound;
-                        slot[j] = s;
-                    } else {
-                        st[j] = claim_walk(L, rn, sm.view[r] + 2, key, t + 1, slot[j]);
-                    }
-                }
-                if (st[j] == kCChain) {
-                    bool claimed = false;
-                    gid = resolve_chain(L, rn, key, spare, claimed);
-                    st[j] = claimed ? kCClaimed : kCFound;
-                } else {
-                    gid = (int)slot_gid(L, rn, slot[j]);
-                }
-                gids[j] = gid;
-            }
-            // the stores after every atomic of the round
-#pragma unroll
-            for (int j = 0; j < kClaimInFlight; j++) {
-                if (st[j] == kCNone) continue;
-                const int r = row[j], u = rb + r, v = col[j], gid = gids[j];
-                const bool owned = pair_owned(sm, u, v);
-                if (gid >= 0 && st[j] == kCClaimed) {
-                    if (!owned) zero_block(L.vals + (size_t)(unsigned)gid * 9);
-                    atomicAdd(&sm.claims[r], 1);
-                }
-                const unsigned word = gid < 0 ? kMapNone : ((unsigned)gid | (owned ? 0u : kPairShared));
-                if (u <= v) {
-                    const int p = pair_index(T, u, v);
-                    map[2 * p] = word;
-                    if (u == v) map[2 * p + 1] = kMapNone;
-                } else {
-                    map[2 * pair_index(T, v, u) + 1] = word;
-                }
-            }
+            map[word_idx] = gid < 0 ? kMapNone : ((unsigned)gid | (owned ? 0u : kPairShared));
+            if (u == v) map[word_idx + 1] = kMapNone;
         }
         __syncthreads();
         for (int r = tid; r < nrows; r += nt)
             if (sm.claims[r]) atomicAdd(L.counts + T.node[rb + r], sm.claims[r]);
-        __syncthreads();  // the batch's copies and counters are free
     }
+    __syncthreads();  // the shared memory is free for the next group
 }
 
 }  // namespace

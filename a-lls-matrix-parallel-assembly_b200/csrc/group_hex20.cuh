@@ -68,6 +68,9 @@ struct GroupTopo {
     unsigned first[kNbWords];              // occurrences that are their node's first
     unsigned short ubase[kGroupOcc + 1];   // pair index of {u, u}; ubase[nu] = number of pairs
     unsigned char lidx[kGroupOcc];         // occurrence -> group-local node
+    unsigned short hslot[kGroupOcc];       // occurrence -> its node's entry in the hash table
+    int hkey[2 * kGroupOcc];               // node id hash table (first occurrences), -1 = empty
+    int hfirst[2 * kGroupOcc];
     int ne, nu, npairs, bad;
 };
 
@@ -84,20 +87,6 @@ __device__ __forceinline__ int pair_index(const GroupTopo& T, int u, int v) {
     return r;
 }
 
-// The k-th (from 0) member of node u's neighbour set.
-__device__ __forceinline__ int nb_member(const GroupTopo& T, int u, int k) {
-    for (int w = 0; w < kNbWords; w++) {
-        unsigned bits = T.nb[u][w];
-        const int c = __popc(bits);
-        if (k < c) {
-            for (int i = 0; i < k; i++) bits &= bits - 1u;
-            return 32 * w + __ffs(bits) - 1;
-        }
-        k -= c;
-    }
-    return -1;
-}
-
 // Topology of the group of positions [g0, g0 + ne) of the visit order perm
 // (NULL: element i is position i). Every thread of the CTA calls it; it ends
 // with a barrier. A node id outside [0, N) sets T.bad (and leaves the rest
@@ -111,6 +100,10 @@ __device__ void group_topology(const MeshView& m, const int* __restrict__ perm, 
     }
     if (tid < kNbWords) T.first[tid] = 0;
     for (int k = tid; k < kGroupOcc * kNbWords; k += nt) (&T.nb[0][0])[k] = 0u;
+    for (int k = tid; k < 2 * kGroupOcc; k += nt) {
+        T.hkey[k] = -1;
+        T.hfirst[k] = kGroupOcc;
+    }
     __syncthreads();
     for (int k = tid; k < nocc; k += nt) {
         const long long i = g0 + k / 20;
@@ -121,11 +114,21 @@ __device__ void group_topology(const MeshView& m, const int* __restrict__ perm, 
     }
     __syncthreads();
     if (T.bad) return;  // uniform
-    // first occurrence of each occurrence's node
+    // first occurrence of each occurrence's node, through a hash table of the node ids
     for (int k = tid; k < nocc; k += nt) {
         const int n = T.occ[k];
-        int j = 0;
-        while (T.occ[j] != n) j++;
+        int h = (int)(((unsigned)n * 2654435761u) >> 23) % (2 * kGroupOcc);
+        for (;;) {
+            const int old = atomicCAS(&T.hkey[h], -1, n);
+            if (old == -1 || old == n) break;
+            h = h + 1 == 2 * kGroupOcc ? 0 : h + 1;
+        }
+        T.hslot[k] = (unsigned short)h;
+        atomicMin(&T.hfirst[h], k);
+    }
+    __syncthreads();
+    for (int k = tid; k < nocc; k += nt) {
+        const int j = T.hfirst[T.hslot[k]];
         T.lidx[k] = (unsigned char)j;
         if (j == k) atomicOr(&T.first[k >> 5], 1u << (k & 31));
     }
