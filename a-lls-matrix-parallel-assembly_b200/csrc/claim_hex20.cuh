@@ -24,7 +24,7 @@ struct ClaimSmem {
         struct {
             int mult[kGroupPairs];                 // blocks of the group's elements on each node pair
             unsigned short tab[kGroup * 210];      // the block table before it is written
-            int inc_lo[kGroupOcc], inc_n[kGroupOcc], inc_base[kGroupOcc + 1];  // incidence of each node
+            int inc_lo[kGroupOcc], inc_n[kGroupOcc];  // incidence list of each node
         } pre;
         struct {
             alignas(16) int view[kClaimRows][kViewStride];  // first chunks of a batch of row nodes
@@ -206,7 +206,6 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         }
     }
     __syncthreads();
-    if (tid < 32) warp_scan_into(nu, sm.pre.inc_base, [&](int u) { return sm.pre.inc_n[u]; });
     for (int k = tid; k < ne * 210; k += nt) {
         const int w = k / 210, d = sm.pdec[k - 210 * w], I = d & 0xFF, J = d >> 8;
         const int u = T.lidx[20 * w + I], v = T.lidx[20 * w + J];
@@ -223,30 +222,25 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
     }
     // ownership masks: the elements outside the group that have a node of
     // the group, numbered through a hash table (the first kOutBits get a bit)
-    const int ninc = sm.pre.inc_base[nu];
-    auto inc_entry = [&](int q, int& u) {
-        int lo = 0, hi = nu - 1;  // the last node whose first entry is <= q
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (sm.pre.inc_base[mid] <= q) lo = mid;
-            else hi = mid - 1;
-        }
-        u = lo;
-        const int e = FEM_LDG(inc + sm.pre.inc_lo[lo] + q - sm.pre.inc_base[lo]);
+    // (thread per node and entry rank modulo 8: no search for the entry's node)
+    auto outside = [&](int u, int k) {
+        const int e = FEM_LDG(inc + sm.pre.inc_lo[u] + k);
         for (int w = 0; w < ne; w++)
             if (sm.gelem[w] == e) return -1;
         return e;
     };
     auto out_slot = [&](int e) { return (int)(((unsigned)e * 2654435761u) >> 24); };
-    for (int q = tid; q < ninc; q += nt) {
-        int u;
-        const int e = inc_entry(q, u);
-        if (e < 0) continue;
-        int h = out_slot(e);
-        for (int i = 0; i < kOutTable; i++) {
-            const int old = atomicCAS(&sm.okey[h], -1, e);
-            if (old == -1 || old == e) break;
-            h = (h + 1) & (kOutTable - 1);
+    for (int t = tid; t < nu * 8; t += nt) {
+        const int u = t >> 3;
+        for (int k = t & 7; k < sm.pre.inc_n[u]; k += 8) {
+            const int e = outside(u, k);
+            if (e < 0) continue;
+            int h = out_slot(e);
+            for (int i = 0; i < kOutTable; i++) {
+                const int old = atomicCAS(&sm.okey[h], -1, e);
+                if (old == -1 || old == e) break;
+                h = (h + 1) & (kOutTable - 1);
+            }
         }
     }
     __syncthreads();
@@ -261,20 +255,22 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         sm.obit[s] = (unsigned char)min(r, kOutBits);
     }
     __syncthreads();
-    for (int q = tid; q < ninc; q += nt) {
-        int u;
-        const int e = inc_entry(q, u);
-        if (e < 0) continue;
-        int h = out_slot(e), b = kOutBits;
-        for (int i = 0; i < kOutTable; i++) {
-            if (sm.okey[h] == e) {
-                b = sm.obit[h];
-                break;
+    for (int t = tid; t < nu * 8; t += nt) {
+        const int u = t >> 3;
+        for (int k = t & 7; k < sm.pre.inc_n[u]; k += 8) {
+            const int e = outside(u, k);
+            if (e < 0) continue;
+            int h = out_slot(e), b = kOutBits;
+            for (int i = 0; i < kOutTable; i++) {
+                if (sm.okey[h] == e) {
+                    b = sm.obit[h];
+                    break;
+                }
+                h = (h + 1) & (kOutTable - 1);
             }
-            h = (h + 1) & (kOutTable - 1);
+            if (b < kOutBits) atomicOr(&sm.extm[u], 1ull << b);
+            else atomicOr(&sm.unk[u >> 5], 1u << (u & 31));
         }
-        if (b < kOutBits) atomicOr(&sm.extm[u], 1ull << b);
-        else atomicOr(&sm.unk[u >> 5], 1u << (u & 31));
     }
     unsigned* map = reinterpret_cast<unsigned*>(rec + kRecMap);
     int spare = -1;
@@ -300,13 +296,7 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         // the batch's ordered pairs, row by row: column, and the record word of
         // the pair's slot (2 pair_index(u, v) for u <= v, 2 pair_index(v, u) + 1 else)
         for (int r = warp; r < nrows; r += nwarps) {
-            const int u = rb + r, base = sm.obase[r];
-            int below = 0;  // neighbours of u before u
-#pragma unroll
-            for (int w = 0; w < kNbWords; w++) {
-                const unsigned bits = T.nb[u][w];
-                below += w < (u >> 5) ? __popc(bits) : (w == (u >> 5) ? __popc(bits & ((1u << (u & 31)) - 1u)) : 0);
-            }
+            const int u = rb + r, base = sm.obase[r], below = T.nbbelow[u];
             int cum = 0;
 #pragma unroll
             for (int w = 0; w < kNbWords; w++) {

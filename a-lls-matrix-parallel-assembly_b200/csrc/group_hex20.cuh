@@ -67,6 +67,8 @@ struct GroupTopo {
     unsigned nb[kGroupOcc][kNbWords];      // neighbour sets
     unsigned first[kNbWords];              // occurrences that are their node's first
     unsigned short ubase[kGroupOcc + 1];   // pair index of {u, u}; ubase[nu] = number of pairs
+    unsigned char nbpre[kGroupOcc][kNbWords];  // neighbours of u in the words before w
+    unsigned char nbbelow[kGroupOcc];      // neighbours of u before u
     unsigned char lidx[kGroupOcc];         // occurrence -> group-local node
     unsigned short hslot[kGroupOcc];       // occurrence -> its node's entry in the hash table
     int hkey[2 * kGroupOcc];               // node id hash table (first occurrences), -1 = empty
@@ -74,17 +76,10 @@ struct GroupTopo {
     int ne, nu, npairs, bad;
 };
 
-// Pair index of {u, v}, u <= v, v in nb[u].
+// Pair index of {u, v}, u <= v, v in nb[u]: v's rank among u's neighbours
+// from u on.
 __device__ __forceinline__ int pair_index(const GroupTopo& T, int u, int v) {
-    int r = T.ubase[u];
-    const int wu = u >> 5, wv = v >> 5;
-    for (int w = wu; w <= wv; w++) {
-        unsigned bits = T.nb[u][w];
-        if (w == wu) bits &= ~0u << (u & 31);
-        if (w == wv) bits &= (1u << (v & 31)) - 1u;
-        r += __popc(bits);
-    }
-    return r;
+    return T.ubase[u] + T.nbpre[u][v >> 5] + __popc(T.nb[u][v >> 5] & ((1u << (v & 31)) - 1u)) - T.nbbelow[u];
 }
 
 // Topology of the group of positions [g0, g0 + ne) of the visit order perm
@@ -149,6 +144,19 @@ __device__ void group_topology(const MeshView& m, const int* __restrict__ perm, 
         atomicOr(&T.nb[u][v >> 5], 1u << (v & 31));
     }
     __syncthreads();
+    // neighbour-rank tables of pair_index
+    for (int u = tid; u < kGroupOcc; u += nt) {
+        int c = 0, below = 0;
+#pragma unroll
+        for (int w = 0; w < kNbWords; w++) {
+            const unsigned bits = T.nb[u][w];
+            T.nbpre[u][w] = (unsigned char)c;
+            if (w < (u >> 5)) below += __popc(bits);
+            else if (w == (u >> 5)) below += __popc(bits & ((1u << (u & 31)) - 1u));
+            c += __popc(bits);
+        }
+        T.nbbelow[u] = (unsigned char)below;
+    }
     // pair numbering: ubase = exclusive prefix of the counts of {u <= v}
     if (tid < 32) {
         int nu = 0;

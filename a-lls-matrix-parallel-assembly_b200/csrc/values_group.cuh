@@ -235,22 +235,39 @@ __device__ void values_group(const MeshView& m, int i0, int i1, const int* __res
         // every block of the group once: stored where the group is the pair's
         // only contributor, added atomically where other groups add too;
         // (row u, column v) as accumulated, (row v, column u) transposed
+        // three threads per pair, one row a of its block each: row a of
+        // (row u, column v), column a of (row v, column u)
         const unsigned* slots = reinterpret_cast<const unsigned*>(R + kRecMap);
-        const int n9 = npairs * 9;
-        for (int idx = tid; idx < n9; idx += nt) {
-            const int r = idx / 9, q = idx - 9 * r;
-            const double val = sm.acc[idx];
-            sm.acc[idx] = 0.0;
+        const int n3 = npairs * 3;
+        for (int idx = tid; idx < n3; idx += nt) {
+            const int r = idx / 3, a = idx - 3 * r;
+            double* src = sm.acc + 3 * idx;
+            const double v0 = src[0], v1 = src[1], v2 = src[2];
+            src[0] = src[1] = src[2] = 0.0;
             const unsigned w0 = slots[2 * r], w1 = slots[2 * r + 1];
             if (map_has_slot(w0)) {
-                double* d = vals + (size_t)(w0 & ~kPairShared) * 9 + q;
-                if (w0 & kPairShared) atomicAdd(d, val);
-                else *d = val;
+                double* d = vals + (size_t)(w0 & ~kPairShared) * 9 + 3 * a;
+                if (w0 & kPairShared) {
+                    atomicAdd(d, v0);
+                    atomicAdd(d + 1, v1);
+                    atomicAdd(d + 2, v2);
+                } else {
+                    d[0] = v0;
+                    d[1] = v1;
+                    d[2] = v2;
+                }
             }
             if (map_has_slot(w1)) {
-                double* d = vals + (size_t)(w1 & ~kPairShared) * 9 + (q % 3) * 3 + q / 3;
-                if (w1 & kPairShared) atomicAdd(d, val);
-                else *d = val;
+                double* d = vals + (size_t)(w1 & ~kPairShared) * 9 + a;
+                if (w1 & kPairShared) {
+                    atomicAdd(d, v0);
+                    atomicAdd(d + 3, v1);
+                    atomicAdd(d + 6, v2);
+                } else {
+                    d[0] = v0;
+                    d[3] = v1;
+                    d[6] = v2;
+                }
             }
         }
         __syncthreads();  // the accumulator is zero again and the record buffer free
