@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                 break;
             }
             case kBpClaim: {
-                const int w0 = sg.arg * kHex20Wave, w1 = min(m.E_count, w0 + kHex20Wave);
+                const int w0 = sg.arg * kBatchHex20Wave, w1 = min(m.E_count, w0 + kBatchHex20Wave);
                 const int b = w0 + k * kBatchClaim, e1 = min(w1, b + kBatchClaim);
                 for (int gb = b; gb < e1; gb += kGroup)
                     claim_group(m, L, nullptr, nullptr, nullptr, gb, min(kGroup, e1 - gb),
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                 break;
             }
             case kBpValues: {
-                const int w0 = sg.arg * kHex20Wave, w1 = min(m.E_count, w0 + kHex20Wave);
+                const int w0 = sg.arg * kBatchHex20Wave, w1 = min(m.E_count, w0 + kBatchHex20Wave);
                 const int b = w0 + k * kBatchValues, ne = min(kGroup, w1 - b);
                 group_topology(m, nullptr, b, ne, sm.gv.topo);
                 if (sm.gv.topo.bad) break;  // the claim item raised it

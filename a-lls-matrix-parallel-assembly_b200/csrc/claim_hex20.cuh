@@ -13,7 +13,7 @@ constexpr int kClaimRows = 96;      // row nodes whose first chunks are copied a
 constexpr int kOutBits = 64;        // elements outside the group that get a bit of the ownership masks
 constexpr int kOutTable = 256;      // hash table of the outside elements
 
-enum : unsigned char { kCFound = 0, kCTry = 1, kCClaimed = 2, kCChain = 3, kCNone = 4 };
+enum : unsigned char { kCFound = 0, kCTry = 1, kCClaimed = 2, kCChain = 3, kCNone = 4, kCFail = 5 };
 
 // Shared memory of one claiming CTA. The block-table scratch and the
 // incidence bounds are used before the row batches, the chunk copies and the
@@ -29,6 +29,7 @@ struct ClaimSmem {
         struct {
             alignas(16) int view[kClaimRows][kViewStride];  // first chunks of a batch of row nodes
             unsigned pairs[kGroup * 400];          // the batch's ordered pairs: row | column << 8 | record word << 16
+            unsigned short res[kGroup * 400];      // each pair's state << 8 | slot (or probe step)
         } batch;
     };
     unsigned long long extm[kGroupOcc];   // node u's elements outside the group (mask bits)
@@ -312,12 +313,52 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         cp_async_wait_all();
         __syncthreads();
         const int total = sm.obase[nrows];
+        // 1. every pair probed in the copies: found, or the step of the first
+        // empty slot of its sequence, or a full sequence
+        for (int f = tid; f < total; f += nt) {
+            const unsigned pr = sm.batch.pairs[f];
+            const int r = pr & 0xFF, key = T.node[(pr >> 8) & 0xFF] + 1;
+            const int* v = sm.batch.view[r] + 2;
+            const int p0 = probe_start(key, S1);
+            unsigned short res = (unsigned short)(kCChain << 8);
+            for (int t = 0; t < S1; t++) {
+                int s = p0 + t;
+                if (s >= S1) s -= S1;
+                const int x = v[s];
+                if (x == key || x == 0) {
+                    res = (unsigned short)(x == key ? (kCFound << 8) | s : (kCTry << 8) | t);
+                    break;
+                }
+            }
+            sm.batch.res[f] = res;
+        }
+        __syncthreads();
+        // 2. the claims, several of a thread in flight at once; each outcome is
+        // written back to the copy (a CAS that met another claimer's column
+        // is walked on in step 3)
+#pragma unroll 8
+        for (int f = tid; f < total; f += nt) {
+            const unsigned res = sm.batch.res[f];
+            if ((res >> 8) != kCTry) continue;
+            const unsigned pr = sm.batch.pairs[f];
+            const int r = pr & 0xFF, key = T.node[(pr >> 8) & 0xFF] + 1;
+            const int t = res & 0xFF;
+            int s = probe_start(key, S1) + t;
+            if (s >= S1) s -= S1;
+            const int old = atomicCAS(L.meta1 + (size_t)T.node[rb + r] * L.H1 + 2 + s, 0, key);
+            sm.batch.view[r][2 + s] = old == 0 ? key : old;
+            sm.batch.res[f] = (unsigned short)(old == 0 ? (kCClaimed << 8) | s : (old == key ? (kCFound << 8) | s : (kCFail << 8) | t));
+        }
+        __syncthreads();
+        // 3. walks of the contested claims, overflow chains, then the stores
         for (int f = tid; f < total; f += nt) {
             const unsigned pr = sm.batch.pairs[f];
             const int r = pr & 0xFF, v = (pr >> 8) & 0xFF, word_idx = pr >> 16, u = rb + r;
             const int rn = T.node[u], key = T.node[v] + 1;
-            int slot = -1;
-            unsigned char st = claim_walk(L, rn, sm.batch.view[r] + 2, key, 0, slot);
+            const unsigned res = sm.batch.res[f];
+            unsigned char st = (unsigned char)(res >> 8);
+            int slot = res & 0xFF;
+            if (st == kCFail) st = claim_walk(L, rn, sm.batch.view[r] + 2, key, slot + 1, slot);
             int gid;
             if (st == kCChain) {
                 bool claimed = false;

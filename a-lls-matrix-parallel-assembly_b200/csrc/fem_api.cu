@@ -54,9 +54,9 @@ fem_status check_mesh(const fem_mesh* m, bool device_pointers_needed = true) {
     return FEM_OK;
 }
 
-// Map records of one wave of the Hex20 scatter for a mesh of E elements.
-size_t hex20_map_bytes(int E) {
-    const size_t groups = ((size_t)std::min(E, kHex20Wave) + kHex20GroupSize - 1) / kHex20GroupSize;
+// Group records of one wave (of `wave` elements) of the Hex20 scatter for a mesh of E elements.
+size_t hex20_map_bytes(int E, int wave = kHex20Wave) {
+    const size_t groups = ((size_t)std::min(E, wave) + kHex20GroupSize - 1) / kHex20GroupSize;
     return groups * kHex20GroupRecWords * sizeof(unsigned);
 }
 
@@ -448,13 +448,13 @@ size_t batch_mesh_bytes(const fem_mesh& m, const fem_opts* opts, fem_status& st)
     HostLayout h;
     st = make_layout(&m, opts, h);
     if (st) return 0;
-    return h.total + (h.kind == FEM_HEX20 ? align_up(hex20_map_bytes(h.E)) : 0);
+    return h.total + (h.kind == FEM_HEX20 ? align_up(hex20_map_bytes(h.E, kBatchHex20Wave)) : 0);
 }
 
 // Work items of one mesh in the batch schedule (an upper bound of the
 // segments too), used to size the schedule.
 int batch_segments_bound(const fem_mesh& m) {
-    const int waves = m.kind == FEM_HEX20 ? (m.num_elems + kHex20Wave - 1) / kHex20Wave : 0;
+    const int waves = m.kind == FEM_HEX20 ? (m.num_elems + kBatchHex20Wave - 1) / kBatchHex20Wave : 0;
     return 8 + 2 * waves;
 }
 
@@ -605,10 +605,10 @@ fem_status fem_assemble_batched(const fem_mesh* meshes, int32_t n, const fem_opt
             const int E = meshes[j].num_elems;
             if (E <= 0) continue;
             if (bms[j].kind == FEM_HEX20) {
-                const int nw = (E + kHex20Wave - 1) / kHex20Wave;
+                const int nw = (E + kBatchHex20Wave - 1) / kBatchHex20Wave;
                 std::vector<int> claims(nw), values(nw);
                 for (int w = 0; w < nw; w++) {
-                    const int ew = std::min(kHex20Wave, E - w * kHex20Wave);
+                    const int ew = std::min(kBatchHex20Wave, E - w * kBatchHex20Wave);
                     claims[w] = (ew + kBatchClaim - 1) / kBatchClaim;
                     values[w] = (ew + kBatchValues - 1) / kBatchValues;
                 }

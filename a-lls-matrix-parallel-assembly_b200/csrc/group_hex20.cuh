@@ -52,7 +52,7 @@ static_assert(kNbWords * 32 == kGroupOcc, "whole words of group-local nodes");
 static_assert(kGroupPairs <= kTabPair + 1, "pair index in 11 bits");
 static_assert(kRecTab % 4 == 0 && kRecMap % 4 == 0 && kGroupRecWords % 4 == 0, "16-byte sections");
 static_assert(kGroup == kHex20GroupSize && kGroupRecWords == kHex20GroupRecWords, "host-side sizes");
-static_assert(kHex20Wave % kGroup == 0, "waves of whole groups");
+static_assert(kHex20Wave % kGroup == 0 && kBatchHex20Wave % kGroup == 0, "waves of whole groups");
 
 // Whether a map word names a slot (slot ids are below 2^31 - 1: the layout
 // keeps the slot count below 2^31).

@@ -124,12 +124,15 @@ cudaError_t launch_values_hex20(const MeshView& m, const ListLayout& L, int prec
 // The packed Ke of the elements perm[i0, i1) on the tensor cores, row q - i0 for position q.
 cudaError_t launch_stage_hex20_tc(const MeshView& m, const int* perm, int i0, int i1, double* stage, int* status,
                                   long long wait_ns, cudaStream_t s);
-// Elements per wave of the two-pass scatter: the value blocks a wave's claims
-// zero stay in L2 until its value pass adds to them.
-constexpr int kHex20Wave = 4096;
+// Elements per wave of the two-pass scatter: a multiple of the group size,
+// large enough that each pass keeps every SM busy (4,096 groups a wave);
+// the batched kernel's waves are smaller (its items interleave many meshes).
+constexpr int kHex20Wave = 32768;
+constexpr int kBatchHex20Wave = 4096;
 constexpr int kHex20GroupSize = 8;            // elements per group (group_hex20.cuh)
 constexpr int kHex20GroupRecWords = 4376;     // record words per group (header, nodes, block table, slots)
 constexpr size_t kHex20WaveMapWords = (size_t)kHex20Wave / kHex20GroupSize * kHex20GroupRecWords;
+static_assert(kBatchHex20Wave <= kHex20Wave, "the batched ring's first map is the single-mesh one");
 
 // Spatial (3-D Morton bucket) element order; hist needs 1 << (3 * morton_bits(E)) ints, bbox 6 words.
 int morton_bits(int num_elems);

@@ -775,7 +775,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 def kernels_per_step(workload: str, mesh) -> int:
     """Library kernels launched by one assembly step."""
     if workload == "hex20":
-        waves = (mesh.num_elems + 4095) // 4096
+        waves = (mesh.num_elems + 32767) // 32768
         # k_info_init, k_bbox_init, k_bbox, Morton count / scan / scatter, k_node_degree,
         # two per wave, k_consolidate_reset, k_scan_reduce, k_scan_tiles, k_row_ptr, k_write
         return 7 + 2 * waves + 5
