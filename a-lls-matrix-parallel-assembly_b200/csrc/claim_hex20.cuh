@@ -251,6 +251,14 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         const unsigned e = sm.pre.tab[k];
         tab[k] = (unsigned short)(sm.pre.mult[e & kTabPair] == 1 ? e | kTabSole : e);
     }
+    for (int wd = tid; wd < (T.npairs + 31) / 32; wd += nt) {
+        unsigned bits = 0u;
+        for (int b = 0; b < 32; b++) {
+            const int r = 32 * wd + b;
+            if (r < T.npairs && sm.pre.mult[r] == 1) bits |= 1u << b;
+        }
+        rec[kRecSole + wd] = (int)bits;
+    }
     // ownership masks: the elements outside the group that have a node of
     // the group, numbered through a hash table (the first kOutBits get a bit)
     if (!kLookup) {

@@ -23,6 +23,7 @@
 //     14 set when both orientations fall on one diagonal block (an element
 //     with a repeated node), bit 13 set when no other block of the group
 //     falls on the pair;
+//   kRecSole: bit r set when pair r has a single block in the group;
 //   kRecMap + 2 r: slot id of (row u, column v) of pair r = {u <= v}, and
 //   kRecMap + 2 r + 1: slot id of (row v, column u) (kMapNone for a diagonal
 //     pair or an unresolved slot). Bit 31 (kPairShared) marks a pair that
@@ -45,12 +46,13 @@ constexpr unsigned kPairShared = 0x80000000u;    // map word flag: other groups 
 constexpr unsigned kMapNone = 0xFFFFFFFFu;       // map word of no slot
 constexpr int kRecOcc = 16;                                 // record words: header, then occurrences,
 constexpr int kRecTab = kRecOcc + kGroupOcc;                // block table (two 16-bit entries a word),
-constexpr int kRecMap = kRecTab + kGroup * 210 / 2;         // slot words
+constexpr int kRecSole = kRecTab + kGroup * 210 / 2;        // single-block pairs (bits),
+constexpr int kRecMap = kRecSole + (kGroupPairs + 127) / 128 * 4;  // slot words
 constexpr int kGroupRecWords = kRecMap + kGroupMapWords;
 constexpr unsigned kTabTransposed = 0x8000u, kTabBoth = 0x4000u, kTabSole = 0x2000u, kTabPair = 0x07FFu;
 static_assert(kNbWords * 32 == kGroupOcc, "whole words of group-local nodes");
 static_assert(kGroupPairs <= kTabPair + 1, "pair index in 11 bits");
-static_assert(kRecTab % 4 == 0 && kRecMap % 4 == 0 && kGroupRecWords % 4 == 0, "16-byte sections");
+static_assert(kRecTab % 4 == 0 && kRecSole % 4 == 0 && kRecMap % 4 == 0 && kGroupRecWords % 4 == 0, "16-byte sections");
 static_assert(kGroup == kHex20GroupSize && kGroupRecWords == kHex20GroupRecWords, "host-side sizes");
 static_assert(kHex20Wave % kGroup == 0 && kBatchHex20Wave % kGroup == 0, "waves of whole groups");
 

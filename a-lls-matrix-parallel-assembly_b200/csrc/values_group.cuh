@@ -22,16 +22,44 @@ __device__ __forceinline__ void cp_async16_v(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
 }
 
+// Writes block b (row-major 3x3, in the orientation (row u, column v) of its
+// pair) to the slots of the pair's two orientations, slot words w0 (row u,
+// column v) and w1 (row v, column u): stored where the group owns the pair,
+// added atomically where it is shared.
+__device__ __forceinline__ void write_pair_block(double* __restrict__ vals, unsigned w0, unsigned w1, const double (&b)[9]) {
+    if (map_has_slot(w0)) {
+        double* d = vals + (size_t)(w0 & ~kPairShared) * 9;
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            if (w0 & kPairShared) atomicAdd(d + q, b[q]);
+            else d[q] = b[q];
+        }
+    }
+    if (map_has_slot(w1)) {
+        double* d = vals + (size_t)(w1 & ~kPairShared) * 9;
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            if (w1 & kPairShared) atomicAdd(d + (q % 3) * 3 + q / 3, b[q]);
+            else d[(q % 3) * 3 + q / 3] = b[q];
+        }
+    }
+}
+
 // Adds the element block Ke_IJ (row-major 3x3, I <= J) of a group element to
 // the group's block of its node pair, as the block table entry says (pair
 // index, transposed, both orientations, sole block of the pair). Shared-memory
 // FP64 atomics, since the group's elements are added at the same time by
-// different warps; a pair's sole block is stored (the accumulator holds zero).
-__device__ __forceinline__ void group_add_block(double* __restrict__ acc, unsigned e, const double (&k)[9]) {
-    double* a = acc + 9 * (e & kTabPair);
+// different warps; a pair's sole block goes to the list at once (slot words
+// of the record).
+__device__ __forceinline__ void group_add_block(double* __restrict__ acc, const unsigned* __restrict__ slots,
+                                                double* __restrict__ vals, unsigned e, const double (&k)[9]) {
+    const int r = e & kTabPair;
+    double* a = acc + 9 * r;
     if (e & kTabSole) {
+        double b[9];
 #pragma unroll
-        for (int q = 0; q < 9; q++) a[(e & kTabTransposed) ? (q % 3) * 3 + q / 3 : q] = k[q];
+        for (int q = 0; q < 9; q++) b[q] = (e & kTabTransposed) ? k[(q % 3) * 3 + q / 3] : k[q];
+        write_pair_block(vals, slots[2 * r], slots[2 * r + 1], b);
     } else if (e & kTabTransposed) {
 #pragma unroll
         for (int q = 0; q < 9; q++) atomicAdd(a + (q % 3) * 3 + q / 3, k[q]);
@@ -65,8 +93,9 @@ __device__ __forceinline__ void values_group_init(GroupValuesSmem& sm) {
 // Ke of element w of the group (coordinates already in sm.X[w], material in
 // sm.lam / sm.mu), computed by one warp and added to the group's blocks
 // through the block table `tab` (210 entries of element w).
-__device__ __forceinline__ void group_element_fp64(int w, const unsigned short* __restrict__ tab, DevInfo* info,
-                                                   GroupValuesSmem& sm) {
+__device__ __forceinline__ void group_element_fp64(int w, const unsigned short* __restrict__ tab,
+                                                   const unsigned* __restrict__ slots, double* __restrict__ vals,
+                                                   DevInfo* info, GroupValuesSmem& sm) {
     const int lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
     if (lane < 27) {
         // Jacobian at Gauss point g = lane: J[3i + j] = sum_n dN[i][n][g] X[n][j]
@@ -159,7 +188,7 @@ __device__ __forceinline__ void group_element_fp64(int w, const unsigned short* 
 #pragma unroll
                 for (int b = 0; b < 3; b++)
                     k[3 * a + b] = fma(lam, c[a][b][h], fma(mu, c[b][a][h], a == b ? mtr : 0.0));
-            group_add_block(sm.acc, tab[packed_block(I, J)], k);
+            group_add_block(sm.acc, slots, vals, tab[packed_block(I, J)], k);
         }
     }
 }
@@ -205,6 +234,7 @@ __device__ void values_group(const MeshView& m, int i0, int i1, const int* __res
         const int ne = R[1], npairs = R[0];
         const int gn = g + gridDim.x;
         if (gn < ngroups) fetch_record(gn, buf ^ 1);
+        const unsigned* slots = reinterpret_cast<const unsigned*>(R + kRecMap);
         if (warp < ne) {
             const unsigned short* tab = reinterpret_cast<const unsigned short*>(R + kRecTab) + warp * 210;
             if (stage) {
@@ -214,7 +244,7 @@ __device__ void values_group(const MeshView& m, int i0, int i1, const int* __res
                     double k[9];
 #pragma unroll
                     for (int q = 0; q < 9; q++) k[q] = FEM_LDG(ke + 9 * p + q);
-                    group_add_block(sm.acc, tab[p], k);
+                    group_add_block(sm.acc, slots, vals, tab[p], k);
                 }
             } else {
                 if (lane < 20) {
@@ -226,7 +256,7 @@ __device__ void values_group(const MeshView& m, int i0, int i1, const int* __res
                     sm.mu[warp] = pE / (2.0 * (1.0 + pnu));
                 }
                 __syncwarp();
-                group_element_fp64(warp, tab, info, sm);
+                group_element_fp64(warp, tab, slots, vals, info, sm);
             }
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
@@ -235,12 +265,13 @@ __device__ void values_group(const MeshView& m, int i0, int i1, const int* __res
         // every block of the group once: stored where the group is the pair's
         // only contributor, added atomically where other groups add too;
         // (row u, column v) as accumulated, (row v, column u) transposed
-        // three threads per pair, one row a of its block each: row a of
-        // (row u, column v), column a of (row v, column u)
-        const unsigned* slots = reinterpret_cast<const unsigned*>(R + kRecMap);
+        // three threads per pair of several blocks, one row a of its block
+        // each: row a of (row u, column v), column a of (row v, column u)
+        const unsigned* sole = reinterpret_cast<const unsigned*>(R + kRecSole);
         const int n3 = npairs * 3;
         for (int idx = tid; idx < n3; idx += nt) {
             const int r = idx / 3, a = idx - 3 * r;
+            if ((sole[r >> 5] >> (r & 31)) & 1u) continue;  // written when it was computed
             double* src = sm.acc + 3 * idx;
             const double v0 = src[0], v1 = src[1], v2 = src[2];
             src[0] = src[1] = src[2] = 0.0;
