@@ -1,4 +1,4 @@
-// Hex20 A-LLS scatter, pass 1 of 2: list entries (the pattern) and the
+// Hex20 A-LLS scatter, pass 1 of 2: list entries (the pattern) and the map
 // records of the element groups.
 //
 // Replaces the insert half of assembleGlobalStiffnessKernelALLSFixedArray
@@ -8,34 +8,29 @@
 //
 // One CTA per element group (group_hex20.cuh: kGroup consecutive positions of
 // the spatial order), persistent over the groups of a wave. The CTA numbers
-// the group's nodes and node pairs and writes the group's record: node ids,
-// the block table of its elements (pair index, orientation, sole block), and
-// the slot word of every ordered pair (row node, column node), found or
-// claimed once however many of the group's elements share it.
+// the group's nodes and node pairs, so an ordered pair (row node, column node)
+// that several of the group's elements share is resolved once. Row nodes go
+// in batches of kClaimRows: the batch's first list chunks (next link + S1
+// hashed slots, at most 384 bytes each) are copied into shared memory with
+// cp.async, then every thread resolves ordered pairs of the batch in the copy:
+// a column found on its probe sequence is an existing entry; otherwise the
+// first slot of the sequence that is empty in the copy is claimed with
+// atomicCAS(0 -> column + 1), moving on along the sequence when the CAS meets
+// a column that another group put there (slots are never freed, so a column
+// is found or placed at the first empty slot of its sequence, never twice). A
+// full first chunk continues in the row's overflow chunks (taken from the pool
+// and linked with atomicCAS), read from global memory.
 //
-// Claims (claim_group, the batched kernel): the group's rows' first chunks
-// are copied into shared memory with cp.async; every ordered pair is probed
-// in the copy; each absent column is claimed with atomicCAS(0 -> column + 1)
-// at the first slot empty in the copy, all of a thread's claims in flight
-// together, each outcome written back to the copy (which so only ever holds
-// what the slot truly holds); a CAS that met another claimer's column walks
-// on along its probe sequence (slots are never freed, so a column is found or
-// placed at the first empty slot of its sequence, never twice); a full first
-// chunk continues in the row's overflow chunks (taken from the pool and
-// linked with atomicCAS). Ownership: a pair belongs to the group alone when
-// no element outside the group has both nodes (64-bit masks of the outside
-// elements, from the mesh's node -> element incidence; without it every pair
-// counts as shared). The claimer of a shared pair's slot zeroes its value
-// block; each claimed entry is counted for its row.
-//
-// Lookup (k_claim_hex20, the single-mesh path): the wave's row pass
-// (rows_hex20.cu) has inserted every column already, with the pairs' shared
-// flags in the slot words; the group finds its slots in the copies and
-// writes the record.
-//
-// The value pass (values_hex20.cu) is a separate launch, so every value block
-// is zeroed before any addition reaches it and no entry is ever in a
-// half-written state: no pending flags, no fences, no waits.
+// Ownership: a pair {u, v} belongs to the group alone when no element outside
+// the group has both nodes: the elements of u and of v outside the group
+// (from the mesh's node -> element incidence lists, built once per mesh)
+// have none in common. The value pass stores such a pair's blocks once; the
+// claimer of any other slot zeroes its value block for the atomic adds of
+// several groups. Each claimed entry is counted for its row, and the slot id
+// (with the shared flag) goes to the group's map record. The two passes are
+// separate launches, so every value block is zeroed before any addition
+// reaches it and no entry is ever in a half-written state: no pending flags,
+// no fences, no waits.
 #include <algorithm>
 
 #include "claim_hex20.cuh"
@@ -44,21 +39,21 @@ namespace fem {
 namespace {
 
 __global__ void __launch_bounds__(kClaimThreads, 3) k_claim_hex20(MeshView m, ListLayout L, const int* __restrict__ perm,
-                                                                   int i0, int i1, int* __restrict__ map) {
+                                                          const int* __restrict__ inc_off, const int* __restrict__ inc,
+                                                          int i0, int i1, int* __restrict__ map) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ClaimSmem& sm = *reinterpret_cast<ClaimSmem*>(smem_raw);
     const int ngroups = (i1 - i0 + kGroup - 1) / kGroup;
     for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
         const long long g0 = (long long)i0 + (long long)g * kGroup;
-        claim_group<true>(m, L, perm, nullptr, nullptr, g0, min(kGroup, i1 - (int)g0), map + (size_t)g * kGroupRecWords,
-                          sm);
+        claim_group(m, L, perm, inc_off, inc, g0, min(kGroup, i1 - (int)g0), map + (size_t)g * kGroupRecWords, sm);
     }
 }
 
 }  // namespace
 
-cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int* perm, int i0, int i1, int* map,
-                               cudaStream_t s) {
+cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int* perm, const int* inc_off,
+                               const int* inc, int i0, int i1, int* map, cudaStream_t s) {
     if (i1 <= i0) return cudaSuccess;
     static DeviceCache cache;
     const size_t smem = sizeof(ClaimSmem);
@@ -71,7 +66,7 @@ cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int
     if (err) return err;
     const long long need = (i1 - i0 + kGroup - 1) / kGroup;
     const long long grid = std::max<long long>(1, std::min<long long>(need, (long long)per_sm * sm_count()));
-    k_claim_hex20<<<(int)grid, kClaimThreads, smem, s>>>(m, L, perm, i0, i1, map);
+    k_claim_hex20<<<(int)grid, kClaimThreads, smem, s>>>(m, L, perm, inc_off, inc, i0, i1, map);
     return cudaGetLastError();
 }
 

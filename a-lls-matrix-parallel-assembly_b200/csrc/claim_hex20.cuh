@@ -159,40 +159,10 @@ __device__ __forceinline__ void warp_scan_into(int n, int* out, F f) {
     if (lane == 0) out[n] = carry;
 }
 
-// Slot of column key `key` in the overflow chunks of row node n (its first
-// chunk holds no empty slot on the key's sequence), with the stored word's
-// shared flag; -1 when the row lacks the column.
-__device__ int find_in_chain(const ListLayout& L, int n, int key, unsigned& flag) {
-    int c = n;
-    for (int step = 0; step < kMaxChainSteps; step++) {
-        const int nx = ld_cg(chunk_meta(L, c) + 1);
-        if (nx == 0) return -1;
-        c = nx - 1;
-        const int* meta = chunk_meta(L, c);
-        const int S = chunk_cap(L, c);
-        const int p0 = probe_start(key, S);
-        for (int t = 0; t < S; t++) {
-            int s = p0 + t;
-            if (s >= S) s -= S;
-            const int v = ld_cg(meta + 2 + s);
-            if ((v & kColMask) == key) {
-                flag = (unsigned)v & kPairShared;
-                return (int)slot_gid(L, c, s);
-            }
-            if (v == 0) return -1;
-        }
-    }
-    return -1;
-}
-
 // Claim pass of the group of positions [g0, g0 + ne) of the visit order
 // (perm NULL: element i). inc_off / inc: the mesh's node -> element incidence
 // lists; NULL makes every pair shared (every claimed block is zeroed). rec:
 // the group's record (group_hex20.cuh). Every thread of the CTA calls it.
-// kLookup: the rows already hold every column of the group, with the pairs'
-// shared flags in their slot words (rows_hex20.cu): the pass only finds the
-// slots and writes the record.
-template <bool kLookup = false>
 __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* __restrict__ perm,
                             const int* __restrict__ inc_off, const int* __restrict__ inc, long long g0, int ne,
                             int* __restrict__ rec, ClaimSmem& sm) {
@@ -261,7 +231,6 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
     }
     // ownership masks: the elements outside the group that have a node of
     // the group, numbered through a hash table (the first kOutBits get a bit)
-    if (!kLookup) {
     // (thread per node and entry rank modulo 8: no search for the entry's node)
     auto outside = [&](int u, int k) {
         const int e = FEM_LDG(inc + sm.pre.inc_lo[u] + k);
@@ -311,7 +280,6 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
             if (b < kOutBits) atomicOr(&sm.extm[u], 1ull << b);
             else atomicOr(&sm.unk[u >> 5], 1u << (u & 31));
         }
-    }
     }
     unsigned* map = reinterpret_cast<unsigned*>(rec + kRecMap);
     int spare = -1;
@@ -364,16 +332,15 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
             for (int t = 0; t < S1; t++) {
                 int s = p0 + t;
                 if (s >= S1) s -= S1;
-                const int x = kLookup ? (v[s] & kColMask) : v[s];
+                const int x = v[s];
                 if (x == key || x == 0) {
-                    res = (unsigned short)(x == key ? (kCFound << 8) | s : ((kLookup ? kCNone : kCTry) << 8) | t);
+                    res = (unsigned short)(x == key ? (kCFound << 8) | s : (kCTry << 8) | t);
                     break;
                 }
             }
             sm.batch.res[f] = res;
         }
         __syncthreads();
-        if (!kLookup) {
         // 2. the claims, several of a thread in flight at once; each outcome is
         // written back to the copy (a CAS that met another claimer's column
         // is walked on in step 3)
@@ -391,7 +358,6 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
             sm.batch.res[f] = (unsigned short)(old == 0 ? (kCClaimed << 8) | s : (old == key ? (kCFound << 8) | s : (kCFail << 8) | t));
         }
         __syncthreads();
-        }
         // 3. walks of the contested claims, overflow chains, then the stores
         for (int f = tid; f < total; f += nt) {
             const unsigned pr = sm.batch.pairs[f];
@@ -400,21 +366,6 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
             const unsigned res = sm.batch.res[f];
             unsigned char st = (unsigned char)(res >> 8);
             int slot = res & 0xFF;
-            if constexpr (kLookup) {
-                // every column is in the row: found in the first chunk, or in its overflow chunks
-                unsigned flag = 0u;
-                int gid = -1;
-                if (st == kCFound) {
-                    gid = (int)slot_gid(L, rn, slot);
-                    flag = (unsigned)sm.batch.view[r][2 + slot] & kPairShared;
-                } else if (st == kCChain) {
-                    gid = find_in_chain(L, rn, key, flag);
-                }
-                if (gid < 0) raise_status(L.info, FEM_ERR_INTERNAL);
-                map[word_idx] = gid < 0 ? kMapNone : ((unsigned)gid | flag);
-                if (u == v) map[word_idx + 1] = kMapNone;
-                continue;
-            }
             if (st == kCFail) st = claim_walk(L, rn, sm.batch.view[r] + 2, key, slot + 1, slot);
             int gid;
             if (st == kCChain) {
@@ -433,9 +384,8 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
             if (u == v) map[word_idx + 1] = kMapNone;
         }
         __syncthreads();
-        if (!kLookup)
-            for (int r = tid; r < nrows; r += nt)
-                if (sm.claims[r]) atomicAdd(L.counts + T.node[rb + r], sm.claims[r]);
+        for (int r = tid; r < nrows; r += nt)
+            if (sm.claims[r]) atomicAdd(L.counts + T.node[rb + r], sm.claims[r]);
     }
     __syncthreads();  // the shared memory is free for the next group
 }

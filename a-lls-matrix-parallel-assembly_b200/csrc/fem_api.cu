@@ -113,17 +113,12 @@ fem_status make_layout(const fem_mesh* m, const fem_opts* o, HostLayout& h) {
         off += align_up((size_t)h.E * sizeof(int)) + align_up(4 * sizeof(int)) + align_up(nbuckets * sizeof(int)) +
                align_up(6 * sizeof(unsigned long long));
     }
-    // Hex20: node -> element incidence (counts, offsets, lists), element
-    // positions and the waves' node lists, the records of one wave of the
-    // two-pass scatter, and (tensor-core form) the staged Ke of one wave
+    // Hex20: node -> element incidence (counts, offsets, lists), the map
+    // records of one wave of the two-pass scatter, and (tensor-core form) the
+    // staged Ke of one wave
     h.off_inc = off;
-    if (h.kind == FEM_HEX20) {
-        const int nw = (h.E + kHex20Wave - 1) / kHex20Wave;
-        if (nw > 64) return FEM_ERR_RANGE;  // Hex20 meshes of up to 64 waves (2,097,152 elements)
+    if (h.kind == FEM_HEX20)
         off += 2 * align_up((size_t)(h.N + 1) * sizeof(int)) + align_up((size_t)h.E * 20 * sizeof(int));
-        off += align_up((size_t)h.E * sizeof(int)) + 2 * align_up(65 * sizeof(int)) +
-               align_up((size_t)std::min<long long>((long long)h.E * 20, (long long)h.N * nw) * sizeof(int));
-    }
     h.off_map = off;
     if (h.kind == FEM_HEX20) off += align_up(hex20_map_bytes(h.E));
     h.off_stage = off;
@@ -264,21 +259,14 @@ fem_status fem_alls_scatter(const fem_mesh* mesh, const fem_opts* opts, void* wo
         int* inc_cnt = reinterpret_cast<int*>(b + h.off_inc);
         int* inc_off = inc_cnt + align_up((size_t)(h.N + 1) * sizeof(int)) / sizeof(int);
         int* inc = inc_off + align_up((size_t)(h.N + 1) * sizeof(int)) / sizeof(int);
-        int* pos_of = inc + align_up((size_t)h.E * 20 * sizeof(int)) / sizeof(int);
-        int* wcount = pos_of + align_up((size_t)h.E * sizeof(int)) / sizeof(int);
-        int* woff = wcount + align_up(65 * sizeof(int)) / sizeof(int);
-        int* wnodes = woff + align_up(65 * sizeof(int)) / sizeof(int);
-        const int nwaves = (h.E + kHex20Wave - 1) / kHex20Wave;
         int* map = reinterpret_cast<int*>(b + h.off_map);
         double* stage = reinterpret_cast<double*>(b + h.off_stage);
         long long* tiles = reinterpret_cast<long long*>(b + h.off_tiles);  // free until the consolidation
         const long long wait_ns = wait_ns_of(opts ? opts->wait_limit_us : 0);
         if (!err) err = launch_incidence(m, inc_cnt, inc_off, inc, tiles, &L.info->status_bits, sm_count(), s);
-        if (!err) err = launch_wave_nodes(m, perm, inc_off, inc, kHex20Wave, nwaves, pos_of, wcount, woff, wnodes, s);
-        for (int w = 0; w < nwaves && !err; w++) {
-            const int i0 = w * kHex20Wave, i1 = std::min(h.E, i0 + kHex20Wave);
-            err = launch_rows_hex20(m, L, inc_off, inc, pos_of, i0, i1, wnodes, woff, w, s);
-            if (!err) err = launch_claim_hex20(m, L, perm, i0, i1, map, s);
+        for (int i0 = 0; i0 < h.E && !err; i0 += kHex20Wave) {
+            const int i1 = std::min(h.E, i0 + kHex20Wave);
+            err = launch_claim_hex20(m, L, perm, inc_off, inc, i0, i1, map, s);
             if (!err) err = launch_values_hex20(m, L, precision, perm, i0, i1, map, stage, wait_ns, s);
         }
     } else {

@@ -106,28 +106,19 @@ cudaError_t launch_colour_hex20(const MeshView& m, const int* perm, const int* r
 // scratch; status gets 1 << FEM_ERR_* bits.
 cudaError_t launch_incidence(const MeshView& m, int* cnt, int* off, int* inc, long long* tiles, int* status, int sms,
                              cudaStream_t s);
-// Hex20 list scatter over the element groups of positions perm[i0, i1) (one
-// wave; i0 a multiple of the group size). Pass 1 inserts the wave's list
-// entries row by row, zeroing the value blocks of the entries several groups
-// add to (rows_hex20.cu), then writes the groups' records (claim_hex20.cu);
-// pass 2 adds the Ke blocks
+// Two-pass Hex20 list scatter over the element groups of positions
+// perm[i0, i1) (one wave; i0 a multiple of the group size). inc_off / inc:
+// the mesh's node -> element incidence lists (launch_incidence; NULL: every
+// node pair counts as shared by several groups). Pass 1 claims the list
+// entries, zeroes the value blocks of the entries several groups add to and
+// writes the groups' records (claim_hex20.cu); pass 2 adds the Ke blocks
 // (values_hex20.cu; in the tensor-core form the wave's Ke are computed into
 // stage first, ke_tcgen05.cu). map: kHex20WaveMapWords words (the groups'
 // records, group_hex20.cuh); stage:
 // kHex20Wave * kPackedHex20 doubles (tensor-core form only). wait_ns: see
 // wait_ns_of.
-// The wave's node lists (once per mesh): pos_of [E], wcount [nwaves],
-// woff [nwaves + 1], wnodes [sum over nodes of their waves]; nwaves <= 64.
-cudaError_t launch_wave_nodes(const MeshView& m, const int* perm, const int* inc_off, const int* inc, int wave,
-                              int nwaves, int* pos_of, int* wcount, int* woff, int* wnodes, cudaStream_t s);
-// Row pass of wave w (positions [i0, i1)): every column of the wave inserted
-// into its rows, with the pairs' shared flags (rows_hex20.cu).
-cudaError_t launch_rows_hex20(const MeshView& m, const ListLayout& L, const int* inc_off, const int* inc,
-                              const int* pos_of, int i0, int i1, const int* wnodes, const int* woff, int w,
-                              cudaStream_t s);
-// The groups' records of a wave after its row pass (claim_hex20.cu).
-cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int* perm, int i0, int i1, int* map,
-                               cudaStream_t s);
+cudaError_t launch_claim_hex20(const MeshView& m, const ListLayout& L, const int* perm, const int* inc_off,
+                               const int* inc, int i0, int i1, int* map, cudaStream_t s);
 cudaError_t launch_values_hex20(const MeshView& m, const ListLayout& L, int precision, const int* perm, int i0,
                                 int i1, const int* map, double* stage, long long wait_ns, cudaStream_t s);
 // The packed Ke of the elements perm[i0, i1) on the tensor cores, row q - i0 for position q.
