@@ -17,6 +17,11 @@ struct GroupValuesSmem {
     alignas(16) int rec[2][kGroupRecWords];  // the current and the next group's record
 };
 
+// FP64 addition to a shared-memory word, no return value.
+__device__ __forceinline__ void red_shared_f64(double* p, double v) {
+    asm volatile("red.shared.add.f64 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)), "d"(v) : "memory");
+}
+
 __device__ __forceinline__ void cp_async16_v(void* dst, const void* src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
@@ -62,14 +67,14 @@ __device__ __forceinline__ void group_add_block(double* __restrict__ acc, const 
         write_pair_block(vals, slots[2 * r], slots[2 * r + 1], b);
     } else if (e & kTabTransposed) {
 #pragma unroll
-        for (int q = 0; q < 9; q++) atomicAdd(a + (q % 3) * 3 + q / 3, k[q]);
+        for (int q = 0; q < 9; q++) red_shared_f64(a + (q % 3) * 3 + q / 3, k[q]);
     } else {
 #pragma unroll
-        for (int q = 0; q < 9; q++) atomicAdd(a + q, k[q]);
+        for (int q = 0; q < 9; q++) red_shared_f64(a + q, k[q]);
     }
     if (e & kTabBoth) {  // an element with a repeated node: both orientations land on one block
 #pragma unroll
-        for (int q = 0; q < 9; q++) atomicAdd(a + (q % 3) * 3 + q / 3, k[q]);
+        for (int q = 0; q < 9; q++) red_shared_f64(a + (q % 3) * 3 + q / 3, k[q]);
     }
 }
 
