@@ -205,7 +205,7 @@ struct BatchSegment {
 // Work item sizes.
 constexpr int kBatchResetBytes = 1 << 20;  // bytes cleared per reset item
 constexpr int kBatchScatter2D = 2048;      // 2-D elements per scatter item
-constexpr int kBatchClaim = 64;            // Hex20 elements per claim item (element groups, one at a time)
+constexpr int kBatchClaim = 8;             // Hex20 elements per claim item (one element group)
 constexpr int kBatchValues = 8;            // Hex20 elements per value item (one group, one element at a time)
 constexpr int kBatchWriteBatches = 16;     // node batches per write item
 

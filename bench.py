@@ -783,9 +783,14 @@ def kernels_per_step(workload: str, mesh) -> int:
 
 
 def batch_launches(meshes) -> int:
-    """Library kernels of one fem_assemble_batched call: each mesh's assembly
-    and its completion kernel (k_finish), plus the start stamp (k_stamp)."""
-    return 1 + sum(kernels_per_step({0: "q4", 1: "t3", 2: "hex20", 3: "mixed"}[m.kind], m) + 1 for m in meshes)
+    """Library kernels of one fem_assemble_batched call: the copies of the mesh
+    descriptors (96 a launch) and of the schedule (700 segments a launch; a
+    mesh's segments: reset, 2-D scatter or a claim and a value segment per
+    4,096-element Hex20 wave, scan tiles, top scan, row pointers, write,
+    finish), the start kernel (counters, ticket, start stamp) and the
+    persistent kernel."""
+    segs = sum(6 + 2 * ((m.num_elems + 4095) // 4096) if m.kind == 2 else 7 for m in meshes)
+    return -(-len(meshes) // 96) + -(-segs // 700) + 2
 
 
 def read_profile_traffic(workload: str):
