@@ -358,7 +358,71 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
             sm.batch.res[f] = (unsigned short)(old == 0 ? (kCClaimed << 8) | s : (old == key ? (kCFound << 8) | s : (kCFail << 8) | t));
         }
         __syncthreads();
-        // 3. walks of the contested claims, overflow chains, then the stores
+        // 3. contested claims (a CAS that met another claimer's column),
+        // in rounds over the warp: every lane takes its next contested pair
+        // and the first slot of the pair's sequence that is empty in the copy
+        // (or holds its column); of the lanes aiming at one slot of one row
+        // the first issues its CAS, and its outcome, written back to the copy,
+        // moves the others on in the next round
+        {
+            int f = tid - nt, t = 0;
+            auto next_fail = [&]() {
+                for (f += nt; f < total; f += nt)
+                    if ((sm.batch.res[f] >> 8) == kCFail) {
+                        t = (sm.batch.res[f] & 0xFF) + 1;
+                        return;
+                    }
+            };
+            next_fail();
+            for (int round = 0; round < 8 * kClaimMaxWords; round++) {
+                const bool active = f < total;
+                if (!__any_sync(0xFFFFFFFFu, active)) break;
+                int r = 0, key = 0, target = -1;
+                if (active) {
+                    const unsigned pr = sm.batch.pairs[f];
+                    r = pr & 0xFF;
+                    key = T.node[(pr >> 8) & 0xFF] + 1;
+                    const volatile int* v = sm.batch.view[r] + 2;
+                    const int p0 = probe_start(key, S1);
+                    int found = -1;
+                    for (; t < S1; t++) {
+                        int s = p0 + t;
+                        if (s >= S1) s -= S1;
+                        const int x = v[s];
+                        if (x == key) {
+                            found = s;
+                            break;
+                        }
+                        if (x == 0) {
+                            target = s;
+                            break;
+                        }
+                    }
+                    if (found >= 0) {
+                        sm.batch.res[f] = (unsigned short)((kCFound << 8) | found);
+                        next_fail();
+                    } else if (target < 0) {
+                        sm.batch.res[f] = (unsigned short)(kCChain << 8);
+                        next_fail();
+                    }
+                }
+                const unsigned mk = target >= 0 ? (((unsigned)r << 8) | (unsigned)target) : (0xFFFF0000u | (unsigned)lane);
+                const unsigned grp = __match_any_sync(0xFFFFFFFFu, mk);
+                if (target >= 0 && __ffs(grp) - 1 == lane) {
+                    const int old = atomicCAS(L.meta1 + (size_t)T.node[rb + r] * L.H1 + 2 + target, 0, key);
+                    sm.batch.view[r][2 + target] = old == 0 ? key : old;
+                    if (old == 0 || old == key) {
+                        sm.batch.res[f] = (unsigned short)(((old == 0 ? kCClaimed : kCFound) << 8) | target);
+                        next_fail();
+                    } else {
+                        t++;  // another claimer's column: on along the sequence
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // 4. what the rounds left (a very long contest), overflow chains, then the stores
         for (int f = tid; f < total; f += nt) {
             const unsigned pr = sm.batch.pairs[f];
             const int r = pr & 0xFF, v = (pr >> 8) & 0xFF, word_idx = pr >> 16, u = rb + r;
