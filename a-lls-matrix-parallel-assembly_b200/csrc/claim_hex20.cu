@@ -44,7 +44,14 @@ __global__ void __launch_bounds__(kClaimThreads, 3) k_claim_hex20(MeshView m, Li
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ClaimSmem& sm = *reinterpret_cast<ClaimSmem*>(smem_raw);
     const int ngroups = (i1 - i0 + kGroup - 1) / kGroup;
-    for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
+    // groups by class g mod 8 (for a brick-structured Morton order, the
+    // parities of the brick's coordinates), classes ordered so that
+    // consecutive ones differ in two or three parities: the groups claiming
+    // at the same time rarely share a row node
+    const int per = (ngroups + 7) / 8;
+    for (int j = blockIdx.x; j < 8 * per; j += gridDim.x) {
+        const int g = (j % per) * 8 + ((0x43526170 >> (4 * (j / per))) & 7);
+        if (g >= ngroups) continue;
         const long long g0 = (long long)i0 + (long long)g * kGroup;
         claim_group(m, L, perm, inc_off, inc, g0, min(kGroup, i1 - (int)g0), map + (size_t)g * kGroupRecWords, sm);
     }

@@ -13,7 +13,19 @@ constexpr int kClaimRows = 96;      // row nodes whose first chunks are copied a
 constexpr int kOutBits = 64;        // elements outside the group that get a bit of the ownership masks
 constexpr int kOutTable = 256;      // hash table of the outside elements
 
-enum : unsigned char { kCFound = 0, kCTry = 1, kCClaimed = 2, kCChain = 3, kCNone = 4, kCFail = 5 };
+enum : unsigned char { kCFound = 0, kCTry = 1, kCClaimed = 2, kCChain = 3, kCNone = 4, kCFail = 5, kCTent = 6 };
+
+// State of a batch pair: the probe step (0xFF: none, a full first chunk) in
+// the high byte, the state in the low byte, so that of two slots found to
+// hold one column the smaller word names the earlier one.
+constexpr int kNoStep = 0xFF;
+__device__ __forceinline__ unsigned short pair_res(int step, int state) { return (unsigned short)((step << 8) | state); }
+
+// Key word of a slot that held a second copy of a column and was retired:
+// occupied for every probe, no column for the consolidation (kColMask clears it).
+constexpr int kTombKey = (int)0x80000000u;
+
+constexpr int kPlaceIters = 8;  // placement rounds before the remaining claims walk one by one
 
 // Shared memory of one claiming CTA. The block-table scratch and the
 // incidence bounds are used before the row batches, the chunk copies and the
@@ -22,14 +34,16 @@ struct ClaimSmem {
     GroupTopo T;
     union {
         struct {
-            int mult[kGroupPairs];                 // blocks of the group's elements on each node pair
+            int mult[kGroupPairs];                 // blocks of the group's elements on each node pair, then fill counters
+            int cofs[kGroupPairs + 1];             // first entry of each pair's blocks
             unsigned short tab[kGroup * 210];      // the block table before it is written
             int inc_lo[kGroupOcc], inc_n[kGroupOcc];  // incidence list of each node
         } pre;
         struct {
             alignas(16) int view[kClaimRows][kViewStride];  // first chunks of a batch of row nodes
             unsigned pairs[kGroup * 400];          // the batch's ordered pairs: row | column << 8 | record word << 16
-            unsigned short res[kGroup * 400];      // each pair's state << 8 | slot (or probe step)
+            unsigned short res[kGroup * 400];      // each pair's probe step << 8 | state (pair_res)
+            unsigned char home[kGroup * 400];      // earliest probe step a met claim showed holding the pair's column (0xFF: none)
         } batch;
     };
     unsigned long long extm[kGroupOcc];   // node u's elements outside the group (mask bits)
@@ -139,6 +153,24 @@ __device__ __forceinline__ unsigned char claim_walk(const ListLayout& L, int rn,
 
 constexpr int kClaimThreads = 256;
 
+// Slot of probe step t of a sequence starting at p0 in a chunk of S slots.
+__device__ __forceinline__ int probe_slot(int p0, int t, int S) {
+    const int s = p0 + t;
+    return s >= S ? s - S : s;
+}
+
+// Group-local node of node id n (-1 when the group has no such node).
+__device__ __forceinline__ int local_node(const GroupTopo& T, int n) {
+    int h = (int)(((unsigned)n * 2654435761u) >> 23) % (2 * kGroupOcc);
+    for (int i = 0; i < 2 * kGroupOcc; i++) {
+        const int k = T.hkey[h];
+        if (k == n) return T.lidx[T.hfirst[h]];
+        if (k == -1) return -1;
+        h = h + 1 == 2 * kGroupOcc ? 0 : h + 1;
+    }
+    return -1;
+}
+
 // Exclusive prefix sum of f(i) for i < n into out[0..n] by the first warp.
 template <typename F>
 __device__ __forceinline__ void warp_scan_into(int n, int* out, F f) {
@@ -213,21 +245,23 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         unsigned e = u <= v ? (unsigned)pair_index(T, u, v) : ((unsigned)pair_index(T, v, u) | kTabTransposed);
         if (u == v && I != J) e |= kTabBoth;
         sm.pre.tab[k] = (unsigned short)e;
-        atomicAdd(&sm.pre.mult[e & kTabPair], (e & kTabBoth) ? 2 : 1);
+        atomicAdd(&sm.pre.mult[e & kTabPair], 1);
     }
     __syncthreads();
-    unsigned short* tab = reinterpret_cast<unsigned short*>(rec + kRecTab);
+    // the element blocks grouped by pair: offsets (a scan of the counts),
+    // then each block placed at its pair's next free entry
+    if (tid < 32) warp_scan_into(T.npairs, sm.pre.cofs, [&](int r) { return sm.pre.mult[r]; });
+    __syncthreads();
+    unsigned short* cofs = reinterpret_cast<unsigned short*>(rec + kRecCofs);
+    for (int r = tid; r <= T.npairs; r += nt) {
+        cofs[r] = (unsigned short)sm.pre.cofs[r];
+        if (r < T.npairs) sm.pre.mult[r] = sm.pre.cofs[r];
+    }
+    __syncthreads();
+    unsigned short* cont = reinterpret_cast<unsigned short*>(rec + kRecCont);
     for (int k = tid; k < ne * 210; k += nt) {
         const unsigned e = sm.pre.tab[k];
-        tab[k] = (unsigned short)(sm.pre.mult[e & kTabPair] == 1 ? e | kTabSole : e);
-    }
-    for (int wd = tid; wd < (T.npairs + 31) / 32; wd += nt) {
-        unsigned bits = 0u;
-        for (int b = 0; b < 32; b++) {
-            const int r = 32 * wd + b;
-            if (r < T.npairs && sm.pre.mult[r] == 1) bits |= 1u << b;
-        }
-        rec[kRecSole + wd] = (int)bits;
+        cont[atomicAdd(&sm.pre.mult[e & kTabPair], 1)] = (unsigned short)(k | (e & (kTabTransposed | kTabBoth)));
     }
     // ownership masks: the elements outside the group that have a node of
     // the group, numbered through a hash table (the first kOutBits get a bit)
@@ -328,109 +362,132 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
             const int r = pr & 0xFF, key = T.node[(pr >> 8) & 0xFF] + 1;
             const int* v = sm.batch.view[r] + 2;
             const int p0 = probe_start(key, S1);
-            unsigned short res = (unsigned short)(kCChain << 8);
+            unsigned short res = pair_res(kNoStep, kCChain);
             for (int t = 0; t < S1; t++) {
-                int s = p0 + t;
-                if (s >= S1) s -= S1;
-                const int x = v[s];
+                const int x = v[probe_slot(p0, t, S1)];
                 if (x == key || x == 0) {
-                    res = (unsigned short)(x == key ? (kCFound << 8) | s : (kCTry << 8) | t);
+                    res = pair_res(t, x == key ? kCFound : kCTry);
                     break;
                 }
             }
             sm.batch.res[f] = res;
+            sm.batch.home[f] = 0xFF;
         }
         __syncthreads();
-        // 2. the claims, several of a thread in flight at once; each outcome is
-        // written back to the copy (a CAS that met another claimer's column
-        // is walked on in step 3)
-#pragma unroll 8
-        for (int f = tid; f < total; f += nt) {
-            const unsigned res = sm.batch.res[f];
-            if ((res >> 8) != kCTry) continue;
-            const unsigned pr = sm.batch.pairs[f];
-            const int r = pr & 0xFF, key = T.node[(pr >> 8) & 0xFF] + 1;
-            const int t = res & 0xFF;
-            int s = probe_start(key, S1) + t;
-            if (s >= S1) s -= S1;
-            const int old = atomicCAS(L.meta1 + (size_t)T.node[rb + r] * L.H1 + 2 + s, 0, key);
-            sm.batch.view[r][2 + s] = old == 0 ? key : old;
-            sm.batch.res[f] = (unsigned short)(old == 0 ? (kCClaimed << 8) | s : (old == key ? (kCFound << 8) | s : (kCFail << 8) | t));
-        }
-        __syncthreads();
-        // 3. contested claims (a CAS that met another claimer's column),
-        // in rounds over the warp: every lane takes its next contested pair
-        // and the first slot of the pair's sequence that is empty in the copy
-        // (or holds its column); of the lanes aiming at one slot of one row
-        // the first issues its CAS, and its outcome, written back to the copy,
-        // moves the others on in the next round
-        {
-            int f = tid - nt, t = 0;
-            auto next_fail = [&]() {
-                for (f += nt; f < total; f += nt)
-                    if ((sm.batch.res[f] >> 8) == kCFail) {
-                        t = (sm.batch.res[f] & 0xFF) + 1;
-                        return;
-                    }
-            };
-            next_fail();
-            for (int round = 0; round < 8 * kClaimMaxWords; round++) {
-                const bool active = f < total;
-                if (!__any_sync(0xFFFFFFFFu, active)) break;
-                int r = 0, key = 0, target = -1;
-                if (active) {
-                    const unsigned pr = sm.batch.pairs[f];
-                    r = pr & 0xFF;
-                    key = T.node[(pr >> 8) & 0xFF] + 1;
-                    const volatile int* v = sm.batch.view[r] + 2;
-                    const int p0 = probe_start(key, S1);
-                    int found = -1;
-                    for (; t < S1; t++) {
-                        int s = p0 + t;
-                        if (s >= S1) s -= S1;
-                        const int x = v[s];
-                        if (x == key) {
-                            found = s;
-                            break;
-                        }
+        // 2.-4. placement rounds. Each round first places every pending
+        // column in the copy (shared-memory CAS: the first slot of its
+        // sequence empty in the copy becomes its tentative slot, so the
+        // CTA's own columns never meet in global memory), then issues all
+        // tentative claims to the list at once (atomicCAS(0 -> key)), and
+        // writes each outcome back to the copy, which so holds only what the
+        // slots truly hold again. A claim that met another group's column
+        // goes on from the next step in the next round.
+        //
+        // A column's tentative slot can lie beyond a slot that another of the
+        // CTA's columns held tentatively. If another group put the column
+        // itself there meanwhile, the claim met there reports it: the column's
+        // entry is the earliest slot of its sequence known to hold it
+        // (collected per pair as a byte minimum, applied after a barrier), and
+        // a later slot this CTA claimed for it is retired with kTombKey. Other groups never map the
+        // column to that later slot: their probes reach the earlier one first.
+        for (int it = 0; it < kPlaceIters; it++) {
+            int pend = 0;
+            for (int f = tid; f < total; f += nt) {
+                const unsigned short res = sm.batch.res[f];
+                const int st = res & 0xFF;
+                if (st != kCTry && st != kCFail) continue;
+                const unsigned pr = sm.batch.pairs[f];
+                const int r = pr & 0xFF, key = T.node[(pr >> 8) & 0xFF] + 1;
+                int* v = sm.batch.view[r] + 2;
+                const int p0 = probe_start(key, S1);
+                unsigned short out = pair_res(kNoStep, kCChain);
+                for (int t = (res >> 8) + (st == kCFail ? 1 : 0); t < S1; t++) {
+                    const int s = probe_slot(p0, t, S1);
+                    int x = reinterpret_cast<volatile int*>(v)[s];
+                    if (x == 0) {
+                        x = atomicCAS(v + s, 0, key);
                         if (x == 0) {
-                            target = s;
+                            out = pair_res(t, kCTent);
                             break;
                         }
                     }
-                    if (found >= 0) {
-                        sm.batch.res[f] = (unsigned short)((kCFound << 8) | found);
-                        next_fail();
-                    } else if (target < 0) {
-                        sm.batch.res[f] = (unsigned short)(kCChain << 8);
-                        next_fail();
+                    if (x == key) {
+                        out = pair_res(t, kCFound);
+                        break;
                     }
                 }
-                const unsigned mk = target >= 0 ? (((unsigned)r << 8) | (unsigned)target) : (0xFFFF0000u | (unsigned)lane);
-                const unsigned grp = __match_any_sync(0xFFFFFFFFu, mk);
-                if (target >= 0 && __ffs(grp) - 1 == lane) {
-                    const int old = atomicCAS(L.meta1 + (size_t)T.node[rb + r] * L.H1 + 2 + target, 0, key);
-                    sm.batch.view[r][2 + target] = old == 0 ? key : old;
-                    if (old == 0 || old == key) {
-                        sm.batch.res[f] = (unsigned short)(((old == 0 ? kCClaimed : kCFound) << 8) | target);
-                        next_fail();
-                    } else {
-                        t++;  // another claimer's column: on along the sequence
-                    }
-                }
-                __syncwarp();
+                sm.batch.res[f] = out;
+                pend = 1;
             }
+            if (!__syncthreads_or(pend)) break;
+#pragma unroll 8
+            for (int f = tid; f < total; f += nt) {
+                const unsigned short res = sm.batch.res[f];
+                if ((res & 0xFF) != kCTent) continue;
+                const unsigned pr = sm.batch.pairs[f];
+                const int r = pr & 0xFF, key = T.node[(pr >> 8) & 0xFF] + 1;
+                const int t = res >> 8, s = probe_slot(probe_start(key, S1), t, S1);
+                const int old = atomicCAS(L.meta1 + (size_t)T.node[rb + r] * L.H1 + 2 + s, 0, key);
+                if (old != 0 && old != key) sm.batch.view[r][2 + s] = old;
+                sm.batch.res[f] = pair_res(t, old == 0 ? kCClaimed : (old == key ? kCFound : kCFail));
+            }
+            __syncthreads();
+            // claims that met a column of this group's row: the earliest step
+            // at which a slot is known to hold it (a byte minimum), ...
+            int met = 0;
+            for (int f = tid; f < total; f += nt) {
+                const unsigned short res = sm.batch.res[f];
+                if ((res & 0xFF) != kCFail) continue;
+                const unsigned pr = sm.batch.pairs[f];
+                const int r = pr & 0xFF, u = rb + r, key = T.node[(pr >> 8) & 0xFF] + 1;
+                const int w = sm.batch.view[r][2 + probe_slot(probe_start(key, S1), res >> 8, S1)];
+                if (w <= 0) continue;  // a retired slot
+                const int vw = local_node(T, w - 1);
+                if (vw < 0 || !((T.nb[u][vw >> 5] >> (vw & 31)) & 1u)) continue;
+                const int fw = sm.obase[r] + T.nbpre[u][vw >> 5] + __popc(T.nb[u][vw >> 5] & ((1u << (vw & 31)) - 1u));
+                int tw = probe_slot(probe_start(key, S1), res >> 8, S1) - probe_start(w, S1);
+                if (tw < 0) tw += S1;
+                unsigned* word = reinterpret_cast<unsigned*>(&sm.batch.home[fw & ~3]);
+                const int sh = (fw & 3) * 8;
+                unsigned cur = *reinterpret_cast<volatile unsigned*>(word);
+                while (((cur >> sh) & 0xFFu) > (unsigned)tw) {
+                    const unsigned seen = atomicCAS(word, cur, (cur & ~(0xFFu << sh)) | ((unsigned)tw << sh));
+                    if (seen == cur) break;
+                    cur = seen;
+                }
+                met = 1;
+            }
+            if (!__syncthreads_or(met)) continue;
+            // ... which becomes the pair's entry unless it already has an
+            // earlier one or its next probe step comes first; a slot this CTA
+            // claimed later in the sequence is retired
+            for (int f = tid; f < total; f += nt) {
+                const int h = sm.batch.home[f];
+                if (h == 0xFF) continue;
+                sm.batch.home[f] = 0xFF;
+                const unsigned short res = sm.batch.res[f];
+                const int st = res & 0xFF, t = res >> 8;
+                if (st == kCFail ? t < h : (st != kCChain && t <= h)) continue;
+                sm.batch.res[f] = pair_res(h, kCFound);
+                if (st == kCClaimed) {
+                    const unsigned pr = sm.batch.pairs[f];
+                    const int r = pr & 0xFF, key = T.node[(pr >> 8) & 0xFF] + 1;
+                    const int so = probe_slot(probe_start(key, S1), t, S1);
+                    atomicExch(L.meta1 + (size_t)T.node[rb + r] * L.H1 + 2 + so, kTombKey);
+                    sm.batch.view[r][2 + so] = kTombKey;
+                }
+            }
+            __syncthreads();
         }
-        __syncthreads();
-        // 4. what the rounds left (a very long contest), overflow chains, then the stores
+        // 5. what the rounds left (claim by claim), overflow chains, then the stores
         for (int f = tid; f < total; f += nt) {
             const unsigned pr = sm.batch.pairs[f];
             const int r = pr & 0xFF, v = (pr >> 8) & 0xFF, word_idx = pr >> 16, u = rb + r;
             const int rn = T.node[u], key = T.node[v] + 1;
             const unsigned res = sm.batch.res[f];
-            unsigned char st = (unsigned char)(res >> 8);
-            int slot = res & 0xFF;
-            if (st == kCFail) st = claim_walk(L, rn, sm.batch.view[r] + 2, key, slot + 1, slot);
+            unsigned char st = (unsigned char)(res & 0xFF);
+            int slot = st == kCChain ? 0 : probe_slot(probe_start(key, S1), res >> 8, S1);
+            if (st == kCFail) st = claim_walk(L, rn, sm.batch.view[r] + 2, key, (res >> 8) + 1, slot);
             int gid;
             if (st == kCChain) {
                 bool claimed = false;

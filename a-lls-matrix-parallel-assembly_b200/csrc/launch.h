@@ -130,7 +130,7 @@ cudaError_t launch_stage_hex20_tc(const MeshView& m, const int* perm, int i0, in
 constexpr int kHex20Wave = 32768;
 constexpr int kBatchHex20Wave = 4096;
 constexpr int kHex20GroupSize = 8;            // elements per group (group_hex20.cuh)
-constexpr int kHex20GroupRecWords = 4432;     // record words per group (header, nodes, block table, slots)
+constexpr int kHex20GroupRecWords = 5220;     // record words per group (header, nodes, blocks by pair, slots)
 constexpr size_t kHex20WaveMapWords = (size_t)kHex20Wave / kHex20GroupSize * kHex20GroupRecWords;
 static_assert(kBatchHex20Wave <= kHex20Wave, "the batched ring's first map is the single-mesh one");
 

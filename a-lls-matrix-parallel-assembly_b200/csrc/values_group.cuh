@@ -9,7 +9,7 @@ namespace fem {
 namespace {
 
 struct GroupValuesSmem {
-    double acc[kGroupPairs * 9];  // the group's node-pair blocks, pair index-major (row node u <= column node v)
+    alignas(16) double ke[kGroup * 210 * 9];  // the group's element blocks: element w's packed upper block p at 9 (210 w + p)
     double dN[3][20][KS];         // dN_n / dxi_i at Gauss point g: [i][n][g]
     double X[kGroup][20][3];      // per warp: its element's node coordinates
     double iJw[kGroup][KS][10];   // per warp: inverse Jacobian (9) and weight * detJ at each Gauss point; row 27 zero
@@ -17,65 +17,9 @@ struct GroupValuesSmem {
     alignas(16) int rec[2][kGroupRecWords];  // the current and the next group's record
 };
 
-// FP64 addition to a shared-memory word, no return value.
-__device__ __forceinline__ void red_shared_f64(double* p, double v) {
-    asm volatile("red.shared.add.f64 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)), "d"(v) : "memory");
-}
-
 __device__ __forceinline__ void cp_async16_v(void* dst, const void* src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-}
-
-// Writes block b (row-major 3x3, in the orientation (row u, column v) of its
-// pair) to the slots of the pair's two orientations, slot words w0 (row u,
-// column v) and w1 (row v, column u): stored where the group owns the pair,
-// added atomically where it is shared.
-__device__ __forceinline__ void write_pair_block(double* __restrict__ vals, unsigned w0, unsigned w1, const double (&b)[9]) {
-    if (map_has_slot(w0)) {
-        double* d = vals + (size_t)(w0 & ~kPairShared) * 9;
-#pragma unroll
-        for (int q = 0; q < 9; q++) {
-            if (w0 & kPairShared) atomicAdd(d + q, b[q]);
-            else d[q] = b[q];
-        }
-    }
-    if (map_has_slot(w1)) {
-        double* d = vals + (size_t)(w1 & ~kPairShared) * 9;
-#pragma unroll
-        for (int q = 0; q < 9; q++) {
-            if (w1 & kPairShared) atomicAdd(d + (q % 3) * 3 + q / 3, b[q]);
-            else d[(q % 3) * 3 + q / 3] = b[q];
-        }
-    }
-}
-
-// Adds the element block Ke_IJ (row-major 3x3, I <= J) of a group element to
-// the group's block of its node pair, as the block table entry says (pair
-// index, transposed, both orientations, sole block of the pair). Shared-memory
-// FP64 atomics, since the group's elements are added at the same time by
-// different warps; a pair's sole block goes to the list at once (slot words
-// of the record).
-__device__ __forceinline__ void group_add_block(double* __restrict__ acc, const unsigned* __restrict__ slots,
-                                                double* __restrict__ vals, unsigned e, const double (&k)[9]) {
-    const int r = e & kTabPair;
-    double* a = acc + 9 * r;
-    if (e & kTabSole) {
-        double b[9];
-#pragma unroll
-        for (int q = 0; q < 9; q++) b[q] = (e & kTabTransposed) ? k[(q % 3) * 3 + q / 3] : k[q];
-        write_pair_block(vals, slots[2 * r], slots[2 * r + 1], b);
-    } else if (e & kTabTransposed) {
-#pragma unroll
-        for (int q = 0; q < 9; q++) red_shared_f64(a + (q % 3) * 3 + q / 3, k[q]);
-    } else {
-#pragma unroll
-        for (int q = 0; q < 9; q++) red_shared_f64(a + q, k[q]);
-    }
-    if (e & kTabBoth) {  // an element with a repeated node: both orientations land on one block
-#pragma unroll
-        for (int q = 0; q < 9; q++) red_shared_f64(a + (q % 3) * 3 + q / 3, k[q]);
-    }
 }
 
 // Tables of the group value pass; every thread of the CTA calls it once.
@@ -91,16 +35,13 @@ __device__ __forceinline__ void values_group_init(GroupValuesSmem& sm) {
     }
     for (int idx = tid; idx < 3 * 20; idx += nt) sm.dN[idx / 20][idx % 20][27] = 0.0;
     for (int idx = tid; idx < kGroup * KS * 10; idx += nt) (&sm.iJw[0][0][0])[idx] = 0.0;
-    for (int idx = tid; idx < kGroupPairs * 9; idx += nt) sm.acc[idx] = 0.0;
     __syncthreads();
 }
 
 // Ke of element w of the group (coordinates already in sm.X[w], material in
-// sm.lam / sm.mu), computed by one warp and added to the group's blocks
-// through the block table `tab` (210 entries of element w).
-__device__ __forceinline__ void group_element_fp64(int w, const unsigned short* __restrict__ tab,
-                                                   const unsigned* __restrict__ slots, double* __restrict__ vals,
-                                                   DevInfo* info, GroupValuesSmem& sm) {
+// sm.lam / sm.mu), computed by one warp; its packed upper blocks go to
+// sm.ke[w] (plain stores: every block has one writer).
+__device__ __forceinline__ void group_element_fp64(int w, DevInfo* info, GroupValuesSmem& sm) {
     const int lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
     if (lane < 27) {
         // Jacobian at Gauss point g = lane: J[3i + j] = sum_n dN[i][n][g] X[n][j]
@@ -187,13 +128,12 @@ __device__ __forceinline__ void group_element_fp64(int w, const unsigned short* 
             const int J = 8 * tj + 2 * fc + h;
             if (I >= 20 || J >= 20 || (ti == tj && J < I)) continue;
             const double mtr = mu * (c[0][0][h] + c[1][1][h] + c[2][2][h]);
-            double k[9];
+            double* k = sm.ke + 9 * (210 * w + packed_block(I, J));
 #pragma unroll
             for (int a = 0; a < 3; a++)
 #pragma unroll
                 for (int b = 0; b < 3; b++)
                     k[3 * a + b] = fma(lam, c[a][b][h], fma(mu, c[b][a][h], a == b ? mtr : 0.0));
-            group_add_block(sm.acc, slots, vals, tab[packed_block(I, J)], k);
         }
     }
 }
@@ -239,18 +179,12 @@ __device__ void values_group(const MeshView& m, int i0, int i1, const int* __res
         const int ne = R[1], npairs = R[0];
         const int gn = g + gridDim.x;
         if (gn < ngroups) fetch_record(gn, buf ^ 1);
-        const unsigned* slots = reinterpret_cast<const unsigned*>(R + kRecMap);
         if (warp < ne) {
-            const unsigned short* tab = reinterpret_cast<const unsigned short*>(R + kRecTab) + warp * 210;
-            if (stage) {
+            if (stage) {  // the element's staged blocks, copied as they are
                 const long long g0 = (long long)i0 + (long long)g * kGroup;
                 const double* ke = stage + (size_t)(g0 + warp - i0) * kPackedHex20;
-                for (int p = lane; p < 210; p += 32) {
-                    double k[9];
-#pragma unroll
-                    for (int q = 0; q < 9; q++) k[q] = FEM_LDG(ke + 9 * p + q);
-                    group_add_block(sm.acc, slots, vals, tab[p], k);
-                }
+                for (int q = lane; q < kPackedHex20 / 2; q += 32) cp_async16_v(sm.ke + 9 * 210 * warp + 2 * q, ke + 2 * q);
+                asm volatile("cp.async.commit_group;" ::: "memory");
             } else {
                 if (lane < 20) {
                     sm.X[warp][lane][0] = px;
@@ -261,25 +195,41 @@ __device__ void values_group(const MeshView& m, int i0, int i1, const int* __res
                     sm.mu[warp] = pE / (2.0 * (1.0 + pnu));
                 }
                 __syncwarp();
-                group_element_fp64(warp, tab, slots, vals, info, sm);
+                group_element_fp64(warp, info, sm);
             }
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
-        __syncthreads();  // the group's blocks are complete; the next record is in
+        __syncthreads();  // the group's element blocks are complete; the next record is in
         if (gn < ngroups && !stage) fetch_element(sm.rec[buf ^ 1]);
-        // every block of the group once: stored where the group is the pair's
-        // only contributor, added atomically where other groups add too;
-        // (row u, column v) as accumulated, (row v, column u) transposed
-        // three threads per pair of several blocks, one row a of its block
-        // each: row a of (row u, column v), column a of (row v, column u)
-        const unsigned* sole = reinterpret_cast<const unsigned*>(R + kRecSole);
+        // every node pair of the group once, the sum of its element blocks:
+        // stored where the group is the pair's only contributor, added
+        // atomically where other groups add too; (row u, column v) as summed,
+        // (row v, column u) transposed. Three threads per pair, one row a of
+        // its block each: row a of (row u, column v), column a of (row v, column u)
+        const unsigned* slots = reinterpret_cast<const unsigned*>(R + kRecMap);
+        const unsigned short* cofs = reinterpret_cast<const unsigned short*>(R + kRecCofs);
+        const unsigned short* cont = reinterpret_cast<const unsigned short*>(R + kRecCont);
         const int n3 = npairs * 3;
         for (int idx = tid; idx < n3; idx += nt) {
             const int r = idx / 3, a = idx - 3 * r;
-            if ((sole[r >> 5] >> (r & 31)) & 1u) continue;  // written when it was computed
-            double* src = sm.acc + 3 * idx;
-            const double v0 = src[0], v1 = src[1], v2 = src[2];
-            src[0] = src[1] = src[2] = 0.0;
+            double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+            for (int i = cofs[r], i1 = cofs[r + 1]; i < i1; i++) {
+                const unsigned c = cont[i];
+                const double* k = sm.ke + 9 * (c & kContBlock);
+                if (c & kTabBoth) {
+                    v0 += k[3 * a] + k[a];
+                    v1 += k[3 * a + 1] + k[3 + a];
+                    v2 += k[3 * a + 2] + k[6 + a];
+                } else if (c & kTabTransposed) {
+                    v0 += k[a];
+                    v1 += k[3 + a];
+                    v2 += k[6 + a];
+                } else {
+                    v0 += k[3 * a];
+                    v1 += k[3 * a + 1];
+                    v2 += k[3 * a + 2];
+                }
+            }
             const unsigned w0 = slots[2 * r], w1 = slots[2 * r + 1];
             if (map_has_slot(w0)) {
                 double* d = vals + (size_t)(w0 & ~kPairShared) * 9 + 3 * a;
@@ -306,7 +256,7 @@ __device__ void values_group(const MeshView& m, int i0, int i1, const int* __res
                 }
             }
         }
-        __syncthreads();  // the accumulator is zero again and the record buffer free
+        __syncthreads();  // the element blocks and the record buffer are free
         buf ^= 1;
     }
 }

@@ -776,9 +776,11 @@ def kernels_per_step(workload: str, mesh) -> int:
     """Library kernels launched by one assembly step."""
     if workload == "hex20":
         waves = (mesh.num_elems + 32767) // 32768
-        # k_info_init, k_bbox_init, k_bbox, Morton count / scan / scatter, k_node_degree,
-        # two per wave, k_consolidate_reset, k_scan_reduce, k_scan_tiles, k_row_ptr, k_write
-        return 7 + 2 * waves + 5
+        # k_info_init, k_bbox_init, k_bbox, Morton key count / bucket scan / scatter;
+        # node -> element incidence (count, tile sums, tile scan, tile apply, fill);
+        # claim + value pass per wave; k_consolidate_reset, k_scan_reduce,
+        # k_scan_tiles, k_row_ptr, k_write (the launch list of one step)
+        return 6 + 5 + 2 * waves + 5
     return {"q4": 10, "t3": 10, "mixed": 11}[workload]
 
 

@@ -160,7 +160,7 @@ def test_upper_output_and_autotuner_arguments(fem):
 def test_batched_workspace_sizing_host_only(fem):
     # Slots are dealt the meshes largest first, one slot per mesh until every
     # slot has one, so a slot's size is that of its first (largest) mesh (a
-    # Hex20 mesh's slot also holds a second wave's group records, 4432 words
+    # Hex20 mesh's slot also holds a second wave's group records, 5220 words
     # per group of 8 elements): the workspace
     # grows with the slot count and is capped by the mesh count. A control
     # block (descriptors, schedule, counters) comes first.
@@ -179,7 +179,7 @@ def test_batched_workspace_sizing_host_only(fem):
     assert all(a <= b for a, b in zip(sizes, sizes[1:]))
     assert sizes[3] == sizes[4] == sizes[5]          # at most one slot per mesh
     up = lambda v: -(-v // 256) * 256  # noqa: E731
-    total = sum(up(fem.workspace_size(m)) + (up(-(-min(m.num_elems, 4096) // 8) * 4432 * 4) if m.kind == 2 else 0)
+    total = sum(up(fem.workspace_size(m)) + (up(-(-min(m.num_elems, 4096) // 8) * 5220 * 4) if m.kind == 2 else 0)
                 for m in meshes)
     assert total < sizes[3] <= total + 64 * 1024
     b = C.c_size_t(0)
