@@ -248,8 +248,8 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         atomicAdd(&sm.pre.mult[e & kTabPair], 1);
     }
     __syncthreads();
-    // the element blocks grouped by pair: offsets (a scan of the counts),
-    // then each block placed at its pair's next free entry
+    // the pair-major order of the element blocks: each pair's first position
+    // (a scan of the counts), then each block's position, its pair's next free one
     if (tid < 32) warp_scan_into(T.npairs, sm.pre.cofs, [&](int r) { return sm.pre.mult[r]; });
     __syncthreads();
     unsigned short* cofs = reinterpret_cast<unsigned short*>(rec + kRecCofs);
@@ -258,10 +258,10 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         if (r < T.npairs) sm.pre.mult[r] = sm.pre.cofs[r];
     }
     __syncthreads();
-    unsigned short* cont = reinterpret_cast<unsigned short*>(rec + kRecCont);
+    unsigned short* cpos = reinterpret_cast<unsigned short*>(rec + kRecCpos);
     for (int k = tid; k < ne * 210; k += nt) {
         const unsigned e = sm.pre.tab[k];
-        cont[atomicAdd(&sm.pre.mult[e & kTabPair], 1)] = (unsigned short)(k | (e & (kTabTransposed | kTabBoth)));
+        cpos[k] = (unsigned short)(atomicAdd(&sm.pre.mult[e & kTabPair], 1) | (e & (kTabTransposed | kTabBoth)));
     }
     // ownership masks: the elements outside the group that have a node of
     // the group, numbered through a hash table (the first kOutBits get a bit)

@@ -17,12 +17,13 @@
 //   [0] number of node pairs, [1] elements (0: the group has a bad node id),
 //   [2 + w] element id of the group's element w;
 //   kRecOcc + 20 w + a: node id of node a of element w;
-//   kRecCont: the group's element blocks grouped by node pair (16-bit
-//     entries): block index 210 w + p of element w's packed upper block p
-//     (I <= J, p = 20 I - I (I - 1) / 2 + J - I), bit 15 set when the block
-//     lies transposed in its pair (u > v), bit 14 set when both orientations
-//     fall on one diagonal block (an element with a repeated node);
-//   kRecCofs: 16-bit offsets, pair r's entries are [cofs[r], cofs[r + 1]);
+//   kRecCpos + (210 w + p) / 2: for element w's packed upper block p (I <= J,
+//     p = 20 I - I (I - 1) / 2 + J - I), a 16-bit entry: the block's position
+//     in the pair-major order of the group's blocks (bits 0-10), bit 15 set
+//     when it lies transposed in its pair (u > v), bit 14 set when both
+//     orientations fall on one diagonal block (an element with a repeated
+//     node);
+//   kRecCofs: 16-bit offsets, pair r's blocks take positions [cofs[r], cofs[r + 1]);
 //   kRecMap + 2 r: slot id of (row u, column v) of pair r = {u <= v}, and
 //   kRecMap + 2 r + 1: slot id of (row v, column u) (kMapNone for a diagonal
 //     pair or an unresolved slot). Bit 31 (kPairShared) marks a pair that
@@ -44,15 +45,15 @@ constexpr int kGroupMapWords = 2 * kGroupPairs;  // map record words per group
 constexpr unsigned kPairShared = 0x80000000u;    // map word flag: other groups add to the pair
 constexpr unsigned kMapNone = 0xFFFFFFFFu;       // map word of no slot
 constexpr int kRecOcc = 16;                                  // record words: header, then occurrences,
-constexpr int kRecCont = kRecOcc + kGroupOcc;                // blocks by pair (two 16-bit entries a word),
-constexpr int kRecCofs = kRecCont + kGroup * 210 / 2;        // their offsets per pair,
+constexpr int kRecCpos = kRecOcc + kGroupOcc;                // block positions (two 16-bit entries a word),
+constexpr int kRecCofs = kRecCpos + kGroup * 210 / 2;        // each pair's first position,
 constexpr int kRecMap = kRecCofs + (kGroupPairs + 1 + 7) / 8 * 4;  // slot words
 constexpr int kGroupRecWords = kRecMap + kGroupMapWords;
-constexpr unsigned kTabTransposed = 0x8000u, kTabBoth = 0x4000u, kTabPair = 0x07FFu, kContBlock = 0x07FFu;
+constexpr unsigned kTabTransposed = 0x8000u, kTabBoth = 0x4000u, kTabPair = 0x07FFu, kPosMask = 0x07FFu;
 static_assert(kNbWords * 32 == kGroupOcc, "whole words of group-local nodes");
 static_assert(kGroupPairs <= kTabPair + 1, "pair index in 11 bits");
-static_assert(kRecCont % 4 == 0 && kRecCofs % 4 == 0 && kRecMap % 4 == 0 && kGroupRecWords % 4 == 0, "16-byte sections");
-static_assert(kGroup * 210 <= kContBlock + 1, "block index in 11 bits");
+static_assert(kRecCpos % 4 == 0 && kRecCofs % 4 == 0 && kRecMap % 4 == 0 && kGroupRecWords % 4 == 0, "16-byte sections");
+static_assert(kGroup * 210 <= kPosMask + 1, "block position in 11 bits");
 static_assert(kGroup == kHex20GroupSize && kGroupRecWords == kHex20GroupRecWords, "host-side sizes");
 static_assert(kHex20Wave % kGroup == 0 && kBatchHex20Wave % kGroup == 0, "waves of whole groups");
 

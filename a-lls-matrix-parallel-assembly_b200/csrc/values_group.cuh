@@ -9,7 +9,7 @@ namespace fem {
 namespace {
 
 struct GroupValuesSmem {
-    alignas(16) double ke[kGroup * 210 * 9];  // the group's element blocks: element w's packed upper block p at 9 (210 w + p)
+    alignas(16) double ke[kGroup * 210 * 9];  // the group's element blocks, pair-major (record positions), each as it adds to its pair's (row u, column v) block
     double dN[3][20][KS];         // dN_n / dxi_i at Gauss point g: [i][n][g]
     double X[kGroup][20][3];      // per warp: its element's node coordinates
     double iJw[kGroup][KS][10];   // per warp: inverse Jacobian (9) and weight * detJ at each Gauss point; row 27 zero
@@ -38,10 +38,30 @@ __device__ __forceinline__ void values_group_init(GroupValuesSmem& sm) {
     __syncthreads();
 }
 
+// Stores block k (row-major 3x3, element orientation (I, J)) at its
+// position in the pair-major order, as it adds to its pair's (row u, column v)
+// block: k, its transpose (bit 15 of the position entry), or k + k^T (bit 14).
+__device__ __forceinline__ void stage_block(double* __restrict__ ke, unsigned c, const double (&k)[9]) {
+    double* d = ke + 9 * (c & kPosMask);
+    const bool tr = c & kTabTransposed, both = c & kTabBoth;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            const double x = k[3 * a + b], y = k[3 * b + a];
+            d[3 * a + b] = both ? x + y : (tr ? y : x);
+        }
+}
+
 // Ke of element w of the group (coordinates already in sm.X[w], material in
-// sm.lam / sm.mu), computed by one warp; its packed upper blocks go to
-// sm.ke[w] (plain stores: every block has one writer).
-__device__ __forceinline__ void group_element_fp64(int w, DevInfo* info, GroupValuesSmem& sm) {
+// sm.lam / sm.mu), computed by one warp; each upper block is staged at its
+// position `cpos` (one writer per position, plain stores) as it adds to its
+// pair: entry (a, b) is alpha M^{ab} + beta M^{ba} + gamma [a = b] mu tr M,
+// with (alpha, beta, gamma) = (lam, mu, 1) for a block in its pair's
+// orientation, (mu, lam, 1) transposed, (lam + mu, lam + mu, 2) for both
+// orientations on one diagonal block.
+__device__ __forceinline__ void group_element_fp64(int w, const unsigned short* __restrict__ cpos, DevInfo* info,
+                                                   GroupValuesSmem& sm) {
     const int lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
     if (lane < 27) {
         // Jacobian at Gauss point g = lane: J[3i + j] = sum_n dN[i][n][g] X[n][j]
@@ -128,12 +148,15 @@ __device__ __forceinline__ void group_element_fp64(int w, DevInfo* info, GroupVa
             const int J = 8 * tj + 2 * fc + h;
             if (I >= 20 || J >= 20 || (ti == tj && J < I)) continue;
             const double mtr = mu * (c[0][0][h] + c[1][1][h] + c[2][2][h]);
-            double* k = sm.ke + 9 * (210 * w + packed_block(I, J));
+            const unsigned e = cpos[packed_block(I, J)];
+            const bool both = e & kTabBoth, tr = e & kTabTransposed;
+            const double al = both ? lam + mu : (tr ? mu : lam), be = both ? lam + mu : (tr ? lam : mu);
+            const double dg = both ? 2.0 * mtr : mtr;
+            double* d = sm.ke + 9 * (e & kPosMask);
 #pragma unroll
             for (int a = 0; a < 3; a++)
 #pragma unroll
-                for (int b = 0; b < 3; b++)
-                    k[3 * a + b] = fma(lam, c[a][b][h], fma(mu, c[b][a][h], a == b ? mtr : 0.0));
+                for (int b = 0; b < 3; b++) d[3 * a + b] = fma(al, c[a][b][h], fma(be, c[b][a][h], a == b ? dg : 0.0));
         }
     }
 }
@@ -180,11 +203,16 @@ __device__ void values_group(const MeshView& m, int i0, int i1, const int* __res
         const int gn = g + gridDim.x;
         if (gn < ngroups) fetch_record(gn, buf ^ 1);
         if (warp < ne) {
-            if (stage) {  // the element's staged blocks, copied as they are
+            const unsigned short* cpos = reinterpret_cast<const unsigned short*>(R + kRecCpos) + 210 * warp;
+            if (stage) {  // the element's blocks from the stage buffer
                 const long long g0 = (long long)i0 + (long long)g * kGroup;
                 const double* ke = stage + (size_t)(g0 + warp - i0) * kPackedHex20;
-                for (int q = lane; q < kPackedHex20 / 2; q += 32) cp_async16_v(sm.ke + 9 * 210 * warp + 2 * q, ke + 2 * q);
-                asm volatile("cp.async.commit_group;" ::: "memory");
+                for (int p = lane; p < 210; p += 32) {
+                    double k[9];
+#pragma unroll
+                    for (int q = 0; q < 9; q++) k[q] = FEM_LDG(ke + 9 * p + q);
+                    stage_block(sm.ke, cpos[p], k);
+                }
             } else {
                 if (lane < 20) {
                     sm.X[warp][lane][0] = px;
@@ -195,42 +223,29 @@ __device__ void values_group(const MeshView& m, int i0, int i1, const int* __res
                     sm.mu[warp] = pE / (2.0 * (1.0 + pnu));
                 }
                 __syncwarp();
-                group_element_fp64(warp, info, sm);
+                group_element_fp64(warp, cpos, info, sm);
             }
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
         __syncthreads();  // the group's element blocks are complete; the next record is in
         if (gn < ngroups && !stage) fetch_element(sm.rec[buf ^ 1]);
-        // every node pair of the group once, the sum of its element blocks:
+        // every node pair of the group once, the sum of its staged blocks:
         // stored where the group is the pair's only contributor, added
         // atomically where other groups add too; (row u, column v) as summed,
         // (row v, column u) transposed. Three threads per pair, one row a of
         // its block each: row a of (row u, column v), column a of (row v, column u)
         const unsigned* slots = reinterpret_cast<const unsigned*>(R + kRecMap);
         const unsigned short* cofs = reinterpret_cast<const unsigned short*>(R + kRecCofs);
-        const unsigned short* cont = reinterpret_cast<const unsigned short*>(R + kRecCont);
-        const int n3 = npairs * 3;
-        for (int idx = tid; idx < n3; idx += nt) {
+        for (int idx = tid; idx < npairs * 3; idx += nt) {
             const int r = idx / 3, a = idx - 3 * r;
+            const unsigned w0 = slots[2 * r], w1 = slots[2 * r + 1];
             double v0 = 0.0, v1 = 0.0, v2 = 0.0;
             for (int i = cofs[r], i1 = cofs[r + 1]; i < i1; i++) {
-                const unsigned c = cont[i];
-                const double* k = sm.ke + 9 * (c & kContBlock);
-                if (c & kTabBoth) {
-                    v0 += k[3 * a] + k[a];
-                    v1 += k[3 * a + 1] + k[3 + a];
-                    v2 += k[3 * a + 2] + k[6 + a];
-                } else if (c & kTabTransposed) {
-                    v0 += k[a];
-                    v1 += k[3 + a];
-                    v2 += k[6 + a];
-                } else {
-                    v0 += k[3 * a];
-                    v1 += k[3 * a + 1];
-                    v2 += k[3 * a + 2];
-                }
+                const double* k = sm.ke + 9 * i + 3 * a;
+                v0 += k[0];
+                v1 += k[1];
+                v2 += k[2];
             }
-            const unsigned w0 = slots[2 * r], w1 = slots[2 * r + 1];
             if (map_has_slot(w0)) {
                 double* d = vals + (size_t)(w0 & ~kPairShared) * 9 + 3 * a;
                 if (w0 & kPairShared) {
