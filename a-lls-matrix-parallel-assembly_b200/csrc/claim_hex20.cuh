@@ -2,10 +2,14 @@
 // batched persistent kernel (batched.cu). See claim_hex20.cu for the method.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "group_hex20.cuh"
 
 namespace fem {
 namespace {
+
+namespace cg = cooperative_groups;
 
 constexpr int kClaimMaxWords = 96;  // first-chunk meta rows of at most 96 words (S1 <= 94, checked on the host)
 constexpr int kViewStride = 100;    // words between the copied rows (16-byte rows, banks spread)
@@ -348,6 +352,8 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
                     const int k = cum + __popc(bits & ((1u << lane) - 1u)), v = 32 * w + lane;
                     const int word = u <= v ? 2 * (T.ubase[u] + k - below) : 2 * pair_index(T, v, u) + 1;
                     sm.batch.pairs[base + k] = (unsigned)r | ((unsigned)v << 8) | ((unsigned)word << 16);
+                    sm.batch.res[base + k] = pair_res(0, kCTry);  // the first round probes from step 0
+                    sm.batch.home[base + k] = 0xFF;
                 }
                 cum += __popc(bits);
             }
@@ -355,26 +361,7 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         cp_async_wait_all();
         __syncthreads();
         const int total = sm.obase[nrows];
-        // 1. every pair probed in the copies: found, or the step of the first
-        // empty slot of its sequence, or a full sequence
-        for (int f = tid; f < total; f += nt) {
-            const unsigned pr = sm.batch.pairs[f];
-            const int r = pr & 0xFF, key = T.node[(pr >> 8) & 0xFF] + 1;
-            const int* v = sm.batch.view[r] + 2;
-            const int p0 = probe_start(key, S1);
-            unsigned short res = pair_res(kNoStep, kCChain);
-            for (int t = 0; t < S1; t++) {
-                const int x = v[probe_slot(p0, t, S1)];
-                if (x == key || x == 0) {
-                    res = pair_res(t, x == key ? kCFound : kCTry);
-                    break;
-                }
-            }
-            sm.batch.res[f] = res;
-            sm.batch.home[f] = 0xFF;
-        }
-        __syncthreads();
-        // 2.-4. placement rounds. Each round first places every pending
+        // 1.-3. placement rounds. Each round first places every pending
         // column in the copy (shared-memory CAS: the first slot of its
         // sequence empty in the copy becomes its tentative slot, so the
         // CTA's own columns never meet in global memory), then issues all
@@ -479,7 +466,7 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
             }
             __syncthreads();
         }
-        // 5. what the rounds left (claim by claim), overflow chains, then the stores
+        // 4. what the rounds left (claim by claim), overflow chains, then the stores
         for (int f = tid; f < total; f += nt) {
             const unsigned pr = sm.batch.pairs[f];
             const int r = pr & 0xFF, v = (pr >> 8) & 0xFF, word_idx = pr >> 16, u = rb + r;
@@ -499,7 +486,10 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
             const bool owned = pair_owned(sm, u, v);
             if (gid >= 0 && st == kCClaimed) {
                 if (!owned) zero_block(L.vals + (size_t)(unsigned)gid * 9);
-                atomicAdd(&sm.claims[r], 1);
+                // one count per row among the lanes claiming together
+                const cg::coalesced_group claimers = cg::coalesced_threads();
+                const cg::coalesced_group row = cg::labeled_partition(claimers, r);
+                if (row.thread_rank() == 0) atomicAdd(&sm.claims[r], (int)row.size());
             }
             map[word_idx] = gid < 0 ? kMapNone : ((unsigned)gid | (owned ? 0u : kPairShared));
             if (u == v) map[word_idx + 1] = kMapNone;
