@@ -12,14 +12,19 @@
 // that several of the group's elements share is resolved once. Row nodes go
 // in batches of kClaimRows: the batch's first list chunks (next link + S1
 // hashed slots, at most 384 bytes each) are copied into shared memory with
-// cp.async, then every thread resolves ordered pairs of the batch in the copy:
-// a column found on its probe sequence is an existing entry; otherwise the
-// first slot of the sequence that is empty in the copy is claimed with
-// atomicCAS(0 -> column + 1), moving on along the sequence when the CAS meets
-// a column that another group put there (slots are never freed, so a column
-// is found or placed at the first empty slot of its sequence, never twice). A
-// full first chunk continues in the row's overflow chunks (taken from the pool
-// and linked with atomicCAS), read from global memory.
+// cp.async, then the batch's ordered pairs are resolved in placement rounds
+// (claim_hex20.cuh): each pending column takes the first slot of its probe
+// sequence that is empty in the copy (a shared-memory CAS, so the group's own
+// columns never meet in global memory), all of a round's claims go to the list
+// as atomicCAS(0 -> column + 1), and a CAS that met another group's column
+// moves on in the next round. Slots are never freed, so a column is found or
+// placed at the first empty slot of its sequence; the rare second copy that a
+// race between groups leaves is retired with a tombstone key before the
+// value pass. A full first chunk continues in the row's overflow chunks
+// (taken from the pool and linked with atomicCAS), read from global memory.
+// The groups are claimed by class g mod 8 (the parities of a brick's
+// coordinates in a brick-structured Morton order), so the groups claiming at
+// the same time rarely share a row.
 //
 // Ownership: a pair {u, v} belongs to the group alone when no element outside
 // the group has both nodes: the elements of u and of v outside the group

@@ -40,7 +40,7 @@ struct ClaimSmem {
         struct {
             int mult[kGroupPairs];                 // blocks of the group's elements on each node pair, then fill counters
             int cofs[kGroupPairs + 1];             // first entry of each pair's blocks
-            unsigned short tab[kGroup * 210];      // the block table before it is written
+            unsigned short tab[kGroup * 210];      // each element block's pair index and orientation bits
             int inc_lo[kGroupOcc], inc_n[kGroupOcc];  // incidence list of each node
         } pre;
         struct {
@@ -223,7 +223,7 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         return;
     }
     const int nu = T.nu;
-    // the record: header, node ids, block table (with the sole-block flag)
+    // the record: header, node ids, then each element block's pair and orientation
     if (tid == 0) {
         rec[0] = T.npairs;
         rec[1] = ne;

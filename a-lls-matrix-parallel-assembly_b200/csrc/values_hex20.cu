@@ -27,15 +27,18 @@
 // group's element w alone: the lanes' gradients G_a(n, g) for the fragment
 // rows n = 8 t + lane / 4 and k-columns g = 4 s + lane % 4 are the same
 // values for the A and the B operands, so they stay in registers (63 per
-// lane) and all six tile positions run from registers. The 210 upper blocks
-// are added with shared-memory FP64 atomics into the group's accumulator,
-// one block per node pair of the group (pair_index), so a pair that several
-// of the group's elements share leaves the CTA once. The flush then writes
-// each pair's block to the slot of (row u, column v) and its transpose to
-// (row v, column u): a plain store for a pair only this group has (its slots
-// were not zeroed), an FP64 atomic add for a shared pair (zeroed by its
-// claimer). The tensor-core form computes the wave's Ke in ke_tcgen05.cu
-// into a staging buffer first, and the same kernel adds the staged blocks.
+// lane) and all six tile positions run from registers. Each of the 210 upper
+// blocks is stored, already oriented as it adds to its node pair (the block,
+// its transpose, or block + transpose for a repeated node), at its position
+// in the group's pair-major block order (from the claim pass's record): one
+// writer per position, plain shared stores. After a barrier, three threads
+// per node pair sum the pair's contiguous blocks, one row each, so a pair
+// that several of the group's elements share leaves the CTA once, and write
+// the sum to the slot of (row u, column v) and its transpose to (row v,
+// column u): a plain store for a pair only this group has (its slots were
+// not zeroed), an FP64 atomic add for a shared pair (zeroed by its claimer).
+// The tensor-core form computes the wave's Ke in ke_tcgen05.cu into a staging
+// buffer first, and the same kernel stages those blocks instead.
 //
 // Element pass (k_values_hex20, kToCsrMap / kToCsrColour): one 6-warp CTA
 // per element at a time, warp w owning tile position w; the shape-function
