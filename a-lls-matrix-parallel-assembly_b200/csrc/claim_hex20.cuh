@@ -243,29 +243,33 @@ __device__ void claim_group(const MeshView& m, const ListLayout& L, const int* _
         }
     }
     __syncthreads();
-    for (int k = tid; k < ne * 210; k += nt) {
-        const int w = k / 210, d = sm.pdec[k - 210 * w], I = d & 0xFF, J = d >> 8;
-        const int u = T.lidx[20 * w + I], v = T.lidx[20 * w + J];
-        unsigned e = u <= v ? (unsigned)pair_index(T, u, v) : ((unsigned)pair_index(T, v, u) | kTabTransposed);
-        if (u == v && I != J) e |= kTabBoth;
-        sm.pre.tab[k] = (unsigned short)e;
-        atomicAdd(&sm.pre.mult[e & kTabPair], 1);
-    }
-    __syncthreads();
-    // the pair-major order of the element blocks: each pair's first position
-    // (a scan of the counts), then each block's position, its pair's next free one
-    if (tid < 32) warp_scan_into(T.npairs, sm.pre.cofs, [&](int r) { return sm.pre.mult[r]; });
-    __syncthreads();
-    unsigned short* cofs = reinterpret_cast<unsigned short*>(rec + kRecCofs);
-    for (int r = tid; r <= T.npairs; r += nt) {
-        cofs[r] = (unsigned short)sm.pre.cofs[r];
-        if (r < T.npairs) sm.pre.mult[r] = sm.pre.cofs[r];
-    }
-    __syncthreads();
-    unsigned short* cpos = reinterpret_cast<unsigned short*>(rec + kRecCpos);
-    for (int k = tid; k < ne * 210; k += nt) {
-        const unsigned e = sm.pre.tab[k];
-        cpos[k] = (unsigned short)(atomicAdd(&sm.pre.mult[e & kTabPair], 1) | (e & (kTabTransposed | kTabBoth)));
+    // the pair-major block order is read by the group value pass only; the
+    // batched kernel (no incidence lists) adds element by element
+    if (inc_off) {
+        for (int k = tid; k < ne * 210; k += nt) {
+            const int w = k / 210, d = sm.pdec[k - 210 * w], I = d & 0xFF, J = d >> 8;
+            const int u = T.lidx[20 * w + I], v = T.lidx[20 * w + J];
+            unsigned e = u <= v ? (unsigned)pair_index(T, u, v) : ((unsigned)pair_index(T, v, u) | kTabTransposed);
+            if (u == v && I != J) e |= kTabBoth;
+            sm.pre.tab[k] = (unsigned short)e;
+            atomicAdd(&sm.pre.mult[e & kTabPair], 1);
+        }
+        __syncthreads();
+        // the pair-major order of the element blocks: each pair's first position
+        // (a scan of the counts), then each block's position, its pair's next free one
+        if (tid < 32) warp_scan_into(T.npairs, sm.pre.cofs, [&](int r) { return sm.pre.mult[r]; });
+        __syncthreads();
+        unsigned short* cofs = reinterpret_cast<unsigned short*>(rec + kRecCofs);
+        for (int r = tid; r <= T.npairs; r += nt) {
+            cofs[r] = (unsigned short)sm.pre.cofs[r];
+            if (r < T.npairs) sm.pre.mult[r] = sm.pre.cofs[r];
+        }
+        __syncthreads();
+        unsigned short* cpos = reinterpret_cast<unsigned short*>(rec + kRecCpos);
+        for (int k = tid; k < ne * 210; k += nt) {
+            const unsigned e = sm.pre.tab[k];
+            cpos[k] = (unsigned short)(atomicAdd(&sm.pre.mult[e & kTabPair], 1) | (e & (kTabTransposed | kTabBoth)));
+        }
     }
     // ownership masks: the elements outside the group that have a node of
     // the group, numbered through a hash table (the first kOutBits get a bit)

@@ -24,6 +24,8 @@
 //     orientations fall on one diagonal block (an element with a repeated
 //     node);
 //   kRecCofs: 16-bit offsets, pair r's blocks take positions [cofs[r], cofs[r + 1]);
+//   (these two sections are written for the group value pass only: a claim
+//   without incidence lists, the batched kernel's, leaves them unset);
 //   kRecMap + 2 r: slot id of (row u, column v) of pair r = {u <= v}, and
 //   kRecMap + 2 r + 1: slot id of (row v, column u) (kMapNone for a diagonal
 //     pair or an unresolved slot). Bit 31 (kPairShared) marks a pair that
